@@ -1,0 +1,15 @@
+"""dynamiqs_b200 -- dynamiqs' ``mesolve`` hot path (Lindblad right-hand side inside the
+Tsit5 / Dopri5 adaptive Runge-Kutta loop) as hand-written sm_100a CUDA kernels behind a
+C ABI (``include/dqb200.h``), with the reference's Python API on top.
+"""
+
+from . import method, operators
+from .mesolve import MESolveB200Integrator, mesolve
+from .method import Dopri5, Tsit5
+from .options import Options
+from .qarrays import SparseDIA, dense, dia
+from .result import AdaptiveStepInfos, MESolveResult
+
+__all__ = ['mesolve', 'MESolveB200Integrator', 'Options', 'Tsit5', 'Dopri5',
+           'MESolveResult', 'AdaptiveStepInfos', 'SparseDIA', 'dense', 'dia', 'method',
+           'operators']

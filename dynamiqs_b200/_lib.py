@@ -1,0 +1,121 @@
+"""ctypes binding of ``libdqb200.so`` (the C ABI declared in ``include/dqb200.h``).
+
+The shared library is built in-tree (``dynamiqs_b200/csrc/Makefile``) and loaded from
+this package directory.  There is no fallback: if the library is missing, or was built
+without CUDA support, every solve raises ``RuntimeError``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / 'libdqb200.so'
+
+# return codes
+DQB_OK = 0
+DQB_ERR_INVALID_ARGUMENT = 1
+DQB_ERR_UNSUPPORTED = 2
+DQB_ERR_WORKSPACE_TOO_SMALL = 3
+DQB_ERR_CUDA = 4
+_RC_NAMES = {
+    DQB_ERR_INVALID_ARGUMENT: 'invalid argument',
+    DQB_ERR_UNSUPPORTED: 'unsupported problem size or option',
+    DQB_ERR_WORKSPACE_TOO_SMALL: 'workspace too small',
+    DQB_ERR_CUDA: 'CUDA launch error',
+}
+
+# per-instance status
+INST_OK = 0
+INST_MAX_STEPS = 1
+INST_NONFINITE = 2
+INST_NOT_HERMITIAN = 3
+
+METHOD_TSIT5 = 0
+METHOD_DOPRI5 = 1
+FORM_HERMITIAN = 0
+FORM_STANDARD = 1
+
+
+class OdeOptions(ctypes.Structure):
+    _fields_ = [
+        ('method', ctypes.c_int32),
+        ('form', ctypes.c_int32),
+        ('rtol', ctypes.c_double),
+        ('atol', ctypes.c_double),
+        ('safety', ctypes.c_double),
+        ('factormin', ctypes.c_double),
+        ('factormax', ctypes.c_double),
+        ('max_steps', ctypes.c_int64),
+        ('t0', ctypes.c_double),
+        ('save_states', ctypes.c_int32),
+        ('check_hermitian', ctypes.c_int32),
+    ]
+
+
+class Outputs(ctypes.Structure):
+    _fields_ = [
+        ('states', ctypes.c_void_p),
+        ('expects', ctypes.c_void_p),
+        ('infos', ctypes.c_void_p),
+        ('status', ctypes.c_void_p),
+    ]
+
+
+class DenseProblem(ctypes.Structure):
+    _fields_ = [
+        ('n', ctypes.c_int32),
+        ('n_jumps', ctypes.c_int32),
+        ('n_exp', ctypes.c_int32),
+        ('n_tsave', ctypes.c_int32),
+        ('batch', ctypes.c_int64),
+        ('H', ctypes.c_void_p),
+        ('L', ctypes.c_void_p),
+        ('rho0', ctypes.c_void_p),
+        ('rho0_is_ket', ctypes.c_int32),
+        ('E', ctypes.c_void_p),
+        ('tsave', ctypes.c_void_p),
+        ('H_index', ctypes.c_void_p),
+        ('L_index', ctypes.c_void_p),
+        ('rho0_index', ctypes.c_void_p),
+    ]
+
+
+# Every symbol include/dqb200.h declares, with (restype, argtypes).
+_P = ctypes.c_void_p
+SIGNATURES = {
+    'dqb_mesolve_dense_workspace_size': (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64]),
+    'dqb_mesolve_dense': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
+                                         ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
+    'dqb_lindblad_rhs_dense': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.c_int32, _P, _P, _P]),
+    'dqb_dense_small_max_n': (ctypes.c_int32, [ctypes.c_int32]),
+    'dqb_version': (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the in-tree library once; raise if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f'{LIB_PATH} is missing: build it with `make -C dynamiqs_b200/csrc` '
+            '(or `python -c "import __graft_entry__ as g; g.build()"`). '
+            'dynamiqs_b200 has no CPU fallback.')
+    lib = ctypes.CDLL(os.fspath(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int, what: str) -> None:
+    if rc != DQB_OK:
+        raise RuntimeError(f'{what} failed: {_RC_NAMES.get(rc, rc)} (code {rc})')

@@ -1,0 +1,679 @@
+// Persistent batched mesolve kernel for dense operators with n <= 64.
+//
+// One CTA solves one instance at a time and fetches the next instance from an atomic
+// counter when it finishes, so instances with different step counts never wait for
+// each other (the reference vmaps diffrax's while loop, which runs every lane for as
+// many iterations as the slowest one: dynamiqs/integrators/apis/mesolve.py:307-336).
+//
+// Per CTA, shared memory holds Hnh = -iH - 1/2 sum L^+L (built once per instance), the
+// jump operators L_k, the current stage input X and a product buffer T, each padded
+// to a row stride of NP+1 complex so that row and column (transposed) reads are both
+// bank-conflict free.  The seven RK stages, y and y1 live in a per-CTA scratch slot in
+// global memory (9 * NP^2 complex64 = 288 KiB at NP = 64; 148 slots = 43 MB, resident
+// in the 126 MB L2).  The products run on the FP32 pipes: 256 threads, each owning an
+// (NP/16) x (NP/16) tile of the output, complex multiply-accumulate as 4 FFMA.
+//
+// Right-hand sides (dynamiqs/integrators/core/diffrax_integrator.py:312-323):
+//   hermitian: tmp = Hnh X + 1/2 sum_k (L_k X) L_k^+ ;  out = tmp + tmp^+
+//   standard : out = Hnh X + X Hnh^+ + sum_k (L_k X) L_k^+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "dqb_common.cuh"
+
+namespace dqb {
+
+constexpr int kSmallThreads = 256;
+constexpr int kSlotMats = 9;  // y, y1, k1..k7
+
+template <int NP>
+struct Small {
+  static constexpr int LD = NP + 1;
+  static constexpr int R = NP / 16;
+  static constexpr int MAT = NP * LD;
+  static constexpr int NN = NP * NP;
+};
+
+struct DenseSmallArgs {
+  int n, K, nE, ntsave;
+  long long batch;
+  const float2* H;
+  const float2* L;
+  const float2* rho0;
+  const float2* E;
+  int rho0_is_ket;
+  const double* tsave;
+  const int* Hidx;
+  const int* Lidx;
+  const int* ridx;
+  float2* states;
+  float2* expects;
+  int* infos;
+  int* status;
+  float2* slots;
+  unsigned int* counter;
+  CtrlOpts o;
+};
+
+struct Ctrl {
+  double t, tnext, h, t1, dtnew;
+  float w[7];
+  int keep, run, status, save_idx;
+  long long nsteps, nacc, nrej;
+  long long inst;
+  int sy, sy1, sk[7];
+};
+
+// acc[r][c] += sum_k op(A)[row][k] * op(B)[k][col], rows ty + 16 r, cols tx + 16 c.
+// CA: op(A) = A^+, CB: op(B) = B^+ (both read transposed from the padded layout).
+template <int NP, bool CA, bool CB>
+__device__ __forceinline__ void gemm(float2 (&acc)[NP / 16][NP / 16], const float2* __restrict__ A,
+                                     const float2* __restrict__ B, int kn) {
+  constexpr int R = NP / 16, LD = NP + 1;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll 4
+  for (int k = 0; k < kn; ++k) {
+    float2 a[R], b[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) a[r] = CA ? cconj(A[k * LD + ty + 16 * r]) : A[(ty + 16 * r) * LD + k];
+#pragma unroll
+    for (int c = 0; c < R; ++c) b[c] = CB ? cconj(B[(tx + 16 * c) * LD + k]) : B[k * LD + tx + 16 * c];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int c = 0; c < R; ++c) cmac(acc[r][c], a[r], b[c]);
+  }
+}
+
+template <int NP>
+__device__ __forceinline__ void zero_tile(float2 (&t)[NP / 16][NP / 16]) {
+#pragma unroll
+  for (int r = 0; r < NP / 16; ++r)
+#pragma unroll
+    for (int c = 0; c < NP / 16; ++c) t[r][c] = make_float2(0.f, 0.f);
+}
+
+template <int NP>
+__device__ __forceinline__ void store_tile(float2* S, const float2 (&t)[NP / 16][NP / 16], float s) {
+  constexpr int LD = NP + 1;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int r = 0; r < NP / 16; ++r)
+#pragma unroll
+    for (int c = 0; c < NP / 16; ++c)
+      S[(ty + 16 * r) * LD + tx + 16 * c] = make_float2(s * t[r][c].x, s * t[r][c].y);
+}
+
+// Load an n x n row-major global matrix into a padded NP x (NP+1) shared buffer.
+template <int NP>
+__device__ __forceinline__ void load_padded(float2* S, const float2* __restrict__ g, int n) {
+  for (int e = threadIdx.x; e < NP * NP; e += blockDim.x) {
+    const int i = e / NP, j = e % NP;
+    S[i * Small<NP>::LD + j] = (i < n && j < n) ? g[i * n + j] : make_float2(0.f, 0.f);
+  }
+}
+
+// Build Hnh = -iH - 1/2 sum_k L_k^+ L_k in place (sH holds H on entry).
+template <int NP>
+__device__ void build_hnh(float2* sH, const float2* sL, int n, int K) {
+  constexpr int LD = NP + 1;
+  float2 acc[NP / 16][NP / 16];
+  zero_tile<NP>(acc);
+  for (int k = 0; k < K; ++k) gemm<NP, true, false>(acc, sL + k * Small<NP>::MAT, sL + k * Small<NP>::MAT, n);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int r = 0; r < NP / 16; ++r)
+#pragma unroll
+    for (int c = 0; c < NP / 16; ++c) {
+      const int idx = (ty + 16 * r) * LD + tx + 16 * c;
+      const float2 h = sH[idx];
+      sH[idx] = make_float2(h.y - 0.5f * acc[r][c].x, -h.x - 0.5f * acc[r][c].y);
+    }
+}
+
+// out[i * ldo + j] = f(X)[i][j] for i, j < nlim.  Ends without a barrier.
+template <int NP>
+__device__ void rhs(const float2* sH, const float2* sL, const float2* sX, float2* sT, int n, int K,
+                    int form, float2* __restrict__ out, int ldo, int nlim) {
+  constexpr int LD = NP + 1;
+  float2 acc[NP / 16][NP / 16];
+  zero_tile<NP>(acc);
+  gemm<NP, false, false>(acc, sH, sX, n);
+  if (form == DQB_FORM_STANDARD) gemm<NP, false, true>(acc, sX, sH, n);
+  const float sc = form == DQB_FORM_HERMITIAN ? 0.5f : 1.0f;
+  for (int k = 0; k < K; ++k) {
+    const float2* Lk = sL + k * Small<NP>::MAT;
+    float2 t[NP / 16][NP / 16];
+    zero_tile<NP>(t);
+    gemm<NP, false, false>(t, Lk, sX, n);
+    __syncthreads();  // readers of the previous T are done
+    store_tile<NP>(sT, t, sc);
+    __syncthreads();
+    gemm<NP, false, true>(acc, sT, Lk, n);
+  }
+  __syncthreads();
+  store_tile<NP>(sT, acc, 1.0f);
+  __syncthreads();
+  const bool herm = form == DQB_FORM_HERMITIAN;
+  for (int e = threadIdx.x; e < NP * NP; e += blockDim.x) {
+    const int i = e / NP, j = e % NP;
+    if (i < nlim && j < nlim) {
+      float2 v = sT[i * LD + j];
+      if (herm) v = cadd(v, cconj(sT[j * LD + i]));
+      out[i * ldo + j] = v;
+    }
+  }
+}
+
+// Write the state at save index `sidx` (y + sum_q cw[q] k_q when `interp`, else y)
+// and its expectation values tr(E_m rho) = sum_ij E_m[j][i] rho[i][j] (FP64 sums).
+template <int NP>
+__device__ void save_point(const DenseSmallArgs& a, long long inst, int sidx, const float2* __restrict__ yv,
+                           float2* const (&kk)[7], const float (&cw)[7], bool interp, double* red) {
+  constexpr int NN = NP * NP;
+  const int n = a.n;
+  for (int m0 = 0; m0 == 0 || m0 < a.nE; m0 += 8) {
+    const int mc = a.nE - m0 < 8 ? a.nE - m0 : 8;
+    double er[8], ei[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) er[m] = ei[m] = 0.0;
+    for (int e = threadIdx.x; e < NN; e += blockDim.x) {
+      const int i = e / NP, j = e % NP;
+      if (i >= n || j >= n) continue;
+      float2 v = yv[e];
+      if (interp) {
+#pragma unroll
+        for (int q = 0; q < 7; ++q) v = caxpy(cw[q], kk[q][e], v);
+      }
+      if (m0 == 0 && a.o.save_states) a.states[((inst * a.ntsave + sidx) * n + i) * n + j] = v;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        if (m < mc) {
+          const float2 ev = a.E[((m0 + m) * n + j) * n + i];
+          er[m] += (double)ev.x * v.x - (double)ev.y * v.y;
+          ei[m] += (double)ev.x * v.y + (double)ev.y * v.x;
+        }
+      }
+    }
+    for (int m = 0; m < mc; ++m) {
+      const double sr = block_sum(er[m], red);
+      const double si = block_sum(ei[m], red);
+      if (threadIdx.x == 0) a.expects[(inst * a.nE + m0 + m) * a.ntsave + sidx] = make_float2((float)sr, (float)si);
+    }
+  }
+}
+
+template <int NP>
+__device__ void solve_one(const DenseSmallArgs& a, long long inst, float2* sH, float2* sX, float2* sT,
+                          float2* sL, float2* slot, double* red, Ctrl& ctl) {
+  constexpr int NN = NP * NP, LD = NP + 1;
+  const int tid = threadIdx.x;
+  const int n = a.n, K = a.K;
+  const CtrlOpts& o = a.o;
+  const Tableau& T = c_tab[o.method];
+  const double inv_nn = 1.0 / (double(n) * double(n));
+
+  // ---- operators ------------------------------------------------------------------
+  const long long hi = a.Hidx ? a.Hidx[inst] : inst;
+  const long long li = a.Lidx ? a.Lidx[inst] : inst;
+  const long long ri = a.ridx ? a.ridx[inst] : inst;
+  load_padded<NP>(sH, a.H + hi * n * n, n);
+  for (int k = 0; k < K; ++k) load_padded<NP>(sL + k * Small<NP>::MAT, a.L + (li * K + k) * n * n, n);
+  __syncthreads();
+  build_hnh<NP>(sH, sL, n, K);
+
+  // ---- initial state (todm for kets) and hermiticity check (rtol = atol = 1e-5) ----
+  if (tid == 0) {
+    ctl.sy = 0;
+    ctl.sy1 = 1;
+    for (int j = 0; j < 7; ++j) ctl.sk[j] = 2 + j;
+    ctl.status = DQB_INST_OK;
+    ctl.nsteps = ctl.nacc = ctl.nrej = 0;
+    ctl.save_idx = 0;
+  }
+  __syncthreads();
+  float2* y = slot + ctl.sy * NN;
+  int bad = 0;
+  for (int e = tid; e < NN; e += blockDim.x) {
+    const int i = e / NP, j = e % NP;
+    float2 v = make_float2(0.f, 0.f);
+    if (i < n && j < n) {
+      if (a.rho0_is_ket) {
+        const float2* psi = a.rho0 + ri * n;
+        v = cmul(psi[i], cconj(psi[j]));
+      } else {
+        const float2* r0 = a.rho0 + ri * n * n;
+        v = r0[i * n + j];
+        if (o.check_hermitian) {
+          const float2 u = cconj(r0[j * n + i]);
+          const float d = cabsf(make_float2(v.x - u.x, v.y - u.y));
+          if (!(d <= 1e-5f + 1e-5f * cabsf(u))) bad = 1;
+        }
+      }
+    }
+    y[e] = v;
+    sX[i * LD + j] = v;
+  }
+  bad = __syncthreads_or(bad);
+  if (bad) {
+    if (tid == 0) {
+      a.status[inst] = DQB_INST_NOT_HERMITIAN;
+      a.infos[inst * 3 + 0] = a.infos[inst * 3 + 1] = a.infos[inst * 3 + 2] = 0;
+    }
+    return;
+  }
+
+  // ---- starting step (Hairer-Norsett-Wanner, RMS norm) --------------------------------
+  const double t1 = a.tsave[a.ntsave - 1];
+  float2* k1 = slot + ctl.sk[0] * NN;
+  float2* kscr = slot + ctl.sk[1] * NN;
+  rhs<NP>(sH, sL, sX, sT, n, K, o.form, k1, NP, NP);
+  __syncthreads();
+  double s0 = 0.0, s1 = 0.0;
+  for (int e = tid; e < NN; e += blockDim.x) {
+    const float2 yv = y[e], fv = k1[e];
+    const double sc = o.atol + o.rtol * (double)cabsf(yv);
+    s0 += (double)cabs2f(yv) / (sc * sc);
+    s1 += (double)cabs2f(fv) / (sc * sc);
+  }
+  s0 = block_sum(s0, red);
+  s1 = block_sum(s1, red);
+  const double d0 = sqrt(s0 * inv_nn), d1 = sqrt(s1 * inv_nn);
+  const double h0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : 0.01 * d0 / d1;
+  const float h0f = (float)h0;
+  for (int e = tid; e < NN; e += blockDim.x) {
+    const int i = e / NP, j = e % NP;
+    sX[i * LD + j] = caxpy(h0f, k1[e], y[e]);
+  }
+  __syncthreads();
+  rhs<NP>(sH, sL, sX, sT, n, K, o.form, kscr, NP, NP);
+  __syncthreads();
+  double s2 = 0.0;
+  for (int e = tid; e < NN; e += blockDim.x) {
+    const float2 yv = y[e], f0 = k1[e], f1 = kscr[e];
+    const double sc = o.atol + o.rtol * (double)cabsf(yv);
+    const double dx = (double)f1.x - (double)f0.x, dy = (double)f1.y - (double)f0.y;
+    s2 += (dx * dx + dy * dy) / (sc * sc);
+  }
+  s2 = block_sum(s2, red);
+  if (tid == 0) {
+    const double d2 = sqrt(s2 * inv_nn) / h0;
+    const double md = d1 > d2 ? d1 : d2;
+    const double h1 = md <= 1e-15 ? fmax(1e-6, h0 * 1e-3) : pow(0.01 / md, 0.2);
+    const double dt = fmin(100.0 * h0, h1);
+    ctl.t = o.t0;
+    ctl.t1 = t1;
+    double tn = o.t0 + dt;
+    if (tn > t1 - 1e-10) tn = t1;
+    ctl.tnext = tn < t1 ? tn : t1;
+    ctl.run = o.t0 < t1;
+  }
+  __syncthreads();
+
+  // ---- degenerate interval: every save is the initial state -------------------------
+  // (handled by the save loop below with theta = 0 when the loop never runs)
+
+  // ---- main loop ----------------------------------------------------------------------
+  while (ctl.run) {
+    if (ctl.nsteps >= o.max_steps) {
+      if (tid == 0) ctl.status = DQB_INST_MAX_STEPS;
+      break;
+    }
+    const double h = ctl.tnext - ctl.t;
+    float2* yv = slot + ctl.sy * NN;
+    float2* y1 = slot + ctl.sy1 * NN;
+    float2* kk[7];
+#pragma unroll
+    for (int j = 0; j < 7; ++j) kk[j] = slot + ctl.sk[j] * NN;
+
+    // stages 2..6
+    for (int s = 1; s < 6; ++s) {
+      float cf[6];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) cf[j] = (float)(h * T.a[s][j]);
+      for (int e = tid; e < NN; e += blockDim.x) {
+        float2 x = yv[e];
+#pragma unroll
+        for (int j = 0; j < 5; ++j)
+          if (j < s) x = caxpy(cf[j], kk[j][e], x);
+        sX[(e / NP) * LD + (e % NP)] = x;
+      }
+      __syncthreads();
+      rhs<NP>(sH, sL, sX, sT, n, K, o.form, kk[s], NP, NP);
+      __syncthreads();
+    }
+    // y1 (FSAL stage input) and k7
+    {
+      float cf[6];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) cf[j] = (float)(h * T.b[j]);
+      for (int e = tid; e < NN; e += blockDim.x) {
+        float2 x = yv[e];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) x = caxpy(cf[j], kk[j][e], x);
+        y1[e] = x;
+        sX[(e / NP) * LD + (e % NP)] = x;
+      }
+      __syncthreads();
+      rhs<NP>(sH, sL, sX, sT, n, K, o.form, kk[6], NP, NP);
+      __syncthreads();
+    }
+    // embedded error, FP64 accumulation
+    double se = 0.0;
+    {
+      double cb[7];
+#pragma unroll
+      for (int j = 0; j < 7; ++j) cb[j] = h * T.btilde[j];
+      for (int e = tid; e < NN; e += blockDim.x) {
+        double ex = 0.0, ey = 0.0;
+#pragma unroll
+        for (int j = 0; j < 7; ++j) {
+          const float2 kv = kk[j][e];
+          ex = fma(cb[j], (double)kv.x, ex);
+          ey = fma(cb[j], (double)kv.y, ey);
+        }
+        const float ya = cabsf(yv[e]), y1a = cabsf(y1[e]);
+        const double sc = o.atol + o.rtol * (double)(ya > y1a ? ya : y1a);
+        se += (ex * ex + ey * ey) / (sc * sc);
+      }
+    }
+    se = block_sum(se, red);
+    if (tid == 0) {
+      const double err = sqrt(se * inv_nn);
+      ctl.nsteps += 1;
+      if (!(err < INFINITY)) {
+        ctl.status = DQB_INST_NONFINITE;
+        ctl.nrej += 1;
+        ctl.run = 0;
+        ctl.keep = 0;
+      } else {
+        const bool keep = err < 1.0;
+        ctl.keep = keep;
+        if (keep) ctl.nacc += 1; else ctl.nrej += 1;
+        ctl.dtnew = h * step_factor(o, err, keep);
+      }
+    }
+    __syncthreads();
+    if (ctl.status != DQB_INST_OK) break;
+
+    if (ctl.keep) {
+      // dense output at every save time in (t, tnext]
+      while (ctl.save_idx < a.ntsave && a.tsave[ctl.save_idx] <= ctl.tnext) {
+        if (tid == 0) {
+          double w[7];
+          const double theta = h > 0.0 ? (a.tsave[ctl.save_idx] - ctl.t) / h : 1.0;
+          dense_weights(o.method, theta, w);
+          for (int j = 0; j < 7; ++j) ctl.w[j] = (float)(h * w[j]);
+        }
+        __syncthreads();
+        float cw[7];
+#pragma unroll
+        for (int j = 0; j < 7; ++j) cw[j] = ctl.w[j];
+        save_point<NP>(a, inst, ctl.save_idx, yv, kk, cw, true, red);
+        __syncthreads();
+        if (tid == 0) ctl.save_idx += 1;
+        __syncthreads();
+      }
+      if (tid == 0) {
+        int tmp = ctl.sy;
+        ctl.sy = ctl.sy1;
+        ctl.sy1 = tmp;
+        tmp = ctl.sk[0];
+        ctl.sk[0] = ctl.sk[6];
+        ctl.sk[6] = tmp;
+        ctl.t = ctl.tnext;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      ctl.tnext = next_tend(ctl.t, ctl.dtnew, ctl.t1, ctl.keep);
+      ctl.run = ctl.t < ctl.t1;
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+
+  // saves left over (t1 <= t0: every save is the initial state)
+  if (ctl.status == DQB_INST_OK) {
+    const float2* yv = slot + ctl.sy * NN;
+    while (ctl.save_idx < a.ntsave && a.tsave[ctl.save_idx] <= ctl.t) {
+      float2* kk[7];
+      float cw[7];
+#pragma unroll
+      for (int j = 0; j < 7; ++j) {
+        kk[j] = slot + ctl.sk[j] * NN;
+        cw[j] = 0.f;
+      }
+      save_point<NP>(a, inst, ctl.save_idx, yv, kk, cw, false, red);
+      __syncthreads();
+      if (tid == 0) ctl.save_idx += 1;
+      __syncthreads();
+    }
+  }
+  // final state when only the last state is kept (SubSaveAt(t1=True))
+  if (!o.save_states) {
+    const float2* yv = slot + ctl.sy * NN;
+    for (int e = tid; e < NN; e += blockDim.x) {
+      const int i = e / NP, j = e % NP;
+      if (i < n && j < n) a.states[(inst * n + i) * n + j] = yv[e];
+    }
+  }
+  if (tid == 0) {
+    a.status[inst] = ctl.status;
+    a.infos[inst * 3 + 0] = (int)ctl.nsteps;
+    a.infos[inst * 3 + 1] = (int)ctl.nacc;
+    a.infos[inst * 3 + 2] = (int)ctl.nrej;
+  }
+}
+
+template <int NP>
+__global__ void __launch_bounds__(kSmallThreads) mesolve_small_kernel(DenseSmallArgs a) {
+  extern __shared__ float4 smem_raw[];
+  __shared__ double red[40];
+  __shared__ Ctrl ctl;
+  float2* sH = reinterpret_cast<float2*>(smem_raw);
+  float2* sX = sH + Small<NP>::MAT;
+  float2* sT = sX + Small<NP>::MAT;
+  float2* sL = sT + Small<NP>::MAT;
+  float2* slot = a.slots + (size_t)blockIdx.x * kSlotMats * Small<NP>::NN;
+  for (;;) {
+    if (threadIdx.x == 0) ctl.inst = (long long)atomicAdd(a.counter, 1u);
+    __syncthreads();
+    const long long inst = ctl.inst;
+    if (inst >= a.batch) break;
+    solve_one<NP>(a, inst, sH, sX, sT, sL, slot, red, ctl);
+    __syncthreads();
+  }
+}
+
+// One right-hand side per instance (no RK loop); out is [batch, n, n].
+template <int NP>
+__global__ void __launch_bounds__(kSmallThreads) rhs_small_kernel(DenseSmallArgs a, int form, const float2* rho,
+                                                                  float2* out) {
+  extern __shared__ float4 smem_raw[];
+  float2* sH = reinterpret_cast<float2*>(smem_raw);
+  float2* sX = sH + Small<NP>::MAT;
+  float2* sT = sX + Small<NP>::MAT;
+  float2* sL = sT + Small<NP>::MAT;
+  const long long b = blockIdx.x;
+  const int n = a.n, K = a.K;
+  const long long hi = a.Hidx ? a.Hidx[b] : b;
+  const long long li = a.Lidx ? a.Lidx[b] : b;
+  load_padded<NP>(sH, a.H + hi * n * n, n);
+  for (int k = 0; k < K; ++k) load_padded<NP>(sL + k * Small<NP>::MAT, a.L + (li * K + k) * n * n, n);
+  load_padded<NP>(sX, rho + b * n * n, n);
+  __syncthreads();
+  build_hnh<NP>(sH, sL, n, K);
+  __syncthreads();
+  rhs<NP>(sH, sL, sX, sT, n, K, form, out + b * n * n, n, n);
+}
+
+// ------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------
+template <int NP>
+static size_t small_smem_bytes(int K) {
+  return (size_t)(3 + K) * Small<NP>::MAT * sizeof(float2);
+}
+
+static int pick_np(int n) { return n <= 16 ? 16 : (n <= 32 ? 32 : (n <= 64 ? 64 : 0)); }
+
+static size_t max_optin_smem() {
+  int dev = 0, v = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return v > 0 ? (size_t)v : (size_t)232448;
+}
+
+static size_t smem_for(int NP, int K) {
+  switch (NP) {
+    case 16: return small_smem_bytes<16>(K);
+    case 32: return small_smem_bytes<32>(K);
+    default: return small_smem_bytes<64>(K);
+  }
+}
+
+// Resident CTAs for (NP, K) on the current device; 0 if the shared memory does not fit.
+template <int NP>
+static int small_grid(int K, long long batch) {
+  const size_t smem = small_smem_bytes<NP>(K);
+  if (smem + 2048 > max_optin_smem()) return 0;
+  cudaFuncSetAttribute(mesolve_small_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mesolve_small_kernel<NP>, kSmallThreads, smem);
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (per_sm < 1) return 0;
+  long long g = (long long)per_sm * sms;
+  if (g > batch) g = batch;
+  return (int)std::max<long long>(g, 1);
+}
+
+static int grid_for(int NP, int K, long long batch) {
+  switch (NP) {
+    case 16: return small_grid<16>(K, batch);
+    case 32: return small_grid<32>(K, batch);
+    default: return small_grid<64>(K, batch);
+  }
+}
+
+}  // namespace dqb
+
+using namespace dqb;
+
+extern "C" int32_t dqb_dense_small_max_n(int32_t n_jumps) {
+  if (n_jumps < 0) return 0;
+  const size_t cap = max_optin_smem() - 2048;
+  if (smem_for(64, n_jumps) <= cap) return 64;
+  if (smem_for(32, n_jumps) <= cap) return 32;
+  if (smem_for(16, n_jumps) <= cap) return 16;
+  return 0;
+}
+
+extern "C" size_t dqb_mesolve_dense_workspace_size(int32_t n, int32_t n_jumps, int64_t batch) {
+  const int NP = pick_np(n);
+  if (NP == 0 || batch <= 0) return 0;
+  const int g = grid_for(NP, n_jumps, batch);
+  if (g <= 0) return 0;
+  return 256 + (size_t)g * kSlotMats * NP * NP * sizeof(float2);
+}
+
+static int validate_dense(const dqb_dense_problem* p, const dqb_ode_options* o) {
+  if (!p || !o) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->n < 1 || p->n_jumps < 0 || p->n_exp < 0 || p->n_tsave < 1 || p->batch < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->batch >= (int64_t)0x7fffffff) return DQB_ERR_INVALID_ARGUMENT;
+  if (!p->H || (p->n_jumps > 0 && !p->L) || !p->rho0 || !p->tsave) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->n_exp > 0 && !p->E) return DQB_ERR_INVALID_ARGUMENT;
+  if (o->method != DQB_METHOD_TSIT5 && o->method != DQB_METHOD_DOPRI5) return DQB_ERR_INVALID_ARGUMENT;
+  if (o->form != DQB_FORM_HERMITIAN && o->form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
+  if (!(o->rtol >= 0) || !(o->atol >= 0) || o->max_steps < 0) return DQB_ERR_INVALID_ARGUMENT;
+  return DQB_OK;
+}
+
+static DenseSmallArgs make_args(const dqb_dense_problem* p, const dqb_ode_options* o, const dqb_outputs* out) {
+  DenseSmallArgs a;
+  a.n = p->n;
+  a.K = p->n_jumps;
+  a.nE = p->n_exp;
+  a.ntsave = p->n_tsave;
+  a.batch = p->batch;
+  a.H = (const float2*)p->H;
+  a.L = (const float2*)p->L;
+  a.rho0 = (const float2*)p->rho0;
+  a.E = (const float2*)p->E;
+  a.rho0_is_ket = p->rho0_is_ket;
+  a.tsave = p->tsave;
+  a.Hidx = p->H_index;
+  a.Lidx = p->L_index;
+  a.ridx = p->rho0_index;
+  a.states = out ? (float2*)out->states : nullptr;
+  a.expects = out ? (float2*)out->expects : nullptr;
+  a.infos = out ? out->infos : nullptr;
+  a.status = out ? out->status : nullptr;
+  a.slots = nullptr;
+  a.counter = nullptr;
+  if (o) a.o = make_ctrl(*o);
+  return a;
+}
+
+extern "C" int dqb_mesolve_dense(const dqb_dense_problem* p, const dqb_ode_options* o, const dqb_outputs* out,
+                                 void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = validate_dense(p, o);
+  if (rc) return rc;
+  if (!out || !out->states || !out->infos || !out->status || (p->n_exp > 0 && !out->expects))
+    return DQB_ERR_INVALID_ARGUMENT;
+  if (p->batch == 0) return DQB_OK;
+  const int NP = pick_np(p->n);
+  if (NP == 0 || dqb_dense_small_max_n(p->n_jumps) < NP) return DQB_ERR_UNSUPPORTED;
+  const size_t need = dqb_mesolve_dense_workspace_size(p->n, p->n_jumps, p->batch);
+  if (need == 0) return DQB_ERR_UNSUPPORTED;
+  if (!workspace || workspace_bytes < need) return DQB_ERR_WORKSPACE_TOO_SMALL;
+  const int grid = grid_for(NP, p->n_jumps, p->batch);
+  cudaStream_t s = (cudaStream_t)stream;
+  DenseSmallArgs a = make_args(p, o, out);
+  a.counter = (unsigned int*)workspace;
+  a.slots = (float2*)((char*)workspace + 256);
+  if (cudaMemsetAsync(workspace, 0, 256, s) != cudaSuccess) return DQB_ERR_CUDA;
+  const size_t smem = smem_for(NP, p->n_jumps);
+  switch (NP) {
+    case 16: mesolve_small_kernel<16><<<grid, kSmallThreads, smem, s>>>(a); break;
+    case 32: mesolve_small_kernel<32><<<grid, kSmallThreads, smem, s>>>(a); break;
+    default: mesolve_small_kernel<64><<<grid, kSmallThreads, smem, s>>>(a); break;
+  }
+  return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+}
+
+extern "C" int dqb_lindblad_rhs_dense(const dqb_dense_problem* p, int32_t form, const void* rho, void* outp,
+                                      void* stream) {
+  if (!p || !rho || !outp) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->n < 1 || p->n_jumps < 0 || p->batch < 0 || !p->H || (p->n_jumps > 0 && !p->L))
+    return DQB_ERR_INVALID_ARGUMENT;
+  if (form != DQB_FORM_HERMITIAN && form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->batch == 0) return DQB_OK;
+  const int NP = pick_np(p->n);
+  if (NP == 0 || dqb_dense_small_max_n(p->n_jumps) < NP) return DQB_ERR_UNSUPPORTED;
+  DenseSmallArgs a = make_args(p, nullptr, nullptr);
+  const size_t smem = smem_for(NP, p->n_jumps);
+  cudaStream_t s = (cudaStream_t)stream;
+  const unsigned grid = (unsigned)p->batch;
+  switch (NP) {
+    case 16:
+      cudaFuncSetAttribute(rhs_small_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      rhs_small_kernel<16><<<grid, kSmallThreads, smem, s>>>(a, form, (const float2*)rho, (float2*)outp);
+      break;
+    case 32:
+      cudaFuncSetAttribute(rhs_small_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      rhs_small_kernel<32><<<grid, kSmallThreads, smem, s>>>(a, form, (const float2*)rho, (float2*)outp);
+      break;
+    default:
+      cudaFuncSetAttribute(rhs_small_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      rhs_small_kernel<64><<<grid, kSmallThreads, smem, s>>>(a, form, (const float2*)rho, (float2*)outp);
+      break;
+  }
+  return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+}
+
+extern "C" const char* dqb_version(void) { return "dqb200 0.1 sm_100a"; }

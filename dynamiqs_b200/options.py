@@ -1,0 +1,44 @@
+"""``Options`` and the per-solver option check, as in ``dynamiqs/options.py:17-123``."""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, fields
+from typing import Any, Callable
+
+__all__ = ['Options', 'check_options']
+
+
+@dataclass(frozen=True)
+class Options:
+    save_states: bool = True
+    save_propagators: bool = True
+    cartesian_batching: bool = True
+    progress_meter: Any = None
+    t0: float | None = None
+    save_extra: Callable | None = None
+    nmaxclick: int = 10_000
+    vectorized: bool = False
+    assume_hermitian: bool = True
+
+    def initialise(self) -> Options:
+        return self
+
+
+_SUPPORTED = {
+    'mesolve': ('save_states', 'cartesian_batching', 'progress_meter', 't0', 'save_extra',
+                'vectorized', 'assume_hermitian'),
+}
+
+
+def check_options(options: Options, solver_name: str) -> None:
+    """Raise if an option that ``solver_name`` ignores differs from its default
+    (``dynamiqs/options.py:80-123``)."""
+    valid = _SUPPORTED[solver_name]
+    default = Options()
+    for f in fields(options):
+        value = getattr(options, f.name)
+        if f.name not in valid and value != getattr(default, f.name):
+            valid_str = ', '.join(f'`{x}`' for x in valid)
+            raise ValueError(
+                f'Option `{f.name}` was set to `{value}` but is not used by '
+                f'the solver `dq.{solver_name}()` (valid options: {valid_str}).')

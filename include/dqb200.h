@@ -1,0 +1,131 @@
+/*
+ * dqb200.h -- C ABI of the B200 (sm_100a) implementation of dynamiqs' mesolve hot
+ * path: the Lindblad right-hand side evaluated inside the Tsit5 / Dopri5 adaptive
+ * Runge-Kutta loop, with embedded error norm, step-size controller and tsave saving.
+ *
+ * Every entry point takes plain pointers and sizes.  Array arguments are DEVICE
+ * pointers (complex64 = interleaved float re/im, like numpy / JAX complex64) unless
+ * stated otherwise; `stream` is a cudaStream_t passed as void*.  Work is enqueued on
+ * `stream` and nothing synchronises the device.  No entry point allocates device
+ * memory: scratch space is the caller's `workspace` buffer, sized by the matching
+ * *_workspace_size() query.  Errors are returned as a DQB_* status code (0 = OK);
+ * per-instance outcomes (max_steps reached, non-finite state, ...) are written to the
+ * caller's `status` array.  No C++ exception crosses this boundary and no kernel traps.
+ *
+ * Reference interfaces replaced (paths relative to the dynamiqs repository):
+ *   - DiffraxIntegrator.run / diffeqsolve       dynamiqs/integrators/core/diffrax_integrator.py:101-147
+ *   - MESolveDiffraxIntegrator vector fields    dynamiqs/integrators/core/diffrax_integrator.py:312-336
+ *   - SolveSaveMixin.save / postprocess_saved   dynamiqs/integrators/core/save_mixin.py:44-68
+ *   - AdaptiveStepInfos                         dynamiqs/integrators/core/diffrax_integrator.py:35-50,149-157
+ *   - sparse-DIA matmul primitives              dynamiqs/qarrays/sparsedia_primitives.py:199-261
+ */
+#ifndef DQB200_H
+#define DQB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DQB_API __attribute__((visibility("default")))
+#else
+#define DQB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ------------------------------------------------------------ */
+#define DQB_OK 0
+#define DQB_ERR_INVALID_ARGUMENT 1
+#define DQB_ERR_UNSUPPORTED 2
+#define DQB_ERR_WORKSPACE_TOO_SMALL 3
+#define DQB_ERR_CUDA 4
+
+/* ---- per-instance status (written to outputs->status[b]) -------------------- */
+#define DQB_INST_OK 0
+#define DQB_INST_MAX_STEPS 1     /* diffrax "maximum number of method steps" error   */
+#define DQB_INST_NONFINITE 2     /* NaN/inf in the state or the error estimate       */
+#define DQB_INST_NOT_HERMITIAN 3 /* check_hermitian(rho0) failed (rtol = atol = 1e-5) */
+
+/* ---- options ----------------------------------------------------------------- */
+#define DQB_METHOD_TSIT5 0
+#define DQB_METHOD_DOPRI5 1
+#define DQB_FORM_HERMITIAN 0 /* tmp = Hnh rho + 1/2 sum L rho L^+ ; out = tmp + tmp^+ */
+#define DQB_FORM_STANDARD 1  /* Hnh rho + rho Hnh^+ + sum L rho L^+                 */
+
+/* Mirrors dq.method.Tsit5 / Dopri5 (dynamiqs/method.py:121-127,356-476) and the
+ * mesolve options that reach the integrator (dynamiqs/options.py:17-77). */
+typedef struct dqb_ode_options {
+  int32_t method;          /* DQB_METHOD_*                                              */
+  int32_t form;            /* DQB_FORM_*                                                */
+  double rtol;             /* relative tolerance (default 1e-6)                         */
+  double atol;             /* absolute tolerance (default 1e-6)                         */
+  double safety;           /* safety factor (default 0.9)                               */
+  double factormin;        /* min step factor after a rejection (default 0.2)           */
+  double factormax;        /* max step factor (default 5.0)                             */
+  int64_t max_steps;       /* attempted steps before DQB_INST_MAX_STEPS (100_000)       */
+  double t0;               /* start time: tsave[0] unless options.t0 is set             */
+  int32_t save_states;     /* 1: state at every tsave; 0: final state only              */
+  int32_t check_hermitian; /* 1: flag rho0 that fails isherm(rtol=atol=1e-5)            */
+} dqb_ode_options;
+
+/* Outputs of a batched solve.  nsave = n_tsave if save_states else 1. */
+typedef struct dqb_outputs {
+  void* states;    /* complex64 [batch, nsave, n, n]                      */
+  void* expects;   /* complex64 [batch, n_exp, n_tsave], NULL if n_exp==0 */
+  int32_t* infos;  /* int32 [batch, 3]: nsteps, naccepted, nrejected      */
+  int32_t* status; /* int32 [batch]: DQB_INST_*                           */
+} dqb_outputs;
+
+/* ---- dense operators ---------------------------------------------------------- */
+/* Instance b solves with H[H_index[b]], jump set L[L_index[b]] (n_jumps matrices)
+ * and rho0[rho0_index[b]]; a NULL index array means "item b".  This is how the
+ * cartesian / flat batching of _vectorized_mesolve (mesolve.py:307-336) reaches the
+ * kernels without materialising broadcast copies. */
+typedef struct dqb_dense_problem {
+  int32_t n;             /* Hilbert dimension                                  */
+  int32_t n_jumps;       /* K                                                  */
+  int32_t n_exp;         /* number of exp_ops                                  */
+  int32_t n_tsave;       /* >= 1                                               */
+  int64_t batch;         /* number of instances                                */
+  const void* H;         /* complex64 [*, n, n]                                */
+  const void* L;         /* complex64 [*, n_jumps, n, n]                       */
+  const void* rho0;      /* complex64 [*, n, n], or [*, n, 1] if rho0_is_ket   */
+  int32_t rho0_is_ket;   /* 1: rho0 = psi psi^+ (todm, utils/general.py:821)   */
+  const void* E;         /* complex64 [n_exp, n, n]                            */
+  const double* tsave;   /* float64 [n_tsave], strictly ascending              */
+  const int32_t* H_index;    /* int32 [batch] or NULL */
+  const int32_t* L_index;    /* int32 [batch] or NULL */
+  const int32_t* rho0_index; /* int32 [batch] or NULL */
+} dqb_dense_problem;
+
+/* Scratch bytes needed by dqb_mesolve_dense on the current device. */
+DQB_API size_t dqb_mesolve_dense_workspace_size(int32_t n, int32_t n_jumps, int64_t batch);
+
+/* Batched adaptive solve with dense operators.  Replaces DiffraxIntegrator.run for
+ * MESolveDiffraxIntegrator with Tsit5 / Dopri5 (diffrax_integrator.py:135-147,
+ * 283-378).  n <= 64: one persistent CTA per in-flight instance, the whole RK loop on
+ * the device (operators and the stage input in shared memory, stages in an
+ * L2-resident per-CTA scratch slot).  Larger n: see dqb_mesolve_dense_large. */
+DQB_API int dqb_mesolve_dense(const dqb_dense_problem* problem, const dqb_ode_options* options,
+                      const dqb_outputs* outputs, void* workspace,
+                      size_t workspace_bytes, void* stream);
+
+/* One Lindblad right-hand-side evaluation per instance, out[b] = f(rho[b]) with
+ * operators H[H_index[b]], L[L_index[b]] (vector_field_unvec_hermitian / _standard,
+ * diffrax_integrator.py:312-323).  rho, out: complex64 [batch, n, n]. n <= 64. */
+DQB_API int dqb_lindblad_rhs_dense(const dqb_dense_problem* problem, int32_t form,
+                           const void* rho, void* out, void* stream);
+
+/* ---- library info ------------------------------------------------------------- */
+/* Largest n handled by the shared-memory persistent kernel for a jump count. */
+DQB_API int32_t dqb_dense_small_max_n(int32_t n_jumps);
+/* Build string (arch, version). */
+DQB_API const char* dqb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DQB200_H */

@@ -1,0 +1,198 @@
+"""GPU parity of the dense persistent kernel (n <= 64) against the oracle, through the
+C ABI (``dqb_lindblad_rhs_dense``, ``dqb_mesolve_dense``) and the public ``mesolve``.
+
+Tolerances: the bar of the build is <= 1e-5 relative Frobenius error on every saved
+state, and |<E> - <E>_ref| <= 1e-5 * max(|<E>_ref|, 1) on every expectation value,
+against the oracle run on the same inputs with the same method, tolerances and
+controller (complex128 state).  Single right-hand sides are compared at 2e-6 relative
+(FP32 products of length <= 64)."""
+
+import numpy as np
+import pytest
+import torch
+
+import dynamiqs_b200 as dq
+from dynamiqs_b200 import _lib
+from dynamiqs_b200 import operators as ops
+from dynamiqs_b200 import workloads
+from oracle import lindblad as lb
+from oracle.mesolve import mesolve as oracle_mesolve
+from tests.systems import ocavity, random_problem, readme_oscillator
+
+pytestmark = pytest.mark.gpu
+
+STATE_RTOL = 1e-5
+EXPECT_TOL = 1e-5
+
+
+def rel_frob(x, ref):
+    x, ref = np.asarray(x), np.asarray(ref)
+    return np.linalg.norm(x - ref, axis=(-2, -1)) / np.maximum(np.linalg.norm(ref, axis=(-2, -1)), 1e-30)
+
+
+def expect_err(x, ref):
+    return np.abs(np.asarray(x) - ref) / np.maximum(np.abs(ref), 1.0)
+
+
+def _dev(x, dtype=torch.complex64):
+    return torch.from_numpy(np.ascontiguousarray(x)).to('cuda', dtype)
+
+
+@pytest.mark.parametrize('n', [2, 7, 16, 33, 64])
+@pytest.mark.parametrize('K', [0, 1, 3])
+@pytest.mark.parametrize('form', [_lib.FORM_HERMITIAN, _lib.FORM_STANDARD])
+def test_rhs_matches_oracle(cuda_device, n, K, form):
+    if _lib.load().dqb_dense_small_max_n(K) < n:
+        pytest.skip('jump count beyond shared memory at this n')
+    B = 3
+    rng = np.random.default_rng(n * 10 + K)
+    Hs, Lsets, rhos = [], [], []
+    for b in range(B):
+        H, Ls, rho = random_problem(n, K, seed=int(rng.integers(1 << 30)),
+                                    hermitian_rho=form == _lib.FORM_HERMITIAN)
+        Hs.append(H)
+        Lsets.append(np.stack(Ls) if K else np.zeros((0, n, n), np.complex64))
+        rhos.append(rho)
+    H_d, L_d, r_d = _dev(np.stack(Hs)), _dev(np.stack(Lsets)), _dev(np.stack(rhos))
+    out = torch.empty_like(r_d)
+    prob = _lib.DenseProblem(n=n, n_jumps=K, batch=B, H=H_d.data_ptr(), L=L_d.data_ptr())
+    lib = _lib.load()
+    rc = lib.dqb_lindblad_rhs_dense(prob, form, r_d.data_ptr(), out.data_ptr(),
+                                    torch.cuda.current_stream().cuda_stream)
+    _lib.check(rc, 'rhs')
+    got = out.cpu().numpy()
+    for b in range(B):
+        Hc = Hs[b].astype(complex)
+        Lc = [L.astype(complex) for L in Lsets[b]]
+        rc_ = rhos[b].astype(complex)
+        ref = lb.vf_hermitian(Hc, Lc, rc_) if form == _lib.FORM_HERMITIAN else lb.vf_standard(Hc, Lc, rc_)
+        assert rel_frob(got[b], ref) < 2e-6
+
+
+def _compare_solve(res, H, Ls, rho0, tsave, exp_ops, method, **okw):
+    r = oracle_mesolve(H, Ls, rho0, tsave, exp_ops=exp_ops,
+                       method='Tsit5' if isinstance(method, dq.Tsit5) else 'Dopri5',
+                       rtol=method.rtol, atol=method.atol, **okw)
+    got = res.states.cpu().numpy()
+    assert rel_frob(got, r.states).max() < STATE_RTOL
+    if exp_ops:
+        assert expect_err(res.expects.cpu().numpy(), r.expects).max() < EXPECT_TOL
+    info = res.infos
+    assert abs(int(info.nsteps) - r.nsteps) <= 1
+    return r
+
+
+@pytest.mark.parametrize('method', [dq.Tsit5(rtol=1e-6, atol=1e-8), dq.Dopri5(rtol=1e-6, atol=1e-8)],
+                         ids=['tsit5', 'dopri5'])
+def test_lossy_oscillator_config(cuda_device, method):
+    """Plain lossy oscillator: n=16, omega=1, kappa=0.1, alpha0=1, 101 saves."""
+    w = workloads.lossy_oscillator()
+    res = dq.mesolve(w['H'], w['jump_ops'], w['rho0'], w['tsave'], exp_ops=w['exp_ops'],
+                     method=method)
+    assert res.states.shape == (101, 16, 16)
+    assert res.expects.shape == (1, 101)
+    _compare_solve(res, w['H'], w['jump_ops'], w['rho0'], w['tsave'], w['exp_ops'], method)
+
+
+def test_readme_step_count_matches_oracle(cuda_device):
+    p = readme_oscillator()
+    res = dq.mesolve(p['H'], p['jump_ops'], p['rho0'], p['tsave'])
+    r = oracle_mesolve(p['H'], p['jump_ops'], p['rho0'], p['tsave'])
+    assert int(res.infos.nsteps) == r.nsteps
+    assert int(res.infos.nrejected) == r.nrejected == 0
+
+
+@pytest.mark.parametrize('layout', ['dense', 'dia'])
+@pytest.mark.parametrize('opts', [dq.Options(), dq.Options(assume_hermitian=False),
+                                  dq.Options(vectorized=True)], ids=['herm', 'std', 'vec'])
+def test_ocavity_analytic(cuda_device, layout, opts):
+    """The reference's TestMESolveAdaptive.test_correctness system and tolerances."""
+    p = ocavity(layout)
+    res = dq.mesolve(p['H'], p['jump_ops'], p['rho0'], p['tsave'], exp_ops=p['exp_ops'],
+                     options=opts)
+    errs = np.linalg.norm(res.states.cpu().numpy() - p['true_states'], axis=(-2, -1))
+    assert np.all(errs <= 1e-3)
+    np.testing.assert_allclose(res.expects.cpu().numpy(), p['true_expects'], rtol=1e-3, atol=1e-4)
+
+
+def test_batched_kerr_subset(cuda_device):
+    """Batched Kerr (n=64, two jumps) on a subset of instances, each against the oracle."""
+    w = workloads.batched_kerr(batch=6, seed=7)
+    res = dq.mesolve(w['H'], w['jump_ops'], w['rho0'], w['tsave'], exp_ops=w['exp_ops'],
+                     method=w['method'])
+    assert res.states.shape == (6, 51, 64, 64)
+    for b in range(6):
+        sub = dq.MESolveResult(None, w['method'], None, None, res.states[b], res.expects[b],
+                               dq.AdaptiveStepInfos(res.infos.nsteps[b], res.infos.naccepted[b],
+                                                    res.infos.nrejected[b]))
+        _compare_solve(sub, w['H'][b], w['jump_ops'], w['rho0'], w['tsave'], w['exp_ops'],
+                       w['method'])
+
+
+def test_standard_form_non_hermitian_rho(cuda_device):
+    H, Ls, rho = random_problem(12, 2, seed=11, hermitian_rho=False)
+    ts = np.linspace(0, 1.5, 7)
+    res = dq.mesolve(H, Ls, rho, ts, options=dq.Options(assume_hermitian=False))
+    _compare_solve(res, H, Ls, rho, ts, None, dq.Tsit5(), form='standard')
+    with pytest.raises(RuntimeError, match='not hermitian'):
+        dq.mesolve(H, Ls, rho, ts)
+
+
+def test_cartesian_batching_equals_single_solves(cuda_device):
+    n = 10
+    a = ops.destroy(n, layout='dense')
+    Hs = np.stack([w * (ops.dag(a) @ a) for w in (0.5, 1.0, 1.5)])
+    L0 = np.stack([np.float32(np.sqrt(k)) * a for k in (0.1, 0.3)])
+    rho0 = np.stack([ops.coherent(n, al) for al in (0.3, 0.6)])
+    ts = np.linspace(0, 2, 5)
+    E = [ops.number(n, layout='dense')]
+    res = dq.mesolve(Hs, [L0], rho0, ts, exp_ops=E)
+    assert res.states.shape == (3, 2, 2, 5, n, n)
+    assert res.expects.shape == (3, 2, 2, 1, 5)
+    for i in range(3):
+        for j in range(2):
+            for k in range(2):
+                single = dq.mesolve(Hs[i], [L0[j]], rho0[k], ts, exp_ops=E)
+                np.testing.assert_array_equal(res.states[i, j, k].cpu().numpy(),
+                                              single.states.cpu().numpy())
+    flat = dq.mesolve(Hs[:2], [L0], rho0, ts, options=dq.Options(cartesian_batching=False))
+    assert flat.states.shape == (2, 5, n, n)
+
+
+def test_save_states_false_and_t0(cuda_device):
+    p = readme_oscillator()
+    full = dq.mesolve(p['H'], p['jump_ops'], p['rho0'], p['tsave'])
+    last = dq.mesolve(p['H'], p['jump_ops'], p['rho0'], p['tsave'],
+                      options=dq.Options(save_states=False))
+    assert last.states.shape == (1, 16, 16)
+    assert rel_frob(last.final_state.cpu().numpy(), full.final_state.cpu().numpy()) < 1e-5
+    shifted = dq.mesolve(p['H'], p['jump_ops'], p['rho0'], p['tsave'][50:],
+                         options=dq.Options(t0=0.0))
+    r = oracle_mesolve(p['H'], p['jump_ops'], p['rho0'], p['tsave'][50:], t0=0.0)
+    assert rel_frob(shifted.states.cpu().numpy(), r.states).max() < STATE_RTOL
+
+
+def test_max_steps_error(cuda_device):
+    p = readme_oscillator()
+    with pytest.raises(RuntimeError, match='maximum number of method steps'):
+        dq.mesolve(p['H'], p['jump_ops'], p['rho0'], p['tsave'], method=dq.Tsit5(max_steps=5))
+
+
+def test_nonfinite_status(cuda_device):
+    H, Ls, rho = random_problem(4, 1, seed=1)
+    H = H.copy()
+    H[0, 0] = np.nan
+    with pytest.raises(RuntimeError, match='non-finite'):
+        dq.mesolve(H, Ls, rho, np.linspace(0, 1, 3))
+
+
+def test_capi_rejects_bad_arguments(cuda_device):
+    lib = _lib.load()
+    opts = _lib.OdeOptions(method=7, rtol=1e-6, atol=1e-6, safety=0.9, factormin=0.2,
+                           factormax=5.0, max_steps=10)
+    prob = _lib.DenseProblem(n=4, n_jumps=0, n_exp=0, n_tsave=2, batch=1)
+    outs = _lib.Outputs()
+    assert lib.dqb_mesolve_dense(prob, opts, outs, None, 0, None) == _lib.DQB_ERR_INVALID_ARGUMENT
+    assert lib.dqb_mesolve_dense(None, opts, outs, None, 0, None) == _lib.DQB_ERR_INVALID_ARGUMENT
+    assert lib.dqb_dense_small_max_n(2) == 64
+    assert lib.dqb_mesolve_dense_workspace_size(64, 2, 4096) > 0

@@ -1,0 +1,102 @@
+"""Host-side logic of the drop-in API: argument checks with the reference's messages,
+batching plans (cartesian and flat, mesolve.py:307-336) and the no-fallback rule."""
+
+import numpy as np
+import pytest
+
+import dynamiqs_b200 as dq
+from dynamiqs_b200 import operators as ops
+from dynamiqs_b200.mesolve import make_batch_plan
+
+
+def _problem(n=4):
+    a = ops.destroy(n, layout='dense')
+    return ops.dag(a) @ a, [a], ops.fock(n, 0), np.linspace(0, 1, 5)
+
+
+def test_check_times_messages():
+    H, Ls, r, _ = _problem()
+    with pytest.raises(ValueError, match='strictly ascending'):
+        dq.mesolve(H, Ls, r, [0.0, 1.0, 0.5])
+    with pytest.raises(ValueError, match='1D array'):
+        dq.mesolve(H, Ls, r, np.zeros((2, 2)))
+
+
+def test_shape_messages():
+    H, Ls, r, ts = _problem()
+    with pytest.raises(ValueError, match=r'Argument `H` must have shape'):
+        dq.mesolve(np.zeros((4, 3)), Ls, r, ts)
+    with pytest.raises(ValueError, match=r'Argument `jump_ops\[0\]` must have shape'):
+        dq.mesolve(H, [np.zeros((4, 3))], r, ts)
+    with pytest.raises(ValueError, match=r'Argument `rho0` must have shape'):
+        dq.mesolve(H, Ls, np.zeros((4, 3)), ts)
+    with pytest.raises(ValueError, match=r'exp_ops\[0\]'):
+        dq.mesolve(H, Ls, r, ts, exp_ops=[np.zeros((2, 4, 4))])
+    with pytest.raises(ValueError, match='layout `dense`'):
+        dq.mesolve(H, Ls, ops.number(4), ts)
+
+
+def test_options_and_method_checks():
+    H, Ls, r, ts = _problem()
+    with pytest.raises(ValueError, match='Option `save_propagators`'):
+        dq.mesolve(H, Ls, r, ts, options=dq.Options(save_propagators=False))
+
+    class Euler(dq.method.Method):
+        pass
+
+    with pytest.raises(TypeError, match='Method of type `Euler` is not supported'):
+        dq.mesolve(H, Ls, r, ts, method=Euler())
+    with pytest.raises(NotImplementedError):
+        dq.mesolve(H, Ls, r, ts, gradient=object())
+
+
+def test_cartesian_batch_plan():
+    n = 3
+    H = np.zeros((2, 3, n, n), np.complex64)
+    L0 = np.zeros((4, n, n), np.complex64)
+    L1 = np.zeros((n, n), np.complex64)
+    r = np.zeros((5, n, 1), np.complex64)
+    p = make_batch_plan(H, [L0, L1], r, cartesian=True)
+    assert p.bshape == (2, 3, 4, 5)
+    idx = np.arange(p.batch).reshape(p.bshape + (1,))
+    hi, li, ri = (x.reshape(p.bshape) for x in (p.H_index, p.L_index, p.rho_index))
+    I = np.indices(p.bshape)
+    np.testing.assert_array_equal(hi, I[0] * 3 + I[1])
+    np.testing.assert_array_equal(li, I[2])
+    np.testing.assert_array_equal(ri, I[3])
+    assert p.L_sets.shape == (4, 2, n, n)
+    del idx
+
+
+def test_flat_batch_plan_broadcasts():
+    n = 2
+    rng = np.random.default_rng(0)
+    H = rng.normal(size=(2, 3, n, n)).astype(np.complex64)
+    L0 = rng.normal(size=(3, n, n)).astype(np.complex64)
+    L1 = rng.normal(size=(2, 1, n, n)).astype(np.complex64)
+    r = rng.normal(size=(3, n, n)).astype(np.complex64)
+    p = make_batch_plan(H, [L0, L1], r, cartesian=False)
+    assert p.bshape == (2, 3)
+    for b in range(6):
+        i, j = divmod(b, 3)
+        np.testing.assert_array_equal(p.H_items[p.H_index[b]], H[i, j])
+        np.testing.assert_array_equal(p.L_sets[p.L_index[b], 0], L0[j])
+        np.testing.assert_array_equal(p.L_sets[p.L_index[b], 1], L1[i, 0])
+        np.testing.assert_array_equal(p.rho_items[p.rho_index[b]], r[j])
+
+
+def test_no_cpu_fallback(monkeypatch):
+    import torch
+
+    monkeypatch.setattr(torch.cuda, 'is_available', lambda: False)
+    H, Ls, r, ts = _problem()
+    with pytest.raises(RuntimeError, match='no CPU fallback'):
+        dq.mesolve(H, Ls, r, ts)
+
+
+def test_operator_constructors_match_reference_examples():
+    # dq.position(3) and dq.displace(4, 0.5) printed in the reference docstrings
+    # (dynamiqs/utils/operators.py:586-590, 496-500)
+    np.testing.assert_allclose(ops.position(3).to_dense(),
+                               [[0, .5, 0], [.5, 0, .70710678], [0, .70710678, 0]], atol=1e-6)
+    np.testing.assert_allclose(ops.displace(4, 0.5)[:, 0], [0.882, 0.441, 0.156, 0.047], atol=1e-3)

@@ -187,7 +187,7 @@ def run_b200(args):
     L_d = torch.from_numpy(np.stack(w['jump_ops'])[None].copy()).to(dev)
     r_d = torch.from_numpy(w['rho0'].copy()).to(dev)
     E_d = torch.from_numpy(np.stack(w['exp_ops']).copy()).to(dev)
-    ts = w['tsave']
+    ts = w['tsave'] if args.tend == 10.0 else np.linspace(0.0, args.tend, 51)
     ts_d = torch.from_numpy(ts).to(dev)
     zeros = torch.zeros(B, dtype=torch.int32, device=dev)
     H_idx = torch.arange(B, dtype=torch.int32, device=dev)
@@ -357,6 +357,8 @@ def main():
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--batch', type=int, default=4096)
     ap.add_argument('--seed', type=int, default=0)
+    ap.add_argument('--tend', type=float, default=10.0, help='end time (10 in the workload; '
+                    'shorter only for profiling captures)')
     ap.add_argument('--e2e-steps', type=int, default=1)
     ap.add_argument('--cpu-sample', type=int, default=3)
     ap.add_argument('--no-e2e', action='store_true')

@@ -20,11 +20,13 @@ DQB_ERR_INVALID_ARGUMENT = 1
 DQB_ERR_UNSUPPORTED = 2
 DQB_ERR_WORKSPACE_TOO_SMALL = 3
 DQB_ERR_CUDA = 4
+DQB_ERR_SCRATCH_TOO_SMALL = 5
 _RC_NAMES = {
     DQB_ERR_INVALID_ARGUMENT: 'invalid argument',
     DQB_ERR_UNSUPPORTED: 'unsupported problem size or option',
     DQB_ERR_WORKSPACE_TOO_SMALL: 'workspace too small',
     DQB_ERR_CUDA: 'CUDA launch error',
+    DQB_ERR_SCRATCH_TOO_SMALL: 'problem needs more than the static scratch array',
 }
 
 # per-instance status
@@ -89,6 +91,8 @@ SIGNATURES = {
     'dqb_mesolve_dense_workspace_size': (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64]),
     'dqb_mesolve_dense': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
                                          ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
+    'dqb_mesolve_dense_noalloc': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
+                                                 ctypes.POINTER(Outputs), _P]),
     'dqb_lindblad_rhs_dense': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.c_int32, _P, _P, _P]),
     'dqb_dense_small_max_n': (ctypes.c_int32, [ctypes.c_int32]),
     'dqb_version': (ctypes.c_char_p, []),

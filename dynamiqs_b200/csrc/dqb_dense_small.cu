@@ -677,3 +677,50 @@ extern "C" int dqb_lindblad_rhs_dense(const dqb_dense_problem* p, int32_t form, 
 }
 
 extern "C" const char* dqb_version(void) { return "dqb200 0.1 sm_100a"; }
+
+// ------------------------------------------------------------------------------------
+// internal helpers for entry points that bring their own scratch (not exported)
+// ------------------------------------------------------------------------------------
+namespace dqb {
+
+// Bytes of one in-flight instance's scratch slot for dimension n (0 if n > 64).
+size_t small_slot_bytes(int n) {
+  const int NP = pick_np(n);
+  return NP ? (size_t)kSlotMats * NP * NP * sizeof(float2) : 0;
+}
+
+// Resident CTAs of the persistent kernel for (n, K, batch) on the current device.
+int small_resident_grid(int n, int K, long long batch) {
+  const int NP = pick_np(n);
+  return NP ? grid_for(NP, K, batch) : 0;
+}
+
+// Argument checks of dqb_mesolve_dense, without the workspace.
+int small_check_args(const dqb_dense_problem* p, const dqb_ode_options* o, const dqb_outputs* out) {
+  int rc = validate_dense(p, o);
+  if (rc) return rc;
+  if (!out || !out->states || !out->infos || !out->status || (p->n_exp > 0 && !out->expects))
+    return DQB_ERR_INVALID_ARGUMENT;
+  const int NP = pick_np(p->n);
+  if (NP == 0 || dqb_dense_small_max_n(p->n_jumps) < NP) return DQB_ERR_UNSUPPORTED;
+  return DQB_OK;
+}
+
+// Launch the persistent kernel on `grid` CTAs with a zeroed work counter at `counter`
+// and grid * small_slot_bytes(n) bytes of slots at `slots` (both device addresses).
+int small_launch_with_scratch(const dqb_dense_problem* p, const dqb_ode_options* o, const dqb_outputs* out,
+                              unsigned int* counter, void* slots, int grid, cudaStream_t s) {
+  const int NP = pick_np(p->n);
+  DenseSmallArgs a = make_args(p, o, out);
+  a.counter = counter;
+  a.slots = (float2*)slots;
+  const size_t smem = smem_for(NP, p->n_jumps);
+  switch (NP) {
+    case 16: mesolve_small_kernel<16><<<grid, kSmallThreads, smem, s>>>(a); break;
+    case 32: mesolve_small_kernel<32><<<grid, kSmallThreads, smem, s>>>(a); break;
+    default: mesolve_small_kernel<64><<<grid, kSmallThreads, smem, s>>>(a); break;
+  }
+  return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+}
+
+}  // namespace dqb

@@ -41,6 +41,7 @@ extern "C" {
 #define DQB_ERR_UNSUPPORTED 2
 #define DQB_ERR_WORKSPACE_TOO_SMALL 3
 #define DQB_ERR_CUDA 4
+#define DQB_ERR_SCRATCH_TOO_SMALL 5 /* problem needs more than DQB_NOALLOC_SCRATCH_BYTES */
 
 /* ---- per-instance status (written to outputs->status[b]) -------------------- */
 #define DQB_INST_OK 0
@@ -117,6 +118,25 @@ DQB_API int dqb_mesolve_dense(const dqb_dense_problem* problem, const dqb_ode_op
  * diffrax_integrator.py:312-323).  rho, out: complex64 [batch, n, n]. n <= 64. */
 DQB_API int dqb_lindblad_rhs_dense(const dqb_dense_problem* problem, int32_t form,
                            const void* rho, void* out, void* stream);
+
+/* Same solve as dqb_mesolve_dense, for callers that cannot allocate device memory.
+ * No counterpart in the reference (it is an addition of this library).  Who needs it:
+ * code running in a process whose framework already holds nearly all device memory in
+ * its own pool (JAX preallocates 75% of it by default), where a cudaMalloc made for this
+ * library fails or takes memory the framework does not track, and deployments whose
+ * device footprint is fixed when the library loads.  Scratch comes from a static device
+ * array of DQB_NOALLOC_SCRATCH_BYTES that every GPU loading the library keeps until the
+ * process exits; nothing is allocated or freed.  At most
+ * (DQB_NOALLOC_SCRATCH_BYTES - 256) / (9 * NP * NP * 8) instances run at once (NP = n
+ * rounded up to 16, 32 or 64: 28 at n = 64), so results equal dqb_mesolve_dense's but
+ * throughput is lower.  n > 64 returns DQB_ERR_UNSUPPORTED; a problem whose single-instance
+ * scratch exceeds the array returns DQB_ERR_SCRATCH_TOO_SMALL.  The first call on each
+ * device looks up the array's address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  All calls share the array: each clears its work counter first; calls
+ * that overlap on the GPU race and must be serialised by the caller. */
+#define DQB_NOALLOC_SCRATCH_BYTES (8u << 20)
+DQB_API int dqb_mesolve_dense_noalloc(const dqb_dense_problem* problem, const dqb_ode_options* options,
+                                      const dqb_outputs* outputs, void* stream);
 
 /* ---- library info ------------------------------------------------------------- */
 /* Largest n handled by the shared-memory persistent kernel for a jump count. */

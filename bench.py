@@ -29,12 +29,17 @@ import subprocess
 import sys
 import time
 
-import numpy as np
+# The oracle legs run numpy; its OpenBLAS is built with MAX_THREADS=64, whose threaded
+# complex GEMM has misbehaved on hosts with more cores.  The CPU legs use one thread per
+# process anyway.
+for _v in ('OPENBLAS_NUM_THREADS', 'OMP_NUM_THREADS', 'MKL_NUM_THREADS'):
+    os.environ.setdefault(_v, '1')
+
+import numpy as np  # noqa: E402
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = 'batched driven Kerr: n=64, B=4096, K=2 jumps, t=[0,10], 51 saves, Tsit5 1e-6/1e-8'
 METRIC = 'mesolve solves/sec vs plain GPU path at equal 1e-5 error; p50/p99 latency'
 
 
@@ -138,7 +143,7 @@ def run_reference(args):
         'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': 1e3 * total / args.steps, 'higher_is_better': True, 'scaling': 'weak',
         'vs_baseline': None, 'dtype': 'c64', 'data': 'synthetic (seeded)',
-        'config': {'workload': WORKLOAD, 'sample_per_step': per_step},
+        'config': {'workload': CASES['kerr'], 'sample_per_step': per_step},
         'cpu_baseline': {'value': value, 'unit': 'solves/s', 'cores': cores, 'kind': 'port',
                          'sample': f'{per_step} instances per step (one per core) through '
                                    'the numpy oracle; the reference (JAX + diffrax) is not '
@@ -153,11 +158,56 @@ def run_reference(args):
 # GPU arm
 # --------------------------------------------------------------------------------------
 
+CASES = {
+    'kerr': 'batched driven Kerr: n=64, B=4096, K=2 jumps, t=[0,10], 51 saves, Tsit5 1e-6/1e-8',
+    'oscillator': 'lossy oscillator: n=16, one instance, omega=1, kappa=0.1, alpha0=1, 101 saves, '
+                  'Tsit5 1e-6/1e-8',
+    'transmon': 'transmon(4) x cavity(64): n=256, B=256, K=2, t=[0,20], 41 saves, Tsit5 1e-6/1e-8',
+    'dia': 'coupled Kerr modes 64x64 in sparse DIA: n=4096, B=8, K=2, t=[0,5], 11 saves, '
+           'Tsit5 1e-5/1e-7',
+}
+
+
+def _workload(name, args, rank):
+    from dynamiqs_b200 import workloads
+
+    seed = args.seed + rank
+    if name == 'kerr':
+        w = workloads.batched_kerr(batch=args.batch or 4096, seed=seed)
+        if args.tend != 10.0:
+            w['tsave'] = np.linspace(0.0, args.tend, 51)
+    elif name == 'oscillator':
+        w = workloads.lossy_oscillator()
+    elif name == 'transmon':
+        w = workloads.transmon_cavity(batch=args.batch or 256, seed=seed)
+        if args.tend != 10.0:
+            w['tsave'] = np.linspace(0.0, args.tend, 41)
+    else:
+        w = workloads.coupled_kerr_dia(batch=args.batch or 8, seed=seed)
+        if args.tend != 10.0:
+            w['tsave'] = np.linspace(0.0, args.tend, 11)
+    return w
+
+
+def _kernels_per_launch(path: str, K: int, iterations: int) -> int:
+    """Kernels of this library executed by one solve call."""
+    if path == 'dqb_mesolve_dense':
+        return 1  # the persistent kernel (plus a 256-byte memset of its work counter)
+    if path == 'dqb_mesolve_dia':
+        body = 6 * 2 + 4          # 6 x (combine + stencil) + error, control, save, commit
+        init = 10                 # set-up, Hnh, rho0, 2 RHS, norms, controls, probe
+        return init + body * iterations + 3
+    rhs = (2 if K else 1) + 1 + ((K + 1) // 4 if K > 3 else 0)  # L X, sums, symmetrize
+    body = 6 * (1 + rhs) + 4
+    init = 3 + 2 * rhs + 5 + (K + 3) // 4
+    return init + body * iterations + 3
+
+
 def run_b200(args):
     import torch
 
     import dynamiqs_b200 as dq
-    from dynamiqs_b200 import _lib, workloads
+    from dynamiqs_b200.mesolve import MESolveB200Integrator, make_batch_plan
 
     world = int(os.environ.get('WORLD_SIZE', 1))
     rank = int(os.environ.get('RANK', 0))
@@ -178,45 +228,22 @@ def run_b200(args):
             dist.barrier(device_ids=[local])
         torch.cuda.synchronize()
 
-    B = args.batch
-    w = workloads.batched_kerr(batch=B, seed=args.seed + rank)
-    n, K = 64, 2
-    lib = _lib.load()
-    c64 = torch.complex64
-    H_d = torch.from_numpy(w['H']).to(dev)
-    L_d = torch.from_numpy(np.stack(w['jump_ops'])[None].copy()).to(dev)
-    r_d = torch.from_numpy(w['rho0'].copy()).to(dev)
-    E_d = torch.from_numpy(np.stack(w['exp_ops']).copy()).to(dev)
-    ts = w['tsave'] if args.tend == 10.0 else np.linspace(0.0, args.tend, 51)
-    ts_d = torch.from_numpy(ts).to(dev)
-    zeros = torch.zeros(B, dtype=torch.int32, device=dev)
-    H_idx = torch.arange(B, dtype=torch.int32, device=dev)
-    nt = len(ts)
-    states = torch.empty((B, nt, n, n), dtype=c64, device=dev)
-    expects = torch.empty((B, 1, nt), dtype=c64, device=dev)
-    infos = torch.empty((B, 3), dtype=torch.int32, device=dev)
-    status = torch.empty((B,), dtype=torch.int32, device=dev)
-    prob = _lib.DenseProblem(n=n, n_jumps=K, n_exp=1, n_tsave=nt, batch=B, H=H_d.data_ptr(),
-                             L=L_d.data_ptr(), rho0=r_d.data_ptr(), rho0_is_ket=1,
-                             E=E_d.data_ptr(), tsave=ts_d.data_ptr(), H_index=H_idx.data_ptr(),
-                             L_index=zeros.data_ptr(), rho0_index=zeros.data_ptr())
-    outs = _lib.Outputs(states=states.data_ptr(), expects=expects.data_ptr(),
-                        infos=infos.data_ptr(), status=status.data_ptr())
-    opts = _lib.OdeOptions(method=_lib.METHOD_TSIT5, form=_lib.FORM_HERMITIAN, rtol=1e-6,
-                           atol=1e-8, safety=0.9, factormin=0.2, factormax=5.0,
-                           max_steps=100_000, t0=float(ts[0]), save_states=1, check_hermitian=1)
-    ws_bytes = lib.dqb_mesolve_dense_workspace_size(n, K, B)
-    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    w = _workload(args.config, args, rank)
+    Es = w.get('exp_ops')
+    plan = make_batch_plan(w['H'], w['jump_ops'], w['rho0'], True)
+    integ = MESolveB200Integrator(ts=w['tsave'], y0=w['rho0'], method=w['method'], gradient=None,
+                                  options=dq.Options(), H=w['H'], Ls=w['jump_ops'], Es=Es, plan=plan)
+    prep = integ.prepare()
+    B = plan.batch
+    n = w['H'].shape[-1]
+    K = len(w['jump_ops'])
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
-    def step():
-        rc = lib.dqb_mesolve_dense(prob, opts, outs, ws.data_ptr(), ws_bytes, stream.cuda_stream)
-        _lib.check(rc, 'dqb_mesolve_dense')
-
     for _ in range(args.warmup):
-        step()
+        prep.launch(stream.cuda_stream)
     torch.cuda.synchronize()
+    status = prep.bufs['status']
     assert int((status != 0).sum()) == 0, 'solver status not OK'
 
     # ---- timed region: device-resident inputs --------------------------------------
@@ -227,87 +254,101 @@ def run_b200(args):
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     barrier()
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_stop = torch.cuda.Event(enable_timing=True)
-    kernel_ms = []
-    t_start.record(stream)
     for i in range(args.steps):
         flush.zero_()  # L2 flush between iterations (256 MiB > 126 MB L2)
         ev[i][0].record(stream)
-        step()
+        prep.launch(stream.cuda_stream)
         ev[i][1].record(stream)
-    t_stop.record(stream)
     barrier()
     if sampler is not None:
         sampler.terminate()
         sampler.wait()
     kernel_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = t_start.elapsed_time(t_stop)
+    infos = prep.bufs['infos']
     nsteps = infos[:, 0].to(torch.float64)
-    rhs_evals = float((6 * nsteps + 2).sum())
-    flops_per_solve_batch = rhs_evals * _flops_per_rhs(n, K)
-    # max over ranks
     kern = float(np.sum(kernel_ms))
     if dist is not None:
-        tt = torch.tensor([kern, total_ms], device=dev, dtype=torch.float64)
+        tt = torch.tensor([kern], device=dev, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        kern, total_ms = float(tt[0]), float(tt[1])
+        kern = float(tt[0])
     value = world * B * args.steps / (kern / 1e3)
-    mean_kernel_ms = kern / args.steps
-    achieved_tflops = flops_per_solve_batch / (mean_kernel_ms / 1e3) / 1e12
+    mean_ms = kern / args.steps
+    peaks, which = _peaks()
+    if args.config == 'dia':
+        # algorithmic HBM bytes per attempted step and instance: stage inputs (25 matrix
+        # passes), y1 (8), six right-hand sides (read X, write k: 12), error (9)
+        nbytes = float((54 * 8.0 * n * n * nsteps).sum())
+        achieved = nbytes / (mean_ms / 1e3) / 1e9
+        roof = {'bound': 'hbm', 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
+                'frac': achieved / peaks['hbm_gbs'], 'peak_source': f'hbm_gbs ({which})',
+                'traffic': None, 'algorithmic_bytes_per_launch': nbytes,
+                'note': 'bytes = 54 n^2 complex64 matrix passes per attempted RK step per instance'}
+    else:
+        rhs_evals = float((6 * nsteps + 2).sum())
+        flops = rhs_evals * _flops_per_rhs(n, K)
+        achieved = flops / (mean_ms / 1e3) / 1e12
+        peak = peaks.get('bf16_tflops_sustained', peaks.get('bf16_tflops'))
+        roof = {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
+                'frac': achieved / peak, 'peak_source': f'bf16_tflops_sustained ({which})',
+                'traffic': None, 'algorithmic_flops_per_launch': flops,
+                'note': 'products run on the FP32 CUDA-core pipe (SIMT); FP32 nominal peak is '
+                        '148 SMs x 128 FMA x 2 x clock'}
 
     # ---- e2e: public API from host inputs --------------------------------------------
-    e2e_value = None
-    h2d = d2h = 0
+    e2e = None
     if not args.no_e2e:
-        H_host = torch.from_numpy(w['H']).pin_memory()
-        Ls = w['jump_ops']
-        e2e_times = []
+        H_host = w['H']
+        if isinstance(H_host, np.ndarray):
+            H_host = torch.from_numpy(H_host).pin_memory()
+        times = []
         for i in range(max(1, args.e2e_steps) + 1):
             barrier()
             t = time.perf_counter()
-            res = dq.mesolve(H_host, Ls, w['rho0'], ts, exp_ops=w['exp_ops'], method=w['method'])
-            ex = res.expects.cpu()
+            res = dq.mesolve(H_host, w['jump_ops'], w['rho0'], w['tsave'], exp_ops=Es,
+                             method=w['method'])
+            ex = res.expects.cpu() if res.expects is not None else torch.zeros(0)
             inf = res.infos.nsteps.cpu()
             torch.cuda.synchronize()
             if i > 0:
-                e2e_times.append(time.perf_counter() - t)
-        e2e_s = max(e2e_times) if dist is None else e2e_times[-1]
+                times.append(time.perf_counter() - t)
+        e2e_s = float(np.mean(times))
         if dist is not None:
-            tt = torch.tensor([float(np.mean(e2e_times))], device=dev, dtype=torch.float64)
+            tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             e2e_s = float(tt[0])
-        else:
-            e2e_s = float(np.mean(e2e_times))
-        e2e_value = world * B / e2e_s
-        h2d = (w['H'].nbytes + sum(L.nbytes for L in Ls) + w['rho0'].nbytes
-               + sum(E.nbytes for E in w['exp_ops']) + ts.nbytes)
+
+        def nb(x):
+            return x.diags.nbytes if hasattr(x, 'diags') else np.asarray(x).nbytes
+
+        h2d = (nb(w['H']) + sum(nb(L) for L in w['jump_ops']) + np.asarray(w['rho0']).nbytes
+               + (sum(np.asarray(E).nbytes for E in Es) if Es else 0) + w['tsave'].nbytes)
         d2h = ex.numel() * ex.element_size() + inf.numel() * inf.element_size()
+        e2e = {'value': world * B / e2e_s, 'unit': 'solves/s', 'h2d_bytes_per_step': int(h2d),
+               'd2h_bytes_per_step': int(d2h)}
 
     # ---- plain path: one instance per launch -------------------------------------------
     plain = None
-    if not args.no_plain and rank == 0:
+    if args.config == 'kerr' and not args.no_plain and rank == 0:
         nplain = 16
-        p1 = _lib.DenseProblem(n=n, n_jumps=K, n_exp=1, n_tsave=nt, batch=1, H=0,
-                               L=L_d.data_ptr(), rho0=r_d.data_ptr(), rho0_is_ket=1,
-                               E=E_d.data_ptr(), tsave=ts_d.data_ptr(), H_index=None,
-                               L_index=zeros.data_ptr(), rho0_index=zeros.data_ptr())
-        ws1 = lib.dqb_mesolve_dense_workspace_size(n, K, 1)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        lat = []
         for b in range(nplain):
-            p1.H = H_d[b].data_ptr()
-            o1 = _lib.Outputs(states=states[b].data_ptr(), expects=expects[b].data_ptr(),
-                              infos=infos[b].data_ptr(), status=status[b].data_ptr())
-            _lib.check(lib.dqb_mesolve_dense(p1, opts, o1, ws.data_ptr(), ws1, stream.cuda_stream),
-                       'plain')
-        e1.record(stream)
-        torch.cuda.synchronize()
-        plain_s = e0.elapsed_time(e1) / 1e3
-        lat = plain_s / nplain
+            p1 = make_batch_plan(w['H'][b], w['jump_ops'], w['rho0'], True)
+            i1 = MESolveB200Integrator(ts=w['tsave'], y0=w['rho0'], method=w['method'],
+                                       gradient=None, options=dq.Options(), H=w['H'][b],
+                                       Ls=w['jump_ops'], Es=Es, plan=p1).prepare()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            i1.launch(stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            lat.append(e0.elapsed_time(e1))
+        plain_s = float(np.sum(lat)) / 1e3
         plain = {'value': nplain / plain_s, 'unit': 'solves/s',
-                 'what': 'same kernel, one instance per launch, launches back to back',
-                 'p50_latency_ms': 1e3 * lat, 'batched_over_plain': value / (world * nplain / plain_s)}
+                 'what': 'same kernel, one instance per launch (16 instances)',
+                 'p50_latency_ms': float(np.percentile(lat, 50)),
+                 'p99_latency_ms': float(np.percentile(lat, 99)),
+                 'batched_over_plain': value / world / (nplain / plain_s)}
 
     if dist is not None:
         dist.barrier(device_ids=[local])
@@ -315,36 +356,26 @@ def run_b200(args):
     if rank != 0:
         return
 
-    peaks, which = _peaks()
-    peak = peaks.get('bf16_tflops_sustained', peaks.get('bf16_tflops'))
     clocks = _clock_summary(clk_path)
-    per_inst_ms = None
     line = {
         'metric': METRIC, 'value': value, 'unit': 'solves/s', 'n_gpus': world,
-        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': mean_kernel_ms,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': mean_ms,
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'c64',
         'data': 'synthetic (seeded numpy generator; no dataset)',
-        'config': {'workload': WORKLOAD, 'batch_per_gpu': B, 'n': n, 'n_jumps': K,
-                   'n_tsave': nt, 'method': 'Tsit5', 'rtol': 1e-6, 'atol': 1e-8,
-                   'l2': 'flushed between iterations (256 MiB write); inputs+outputs > L2',
+        'config': {'workload': CASES[args.config], 'batch_per_gpu': B, 'n': n, 'n_jumps': K,
+                   'n_tsave': len(w['tsave']), 'method': type(w['method']).__name__,
+                   'rtol': w['method'].rtol, 'atol': w['method'].atol, 'path': prep.name,
+                   'l2': 'flushed between iterations (256 MiB write)',
                    'parallelism': f'instances sharded over {world} GPU(s), no collective',
-                   'avg_rk_steps': float(nsteps.mean())},
-        'e2e': ({'value': e2e_value, 'unit': 'solves/s', 'h2d_bytes_per_step': int(h2d),
-                 'd2h_bytes_per_step': int(d2h)} if e2e_value else None),
-        'gpu_launches': args.steps,
-        'roofline': {'bound': 'tensor', 'achieved': achieved_tflops, 'peak': peak,
-                     'unit': 'TFLOP/s', 'frac': achieved_tflops / peak,
-                     'peak_source': f'bf16_tflops_sustained ({which})',
-                     'traffic': None,
-                     'algorithmic_flops_per_launch': flops_per_solve_batch,
-                     'note': 'mesolve_small_kernel<64> runs its products on the FP32 '
-                             'CUDA-core pipe; FP32 SIMT nominal peak is 148 SMs x 128 FMA '
-                             'x 2 x clock'},
+                   'avg_rk_steps': float(nsteps.mean()), 'max_rk_steps': float(nsteps.max())},
+        'e2e': e2e,
+        'gpu_launches': args.steps * _kernels_per_launch(prep.name, K, int(nsteps.max())),
+        'roofline': roof,
         'clocks': clocks,
         'plain_path': plain,
-        'latency_ms': {'per_batch': mean_kernel_ms, 'p50': per_inst_ms, 'p99': per_inst_ms},
+        'latency_ms': {'per_batch': mean_ms},
     }
-    if not args.no_cpu_baseline:
+    if args.config == 'kerr' and not args.no_cpu_baseline:
         line['cpu_baseline'] = cpu_baseline(sample=args.cpu_sample)
     print(json.dumps(line), flush=True)
 
@@ -355,7 +386,8 @@ def main():
     ap.add_argument('--steps', type=int, default=3)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
-    ap.add_argument('--batch', type=int, default=4096)
+    ap.add_argument('--config', default='kerr', choices=sorted(CASES))
+    ap.add_argument('--batch', type=int, default=0, help='instances (0: the workload default)')
     ap.add_argument('--seed', type=int, default=0)
     ap.add_argument('--tend', type=float, default=10.0, help='end time (10 in the workload; '
                     'shorter only for profiling captures)')

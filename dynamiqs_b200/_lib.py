@@ -85,6 +85,29 @@ class DenseProblem(ctypes.Structure):
     ]
 
 
+class DiaProblem(ctypes.Structure):
+    _fields_ = [
+        ('n', ctypes.c_int32),
+        ('n_jumps', ctypes.c_int32),
+        ('n_exp', ctypes.c_int32),
+        ('n_tsave', ctypes.c_int32),
+        ('batch', ctypes.c_int64),
+        ('h_ndiag', ctypes.c_int32),
+        ('h_offsets', ctypes.c_void_p),
+        ('h_diags', ctypes.c_void_p),
+        ('l_ndiag', ctypes.c_void_p),
+        ('l_offsets', ctypes.c_void_p),
+        ('l_diags', ctypes.c_void_p),
+        ('rho0', ctypes.c_void_p),
+        ('rho0_is_ket', ctypes.c_int32),
+        ('E', ctypes.c_void_p),
+        ('tsave', ctypes.c_void_p),
+        ('H_index', ctypes.c_void_p),
+        ('L_index', ctypes.c_void_p),
+        ('rho0_index', ctypes.c_void_p),
+    ]
+
+
 # Every symbol include/dqb200.h declares, with (restype, argtypes).
 _P = ctypes.c_void_p
 SIGNATURES = {
@@ -94,6 +117,18 @@ SIGNATURES = {
     'dqb_mesolve_dense_noalloc': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
                                                  ctypes.POINTER(Outputs), _P]),
     'dqb_lindblad_rhs_dense': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.c_int32, _P, _P, _P]),
+    'dqb_mesolve_dense_large_workspace_size': (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32,
+                                                                 ctypes.c_int32, ctypes.c_int32,
+                                                                 ctypes.c_int64]),
+    'dqb_mesolve_dense_large': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
+                                               ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
+    'dqb_lindblad_rhs_dense_large': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.c_int32, _P,
+                                                    _P, _P, ctypes.c_size_t, _P]),
+    'dqb_mesolve_dia_workspace_size': (ctypes.c_size_t, [ctypes.POINTER(DiaProblem)]),
+    'dqb_mesolve_dia': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.POINTER(OdeOptions),
+                                       ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
+    'dqb_lindblad_rhs_dia': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.c_int32, _P, _P, _P,
+                                            ctypes.c_size_t, _P]),
     'dqb_dense_small_max_n': (ctypes.c_int32, [ctypes.c_int32]),
     'dqb_version': (ctypes.c_char_p, []),
 }

@@ -1,0 +1,436 @@
+// Batched RK stepper for problems too large for one CTA (n > 64 dense, or sparse DIA).
+//
+// One RK step of every running instance is a fixed sequence of grid-wide kernels:
+//   for s = 2..6:  combine  X   = y + h sum_{j<s} a_sj k_j        (elementwise)
+//                  rhs      k_s = f(X)                            (DIA stencil or GEMMs)
+//                  combine  y1  = y + h sum_{j<7} b_j k_j ; rhs k7 = f(y1)
+//                  error    acc += |h sum_j btilde_j k_j|^2 / sc^2 (FP64 atomics)
+//                  control  (one thread per instance, FP64): accept / reject, save range
+//                  save     dense output at the tsave points crossed, tr(E rho) sums
+//                  commit   swap y <-> y1 and k1 <-> k7 on accept, next trial step
+// The sequence is the body of a CUDA-graph WHILE node whose condition the commit kernel
+// sets to "some instance is still running", so a whole batched solve is one graph launch
+// with no host round trip.  Every instance keeps its own t, dt, accept/reject state and
+// step counters; finished instances are skipped by every kernel.  The loop ends because
+// every iteration advances each running instance's attempted-step counter, which is
+// bounded by max_steps, and the commit kernel also stops after max_steps + 2 iterations.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "dqb_common.cuh"
+
+namespace dqb {
+namespace big {
+
+constexpr int kSlots = 10;  // y, y1, k1..k7, X
+constexpr int kX = 9;
+constexpr int kElemThreads = 256;
+
+struct Inst {
+  double t, tnext, h, dtnew, t1, h0;
+  double acc[3];  // error / starting-step norm accumulators
+  int status, run, keep, save_idx, save_lo, save_hi, herm_bad, pad;
+  long long nsteps, nacc, nrej;
+  int sy, sy1, sk[7];
+};
+
+struct Common {
+  int n;
+  long long nn;  // n * n
+  int B, nE, ntsave, form, save_states, rho0_is_ket;
+  CtrlOpts o;
+  const double* tsave;
+  Inst* inst;
+  float2* mats;    // [B][kSlots][nn]
+  double2* eacc;   // [B][nE][ntsave]
+  float2* states;  // [B][nsave][n][n]
+  float2* expects; // [B][nE][ntsave]
+  int* infos;
+  int* status;
+  const float2* E;  // [nE][n][n]
+  const float2* rho0;
+  const int* ridx;
+  long long* iter;  // graph-loop iteration counter
+};
+
+__device__ __forceinline__ float2* slot(const Common& c, int b, int s) {
+  return c.mats + ((long long)b * kSlots + s) * c.nn;
+}
+
+__device__ __forceinline__ void block_atomic_add(double v, double* dst, double* red) {
+  v = block_sum(v, red);
+  if (threadIdx.x == 0) atomicAdd(dst, v);
+}
+
+// ------------------------------------------------------------------------------------
+// set-up
+// ------------------------------------------------------------------------------------
+
+// One thread per instance.
+static __global__ void setup_kernel(Common c) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b == 0) *c.iter = 0;
+  if (b >= c.B) return;
+  Inst& I = c.inst[b];
+  I.t = c.o.t0;
+  I.t1 = c.tsave[c.ntsave - 1];
+  I.tnext = I.t1;
+  I.h = I.dtnew = I.h0 = 0.0;
+  I.acc[0] = I.acc[1] = I.acc[2] = 0.0;
+  I.status = DQB_INST_OK;
+  I.run = 0;
+  I.keep = 0;
+  I.save_idx = I.save_lo = I.save_hi = 0;
+  I.herm_bad = 0;
+  I.nsteps = I.nacc = I.nrej = 0;
+  I.sy = 0;
+  I.sy1 = 1;
+  for (int j = 0; j < 7; ++j) I.sk[j] = 2 + j;
+}
+
+// grid (tiles, B): rho0 (or psi psi^+) into y, hermiticity check, expects sums zeroed.
+static __global__ void load_rho0_kernel(Common c) {
+  const int b = blockIdx.y;
+  Inst& I = c.inst[b];
+  const int n = c.n;
+  const long long ri = c.ridx ? c.ridx[b] : b;
+  float2* y = slot(c, b, 0);
+  int bad = 0;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / n), j = (int)(e % n);
+    float2 v;
+    if (c.rho0_is_ket) {
+      const float2* psi = c.rho0 + ri * n;
+      v = cmul(psi[i], cconj(psi[j]));
+    } else {
+      const float2* r0 = c.rho0 + ri * c.nn;
+      v = r0[e];
+      if (c.o.check_hermitian) {
+        const float2 u = cconj(r0[(long long)j * n + i]);
+        const float d = cabsf(make_float2(v.x - u.x, v.y - u.y));
+        if (!(d <= 1e-5f + 1e-5f * cabsf(u))) bad = 1;
+      }
+    }
+    y[e] = v;
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) I.herm_bad = 1;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)c.nE * c.ntsave;
+       e += (long long)gridDim.x * blockDim.x)
+    c.eacc[(long long)b * c.nE * c.ntsave + e] = make_double2(0.0, 0.0);
+}
+
+// ------------------------------------------------------------------------------------
+// elementwise kernels: grid (tiles, B)
+// ------------------------------------------------------------------------------------
+
+// mode 0..4: X = y + h sum_{j<=mode} a[mode+1][j] k_j    (stage mode+2 input)
+// mode 5:    y1 = y + h sum_{j<6} b_j k_j
+// mode 6:    X = y + h0 k1                              (starting-step probe)
+static __global__ void combine_kernel(Common c, int mode) {
+  const int b = blockIdx.y;
+  const Inst& I = c.inst[b];
+  if (mode == 6) {
+    if (I.status != DQB_INST_OK) return;
+  } else if (!I.run) {
+    return;
+  }
+  const Tableau& T = c_tab[c.o.method];
+  float cf[6];
+  int nterm;
+  if (mode == 6) {
+    cf[0] = (float)I.h0;
+    nterm = 1;
+  } else if (mode == 5) {
+    for (int j = 0; j < 6; ++j) cf[j] = (float)(I.h * T.b[j]);
+    nterm = 6;
+  } else {
+    for (int j = 0; j < 6; ++j) cf[j] = (float)(I.h * T.a[mode + 1][j]);
+    nterm = mode + 1;
+  }
+  const float2* y = slot(c, b, I.sy);
+  const float2* k[6];
+  for (int j = 0; j < 6; ++j) k[j] = slot(c, b, I.sk[j]);
+  float2* out = slot(c, b, mode == 5 ? I.sy1 : kX);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
+       e += (long long)gridDim.x * blockDim.x) {
+    float2 x = y[e];
+#pragma unroll
+    for (int j = 0; j < 6; ++j)
+      if (j < nterm) x = caxpy(cf[j], k[j][e], x);
+    out[e] = x;
+  }
+}
+
+// Embedded-error accumulation: acc[0] += sum |h sum_j btilde_j k_j|^2 / sc^2.
+static __global__ void error_kernel(Common c) {
+  __shared__ double red[40];
+  const int b = blockIdx.y;
+  Inst& I = c.inst[b];
+  if (!I.run) return;
+  const Tableau& T = c_tab[c.o.method];
+  double cb[7];
+  for (int j = 0; j < 7; ++j) cb[j] = I.h * T.btilde[j];
+  const float2* y = slot(c, b, I.sy);
+  const float2* y1 = slot(c, b, I.sy1);
+  const float2* k[7];
+  for (int j = 0; j < 7; ++j) k[j] = slot(c, b, I.sk[j]);
+  double s = 0.0;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
+       e += (long long)gridDim.x * blockDim.x) {
+    double ex = 0.0, ey = 0.0;
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+      const float2 v = k[j][e];
+      ex = fma(cb[j], (double)v.x, ex);
+      ey = fma(cb[j], (double)v.y, ey);
+    }
+    const float ya = cabsf(y[e]), y1a = cabsf(y1[e]);
+    const double sc = c.o.atol + c.o.rtol * (double)(ya > y1a ? ya : y1a);
+    s += (ex * ex + ey * ey) / (sc * sc);
+  }
+  block_atomic_add(s, &I.acc[0], red);
+}
+
+// Starting-step norms.  phase 0: acc[0] += |y/sc|^2, acc[1] += |k1/sc|^2;
+// phase 1: acc[2] += |(k2 - k1)/sc|^2 (k2 = f(y + h0 k1)).
+static __global__ void init_norm_kernel(Common c, int phase) {
+  __shared__ double red[40];
+  const int b = blockIdx.y;
+  Inst& I = c.inst[b];
+  if (I.status != DQB_INST_OK) return;
+  const float2* y = slot(c, b, I.sy);
+  const float2* k1 = slot(c, b, I.sk[0]);
+  const float2* k2 = slot(c, b, I.sk[1]);
+  double s0 = 0.0, s1 = 0.0;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
+       e += (long long)gridDim.x * blockDim.x) {
+    const float2 yv = y[e];
+    const double sc = c.o.atol + c.o.rtol * (double)cabsf(yv);
+    const float2 f0 = k1[e];
+    if (phase == 0) {
+      s0 += (double)cabs2f(yv) / (sc * sc);
+      s1 += (double)cabs2f(f0) / (sc * sc);
+    } else {
+      const float2 f1 = k2[e];
+      const double dx = (double)f1.x - f0.x, dy = (double)f1.y - f0.y;
+      s0 += (dx * dx + dy * dy) / (sc * sc);
+    }
+  }
+  if (phase == 0) {
+    block_atomic_add(s0, &I.acc[0], red);
+    block_atomic_add(s1, &I.acc[1], red);
+  } else {
+    block_atomic_add(s0, &I.acc[2], red);
+  }
+}
+
+// One thread per instance.  phase 0: hermiticity verdict and h0 from d0, d1.
+// phase 1: first trial step (Hairer-Norsett-Wanner).
+static __global__ void init_ctrl_kernel(Common c, int phase) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= c.B) return;
+  Inst& I = c.inst[b];
+  const double inv_nn = 1.0 / (double)c.nn;
+  if (phase == 0) {
+    if (I.herm_bad) I.status = DQB_INST_NOT_HERMITIAN;
+    const double d0 = sqrt(I.acc[0] * inv_nn), d1 = sqrt(I.acc[1] * inv_nn);
+    I.h0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : 0.01 * d0 / d1;
+    I.acc[0] = d0;
+    I.acc[1] = d1;
+    I.acc[2] = 0.0;
+  } else {
+    if (I.status != DQB_INST_OK) {
+      I.run = 0;
+      return;
+    }
+    const double d1 = I.acc[1];
+    const double d2 = sqrt(I.acc[2] * inv_nn) / I.h0;
+    const double md = d1 > d2 ? d1 : d2;
+    const double h1 = md <= 1e-15 ? fmax(1e-6, I.h0 * 1e-3) : pow(0.01 / md, 0.2);
+    const double dt = fmin(100.0 * I.h0, h1);
+    double tn = I.t + dt;
+    if (tn > I.t1 - 1e-10) tn = I.t1;
+    I.tnext = tn < I.t1 ? tn : I.t1;
+    I.h = I.tnext - I.t;
+    I.run = I.t < I.t1;
+    I.acc[0] = I.acc[1] = I.acc[2] = 0.0;
+  }
+}
+
+// One thread per instance: accept / reject and the range of saves the step crosses.
+static __global__ void control_kernel(Common c) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= c.B) return;
+  Inst& I = c.inst[b];
+  I.keep = 0;
+  I.save_lo = I.save_hi = I.save_idx;
+  if (!I.run) return;
+  if (I.nsteps >= c.o.max_steps) {
+    I.status = DQB_INST_MAX_STEPS;
+    I.run = 0;
+    return;
+  }
+  const double err = sqrt(I.acc[0] / (double)c.nn);
+  I.acc[0] = 0.0;
+  I.nsteps += 1;
+  if (!(err < INFINITY)) {
+    I.status = DQB_INST_NONFINITE;
+    I.nrej += 1;
+    I.run = 0;
+    return;
+  }
+  const bool keep = err < 1.0;
+  I.keep = keep;
+  if (keep) I.nacc += 1; else I.nrej += 1;
+  I.dtnew = I.h * step_factor(c.o, err, keep);
+  if (keep) {
+    int hi = I.save_idx;
+    while (hi < c.ntsave && c.tsave[hi] <= I.tnext) ++hi;
+    I.save_hi = hi;
+  }
+}
+
+// grid (tiles, B): states and tr(E rho) at the saves crossed by an accepted step.
+// interp = 0 saves y itself (saves at or before t0 when t1 <= t0).
+static __global__ void save_kernel(Common c, int interp) {
+  __shared__ double red[40];
+  const int b = blockIdx.y;
+  const Inst& I = c.inst[b];
+  const int lo = I.save_lo, hi = I.save_hi;
+  if (hi <= lo) return;
+  const float2* y = slot(c, b, I.sy);
+  const float2* k[7];
+  for (int j = 0; j < 7; ++j) k[j] = slot(c, b, I.sk[j]);
+  const int n = c.n;
+  const bool herm = c.form == DQB_FORM_HERMITIAN;
+  for (int s = lo; s < hi; ++s) {
+    float cw[7];
+    if (interp) {
+      double w[7];
+      const double theta = I.h > 0.0 ? (c.tsave[s] - I.t) / I.h : 1.0;
+      dense_weights(c.o.method, theta, w);
+      for (int j = 0; j < 7; ++j) cw[j] = (float)(I.h * w[j]);
+    }
+    float2* dst = c.states + ((long long)b * c.ntsave + s) * c.nn;
+    for (int m0 = 0; m0 == 0 || m0 < c.nE; m0 += 4) {
+      const int mc = c.nE - m0 < 4 ? c.nE - m0 : 4;
+      double er[4] = {0, 0, 0, 0}, ei[4] = {0, 0, 0, 0};
+      for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
+           e += (long long)gridDim.x * blockDim.x) {
+        float2 v = y[e];
+        if (interp) {
+#pragma unroll
+          for (int j = 0; j < 7; ++j) v = caxpy(cw[j], k[j][e], v);
+        }
+        if (m0 == 0 && c.save_states) dst[e] = v;
+        if (mc > 0) {
+          // tr(E rho) = sum_ij E_ij rho_ji; rho_ji = conj(rho_ij) when rho is hermitian
+          float2 rt;
+          if (herm) {
+            rt = cconj(v);
+          } else {
+            const int i = (int)(e / n), j = (int)(e % n);
+            const long long et = (long long)j * n + i;
+            rt = y[et];
+            if (interp) {
+#pragma unroll
+              for (int q = 0; q < 7; ++q) rt = caxpy(cw[q], k[q][et], rt);
+            }
+          }
+#pragma unroll
+          for (int m = 0; m < 4; ++m) {
+            if (m < mc) {
+              const float2 ev = c.E[(long long)(m0 + m) * c.nn + e];
+              er[m] += (double)ev.x * rt.x - (double)ev.y * rt.y;
+              ei[m] += (double)ev.x * rt.y + (double)ev.y * rt.x;
+            }
+          }
+        }
+      }
+      for (int m = 0; m < mc; ++m) {
+        double2* acc = c.eacc + ((long long)b * c.nE + m0 + m) * c.ntsave + s;
+        const double sr = block_sum(er[m], red);
+        const double si = block_sum(ei[m], red);
+        if (threadIdx.x == 0) {
+          atomicAdd(&acc->x, sr);
+          atomicAdd(&acc->y, si);
+        }
+      }
+    }
+  }
+}
+
+// One block: per-instance commit, then the WHILE-node condition.
+static __global__ void commit_kernel(Common c, cudaGraphConditionalHandle handle) {
+  int any = 0;
+  for (int b = threadIdx.x; b < c.B; b += blockDim.x) {
+    Inst& I = c.inst[b];
+    if (I.run) {
+      if (I.keep) {
+        int tmp = I.sy;
+        I.sy = I.sy1;
+        I.sy1 = tmp;
+        tmp = I.sk[0];
+        I.sk[0] = I.sk[6];
+        I.sk[6] = tmp;
+        I.t = I.tnext;
+        I.save_idx = I.save_hi;
+      }
+      I.tnext = next_tend(I.t, I.dtnew, I.t1, I.keep);
+      I.h = I.tnext - I.t;
+      I.run = I.t < I.t1;
+    }
+    I.save_lo = I.save_hi = I.save_idx;
+    any |= I.run;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    const long long it = ++(*c.iter);
+    const bool more = any && it < c.o.max_steps + 2;
+    cudaGraphSetConditional(handle, more ? 1u : 0u);
+  }
+}
+
+// One block per instance after the loop: the saves left over (t1 <= t0, or a
+// stopped instance), final state when only it is kept, expects, infos, status.
+static __global__ void pre_finalize_kernel(Common c) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= c.B) return;
+  Inst& I = c.inst[b];
+  I.save_lo = I.save_idx;
+  I.save_hi = I.save_idx;
+  if (I.status == DQB_INST_OK) {
+    int hi = I.save_idx;
+    while (hi < c.ntsave && c.tsave[hi] <= I.t) ++hi;
+    I.save_hi = hi;
+  }
+}
+
+static __global__ void finalize_kernel(Common c) {
+  const int b = blockIdx.y;
+  Inst& I = c.inst[b];
+  if (!c.save_states) {
+    const float2* y = slot(c, b, I.sy);
+    float2* dst = c.states + (long long)b * c.nn;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
+         e += (long long)gridDim.x * blockDim.x)
+      dst[e] = y[e];
+  }
+  if (blockIdx.x == 0) {
+    for (int e = threadIdx.x; e < c.nE * c.ntsave; e += blockDim.x) {
+      const double2 v = c.eacc[(long long)b * c.nE * c.ntsave + e];
+      c.expects[(long long)b * c.nE * c.ntsave + e] = make_float2((float)v.x, (float)v.y);
+    }
+    if (threadIdx.x == 0) {
+      c.status[b] = I.status;
+      c.infos[b * 3 + 0] = (int)I.nsteps;
+      c.infos[b * 3 + 1] = (int)I.nacc;
+      c.infos[b * 3 + 2] = (int)I.nrej;
+    }
+  }
+}
+
+}  // namespace big
+}  // namespace dqb

@@ -28,7 +28,7 @@ struct Tableau {
   double cmid[7];    // Dopri5 midpoint weights (Shampine); unused for Tsit5
 };
 
-__constant__ Tableau c_tab[2] = {
+static __constant__ Tableau c_tab[2] = {
     // Tsit5 (Tsitouras 2011)
     {{0.0, 0.161, 0.327, 0.9, 0.9800255409045097, 1.0, 1.0},
      {{0, 0, 0, 0, 0, 0, 0},

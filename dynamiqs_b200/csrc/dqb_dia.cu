@@ -1,0 +1,375 @@
+// Sparse-DIA mesolve for large n (e.g. two 64-level modes, n = 4096, rho = 128 MiB).
+//
+// Right-hand side, element by element, from the DIA diagonals (column-indexed:
+// A[c - k][c] = diag_k[c]; dynamiqs/qarrays/sparsedia_primitives.py:232-261):
+//   (Hnh X)[i][j]   = sum_d hnh_d[i + k_d] X[i + k_d][j]                 (row shifts)
+//   (X Hnh^+)[i][j] = sum_d conj(hnh_d[j + k_d]) X[i][j + k_d]           (column shifts)
+//   (L X L^+)[i][j] = sum_{p,q} l_p[i + q_p] conj(l_q[j + q_q]) X[i + q_p][j + q_q]
+// and f(X) = Hnh X + X Hnh^+ + sum_k L_k X L_k^+.  For a hermitian X this equals the
+// reference's hermitian form tmp + tmp^+ with tmp = Hnh X + 1/2 sum L X L^+
+// (diffrax_integrator.py:319-323) and it is the standard form (:312-317) for any X, so
+// one stencil serves both.  Every term is a shifted, coalesced read of X; the kernel is
+// HBM/L2-bandwidth bound (algorithmic traffic: read X once, write f(X) once).
+//
+// Hnh's diagonals are built once per instance on the device (the reference rebuilds
+// them with matmul_sparsedia_sparsedia + add_sparsedia_sparsedia on every RHS,
+// sparsedia_primitives.py:172-229).  The RK loop is the stepper of dqb_big.cuh run as a
+// CUDA graph WHILE node.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <set>
+#include <vector>
+
+#include "dqb_big.cuh"
+#include "dqb_graph.cuh"
+
+namespace dqb {
+
+struct DiaOps {
+  int n;
+  int nh;                             // diagonals of Hnh
+  int hoff[DQB_DIA_MAX_HNH_DIAGS];
+  int hmap[DQB_DIA_MAX_HNH_DIAGS];    // index of the same offset in H, or -1
+  int h_nd;                           // diagonals of H
+  int K;
+  int nl;                             // sum of jump diagonals
+  int lstart[DQB_DIA_MAX_JUMPS + 1];
+  int loff[DQB_DIA_MAX_JUMP_DIAGS];
+  const float2* H;                    // [*, h_nd, n]
+  const float2* L;                    // [*, nl, n]
+  const int* Hidx;
+  const int* Lidx;
+  float2* hnh;                        // [B, nh, n]
+};
+
+namespace {
+
+// One thread per (column c, instance b): Hnh diagonals of instance b.
+__global__ void hnh_dia_kernel(DiaOps d, int B) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (c >= d.n || b >= B) return;
+  const int n = d.n;
+  const long long hi = d.Hidx ? d.Hidx[b] : b;
+  const long long li = d.Lidx ? d.Lidx[b] : b;
+  const float2* H = d.H + hi * d.h_nd * n;
+  const float2* L = d.L + li * d.nl * n;
+  float2* out = d.hnh + (long long)b * d.nh * n;
+  for (int q = 0; q < d.nh; ++q) {
+    const int k = d.hoff[q];
+    float2 v = make_float2(0.f, 0.f);
+    if (c - k >= 0 && c - k < n) {
+      if (d.hmap[q] >= 0) {
+        const float2 h = H[d.hmap[q] * n + c];
+        v = make_float2(h.y, -h.x);  // -i h
+      }
+      for (int jk = 0; jk < d.K; ++jk) {
+        for (int p = d.lstart[jk]; p < d.lstart[jk + 1]; ++p) {
+          for (int r = d.lstart[jk]; r < d.lstart[jk + 1]; ++r) {
+            if (d.loff[r] - d.loff[p] != k) continue;
+            // (L^+ L)[c - k][c] += conj(l_p[c - k]) l_r[c]
+            const float2 t = cmul(cconj(L[p * n + (c - k)]), L[r * n + c]);
+            v.x -= 0.5f * t.x;
+            v.y -= 0.5f * t.y;
+          }
+        }
+      }
+    }
+    out[q * n + c] = v;
+  }
+}
+
+constexpr int kRhsCols = 128;
+constexpr int kRhsRows = 8;
+
+// f(X) for DIA operators.  grid (n / 128, n / 8, B), block 128: each thread owns one
+// column and 8 consecutive rows.
+// in_sel: 0 = y, 1 = y1, 2 = X.  need_run: 1 = running instances, 0 = status OK.
+__global__ void __launch_bounds__(kRhsCols) rhs_dia_kernel(big::Common c, DiaOps d, int in_sel, int out_k,
+                                                           int need_run, const float2* ext_in, float2* ext_out) {
+  const int b = blockIdx.z;
+  const float2* X;
+  float2* out;
+  const float2* L;
+  if (ext_in) {  // stand-alone evaluation (dqb_lindblad_rhs_dia)
+    X = ext_in + (long long)b * d.n * d.n;
+    out = ext_out + (long long)b * d.n * d.n;
+  } else {
+    const big::Inst& I = c.inst[b];
+    if (need_run ? !I.run : I.status != DQB_INST_OK) return;
+    X = big::slot(c, b, in_sel == 0 ? I.sy : (in_sel == 1 ? I.sy1 : big::kX));
+    out = big::slot(c, b, I.sk[out_k]);
+  }
+  const long long li = d.Lidx ? d.Lidx[b] : b;
+  L = d.L + li * d.nl * d.n;
+  const float2* hnh = d.hnh + (long long)b * d.nh * d.n;
+  const int n = d.n;
+  const int j = blockIdx.x * kRhsCols + threadIdx.x;
+  if (j >= n) return;
+  const int i0 = blockIdx.y * kRhsRows;
+  for (int r = 0; r < kRhsRows; ++r) {
+    const int i = i0 + r;
+    if (i >= n) break;
+    float2 acc = make_float2(0.f, 0.f);
+    for (int q = 0; q < d.nh; ++q) {
+      const int k = d.hoff[q];
+      float2 pair = make_float2(0.f, 0.f);
+      const int ik = i + k, jk = j + k;
+      if (ik >= 0 && ik < n) pair = cmul(__ldg(&hnh[q * n + ik]), __ldg(&X[(long long)ik * n + j]));
+      if (jk >= 0 && jk < n) {
+        const float2 t = cmul(cconj(__ldg(&hnh[q * n + jk])), __ldg(&X[(long long)i * n + jk]));
+        pair = cadd(pair, t);
+      }
+      acc = cadd(acc, pair);
+    }
+    for (int jk = 0; jk < d.K; ++jk) {
+      for (int p = d.lstart[jk]; p < d.lstart[jk + 1]; ++p) {
+        const int ip = i + d.loff[p];
+        if (ip < 0 || ip >= n) continue;
+        const float2 lp = __ldg(&L[p * n + ip]);
+        for (int s = d.lstart[jk]; s < d.lstart[jk + 1]; ++s) {
+          const int jq = j + d.loff[s];
+          if (jq < 0 || jq >= n) continue;
+          const float2 coef = cmul(lp, cconj(__ldg(&L[s * n + jq])));
+          acc = cadd(acc, cmul(coef, __ldg(&X[(long long)ip * n + jq])));
+        }
+      }
+    }
+    out[(long long)i * n + j] = acc;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------
+
+size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct DiaLayout {
+  size_t off_iter, off_inst, off_eacc, off_hnh, off_mats, total;
+};
+
+int build_ops(const dqb_dia_problem* p, DiaOps* d) {
+  std::memset(d, 0, sizeof(*d));
+  if (p->h_ndiag < 0 || p->h_ndiag > DQB_DIA_MAX_HNH_DIAGS) return DQB_ERR_UNSUPPORTED;
+  if (p->n_jumps < 0 || p->n_jumps > DQB_DIA_MAX_JUMPS) return DQB_ERR_UNSUPPORTED;
+  if (p->h_ndiag > 0 && !p->h_offsets) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->n_jumps > 0 && (!p->l_ndiag || !p->l_offsets)) return DQB_ERR_INVALID_ARGUMENT;
+  d->n = p->n;
+  d->h_nd = p->h_ndiag;
+  d->K = p->n_jumps;
+  int nl = 0;
+  d->lstart[0] = 0;
+  for (int k = 0; k < p->n_jumps; ++k) {
+    if (p->l_ndiag[k] < 0) return DQB_ERR_INVALID_ARGUMENT;
+    nl += p->l_ndiag[k];
+    if (nl > DQB_DIA_MAX_JUMP_DIAGS) return DQB_ERR_UNSUPPORTED;
+    d->lstart[k + 1] = nl;
+  }
+  d->nl = nl;
+  std::set<int> offs;
+  for (int q = 0; q < p->h_ndiag; ++q) {
+    const int k = p->h_offsets[q];
+    if (k <= -p->n || k >= p->n) return DQB_ERR_INVALID_ARGUMENT;
+    offs.insert(k);
+  }
+  for (int q = 0; q < nl; ++q) {
+    d->loff[q] = p->l_offsets[q];
+    if (d->loff[q] <= -p->n || d->loff[q] >= p->n) return DQB_ERR_INVALID_ARGUMENT;
+  }
+  for (int k = 0; k < p->n_jumps; ++k)
+    for (int a = d->lstart[k]; a < d->lstart[k + 1]; ++a)
+      for (int c = d->lstart[k]; c < d->lstart[k + 1]; ++c) {
+        const int o = d->loff[c] - d->loff[a];
+        if (o > -p->n && o < p->n) offs.insert(o);
+      }
+  if ((int)offs.size() > DQB_DIA_MAX_HNH_DIAGS) return DQB_ERR_UNSUPPORTED;
+  d->nh = 0;
+  for (int o : offs) {
+    d->hoff[d->nh] = o;
+    d->hmap[d->nh] = -1;
+    for (int q = 0; q < p->h_ndiag; ++q)
+      if (p->h_offsets[q] == o) d->hmap[d->nh] = q;
+    d->nh++;
+  }
+  d->H = (const float2*)p->h_diags;
+  d->L = (const float2*)p->l_diags;
+  d->Hidx = p->H_index;
+  d->Lidx = p->L_index;
+  return DQB_OK;
+}
+
+DiaLayout layout_for(const dqb_dia_problem* p, int nh) {
+  DiaLayout l;
+  const size_t B = (size_t)p->batch, n = (size_t)p->n;
+  l.off_iter = 0;
+  l.off_inst = 256;
+  l.off_eacc = align_up(l.off_inst + B * sizeof(big::Inst));
+  l.off_hnh = align_up(l.off_eacc + B * (size_t)p->n_exp * p->n_tsave * sizeof(double2));
+  l.off_mats = align_up(l.off_hnh + B * (size_t)nh * n * sizeof(float2));
+  l.total = l.off_mats + B * big::kSlots * n * n * sizeof(float2);
+  return l;
+}
+
+// Operator fields (what a right-hand side needs).
+int check_ops(const dqb_dia_problem* p) {
+  if (!p) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->n < 2 || p->n_jumps < 0 || p->batch < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->batch > 65535) return DQB_ERR_UNSUPPORTED;
+  if ((p->h_ndiag > 0 && !p->h_diags) || (p->n_jumps > 0 && !p->l_diags)) return DQB_ERR_INVALID_ARGUMENT;
+  return DQB_OK;
+}
+
+// Everything a solve needs.
+int check_problem(const dqb_dia_problem* p) {
+  int rc = check_ops(p);
+  if (rc) return rc;
+  if (p->n_exp < 0 || p->n_tsave < 1 || !p->rho0 || !p->tsave) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->n_exp > 0 && !p->E) return DQB_ERR_INVALID_ARGUMENT;
+  return DQB_OK;
+}
+
+GraphCache g_cache;
+
+struct LaunchKey {
+  big::Common c;
+  DiaOps d;
+  int grid_e, grid_r_x, grid_r_y;
+};
+
+}  // namespace
+}  // namespace dqb
+
+using namespace dqb;
+
+extern "C" size_t dqb_mesolve_dia_workspace_size(const dqb_dia_problem* p) {
+  if (check_problem(p)) return 0;
+  DiaOps d;
+  if (build_ops(p, &d)) return 0;
+  return layout_for(p, d.nh).total;
+}
+
+extern "C" int dqb_lindblad_rhs_dia(const dqb_dia_problem* p, int32_t form, const void* rho, void* outp,
+                                    void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_ops(p);
+  if (rc) return rc;
+  if (!rho || !outp) return DQB_ERR_INVALID_ARGUMENT;
+  if (form != DQB_FORM_HERMITIAN && form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->batch == 0) return DQB_OK;
+  DiaOps d;
+  rc = build_ops(p, &d);
+  if (rc) return rc;
+  const size_t need = (size_t)p->batch * d.nh * p->n * sizeof(float2);
+  if (!workspace || workspace_bytes < need) return DQB_ERR_WORKSPACE_TOO_SMALL;
+  d.hnh = (float2*)workspace;
+  cudaStream_t s = (cudaStream_t)stream;
+  hnh_dia_kernel<<<dim3((p->n + 255) / 256, (unsigned)p->batch), 256, 0, s>>>(d, (int)p->batch);
+  big::Common c;
+  std::memset(&c, 0, sizeof(c));
+  rhs_dia_kernel<<<dim3((p->n + kRhsCols - 1) / kRhsCols, (p->n + kRhsRows - 1) / kRhsRows, (unsigned)p->batch),
+                   kRhsCols, 0, s>>>(c, d, 2, 0, 0, (const float2*)rho, (float2*)outp);
+  return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+}
+
+extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* o, const dqb_outputs* out,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_problem(p);
+  if (rc) return rc;
+  if (!o || !out || !out->states || !out->infos || !out->status || (p->n_exp > 0 && !out->expects))
+    return DQB_ERR_INVALID_ARGUMENT;
+  if (o->method != DQB_METHOD_TSIT5 && o->method != DQB_METHOD_DOPRI5) return DQB_ERR_INVALID_ARGUMENT;
+  if (o->form != DQB_FORM_HERMITIAN && o->form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
+  if (!(o->rtol >= 0) || !(o->atol >= 0) || o->max_steps < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->batch == 0) return DQB_OK;
+  DiaOps d;
+  rc = build_ops(p, &d);
+  if (rc) return rc;
+  const DiaLayout lay = layout_for(p, d.nh);
+  if (!workspace || workspace_bytes < lay.total) return DQB_ERR_WORKSPACE_TOO_SMALL;
+  char* ws = (char*)workspace;
+  d.hnh = (float2*)(ws + lay.off_hnh);
+
+  big::Common c;
+  std::memset(&c, 0, sizeof(c));
+  c.n = p->n;
+  c.nn = (long long)p->n * p->n;
+  c.B = (int)p->batch;
+  c.nE = p->n_exp;
+  c.ntsave = p->n_tsave;
+  c.form = o->form;
+  c.save_states = o->save_states;
+  c.rho0_is_ket = p->rho0_is_ket;
+  c.o = make_ctrl(*o);
+  c.tsave = p->tsave;
+  c.inst = (big::Inst*)(ws + lay.off_inst);
+  c.mats = (float2*)(ws + lay.off_mats);
+  c.eacc = (double2*)(ws + lay.off_eacc);
+  c.states = (float2*)out->states;
+  c.expects = (float2*)out->expects;
+  c.infos = out->infos;
+  c.status = out->status;
+  c.E = (const float2*)p->E;
+  c.rho0 = (const float2*)p->rho0;
+  c.ridx = p->rho0_index;
+  c.iter = (long long*)(ws + lay.off_iter);
+
+  cudaStream_t s = (cudaStream_t)stream;
+  const int B = c.B;
+  const long long nn = c.nn;
+  int grid_e = (int)std::min<long long>((nn + big::kElemThreads - 1) / big::kElemThreads, 1184);
+  if (grid_e < 1) grid_e = 1;
+  const dim3 ge(grid_e, B);
+  const dim3 gr((p->n + kRhsCols - 1) / kRhsCols, (p->n + kRhsRows - 1) / kRhsRows, B);
+  const dim3 gi((B + 127) / 128);
+  const int T = big::kElemThreads;
+
+  // ---- set-up and starting step (outside the graph) ----------------------------------
+  big::setup_kernel<<<gi, 128, 0, s>>>(c);
+  hnh_dia_kernel<<<dim3((p->n + 255) / 256, B), 256, 0, s>>>(d, B);
+  big::load_rho0_kernel<<<ge, T, 0, s>>>(c);
+  rhs_dia_kernel<<<gr, kRhsCols, 0, s>>>(c, d, 0, 0, 0, nullptr, nullptr);
+  big::init_norm_kernel<<<ge, T, 0, s>>>(c, 0);
+  big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 0);
+  big::combine_kernel<<<ge, T, 0, s>>>(c, 6);
+  rhs_dia_kernel<<<gr, kRhsCols, 0, s>>>(c, d, 2, 1, 0, nullptr, nullptr);
+  big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
+  big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 1);
+  if (cudaGetLastError() != cudaSuccess) return DQB_ERR_CUDA;
+
+  // ---- the RK loop: graph with a WHILE node ------------------------------------------
+  LaunchKey key;
+  std::memset(&key, 0, sizeof(key));
+  key.c = c;
+  key.d = d;
+  key.grid_e = grid_e;
+  key.grid_r_x = gr.x;
+  key.grid_r_y = gr.y;
+  cudaGraphExec_t exec = g_cache.find(&key, sizeof(key));
+  if (!exec) {
+    auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
+      for (int st = 0; st < 5; ++st) {
+        big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
+        rhs_dia_kernel<<<gr, kRhsCols, 0, cs>>>(c, d, 2, st + 1, 1, nullptr, nullptr);
+      }
+      big::combine_kernel<<<ge, T, 0, cs>>>(c, 5);
+      rhs_dia_kernel<<<gr, kRhsCols, 0, cs>>>(c, d, 1, 6, 1, nullptr, nullptr);
+      big::error_kernel<<<ge, T, 0, cs>>>(c);
+      big::control_kernel<<<gi, 128, 0, cs>>>(c);
+      big::save_kernel<<<ge, T, 0, cs>>>(c, 1);
+      big::commit_kernel<<<1, 1024, 0, cs>>>(c, h);
+    };
+    if (build_while_graph(body, &exec) != cudaSuccess) return DQB_ERR_CUDA;
+    g_cache.insert(&key, sizeof(key), exec, s);
+  } else {
+    g_cache.touch(&key, sizeof(key), s);
+  }
+  if (cudaGraphLaunch(exec, s) != cudaSuccess) return DQB_ERR_CUDA;
+
+  // ---- leftovers and outputs -----------------------------------------------------------
+  big::pre_finalize_kernel<<<gi, 128, 0, s>>>(c);
+  big::save_kernel<<<ge, T, 0, s>>>(c, 0);
+  big::finalize_kernel<<<ge, T, 0, s>>>(c);
+  return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+}

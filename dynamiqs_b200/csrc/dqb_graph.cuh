@@ -1,0 +1,96 @@
+// Host helpers shared by the large-problem entry points: the CUDA graph that runs the
+// RK loop as a device-side WHILE node, and a small cache of its executables.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+namespace dqb {
+
+// Executable graphs keyed by the bytes of the launch parameters (pointers and sizes):
+// a repeated call with the same buffers reuses its executable.  Evicted executables are
+// destroyed after the stream they were last launched on has drained.
+class GraphCache {
+ public:
+  struct Entry {
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t stream = nullptr;
+  };
+
+  cudaGraphExec_t find(const void* key, size_t len) {
+    std::lock_guard<std::mutex> lock(mu_);
+    for (auto& e : entries_)
+      if (e.key.size() == len && std::memcmp(e.key.data(), key, len) == 0) return e.exec;
+    return nullptr;
+  }
+
+  void insert(const void* key, size_t len, cudaGraphExec_t exec, cudaStream_t s) {
+    std::lock_guard<std::mutex> lock(mu_);
+    if (entries_.size() >= kMax) {
+      Entry& old = entries_.front();
+      cudaStreamSynchronize(old.stream);
+      cudaGraphExecDestroy(old.exec);
+      entries_.erase(entries_.begin());
+    }
+    Entry e;
+    e.key.assign((const unsigned char*)key, (const unsigned char*)key + len);
+    e.exec = exec;
+    e.stream = s;
+    entries_.push_back(std::move(e));
+  }
+
+  void touch(const void* key, size_t len, cudaStream_t s) {
+    std::lock_guard<std::mutex> lock(mu_);
+    for (auto& e : entries_)
+      if (e.key.size() == len && std::memcmp(e.key.data(), key, len) == 0) e.stream = s;
+  }
+
+ private:
+  static constexpr size_t kMax = 8;
+  std::mutex mu_;
+  std::vector<Entry> entries_;
+};
+
+// Build "WHILE (cond) { body }" where `body(stream, handle)` enqueues one loop iteration
+// on the capture stream and must end with a kernel that sets the condition.
+template <class Body>
+cudaError_t build_while_graph(Body body, cudaGraphExec_t* out) {
+  cudaGraph_t g = nullptr;
+  cudaError_t err = cudaGraphCreate(&g, 0);
+  if (err != cudaSuccess) return err;
+  cudaGraphConditionalHandle handle;
+  err = cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault);
+  if (err == cudaSuccess) {
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = handle;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    err = cudaGraphAddNode(&node, g, nullptr, 0, &p);
+    if (err == cudaSuccess) {
+      cudaGraph_t bodyg = p.conditional.phGraph_out[0];
+      cudaStream_t cap;
+      err = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+      if (err == cudaSuccess) {
+        err = cudaStreamBeginCaptureToGraph(cap, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (err == cudaSuccess) {
+          body(cap, handle);
+          cudaError_t e2 = cudaStreamEndCapture(cap, &bodyg);
+          if (err == cudaSuccess) err = e2;
+          if (err == cudaSuccess) err = cudaGetLastError();
+        }
+        cudaStreamDestroy(cap);
+      }
+      if (err == cudaSuccess) err = cudaGraphInstantiate(out, g, 0);
+    }
+  }
+  cudaGraphDestroy(g);
+  return err;
+}
+
+}  // namespace dqb

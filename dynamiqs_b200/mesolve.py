@@ -121,8 +121,8 @@ def assert_method_supported(method) -> None:
 @dataclass
 class BatchPlan:
     bshape: tuple  # leading result dims
-    H_items: np.ndarray  # (nH, n, n) or SparseDIA with diags (nH, nd, n)
-    L_sets: np.ndarray  # (nLsets, K, n, n)
+    H_items: object  # (nH, n, n) dense, or SparseDIA with diags (nH, nd, n)
+    L_sets: object  # (nLsets, K, n, n) dense, or list of K SparseDIA with diags (nLsets, nd_k, n)
     rho_items: np.ndarray  # (nrho, n, n) or (nrho, n, 1)
     H_index: np.ndarray  # int32 [B]
     L_index: np.ndarray
@@ -131,6 +131,16 @@ class BatchPlan:
     @property
     def batch(self) -> int:
         return int(np.prod(self.bshape, dtype=np.int64)) if self.bshape else 1
+
+    def L_sets_dense(self) -> np.ndarray:
+        if isinstance(self.L_sets, np.ndarray):
+            return self.L_sets
+        if not self.L_sets:
+            return np.zeros((1, 0, 1, 1), np.complex64)
+        return np.stack([L.to_dense() for L in self.L_sets], axis=1)
+
+    def H_items_dense(self) -> np.ndarray:
+        return self.H_items.to_dense() if isinstance(self.H_items, SparseDIA) else self.H_items
 
 
 def _place(n_items_shape: tuple, start: int, full: tuple) -> np.ndarray:
@@ -141,17 +151,46 @@ def _place(n_items_shape: tuple, start: int, full: tuple) -> np.ndarray:
     return np.broadcast_to(a.reshape(shape), full).reshape(-1)
 
 
+def _stack_sets(Ls, L_bs, n, cartesian, full):
+    """Jump sets indexed like ``L_index``: dense (nsets, K, n, n) when every operator is
+    dense, else one SparseDIA per jump with diags (nsets, nd_k, n)."""
+    K = len(Ls)
+    dia_mode = any(isinstance(L, SparseDIA) for L in Ls)
+    if dia_mode:
+        Ls = [L if isinstance(L, SparseDIA) else SparseDIA.from_dense(L) for L in Ls]
+        items = [(L.diags, L.diags.shape[-2:]) for L in Ls]
+    else:
+        items = [(np.asarray(L), (n, n)) for L in Ls]
+    if cartesian:
+        Lcat = tuple(d for b in L_bs for d in b)
+        mats, pos = [], 0
+        for (arr, tail), b in zip(items, L_bs):
+            shape = (1,) * pos + b + (1,) * (len(Lcat) - pos - len(b)) + tail
+            mats.append(np.broadcast_to(arr.reshape(shape), Lcat + tail).reshape(-1, *tail))
+            pos += len(b)
+        L_index_shape = Lcat
+    elif all(len(b) == 0 for b in L_bs):
+        mats = [arr.reshape(1, *tail) for arr, tail in items]
+        L_index_shape = None
+    else:
+        mats = [np.broadcast_to(arr, full + tail).reshape(-1, *tail) for arr, tail in items]
+        L_index_shape = full
+    if dia_mode:
+        sets = [SparseDIA(L.offsets, np.ascontiguousarray(m)) for L, m in zip(Ls, mats)]
+    else:
+        sets = (np.ascontiguousarray(np.stack(mats, axis=1)) if K
+                else np.zeros((1, 0, n, n), np.complex64))
+    return sets, L_index_shape
+
+
 def make_batch_plan(H, Ls, rho0, cartesian: bool) -> BatchPlan:
     """Flatten the reference's batching into per-instance index arrays
     (``mesolve.py:307-336``; ``cartesian_vmap`` / ``multi_vmap``,
     ``dynamiqs/integrators/_utils.py:93-187``)."""
-    Hd = to_dense(H) if not isinstance(H, SparseDIA) else H
     n = _shape(H)[-1]
     H_b = _shape(H)[:-2]
     L_bs = [_shape(L)[:-2] for L in Ls]
     r_b = _shape(rho0)[:-2]
-    K = len(Ls)
-    Ld = [to_dense(L) for L in Ls]
     rd = np.asarray(rho0)
     if cartesian:
         Lcat = tuple(d for b in L_bs for d in b)
@@ -159,33 +198,21 @@ def make_batch_plan(H, Ls, rho0, cartesian: bool) -> BatchPlan:
         H_index = _place(H_b, 0, full)
         L_index = _place(Lcat, len(H_b), full)
         rho_index = _place(r_b, len(H_b) + len(Lcat), full)
-        # materialise one stacked jump set per combination of the L batch indices
-        mats = []
-        pos = 0
-        for Lk, b in zip(Ld, L_bs):
-            shape = (1,) * pos + b + (1,) * (len(Lcat) - pos - len(b)) + (n, n)
-            mats.append(np.broadcast_to(Lk.reshape(shape), Lcat + (n, n)).reshape(-1, n, n))
-            pos += len(b)
-        L_sets = np.stack(mats, axis=1) if K else np.zeros((1, 0, n, n), np.complex64)
+        L_sets, _ = _stack_sets(Ls, L_bs, n, True, full)
     else:
-        full = np.broadcast_shapes(H_b, *L_bs, r_b)
+        full = tuple(np.broadcast_shapes(H_b, *L_bs, r_b))
         H_index = np.broadcast_to(np.arange(int(np.prod(H_b, dtype=np.int64))).reshape(H_b), full).reshape(-1)
         rho_index = np.broadcast_to(np.arange(int(np.prod(r_b, dtype=np.int64))).reshape(r_b), full).reshape(-1)
-        if all(len(b) == 0 for b in L_bs):
-            L_sets = np.stack(Ld, axis=0)[None] if K else np.zeros((1, 0, n, n), np.complex64)
-            L_index = np.zeros(int(np.prod(full, dtype=np.int64)), dtype=np.int64)
-        else:
-            mats = [np.broadcast_to(Lk, full + (n, n)).reshape(-1, n, n) for Lk in Ld]
-            L_sets = np.stack(mats, axis=1)
-            L_index = np.arange(int(np.prod(full, dtype=np.int64)))
-    if isinstance(Hd, SparseDIA):
-        H_items = SparseDIA(Hd.offsets, Hd.diags.reshape(-1, len(Hd.offsets), n))
+        L_sets, shp = _stack_sets(Ls, L_bs, n, False, full)
+        nb = int(np.prod(full, dtype=np.int64))
+        L_index = np.zeros(nb, dtype=np.int64) if shp is None else np.arange(nb)
+    if isinstance(H, SparseDIA):
+        H_items = SparseDIA(H.offsets, H.diags.reshape(-1, len(H.offsets), n))
     else:
-        H_items = Hd.reshape(-1, n, n)
+        H_items = np.asarray(H).reshape(-1, n, n)
     rho_items = rd.reshape(-1, *rd.shape[-2:])
-    return BatchPlan(tuple(full), H_items, np.ascontiguousarray(L_sets), rho_items,
-                     H_index.astype(np.int32), L_index.astype(np.int32),
-                     rho_index.astype(np.int32))
+    return BatchPlan(tuple(full), H_items, L_sets, rho_items, H_index.astype(np.int32),
+                     L_index.astype(np.int32), rho_index.astype(np.int32))
 
 
 # --------------------------------------------------------------------------------------
@@ -208,6 +235,35 @@ def _to_dev(x, dtype, device):
     if isinstance(x, torch.Tensor):
         return x.to(device=device, dtype=dtype).contiguous()
     return torch.from_numpy(np.ascontiguousarray(x)).to(device=device, dtype=dtype).contiguous()
+
+
+class PreparedSolve:
+    """A bound C-ABI solve with device-resident inputs, outputs and workspace."""
+
+    def __init__(self, integrator, fn, name, prob, outs, bufs, ws_bytes, dev, nE):
+        self.integrator = integrator
+        self.fn = fn
+        self.name = name
+        self.prob = prob
+        self.outs = outs
+        self.bufs = bufs
+        self.ws_bytes = ws_bytes
+        self.dev = dev
+        self.nE = nE
+
+    def launch(self, stream=None) -> PreparedSolve:
+        import torch
+
+        s = stream if stream is not None else torch.cuda.current_stream(self.dev).cuda_stream
+        rc = self.fn(self.prob, self.integrator._ode_options(), self.outs,
+                     self.bufs['workspace'].data_ptr(), self.ws_bytes, s)
+        _lib.check(rc, self.name)
+        return self
+
+    def result(self) -> MESolveResult:
+        b = self.bufs
+        return self.integrator._result(b['states'], b['expects'] if self.nE else None,
+                                       b['infos'], b['status'])
 
 
 class MESolveB200Integrator:
@@ -243,50 +299,125 @@ class MESolveB200Integrator:
             check_hermitian=int(bool(o.assume_hermitian)))
 
     def run(self) -> MESolveResult:
-        import torch
+        return self.prepare().launch().result()
 
+    def prepare(self) -> PreparedSolve:
+        """Copy the inputs to the device, size the workspace and bind the C-ABI call;
+        ``launch()`` may then be called repeatedly (the device inputs stay resident)."""
         lib = _lib.load()
-        dev = _device()
-        plan = self.plan
         n = _shape(self.H)[-1]
         K = len(self.Ls)
-        ntsave = len(self.ts)
-        B = plan.batch
-        nE = len(self.Es) if self.Es else 0
-        nsave = ntsave if self.options.save_states else 1
-        if n > lib.dqb_dense_small_max_n(K):
-            raise NotImplementedError(
-                f'Hilbert dimension n={n} with {K} jump operators is beyond the dense '
-                'shared-memory kernel of this build.')
-        H_items = plan.H_items.to_dense() if isinstance(plan.H_items, SparseDIA) else plan.H_items
+        dia_ops = isinstance(self.H, SparseDIA) or any(isinstance(L, SparseDIA) for L in self.Ls)
+        if n <= lib.dqb_dense_small_max_n(K):
+            return self._prepare_dense(lib, 'small')
+        if dia_ops:
+            return self._prepare_dia(lib)
+        return self._prepare_dense(lib, 'large')
+
+    def _common_buffers(self, dev, n, ntsave, nE, B, nsave):
+        import torch
+
         c64 = torch.complex64
-        H_d = _to_dev(H_items, c64, dev)
-        L_d = _to_dev(plan.L_sets, c64, dev)
+        plan = self.plan
         r_items = plan.rho_items
         is_ket = r_items.shape[-1] == 1 and n > 1
-        r_d = _to_dev(r_items, c64, dev)
-        E_d = (_to_dev(np.stack([to_dense(E) for E in self.Es]), c64, dev) if nE
-               else torch.zeros(1, dtype=c64, device=dev))
-        ts_d = _to_dev(np.asarray(self.ts, dtype=np.float64), torch.float64, dev)
-        idx = [_to_dev(a, torch.int32, dev) for a in (plan.H_index, plan.L_index, plan.rho_index)]
-        states = torch.empty((B, nsave, n, n), dtype=c64, device=dev)
-        expects = torch.empty((B, max(nE, 1), ntsave), dtype=c64, device=dev)
-        infos = torch.empty((B, 3), dtype=torch.int32, device=dev)
-        status = torch.empty((B,), dtype=torch.int32, device=dev)
+        bufs = {
+            'rho0': _to_dev(r_items, c64, dev),
+            'E': (_to_dev(np.stack([to_dense(E) for E in self.Es]), c64, dev) if nE
+                  else torch.zeros(1, dtype=c64, device=dev)),
+            'tsave': _to_dev(np.asarray(self.ts, dtype=np.float64), torch.float64, dev),
+            'H_index': _to_dev(plan.H_index, torch.int32, dev),
+            'L_index': _to_dev(plan.L_index, torch.int32, dev),
+            'rho0_index': _to_dev(plan.rho_index, torch.int32, dev),
+            'states': torch.empty((B, nsave, n, n), dtype=c64, device=dev),
+            'expects': torch.empty((B, max(nE, 1), ntsave), dtype=c64, device=dev),
+            'infos': torch.empty((B, 3), dtype=torch.int32, device=dev),
+            'status': torch.empty((B,), dtype=torch.int32, device=dev),
+        }
+        outs = _lib.Outputs(states=bufs['states'].data_ptr(), expects=bufs['expects'].data_ptr(),
+                            infos=bufs['infos'].data_ptr(), status=bufs['status'].data_ptr())
+        return bufs, outs, is_ket
+
+    def _sizes(self):
+        n = _shape(self.H)[-1]
+        ntsave = len(self.ts)
+        nE = len(self.Es) if self.Es else 0
+        nsave = ntsave if self.options.save_states else 1
+        return n, len(self.Ls), ntsave, self.plan.batch, nE, nsave
+
+    def _prepare_dense(self, lib, kind) -> PreparedSolve:
+        import torch
+
+        dev = _device()
+        n, K, ntsave, B, nE, nsave = self._sizes()
+        c64 = torch.complex64
+        bufs, outs, is_ket = self._common_buffers(dev, n, ntsave, nE, B, nsave)
+        bufs['H'] = _to_dev(self.plan.H_items_dense(), c64, dev)
+        bufs['L'] = _to_dev(self.plan.L_sets_dense(), c64, dev)
         prob = _lib.DenseProblem(
-            n=n, n_jumps=K, n_exp=nE, n_tsave=ntsave, batch=B, H=H_d.data_ptr(),
-            L=L_d.data_ptr(), rho0=r_d.data_ptr(), rho0_is_ket=int(is_ket),
-            E=E_d.data_ptr(), tsave=ts_d.data_ptr(), H_index=idx[0].data_ptr(),
-            L_index=idx[1].data_ptr(), rho0_index=idx[2].data_ptr())
-        outs = _lib.Outputs(states=states.data_ptr(), expects=expects.data_ptr(),
-                            infos=infos.data_ptr(), status=status.data_ptr())
-        opts = self._ode_options()
-        ws_bytes = lib.dqb_mesolve_dense_workspace_size(n, K, B)
-        ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
-        stream = torch.cuda.current_stream(dev).cuda_stream
-        rc = lib.dqb_mesolve_dense(prob, opts, outs, ws.data_ptr(), ws_bytes, stream)
-        _lib.check(rc, 'dqb_mesolve_dense')
-        return self._result(states, expects if nE else None, infos, status)
+            n=n, n_jumps=K, n_exp=nE, n_tsave=ntsave, batch=B, H=bufs['H'].data_ptr(),
+            L=bufs['L'].data_ptr(), rho0=bufs['rho0'].data_ptr(), rho0_is_ket=int(is_ket),
+            E=bufs['E'].data_ptr(), tsave=bufs['tsave'].data_ptr(),
+            H_index=bufs['H_index'].data_ptr(), L_index=bufs['L_index'].data_ptr(),
+            rho0_index=bufs['rho0_index'].data_ptr())
+        if kind == 'small':
+            ws_bytes = lib.dqb_mesolve_dense_workspace_size(n, K, B)
+            fn, name = lib.dqb_mesolve_dense, 'dqb_mesolve_dense'
+        else:
+            ws_bytes = lib.dqb_mesolve_dense_large_workspace_size(n, K, nE, ntsave, B)
+            fn, name = lib.dqb_mesolve_dense_large, 'dqb_mesolve_dense_large'
+        bufs['workspace'] = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+        return PreparedSolve(self, fn, name, prob, outs, bufs, ws_bytes, dev, nE)
+
+    def _prepare_dia(self, lib) -> PreparedSolve:
+        import ctypes
+
+        import torch
+
+        dev = _device()
+        n, K, ntsave, B, nE, nsave = self._sizes()
+        plan = self.plan
+        c64 = torch.complex64
+        bufs, outs, is_ket = self._common_buffers(dev, n, ntsave, nE, B, nsave)
+        H = plan.H_items if isinstance(plan.H_items, SparseDIA) else SparseDIA.from_dense(plan.H_items)
+        Lsets = plan.L_sets if isinstance(plan.L_sets, list) else [
+            SparseDIA.from_dense(plan.L_sets[:, k]) for k in range(plan.L_sets.shape[1])]
+        bufs['H'] = _to_dev(H.diags, c64, dev)
+        bufs['L'] = (_to_dev(np.concatenate([L.diags for L in Lsets], axis=-2), c64, dev)
+                     if Lsets else torch.zeros(1, dtype=c64, device=dev))
+        l_off_list = [k for L in Lsets for k in L.offsets]
+        host = {  # host arrays the C ABI reads during the call
+            'h_off': (ctypes.c_int32 * max(len(H.offsets), 1))(*H.offsets),
+            'l_nd': (ctypes.c_int32 * max(len(Lsets), 1))(*[len(L.offsets) for L in Lsets]),
+            'l_off': (ctypes.c_int32 * max(len(l_off_list), 1))(*l_off_list),
+        }
+        vp = ctypes.c_void_p
+        prob = _lib.DiaProblem(
+            n=n, n_jumps=len(Lsets), n_exp=nE, n_tsave=ntsave, batch=B, h_ndiag=len(H.offsets),
+            h_offsets=ctypes.cast(host['h_off'], vp), h_diags=bufs['H'].data_ptr(),
+            l_ndiag=ctypes.cast(host['l_nd'], vp), l_offsets=ctypes.cast(host['l_off'], vp),
+            l_diags=bufs['L'].data_ptr(), rho0=bufs['rho0'].data_ptr(), rho0_is_ket=int(is_ket),
+            E=bufs['E'].data_ptr(), tsave=bufs['tsave'].data_ptr(),
+            H_index=bufs['H_index'].data_ptr(), L_index=bufs['L_index'].data_ptr(),
+            rho0_index=bufs['rho0_index'].data_ptr())
+        ws_bytes = lib.dqb_mesolve_dia_workspace_size(prob)
+        if ws_bytes == 0:
+            raise NotImplementedError('DIA problem outside the limits of this build '
+                                      '(diagonal counts or batch size).')
+        bufs['workspace'] = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+        bufs['host'] = host
+        return PreparedSolve(self, lib.dqb_mesolve_dia, 'dqb_mesolve_dia', prob, outs, bufs,
+                             ws_bytes, dev, nE)
+
+    # kept for callers that select a path explicitly (tests)
+    def _run_dense_small(self, lib) -> MESolveResult:
+        return self._prepare_dense(lib, 'small').launch().result()
+
+    def _run_dense_large(self, lib) -> MESolveResult:
+        return self._prepare_dense(lib, 'large').launch().result()
+
+    def _run_dia(self, lib) -> MESolveResult:
+        return self._prepare_dia(lib).launch().result()
 
     def _result(self, states, expects, infos, status) -> MESolveResult:
         import torch

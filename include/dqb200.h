@@ -108,7 +108,8 @@ DQB_API size_t dqb_mesolve_dense_workspace_size(int32_t n, int32_t n_jumps, int6
  * MESolveDiffraxIntegrator with Tsit5 / Dopri5 (diffrax_integrator.py:135-147,
  * 283-378).  n <= 64: one persistent CTA per in-flight instance, the whole RK loop on
  * the device (operators and the stage input in shared memory, stages in an
- * L2-resident per-CTA scratch slot).  Larger n: see dqb_mesolve_dense_large. */
+ * L2-resident per-CTA scratch slot).  n > 64 returns DQB_ERR_UNSUPPORTED: use
+ * dqb_mesolve_dense_large. */
 DQB_API int dqb_mesolve_dense(const dqb_dense_problem* problem, const dqb_ode_options* options,
                       const dqb_outputs* outputs, void* workspace,
                       size_t workspace_bytes, void* stream);
@@ -137,6 +138,73 @@ DQB_API int dqb_lindblad_rhs_dense(const dqb_dense_problem* problem, int32_t for
 #define DQB_NOALLOC_SCRATCH_BYTES (8u << 20)
 DQB_API int dqb_mesolve_dense_noalloc(const dqb_dense_problem* problem, const dqb_ode_options* options,
                                       const dqb_outputs* outputs, void* stream);
+
+/* ---- dense operators, large n ---------------------------------------------------- */
+/* Scratch bytes for dqb_mesolve_dense_large (10 n x n slots per instance, Hnh, K product
+ * buffers, one sum buffer, controller state, FP64 expectation accumulators). */
+DQB_API size_t dqb_mesolve_dense_large_workspace_size(int32_t n, int32_t n_jumps, int32_t n_exp,
+                                                     int32_t n_tsave, int64_t batch);
+
+/* Batched adaptive solve with dense operators of any n (meant for n > 64, where one
+ * instance no longer fits a CTA).  Same problem, options and outputs as
+ * dqb_mesolve_dense (DiffraxIntegrator.run, diffrax_integrator.py:135-147, 283-378):
+ * each right-hand side is T_k = s L_k X, tmp = Hnh X + sum T_k L_k^+ (+ X Hnh^+), then
+ * tmp + tmp^+, as batched complex GEMMs; the RK loop runs as a CUDA-graph WHILE node. */
+DQB_API int dqb_mesolve_dense_large(const dqb_dense_problem* problem, const dqb_ode_options* options,
+                                    const dqb_outputs* outputs, void* workspace,
+                                    size_t workspace_bytes, void* stream);
+
+/* One right-hand side per instance for any n through the GEMM path.  `workspace` needs
+ * dqb_mesolve_dense_large_workspace_size(n, n_jumps, 0, 1, batch) bytes. */
+DQB_API int dqb_lindblad_rhs_dense_large(const dqb_dense_problem* problem, int32_t form,
+                                         const void* rho, void* out, void* workspace,
+                                         size_t workspace_bytes, void* stream);
+
+/* ---- sparse-DIA operators (large n) ---------------------------------------------- */
+/* Storage of the reference's SparseDIADataArray (dynamiqs/qarrays/sparsedia_dataarray.py:
+ * 42-71): static offsets (HOST arrays here, as they are static in the reference) and
+ * column-indexed diagonals diags[d][j] = A[j - offset_d][j] (DEVICE arrays), zero where
+ * the row falls outside the matrix.  Jump operator k owns l_ndiag[k] consecutive entries
+ * of l_offsets / of the diagonal axis of l_diags.  exp_ops are dense. */
+#define DQB_DIA_MAX_HNH_DIAGS 64
+#define DQB_DIA_MAX_JUMP_DIAGS 32
+#define DQB_DIA_MAX_JUMPS 16
+typedef struct dqb_dia_problem {
+  int32_t n, n_jumps, n_exp, n_tsave;
+  int64_t batch;
+  int32_t h_ndiag;
+  const int32_t* h_offsets;  /* HOST int32 [h_ndiag]                       */
+  const void* h_diags;       /* complex64 [*, h_ndiag, n]                  */
+  const int32_t* l_ndiag;    /* HOST int32 [n_jumps]                       */
+  const int32_t* l_offsets;  /* HOST int32 [sum l_ndiag]                   */
+  const void* l_diags;       /* complex64 [*, sum l_ndiag, n]              */
+  const void* rho0;          /* complex64 [*, n, n] or [*, n, 1] (ket)     */
+  int32_t rho0_is_ket;
+  const void* E;             /* complex64 [n_exp, n, n] (dense)            */
+  const double* tsave;       /* float64 [n_tsave]                          */
+  const int32_t* H_index;
+  const int32_t* L_index;
+  const int32_t* rho0_index;
+} dqb_dia_problem;
+
+/* Scratch bytes for dqb_mesolve_dia (10 n x n complex64 matrices per instance, plus
+ * Hnh diagonals, controller state and FP64 expectation accumulators). */
+DQB_API size_t dqb_mesolve_dia_workspace_size(const dqb_dia_problem* problem);
+
+/* Batched adaptive solve with sparse-DIA H and jump operators and a dense rho
+ * (matmul_sparsedia_array / matmul_array_sparsedia, sparsedia_primitives.py:232-261, in
+ * the vector fields of diffrax_integrator.py:312-323).  Hnh = -iH - 1/2 sum L^+L is built
+ * once per instance in DIA form (matmul_sparsedia_sparsedia / add_sparsedia_sparsedia,
+ * :172-229, hoisted out of the loop).  The RK loop runs as a CUDA graph with a device-side
+ * WHILE node: the call enqueues the whole solve on `stream` and returns. */
+DQB_API int dqb_mesolve_dia(const dqb_dia_problem* problem, const dqb_ode_options* options,
+                            const dqb_outputs* outputs, void* workspace, size_t workspace_bytes,
+                            void* stream);
+
+/* One right-hand side per instance with DIA operators: out[b] = f(rho[b]).  `workspace`
+ * holds the Hnh diagonals (size from dqb_mesolve_dia_workspace_size suffices). */
+DQB_API int dqb_lindblad_rhs_dia(const dqb_dia_problem* problem, int32_t form, const void* rho,
+                                 void* out, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- library info ------------------------------------------------------------- */
 /* Largest n handled by the shared-memory persistent kernel for a jump count. */

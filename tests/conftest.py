@@ -1,7 +1,20 @@
 import os
 import sys
 
-import pytest
+# The oracle's numpy uses OpenBLAS built with MAX_THREADS=64; on hosts with more cores
+# its multithreaded complex GEMM (n >= 128) has returned wrong results.  Cap the threads
+# before numpy loads, and again at run time in case a plugin imported it first.
+for _v in ('OPENBLAS_NUM_THREADS', 'OMP_NUM_THREADS', 'MKL_NUM_THREADS'):
+    os.environ.setdefault(_v, '8')
+
+import pytest  # noqa: E402
+
+try:
+    from threadpoolctl import threadpool_limits
+
+    threadpool_limits(8)
+except ImportError:  # pragma: no cover
+    pass
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:

@@ -38,3 +38,25 @@ def test_library_exports_every_declared_symbol():
 def test_version_string():
     lib = _lib.load()
     assert b'sm_100a' in lib.dqb_version()
+
+
+def test_argument_validation_without_gpu():
+    """Entry points reject bad arguments before touching the device."""
+    lib = _lib.load()
+    opts = _lib.OdeOptions(method=0, form=0, rtol=1e-6, atol=1e-6, safety=0.9, factormin=0.2,
+                           factormax=5.0, max_steps=10)
+    outs = _lib.Outputs()
+    assert lib.dqb_mesolve_dense(None, opts, outs, None, 0, None) == _lib.DQB_ERR_INVALID_ARGUMENT
+    assert lib.dqb_lindblad_rhs_dense(None, 0, None, None, None) == _lib.DQB_ERR_INVALID_ARGUMENT
+    assert lib.dqb_mesolve_dia(None, opts, outs, None, 0, None) == _lib.DQB_ERR_INVALID_ARGUMENT
+    p = _lib.DiaProblem(n=8, n_jumps=0, batch=1, h_ndiag=1)
+    # h_diags missing
+    assert lib.dqb_lindblad_rhs_dia(p, 0, 1, 1, None, 0, None) == _lib.DQB_ERR_INVALID_ARGUMENT
+    # operator fields suffice for a right-hand side; a too-small workspace is reported
+    off = (ctypes.c_int32 * 1)(0)
+    p = _lib.DiaProblem(n=8, n_jumps=0, batch=1, h_ndiag=1, h_offsets=ctypes.cast(off, ctypes.c_void_p),
+                        h_diags=1)
+    assert lib.dqb_lindblad_rhs_dia(p, 0, 1, 1, None, 0, None) == _lib.DQB_ERR_WORKSPACE_TOO_SMALL
+    # workspace query of a complete problem is host arithmetic
+    p.n_tsave, p.rho0, p.tsave = 3, 1, 1
+    assert lib.dqb_mesolve_dia_workspace_size(p) > 10 * 64 * 8

@@ -1,0 +1,111 @@
+"""GPU parity of the dense GEMM path for n > 64 (``dqb_lindblad_rhs_dense_large``,
+``dqb_mesolve_dense_large``) against the oracle, and against the shared-memory kernel
+at n <= 64.  Bars as in test_gpu_dense."""
+
+import numpy as np
+import pytest
+import torch
+
+import dynamiqs_b200 as dq
+from dynamiqs_b200 import _lib, workloads
+from dynamiqs_b200.mesolve import MESolveB200Integrator, make_batch_plan
+from oracle import lindblad as lb
+from oracle.mesolve import mesolve as oracle_mesolve
+from tests.systems import random_problem
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_frob(x, ref):
+    return np.linalg.norm(np.asarray(x) - ref, axis=(-2, -1)) / np.maximum(
+        np.linalg.norm(ref, axis=(-2, -1)), 1e-30)
+
+
+@pytest.mark.parametrize('n', [65, 100, 256])
+@pytest.mark.parametrize('K', [0, 1, 3, 5])
+@pytest.mark.parametrize('form', [_lib.FORM_HERMITIAN, _lib.FORM_STANDARD])
+def test_rhs_large_matches_oracle(cuda_device, n, K, form):
+    B = 2
+    Hs, Lsets, rhos = [], [], []
+    for b in range(B):
+        H, Ls, rho = random_problem(n, K, seed=100 * n + 10 * K + b,
+                                    hermitian_rho=form == _lib.FORM_HERMITIAN)
+        Hs.append(H)
+        Lsets.append(np.stack(Ls) if K else np.zeros((0, n, n), np.complex64))
+        rhos.append(rho)
+    dev = 'cuda'
+    H_d = torch.from_numpy(np.stack(Hs)).to(dev)
+    L_d = torch.from_numpy(np.stack(Lsets)).to(dev)
+    r_d = torch.from_numpy(np.stack(rhos)).to(dev)
+    out = torch.empty_like(r_d)
+    lib = _lib.load()
+    wsb = lib.dqb_mesolve_dense_large_workspace_size(n, K, 0, 1, B)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    prob = _lib.DenseProblem(n=n, n_jumps=K, batch=B, H=H_d.data_ptr(), L=L_d.data_ptr())
+    _lib.check(lib.dqb_lindblad_rhs_dense_large(prob, form, r_d.data_ptr(), out.data_ptr(),
+                                                 ws.data_ptr(), wsb,
+                                                 torch.cuda.current_stream().cuda_stream), 'rhs')
+    got = out.cpu().numpy()
+    for b in range(B):
+        Hc = Hs[b].astype(complex)
+        Lc = [L.astype(complex) for L in Lsets[b]]
+        rc = rhos[b].astype(complex)
+        ref = lb.vf_hermitian(Hc, Lc, rc) if form == _lib.FORM_HERMITIAN else lb.vf_standard(Hc, Lc, rc)
+        assert rel_frob(got[b], ref) < 3e-6
+
+
+def _check_vs_oracle(res, H, Ls, rho0, ts, Es, method, b=None):
+    kw = dict(exp_ops=Es, rtol=method.rtol, atol=method.atol)
+    r = oracle_mesolve(H, Ls, rho0, ts, **kw)
+    r64 = oracle_mesolve(H, Ls, rho0, ts, dtype=np.complex64, **kw)
+    st = res.states if b is None else res.states[b]
+    tol = max(1e-5, 2 * rel_frob(r64.states, r.states).max())
+    assert rel_frob(st.cpu().numpy(), r.states).max() < tol
+    if Es:
+        ex = res.expects if b is None else res.expects[b]
+        err = np.abs(ex.cpu().numpy() - r.expects) / np.maximum(np.abs(r.expects), 1.0)
+        etol = max(1e-5, 2 * (np.abs(r64.expects - r.expects) / np.maximum(np.abs(r.expects), 1.0)).max())
+        assert err.max() < etol
+    ns = int(res.infos.nsteps if b is None else res.infos.nsteps[b])
+    assert abs(ns - r.nsteps) <= max(1, int(0.002 * r.nsteps))
+
+
+def test_transmon_cavity_small_vs_oracle(cuda_device):
+    """Transmon(2) x cavity(40): n = 80 through the GEMM path, 3 instances."""
+    w = workloads.transmon_cavity(batch=3, nq=2, nc=40, seed=1)
+    ts = np.linspace(0.0, 5.0, 11)
+    res = dq.mesolve(w['H'], w['jump_ops'], w['rho0'], ts, exp_ops=w['exp_ops'], method=w['method'])
+    assert res.states.shape == (3, 11, 80, 80)
+    for b in range(3):
+        _check_vs_oracle(res, w['H'][b], w['jump_ops'], w['rho0'], ts, w['exp_ops'], w['method'], b)
+
+
+def test_transmon_cavity_full_dim_short_horizon(cuda_device):
+    """n = 256 (transmon 4 x cavity 64), 2 instances, t in [0, 2]."""
+    w = workloads.transmon_cavity(batch=2, seed=3)
+    ts = np.linspace(0.0, 2.0, 5)
+    res = dq.mesolve(w['H'], w['jump_ops'], w['rho0'], ts, exp_ops=w['exp_ops'], method=w['method'])
+    _check_vs_oracle(res, w['H'][0], w['jump_ops'], w['rho0'], ts, w['exp_ops'], w['method'], 0)
+
+
+def test_large_path_equals_small_kernel_at_n48(cuda_device):
+    H, Ls, rho = random_problem(48, 2, seed=9)
+    ts = np.linspace(0, 2.0, 6)
+    small = dq.mesolve(H, Ls, rho, ts)
+    plan = make_batch_plan(H, Ls, rho, True)
+    integ = MESolveB200Integrator(ts=ts, y0=rho, method=dq.Tsit5(), gradient=None,
+                                  options=dq.Options(), H=H, Ls=Ls, Es=None, plan=plan)
+    large = integ._run_dense_large(_lib.load())
+    assert rel_frob(large.states.cpu().numpy(), small.states.cpu().numpy()).max() < 1e-5
+    assert abs(int(large.infos.nsteps) - int(small.infos.nsteps)) <= 1
+
+
+def test_large_standard_form_and_save_states_false(cuda_device):
+    H, Ls, rho = random_problem(90, 3, seed=12, hermitian_rho=False)
+    ts = np.linspace(0, 1.0, 4)
+    res = dq.mesolve(H, Ls, rho, ts, options=dq.Options(assume_hermitian=False))
+    r = oracle_mesolve(H, Ls, rho, ts, form='standard')
+    assert rel_frob(res.states.cpu().numpy(), r.states).max() < 1e-5
+    last = dq.mesolve(H, Ls, rho, ts, options=dq.Options(assume_hermitian=False, save_states=False))
+    assert last.states.shape == (1, 90, 90)
+    assert rel_frob(last.states[0].cpu().numpy(), r.states[-1]) < 1e-5

@@ -65,4 +65,5 @@ def random_problem(n, K, seed=0, hermitian_rho=True, batch=None):
     rho = rho / np.trace(rho)
     if not hermitian_rho:
         rho = rho + 0.05 * cplx(n, n)
-    return H.astype(np.complex64), [L.astype(np.complex64) for L in Ls], rho.astype(np.complex64)
+    c = np.ascontiguousarray
+    return c(H, np.complex64), [c(L, np.complex64) for L in Ls], c(rho, np.complex64)

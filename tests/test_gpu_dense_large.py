@@ -34,9 +34,10 @@ def test_rhs_large_matches_oracle(cuda_device, n, K, form):
         Lsets.append(np.stack(Ls) if K else np.zeros((0, n, n), np.complex64))
         rhos.append(rho)
     dev = 'cuda'
-    H_d = torch.from_numpy(np.stack(Hs)).to(dev)
-    L_d = torch.from_numpy(np.stack(Lsets)).to(dev)
-    r_d = torch.from_numpy(np.stack(rhos)).to(dev)
+    # the C ABI reads raw row-major buffers: make every input C-contiguous
+    H_d = torch.from_numpy(np.ascontiguousarray(np.stack(Hs))).to(dev)
+    L_d = torch.from_numpy(np.ascontiguousarray(np.stack(Lsets))).to(dev)
+    r_d = torch.from_numpy(np.ascontiguousarray(np.stack(rhos))).to(dev)
     out = torch.empty_like(r_d)
     lib = _lib.load()
     wsb = lib.dqb_mesolve_dense_large_workspace_size(n, K, 0, 1, B)

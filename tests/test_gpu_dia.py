@@ -67,7 +67,7 @@ def test_rhs_dia_matches_oracle(cuda_device, form, n):
         rho = rho + 0.1 * Y
     rho = rho.astype(np.complex64)
     p, keep = _problem_struct(H, Ls, n, B)
-    r_d = torch.from_numpy(rho).to('cuda')
+    r_d = torch.from_numpy(np.ascontiguousarray(rho)).to('cuda')
     out = torch.empty_like(r_d)
     ws = torch.empty(1 << 20, dtype=torch.uint8, device='cuda')
     lib = _lib.load()

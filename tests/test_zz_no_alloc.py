@@ -29,10 +29,10 @@ def _problem(batch, seed):
     dev = torch.device('cuda', 0)
     n, K = 64, 2
     bufs = dict(
-        H=torch.from_numpy(w['H']).to(dev),
-        L=torch.from_numpy(np.stack(w['jump_ops'])[None].copy()).to(dev),
-        rho0=torch.from_numpy(w['rho0'].copy()).to(dev),
-        E=torch.from_numpy(np.stack(w['exp_ops']).copy()).to(dev),
+        H=torch.from_numpy(np.ascontiguousarray(w['H'])).to(dev),
+        L=torch.from_numpy(np.ascontiguousarray(np.stack(w['jump_ops'])[None])).to(dev),
+        rho0=torch.from_numpy(np.ascontiguousarray(w['rho0'])).to(dev),
+        E=torch.from_numpy(np.ascontiguousarray(np.stack(w['exp_ops']))).to(dev),
         ts=torch.from_numpy(ts).to(dev),
         zeros=torch.zeros(batch, dtype=torch.int32, device=dev),
     )

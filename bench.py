@@ -34,6 +34,9 @@ import time
 # process anyway.
 for _v in ('OPENBLAS_NUM_THREADS', 'OMP_NUM_THREADS', 'MKL_NUM_THREADS'):
     os.environ.setdefault(_v, '1')
+# Streams share CUDA_DEVICE_MAX_CONNECTIONS hardware queues (8 by default); the serving
+# configuration runs up to 16 streams whose waves must not queue behind each other.
+os.environ.setdefault('CUDA_DEVICE_MAX_CONNECTIONS', '32')
 
 import numpy as np  # noqa: E402
 
@@ -165,7 +168,117 @@ CASES = {
     'transmon': 'transmon(4) x cavity(64): n=256, B=256, K=2, t=[0,20], 41 saves, Tsit5 1e-6/1e-8',
     'dia': 'coupled Kerr modes 64x64 in sparse DIA: n=4096, B=8, K=2, t=[0,5], 11 saves, '
            'Tsit5 1e-5/1e-7',
+    'serving': 'Poisson stream (2000 req/s) of Kerr requests, n in {8..256} weights '
+               '(.30,.25,.20,.15,.07,.03), 1-3 jumps, t_end~U(1,20), 11-201 saves, Tsit5 1e-6',
 }
+
+
+def run_serving(args):
+    """Replay a seeded Poisson arrival schedule against MESolveServer in real time."""
+    import threading
+
+    import torch
+
+    import dynamiqs_b200 as dq
+    from dynamiqs_b200 import workloads
+    from dynamiqs_b200.server import MESolveServer
+
+    rank = int(os.environ.get('RANK', 0))
+    if rank != 0:
+        return
+    torch.cuda.set_device(0)
+    N = args.batch or 2000
+    reqs = workloads.serving_requests(N, rate=2000.0, seed=args.seed)
+    warm = workloads.serving_requests(24, rate=2000.0, seed=args.seed + 999)
+    srv = MESolveServer(n_streams=args.streams)
+    srv.warmup()
+    for r in warm:
+        srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'], exp_ops=r['exp_ops'],
+                   method=r['method'])
+    while len(srv.finished) < len(warm):
+        time.sleep(0.01)
+    for t in srv.finished:
+        t.release()
+    srv.finished.clear()
+    clk_path = os.path.join(ROOT, 'gpurun_out', 'clocks_rank0.csv')
+    os.makedirs(os.path.dirname(clk_path), exist_ok=True)
+    sampler = _clock_sampler(clk_path)
+    tickets = []
+
+    def feed():
+        t0 = time.perf_counter()
+        for r in reqs:
+            delay = r['arrival'] - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            tickets.append(srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'],
+                                      exp_ops=r['exp_ops'], method=r['method']))
+
+    th = threading.Thread(target=feed)
+    th.start()
+    th.join()
+    for t in tickets:
+        t.result()
+    srv.close()
+    nsteps_of = {t.id: int(t.result().infos.nsteps) for t in tickets}
+    for t in tickets:
+        t.release()
+    if sampler is not None:
+        sampler.terminate()
+        sampler.wait()
+    st = srv.stats()
+    flops = 0.0
+    for t in tickets:
+        flops += (6 * nsteps_of[t.id] + 2) * _flops_per_rhs(t.n, len(t.Ls))
+    achieved = flops / st['makespan_s'] / 1e12
+    peaks, which = _peaks()
+    peak = peaks.get('bf16_tflops_sustained', peaks.get('bf16_tflops'))
+    # plain path: the same requests one per launch, in arrival order, no overlap
+    plain = None
+    if not args.no_plain:
+        sample = reqs[: min(len(reqs), args.plain_sample)]
+        lat = []
+        t0 = time.perf_counter()
+        for r in sample:
+            a = time.perf_counter()
+            res = dq.mesolve(r['H'], r['jump_ops'], r['rho0'], r['tsave'], exp_ops=r['exp_ops'],
+                             method=r['method'])
+            res.infos.nsteps.cpu()
+            lat.append(time.perf_counter() - a)
+        tot = time.perf_counter() - t0
+        plain = {'value': len(sample) / tot, 'unit': 'solves/s',
+                 'what': f'dq.mesolve one request per launch, {len(sample)} requests back to back',
+                 'p50_latency_ms': 1e3 * float(np.percentile(lat, 50)),
+                 'p99_latency_ms': 1e3 * float(np.percentile(lat, 99)),
+                 'served_over_plain': st['solves_per_s'] / (len(sample) / tot)}
+    by_n = {}
+    for t in tickets:
+        by_n.setdefault(t.n, []).append(1e3 * t.latency)
+    per_size = {str(n): {'count': len(v), 'p50_ms': float(np.percentile(v, 50)),
+                         'p99_ms': float(np.percentile(v, 99))} for n, v in sorted(by_n.items())}
+    line = {
+        'metric': METRIC, 'value': st['solves_per_s'], 'unit': 'solves/s', 'n_gpus': 1,
+        'steps': 1, 'warmup': 1, 'ms_per_step': 1e3 * st['makespan_s'], 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'c64',
+        'data': 'synthetic (seeded Poisson arrivals and Kerr problems)',
+        'config': {'workload': CASES['serving'], 'requests': N, 'streams': args.streams,
+                   'waves': st['waves'], 'errors': st['errors'],
+                   'max_launch_s': max((x[2] for x in srv.launch_seconds), default=0.0),
+                   'slow_launches': [(str(k), c, round(sec, 3)) for k, c, sec in srv.launch_seconds
+                                     if sec > 0.5][:10],
+                   'slow_steps': [(str(k), {a: round(b, 3) for a, b in pr.items() if b > 0.1})
+                                  for k, pr in srv.launch_profile if max(pr.values()) > 0.1][:12]},
+        'latency_ms': {'p50': st['p50_ms'], 'p99': st['p99_ms'], 'mean': st['mean_ms'],
+                       'per_dim': per_size},
+        'e2e': {'value': st['solves_per_s'], 'unit': 'solves/s',
+                'h2d_bytes_per_step': None, 'd2h_bytes_per_step': None},
+        'roofline': {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
+                     'frac': achieved / peak, 'peak_source': f'bf16_tflops_sustained ({which})',
+                     'traffic': None},
+        'clocks': _clock_summary(clk_path),
+        'plain_path': plain,
+    }
+    print(json.dumps(line), flush=True)
 
 
 def _workload(name, args, rank):
@@ -393,12 +506,16 @@ def main():
                     'shorter only for profiling captures)')
     ap.add_argument('--e2e-steps', type=int, default=1)
     ap.add_argument('--cpu-sample', type=int, default=3)
+    ap.add_argument('--streams', type=int, default=16, help='serving: CUDA streams')
+    ap.add_argument('--plain-sample', type=int, default=100, help='serving: plain-path sample')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-plain', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
+    elif args.config == 'serving':
+        run_serving(args)
     else:
         run_b200(args)
 

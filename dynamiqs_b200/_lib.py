@@ -108,6 +108,27 @@ class DiaProblem(ctypes.Structure):
     ]
 
 
+class RaggedInstance(ctypes.Structure):
+    _fields_ = [
+        ('n', ctypes.c_int32),
+        ('n_jumps', ctypes.c_int32),
+        ('n_exp', ctypes.c_int32),
+        ('n_tsave', ctypes.c_int32),
+        ('rho0_is_ket', ctypes.c_int32),
+        ('save_states', ctypes.c_int32),
+        ('t0', ctypes.c_double),
+        ('H', ctypes.c_void_p),
+        ('L', ctypes.c_void_p),
+        ('rho0', ctypes.c_void_p),
+        ('E', ctypes.c_void_p),
+        ('tsave', ctypes.c_void_p),
+        ('states', ctypes.c_void_p),
+        ('expects', ctypes.c_void_p),
+        ('infos', ctypes.c_void_p),
+        ('status', ctypes.c_void_p),
+    ]
+
+
 # Every symbol include/dqb200.h declares, with (restype, argtypes).
 _P = ctypes.c_void_p
 SIGNATURES = {
@@ -124,6 +145,15 @@ SIGNATURES = {
                                                ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
     'dqb_lindblad_rhs_dense_large': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.c_int32, _P,
                                                     _P, _P, ctypes.c_size_t, _P]),
+    'dqb_mesolve_ragged_workspace_size': (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64]),
+    'dqb_mesolve_ragged': (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.POINTER(OdeOptions), _P, ctypes.c_size_t, _P]),
+    'dqb_mesolve_dense_large_ragged_workspace_size': (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32,
+                                                                        ctypes.c_int32, ctypes.c_int32,
+                                                                        ctypes.c_int64]),
+    'dqb_mesolve_dense_large_ragged': (ctypes.c_int, [_P, ctypes.c_int64, _P, ctypes.c_int32,
+                                                      ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                      ctypes.POINTER(OdeOptions), _P, ctypes.c_size_t, _P]),
     'dqb_mesolve_dia_workspace_size': (ctypes.c_size_t, [ctypes.POINTER(DiaProblem)]),
     'dqb_mesolve_dia': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.POINTER(OdeOptions),
                                        ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),

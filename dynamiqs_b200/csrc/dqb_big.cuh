@@ -24,6 +24,7 @@ namespace dqb {
 namespace big {
 
 constexpr int kSlots = 10;  // y, y1, k1..k7, X
+constexpr int kInactive = 99;  // status of a capacity slot beyond the wave's instance count
 constexpr int kX = 9;
 constexpr int kElemThreads = 256;
 
@@ -33,6 +34,16 @@ struct Inst {
   int status, run, keep, save_idx, save_lo, save_hi, herm_bad, pad;
   long long nsteps, nacc, nrej;
   int sy, sy1, sk[7];
+  // the instance's own problem data and outputs (shared arrays or a ragged descriptor)
+  int nts, nE, save_states, is_ket;
+  const double* ts;
+  const float2* rho0;
+  const float2* E;
+  float2* states;
+  float2* expects;
+  double2* eacc;
+  int* infos;
+  int* status_out;
 };
 
 struct Common {
@@ -52,6 +63,9 @@ struct Common {
   const float2* rho0;
   const int* ridx;
   long long* iter;  // graph-loop iteration counter
+  const dqb_ragged_instance* rag;  // per-instance descriptors, or null
+  long long eacc_stride;           // expectation accumulators per instance (ragged)
+  const int* count_dev;            // live instances (<= B) read at run time, or null
 };
 
 __device__ __forceinline__ float2* slot(const Common& c, int b, int s) {
@@ -73,8 +87,47 @@ static __global__ void setup_kernel(Common c) {
   if (b == 0) *c.iter = 0;
   if (b >= c.B) return;
   Inst& I = c.inst[b];
-  I.t = c.o.t0;
-  I.t1 = c.tsave[c.ntsave - 1];
+  if (c.count_dev && b >= *c.count_dev) {  // unused capacity: every kernel skips it
+    I.status = kInactive;
+    I.run = 0;
+    I.nts = I.nE = 0;
+    I.save_idx = I.save_lo = I.save_hi = 0;
+    I.herm_bad = 0;
+    I.nsteps = I.nacc = I.nrej = 0;
+    return;
+  }
+  if (c.rag) {
+    const dqb_ragged_instance& r = c.rag[b];
+    I.nts = r.n_tsave;
+    I.nE = r.n_exp;
+    I.save_states = r.save_states;
+    I.is_ket = r.rho0_is_ket;
+    I.ts = r.tsave;
+    I.rho0 = (const float2*)r.rho0;
+    I.E = (const float2*)r.E;
+    I.states = (float2*)r.states;
+    I.expects = (float2*)r.expects;
+    I.eacc = c.eacc + (long long)b * c.eacc_stride;
+    I.infos = r.infos;
+    I.status_out = r.status;
+    I.t = r.t0;
+  } else {
+    const long long ri = c.ridx ? c.ridx[b] : b;
+    I.nts = c.ntsave;
+    I.nE = c.nE;
+    I.save_states = c.save_states;
+    I.is_ket = c.rho0_is_ket;
+    I.ts = c.tsave;
+    I.rho0 = c.rho0 + ri * (c.rho0_is_ket ? (long long)c.n : c.nn);
+    I.E = c.E;
+    I.states = c.states + (long long)b * (c.save_states ? c.ntsave : 1) * c.nn;
+    I.expects = c.expects + (long long)b * c.nE * c.ntsave;
+    I.eacc = c.eacc + (long long)b * c.nE * c.ntsave;
+    I.infos = c.infos + 3 * b;
+    I.status_out = c.status + b;
+    I.t = c.o.t0;
+  }
+  I.t1 = I.ts[I.nts - 1];
   I.tnext = I.t1;
   I.h = I.dtnew = I.h0 = 0.0;
   I.acc[0] = I.acc[1] = I.acc[2] = 0.0;
@@ -93,19 +146,19 @@ static __global__ void setup_kernel(Common c) {
 static __global__ void load_rho0_kernel(Common c) {
   const int b = blockIdx.y;
   Inst& I = c.inst[b];
+  if (I.status == kInactive) return;
   const int n = c.n;
-  const long long ri = c.ridx ? c.ridx[b] : b;
   float2* y = slot(c, b, 0);
   int bad = 0;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
        e += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(e / n), j = (int)(e % n);
     float2 v;
-    if (c.rho0_is_ket) {
-      const float2* psi = c.rho0 + ri * n;
+    if (I.is_ket) {
+      const float2* psi = I.rho0;
       v = cmul(psi[i], cconj(psi[j]));
     } else {
-      const float2* r0 = c.rho0 + ri * c.nn;
+      const float2* r0 = I.rho0;
       v = r0[e];
       if (c.o.check_hermitian) {
         const float2 u = cconj(r0[(long long)j * n + i]);
@@ -116,9 +169,9 @@ static __global__ void load_rho0_kernel(Common c) {
     y[e] = v;
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) I.herm_bad = 1;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)c.nE * c.ntsave;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)I.nE * I.nts;
        e += (long long)gridDim.x * blockDim.x)
-    c.eacc[(long long)b * c.nE * c.ntsave + e] = make_double2(0.0, 0.0);
+    I.eacc[e] = make_double2(0.0, 0.0);
 }
 
 // ------------------------------------------------------------------------------------
@@ -233,6 +286,7 @@ static __global__ void init_ctrl_kernel(Common c, int phase) {
   if (b >= c.B) return;
   Inst& I = c.inst[b];
   const double inv_nn = 1.0 / (double)c.nn;
+  if (I.status == kInactive) return;
   if (phase == 0) {
     if (I.herm_bad) I.status = DQB_INST_NOT_HERMITIAN;
     const double d0 = sqrt(I.acc[0] * inv_nn), d1 = sqrt(I.acc[1] * inv_nn);
@@ -287,7 +341,7 @@ static __global__ void control_kernel(Common c) {
   I.dtnew = I.h * step_factor(c.o, err, keep);
   if (keep) {
     int hi = I.save_idx;
-    while (hi < c.ntsave && c.tsave[hi] <= I.tnext) ++hi;
+    while (hi < I.nts && I.ts[hi] <= I.tnext) ++hi;
     I.save_hi = hi;
   }
 }
@@ -309,13 +363,13 @@ static __global__ void save_kernel(Common c, int interp) {
     float cw[7];
     if (interp) {
       double w[7];
-      const double theta = I.h > 0.0 ? (c.tsave[s] - I.t) / I.h : 1.0;
+      const double theta = I.h > 0.0 ? (I.ts[s] - I.t) / I.h : 1.0;
       dense_weights(c.o.method, theta, w);
       for (int j = 0; j < 7; ++j) cw[j] = (float)(I.h * w[j]);
     }
-    float2* dst = c.states + ((long long)b * c.ntsave + s) * c.nn;
-    for (int m0 = 0; m0 == 0 || m0 < c.nE; m0 += 4) {
-      const int mc = c.nE - m0 < 4 ? c.nE - m0 : 4;
+    float2* dst = I.states + (long long)s * c.nn;
+    for (int m0 = 0; m0 == 0 || m0 < I.nE; m0 += 4) {
+      const int mc = I.nE - m0 < 4 ? I.nE - m0 : 4;
       double er[4] = {0, 0, 0, 0}, ei[4] = {0, 0, 0, 0};
       for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
            e += (long long)gridDim.x * blockDim.x) {
@@ -324,7 +378,7 @@ static __global__ void save_kernel(Common c, int interp) {
 #pragma unroll
           for (int j = 0; j < 7; ++j) v = caxpy(cw[j], k[j][e], v);
         }
-        if (m0 == 0 && c.save_states) dst[e] = v;
+        if (m0 == 0 && I.save_states) dst[e] = v;
         if (mc > 0) {
           // tr(E rho) = sum_ij E_ij rho_ji; rho_ji = conj(rho_ij) when rho is hermitian
           float2 rt;
@@ -342,7 +396,7 @@ static __global__ void save_kernel(Common c, int interp) {
 #pragma unroll
           for (int m = 0; m < 4; ++m) {
             if (m < mc) {
-              const float2 ev = c.E[(long long)(m0 + m) * c.nn + e];
+              const float2 ev = I.E[(long long)(m0 + m) * c.nn + e];
               er[m] += (double)ev.x * rt.x - (double)ev.y * rt.y;
               ei[m] += (double)ev.x * rt.y + (double)ev.y * rt.x;
             }
@@ -350,7 +404,7 @@ static __global__ void save_kernel(Common c, int interp) {
         }
       }
       for (int m = 0; m < mc; ++m) {
-        double2* acc = c.eacc + ((long long)b * c.nE + m0 + m) * c.ntsave + s;
+        double2* acc = I.eacc + (long long)(m0 + m) * I.nts + s;
         const double sr = block_sum(er[m], red);
         const double si = block_sum(ei[m], red);
         if (threadIdx.x == 0) {
@@ -403,7 +457,7 @@ static __global__ void pre_finalize_kernel(Common c) {
   I.save_hi = I.save_idx;
   if (I.status == DQB_INST_OK) {
     int hi = I.save_idx;
-    while (hi < c.ntsave && c.tsave[hi] <= I.t) ++hi;
+    while (hi < I.nts && I.ts[hi] <= I.t) ++hi;
     I.save_hi = hi;
   }
 }
@@ -411,23 +465,23 @@ static __global__ void pre_finalize_kernel(Common c) {
 static __global__ void finalize_kernel(Common c) {
   const int b = blockIdx.y;
   Inst& I = c.inst[b];
-  if (!c.save_states) {
+  if (I.status == kInactive) return;
+  if (!I.save_states) {
     const float2* y = slot(c, b, I.sy);
-    float2* dst = c.states + (long long)b * c.nn;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
          e += (long long)gridDim.x * blockDim.x)
-      dst[e] = y[e];
+      I.states[e] = y[e];
   }
   if (blockIdx.x == 0) {
-    for (int e = threadIdx.x; e < c.nE * c.ntsave; e += blockDim.x) {
-      const double2 v = c.eacc[(long long)b * c.nE * c.ntsave + e];
-      c.expects[(long long)b * c.nE * c.ntsave + e] = make_float2((float)v.x, (float)v.y);
+    for (int e = threadIdx.x; e < I.nE * I.nts; e += blockDim.x) {
+      const double2 v = I.eacc[e];
+      I.expects[e] = make_float2((float)v.x, (float)v.y);
     }
     if (threadIdx.x == 0) {
-      c.status[b] = I.status;
-      c.infos[b * 3 + 0] = (int)I.nsteps;
-      c.infos[b * 3 + 1] = (int)I.nacc;
-      c.infos[b * 3 + 2] = (int)I.nrej;
+      I.status_out[0] = I.status;
+      I.infos[0] = (int)I.nsteps;
+      I.infos[1] = (int)I.nacc;
+      I.infos[2] = (int)I.nrej;
     }
   }
 }

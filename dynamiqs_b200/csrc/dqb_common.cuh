@@ -193,4 +193,19 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return red[32];
 }
 
+// Zero a few words on a stream with a kernel (a memset would order itself against the
+// work of every other stream).
+static __global__ void zero_words_kernel(unsigned int* p, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = 0u;
+}
+
+// Every kernel of the library asks for the largest shared-memory carveout, so that kernels
+// of different entry points can share an SM without reconfiguring it (a carveout switch
+// serialises concurrent streams).
+template <class Kern>
+__host__ inline void prefer_max_shared(Kern kern) {
+  cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+}
+
 }  // namespace dqb

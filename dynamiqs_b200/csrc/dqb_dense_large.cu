@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "dqb_big.cuh"
 #include "dqb_graph.cuh"
@@ -41,7 +42,10 @@ struct LargeOps {
   float2* hnh;  // [B, n, n]
   float2* T;    // [B, K, n, n]
   float2* tmp;  // [B, n, n]
+  const dqb_ragged_instance* rag;  // per-instance operators (ragged batches), or null
 };
+
+__device__ __forceinline__ int jumps_of(const LargeOps& d, int b) { return d.rag ? d.rag[b].n_jumps : d.K; }
 
 struct GemmJob {
   int nterms;
@@ -68,12 +72,14 @@ __device__ __forceinline__ const float2* src_ptr(const big::Common& c, const Lar
       }
     case SRC_HNH: return d.hnh + b * nn;
     case SRC_L: {
+      if (d.rag) return (const float2*)d.rag[b].L + k * nn;
       const long long li = d.Lidx ? d.Lidx[b] : b;
       return d.L + (li * d.K + k) * nn;
     }
     case SRC_T: return d.T + ((long long)b * d.K + k) * nn;
     case SRC_TMP: return d.tmp + b * nn;
     default: {
+      if (d.rag) return (const float2*)d.rag[b].H;
       const long long hi = d.Hidx ? d.Hidx[b] : b;
       return d.H + hi * nn;
     }
@@ -135,6 +141,8 @@ __global__ void __launch_bounds__(NT) cgemm_kernel(big::Common c, LargeOps d, Ge
     const big::Inst& I = c.inst[b];
     if (job.need_run == 1 ? !I.run : I.status != DQB_INST_OK) return;
   }
+  const int Kb = jumps_of(d, b);
+  if (job.kdst < 0 && kz >= Kb) return;  // this instance has fewer jumps
   const int tiles = (n + BM - 1) / BM;
   const int tr = blockIdx.x / tiles, tc = blockIdx.x % tiles;
   const int r0 = tr * BM, c0 = tc * BN;
@@ -147,6 +155,7 @@ __global__ void __launch_bounds__(NT) cgemm_kernel(big::Common c, LargeOps d, Ge
 
   for (int t = 0; t < job.nterms; ++t) {
     const Term T = job.t[t];
+    if ((T.srcA == SRC_T || T.srcA == SRC_L) && T.kA >= Kb) continue;  // missing jump
     const float2* A = src_ptr(c, d, b, T.srcA, T.kA < 0 ? kz : T.kA, job.in_sel, ext_in);
     const float2* B = src_ptr(c, d, b, T.srcB, T.kB < 0 ? kz : T.kB, job.in_sel, ext_in);
     float2 ra[4], rb[4];
@@ -397,6 +406,82 @@ void launch_hnh(cudaStream_t s, const big::Common& c, const LargeOps& d, int B, 
 
 using namespace dqb;
 
+// One-time: every kernel of this file asks for the same (largest) shared-memory carveout.
+static void init_carveouts() {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    prefer_max_shared(big::setup_kernel);
+    prefer_max_shared(big::load_rho0_kernel);
+    prefer_max_shared(big::combine_kernel);
+    prefer_max_shared(big::error_kernel);
+    prefer_max_shared(big::init_norm_kernel);
+    prefer_max_shared(big::init_ctrl_kernel);
+    prefer_max_shared(big::control_kernel);
+    prefer_max_shared(big::save_kernel);
+    prefer_max_shared(big::commit_kernel);
+    prefer_max_shared(big::pre_finalize_kernel);
+    prefer_max_shared(big::finalize_kernel);
+    prefer_max_shared(zero_words_kernel);
+    prefer_max_shared(cgemm_kernel);
+    prefer_max_shared(symmetrize_kernel);
+  });
+}
+
+static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s) {
+  init_carveouts();
+  const int B = c.B;
+  int grid_e = (int)std::min<long long>((c.nn + big::kElemThreads - 1) / big::kElemThreads, 1184);
+  if (grid_e < 1) grid_e = 1;
+  const dim3 ge(grid_e, B);
+  const dim3 gi((B + 127) / 128);
+  const int T = big::kElemThreads;
+  const int form = c.form;
+
+  big::setup_kernel<<<gi, 128, 0, s>>>(c);
+  big::load_rho0_kernel<<<ge, T, 0, s>>>(c);
+  launch_hnh(s, c, d, B, 0);
+  launch_rhs(s, c, d, B, 0, 0, 0, form, nullptr, nullptr);
+  big::init_norm_kernel<<<ge, T, 0, s>>>(c, 0);
+  big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 0);
+  big::combine_kernel<<<ge, T, 0, s>>>(c, 6);
+  launch_rhs(s, c, d, B, 2, 1, 0, form, nullptr, nullptr);
+  big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
+  big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 1);
+  if (cudaGetLastError() != cudaSuccess) return DQB_ERR_CUDA;
+
+  LaunchKey key;
+  std::memset(&key, 0, sizeof(key));
+  key.c = c;
+  key.d = d;
+  key.form = form;
+  cudaGraphExec_t exec = g_cache.find(&key, sizeof(key));
+  if (!exec) {
+    auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
+      for (int st = 0; st < 5; ++st) {
+        big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
+        launch_rhs(cs, c, d, B, 2, st + 1, 1, form, nullptr, nullptr);
+      }
+      big::combine_kernel<<<ge, T, 0, cs>>>(c, 5);
+      launch_rhs(cs, c, d, B, 1, 6, 1, form, nullptr, nullptr);
+      big::error_kernel<<<ge, T, 0, cs>>>(c);
+      big::control_kernel<<<gi, 128, 0, cs>>>(c);
+      big::save_kernel<<<ge, T, 0, cs>>>(c, 1);
+      big::commit_kernel<<<1, 1024, 0, cs>>>(c, h);
+    };
+    if (build_while_graph(body, &exec) != cudaSuccess) return DQB_ERR_CUDA;
+    g_cache.insert(&key, sizeof(key), exec, s);
+  } else {
+    g_cache.touch(&key, sizeof(key), s);
+  }
+  if (cudaGraphLaunch(exec, s) != cudaSuccess) return DQB_ERR_CUDA;
+  big::pre_finalize_kernel<<<gi, 128, 0, s>>>(c);
+  big::save_kernel<<<ge, T, 0, s>>>(c, 0);
+  big::finalize_kernel<<<ge, T, 0, s>>>(c);
+  return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+}
+
+
+
 extern "C" size_t dqb_mesolve_dense_large_workspace_size(int32_t n, int32_t n_jumps, int32_t n_exp,
                                                          int32_t n_tsave, int64_t batch) {
   if (n < 2 || n_jumps < 0 || n_exp < 0 || n_tsave < 1 || batch <= 0) return 0;
@@ -416,9 +501,54 @@ extern "C" int dqb_lindblad_rhs_dense_large(const dqb_dense_problem* p, int32_t 
   big::Common c;
   std::memset(&c, 0, sizeof(c));
   cudaStream_t s = (cudaStream_t)stream;
+  init_carveouts();
   launch_hnh(s, c, d, (int)p->batch, 2);
   launch_rhs(s, c, d, (int)p->batch, 2, 0, 2, form, (const float2*)rho, (float2*)outp);
   return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+}
+
+extern "C" size_t dqb_mesolve_dense_large_ragged_workspace_size(int32_t n, int32_t max_jumps, int32_t max_exp,
+                                                                int32_t max_tsave, int64_t count) {
+  return dqb_mesolve_dense_large_workspace_size(n, max_jumps, max_exp, max_tsave, count);
+}
+
+extern "C" int dqb_mesolve_dense_large_ragged(const dqb_ragged_instance* instances, int64_t count,
+                                              const int32_t* count_device, int32_t n, int32_t max_jumps,
+                                              int32_t max_exp, int32_t max_tsave, const dqb_ode_options* o,
+                                              void* workspace, size_t workspace_bytes, void* stream) {
+  if (!o || count < 0 || n < 2 || max_jumps < 0 || max_jumps > 16 || max_exp < 0 || max_tsave < 1)
+    return DQB_ERR_INVALID_ARGUMENT;
+  if (count > 65535 / std::max(1, (int)max_jumps)) return DQB_ERR_UNSUPPORTED;
+  if (o->method != DQB_METHOD_TSIT5 && o->method != DQB_METHOD_DOPRI5) return DQB_ERR_INVALID_ARGUMENT;
+  if (o->form != DQB_FORM_HERMITIAN && o->form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
+  if (!(o->rtol >= 0) || !(o->atol >= 0) || o->max_steps < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if (count == 0) return DQB_OK;
+  if (!instances) return DQB_ERR_INVALID_ARGUMENT;
+  const LargeLayout lay = large_layout(n, max_jumps, max_exp, max_tsave, count);
+  if (!workspace || workspace_bytes < lay.total) return DQB_ERR_WORKSPACE_TOO_SMALL;
+  char* ws = (char*)workspace;
+  dqb_dense_problem p;
+  std::memset(&p, 0, sizeof(p));
+  p.n = n;
+  p.n_jumps = max_jumps;
+  p.batch = count;
+  LargeOps d = make_ops(&p, ws, lay);
+  d.rag = instances;
+  big::Common c;
+  std::memset(&c, 0, sizeof(c));
+  c.n = n;
+  c.nn = (long long)n * n;
+  c.B = (int)count;
+  c.form = o->form;
+  c.o = make_ctrl(*o);
+  c.inst = (big::Inst*)(ws + lay.off_inst);
+  c.mats = (float2*)(ws + lay.off_mats);
+  c.eacc = (double2*)(ws + lay.off_eacc);
+  c.eacc_stride = (long long)max_exp * max_tsave;
+  c.iter = (long long*)(ws + lay.off_iter);
+  c.rag = instances;
+  c.count_dev = count_device;
+  return run_large(c, d, (cudaStream_t)stream);
 }
 
 extern "C" int dqb_mesolve_dense_large(const dqb_dense_problem* p, const dqb_ode_options* o, const dqb_outputs* out,
@@ -462,54 +592,5 @@ extern "C" int dqb_mesolve_dense_large(const dqb_dense_problem* p, const dqb_ode
   c.ridx = p->rho0_index;
   c.iter = (long long*)(ws + lay.off_iter);
 
-  cudaStream_t s = (cudaStream_t)stream;
-  const int B = c.B;
-  int grid_e = (int)std::min<long long>((c.nn + big::kElemThreads - 1) / big::kElemThreads, 1184);
-  if (grid_e < 1) grid_e = 1;
-  const dim3 ge(grid_e, B);
-  const dim3 gi((B + 127) / 128);
-  const int T = big::kElemThreads;
-  const int form = o->form;
-
-  big::setup_kernel<<<gi, 128, 0, s>>>(c);
-  big::load_rho0_kernel<<<ge, T, 0, s>>>(c);
-  launch_hnh(s, c, d, B, 2);
-  launch_rhs(s, c, d, B, 0, 0, 0, form, nullptr, nullptr);
-  big::init_norm_kernel<<<ge, T, 0, s>>>(c, 0);
-  big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 0);
-  big::combine_kernel<<<ge, T, 0, s>>>(c, 6);
-  launch_rhs(s, c, d, B, 2, 1, 0, form, nullptr, nullptr);
-  big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
-  big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 1);
-  if (cudaGetLastError() != cudaSuccess) return DQB_ERR_CUDA;
-
-  LaunchKey key;
-  std::memset(&key, 0, sizeof(key));
-  key.c = c;
-  key.d = d;
-  key.form = form;
-  cudaGraphExec_t exec = g_cache.find(&key, sizeof(key));
-  if (!exec) {
-    auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
-      for (int st = 0; st < 5; ++st) {
-        big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
-        launch_rhs(cs, c, d, B, 2, st + 1, 1, form, nullptr, nullptr);
-      }
-      big::combine_kernel<<<ge, T, 0, cs>>>(c, 5);
-      launch_rhs(cs, c, d, B, 1, 6, 1, form, nullptr, nullptr);
-      big::error_kernel<<<ge, T, 0, cs>>>(c);
-      big::control_kernel<<<gi, 128, 0, cs>>>(c);
-      big::save_kernel<<<ge, T, 0, cs>>>(c, 1);
-      big::commit_kernel<<<1, 1024, 0, cs>>>(c, h);
-    };
-    if (build_while_graph(body, &exec) != cudaSuccess) return DQB_ERR_CUDA;
-    g_cache.insert(&key, sizeof(key), exec, s);
-  } else {
-    g_cache.touch(&key, sizeof(key), s);
-  }
-  if (cudaGraphLaunch(exec, s) != cudaSuccess) return DQB_ERR_CUDA;
-  big::pre_finalize_kernel<<<gi, 128, 0, s>>>(c);
-  big::save_kernel<<<ge, T, 0, s>>>(c, 0);
-  big::finalize_kernel<<<ge, T, 0, s>>>(c);
-  return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+  return run_large(c, d, (cudaStream_t)stream);
 }

@@ -20,6 +20,8 @@
 
 #include <algorithm>
 #include <mutex>
+#include <utility>
+#include <vector>
 
 #include "dqb_common.cuh"
 
@@ -65,6 +67,47 @@ struct Ctrl {
   long long inst;
   int sy, sy1, sk[7];
 };
+
+// Everything one instance's solve reads and writes (pointers at the instance's own data).
+struct InstView {
+  int n, K, nE, ntsave, is_ket, save_states;
+  double t0;
+  const float2* H;     // n x n
+  const float2* L;     // K x n x n
+  const float2* rho0;  // n x n, or n x 1 when is_ket
+  const float2* E;     // nE x n x n
+  const double* tsave;
+  float2* states;      // nsave x n x n
+  float2* expects;     // nE x ntsave
+  int* infos;          // 3
+  int* status;         // 1
+};
+
+__device__ __forceinline__ InstView view_of(const DenseSmallArgs& a, long long inst) {
+  InstView v;
+  const int n = a.n;
+  const long long nn = (long long)n * n;
+  const long long hi = a.Hidx ? a.Hidx[inst] : inst;
+  const long long li = a.Lidx ? a.Lidx[inst] : inst;
+  const long long ri = a.ridx ? a.ridx[inst] : inst;
+  v.n = n;
+  v.K = a.K;
+  v.nE = a.nE;
+  v.ntsave = a.ntsave;
+  v.is_ket = a.rho0_is_ket;
+  v.save_states = a.o.save_states;
+  v.t0 = a.o.t0;
+  v.H = a.H + hi * nn;
+  v.L = a.L + li * a.K * nn;
+  v.rho0 = a.rho0 + ri * (a.rho0_is_ket ? (long long)n : nn);
+  v.E = a.E;
+  v.tsave = a.tsave;
+  v.states = a.states ? a.states + inst * (a.o.save_states ? a.ntsave : 1) * nn : nullptr;
+  v.expects = a.expects ? a.expects + inst * a.nE * a.ntsave : nullptr;
+  v.infos = a.infos ? a.infos + inst * 3 : nullptr;
+  v.status = a.status ? a.status + inst : nullptr;
+  return v;
+}
 
 // acc[r][c] += sum_k op(A)[row][k] * op(B)[k][col], rows ty + 16 r, cols tx + 16 c.
 // CA: op(A) = A^+, CB: op(B) = B^+ (both read transposed from the padded layout).
@@ -170,57 +213,53 @@ __device__ void rhs(const float2* sH, const float2* sL, const float2* sX, float2
 // Write the state at save index `sidx` (y + sum_q cw[q] k_q when `interp`, else y)
 // and its expectation values tr(E_m rho) = sum_ij E_m[j][i] rho[i][j] (FP64 sums).
 template <int NP>
-__device__ void save_point(const DenseSmallArgs& a, long long inst, int sidx, const float2* __restrict__ yv,
+__device__ void save_point(const InstView& v, int sidx, const float2* __restrict__ yv,
                            float2* const (&kk)[7], const float (&cw)[7], bool interp, double* red) {
   constexpr int NN = NP * NP;
-  const int n = a.n;
-  for (int m0 = 0; m0 == 0 || m0 < a.nE; m0 += 8) {
-    const int mc = a.nE - m0 < 8 ? a.nE - m0 : 8;
+  const int n = v.n;
+  for (int m0 = 0; m0 == 0 || m0 < v.nE; m0 += 8) {
+    const int mc = v.nE - m0 < 8 ? v.nE - m0 : 8;
     double er[8], ei[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) er[m] = ei[m] = 0.0;
     for (int e = threadIdx.x; e < NN; e += blockDim.x) {
       const int i = e / NP, j = e % NP;
       if (i >= n || j >= n) continue;
-      float2 v = yv[e];
+      float2 val = yv[e];
       if (interp) {
 #pragma unroll
-        for (int q = 0; q < 7; ++q) v = caxpy(cw[q], kk[q][e], v);
+        for (int q = 0; q < 7; ++q) val = caxpy(cw[q], kk[q][e], val);
       }
-      if (m0 == 0 && a.o.save_states) a.states[((inst * a.ntsave + sidx) * n + i) * n + j] = v;
+      if (m0 == 0 && v.save_states) v.states[((long long)sidx * n + i) * n + j] = val;
 #pragma unroll
       for (int m = 0; m < 8; ++m) {
         if (m < mc) {
-          const float2 ev = a.E[((m0 + m) * n + j) * n + i];
-          er[m] += (double)ev.x * v.x - (double)ev.y * v.y;
-          ei[m] += (double)ev.x * v.y + (double)ev.y * v.x;
+          const float2 ev = v.E[((long long)(m0 + m) * n + j) * n + i];
+          er[m] += (double)ev.x * val.x - (double)ev.y * val.y;
+          ei[m] += (double)ev.x * val.y + (double)ev.y * val.x;
         }
       }
     }
     for (int m = 0; m < mc; ++m) {
       const double sr = block_sum(er[m], red);
       const double si = block_sum(ei[m], red);
-      if (threadIdx.x == 0) a.expects[(inst * a.nE + m0 + m) * a.ntsave + sidx] = make_float2((float)sr, (float)si);
+      if (threadIdx.x == 0) v.expects[(m0 + m) * v.ntsave + sidx] = make_float2((float)sr, (float)si);
     }
   }
 }
 
 template <int NP>
-__device__ void solve_one(const DenseSmallArgs& a, long long inst, float2* sH, float2* sX, float2* sT,
+__device__ void solve_one(const InstView& a, const CtrlOpts& o, float2* sH, float2* sX, float2* sT,
                           float2* sL, float2* slot, double* red, Ctrl& ctl) {
   constexpr int NN = NP * NP, LD = NP + 1;
   const int tid = threadIdx.x;
   const int n = a.n, K = a.K;
-  const CtrlOpts& o = a.o;
   const Tableau& T = c_tab[o.method];
   const double inv_nn = 1.0 / (double(n) * double(n));
 
   // ---- operators ------------------------------------------------------------------
-  const long long hi = a.Hidx ? a.Hidx[inst] : inst;
-  const long long li = a.Lidx ? a.Lidx[inst] : inst;
-  const long long ri = a.ridx ? a.ridx[inst] : inst;
-  load_padded<NP>(sH, a.H + hi * n * n, n);
-  for (int k = 0; k < K; ++k) load_padded<NP>(sL + k * Small<NP>::MAT, a.L + (li * K + k) * n * n, n);
+  load_padded<NP>(sH, a.H, n);
+  for (int k = 0; k < K; ++k) load_padded<NP>(sL + k * Small<NP>::MAT, a.L + (long long)k * n * n, n);
   __syncthreads();
   build_hnh<NP>(sH, sL, n, K);
 
@@ -240,11 +279,11 @@ __device__ void solve_one(const DenseSmallArgs& a, long long inst, float2* sH, f
     const int i = e / NP, j = e % NP;
     float2 v = make_float2(0.f, 0.f);
     if (i < n && j < n) {
-      if (a.rho0_is_ket) {
-        const float2* psi = a.rho0 + ri * n;
+      if (a.is_ket) {
+        const float2* psi = a.rho0;
         v = cmul(psi[i], cconj(psi[j]));
       } else {
-        const float2* r0 = a.rho0 + ri * n * n;
+        const float2* r0 = a.rho0;
         v = r0[i * n + j];
         if (o.check_hermitian) {
           const float2 u = cconj(r0[j * n + i]);
@@ -259,8 +298,8 @@ __device__ void solve_one(const DenseSmallArgs& a, long long inst, float2* sH, f
   bad = __syncthreads_or(bad);
   if (bad) {
     if (tid == 0) {
-      a.status[inst] = DQB_INST_NOT_HERMITIAN;
-      a.infos[inst * 3 + 0] = a.infos[inst * 3 + 1] = a.infos[inst * 3 + 2] = 0;
+      a.status[0] = DQB_INST_NOT_HERMITIAN;
+      a.infos[0] = a.infos[1] = a.infos[2] = 0;
     }
     return;
   }
@@ -303,12 +342,12 @@ __device__ void solve_one(const DenseSmallArgs& a, long long inst, float2* sH, f
     const double md = d1 > d2 ? d1 : d2;
     const double h1 = md <= 1e-15 ? fmax(1e-6, h0 * 1e-3) : pow(0.01 / md, 0.2);
     const double dt = fmin(100.0 * h0, h1);
-    ctl.t = o.t0;
+    ctl.t = a.t0;
     ctl.t1 = t1;
-    double tn = o.t0 + dt;
+    double tn = a.t0 + dt;
     if (tn > t1 - 1e-10) tn = t1;
     ctl.tnext = tn < t1 ? tn : t1;
-    ctl.run = o.t0 < t1;
+    ctl.run = a.t0 < t1;
   }
   __syncthreads();
 
@@ -411,7 +450,7 @@ __device__ void solve_one(const DenseSmallArgs& a, long long inst, float2* sH, f
         float cw[7];
 #pragma unroll
         for (int j = 0; j < 7; ++j) cw[j] = ctl.w[j];
-        save_point<NP>(a, inst, ctl.save_idx, yv, kk, cw, true, red);
+        save_point<NP>(a, ctl.save_idx, yv, kk, cw, true, red);
         __syncthreads();
         if (tid == 0) ctl.save_idx += 1;
         __syncthreads();
@@ -446,25 +485,25 @@ __device__ void solve_one(const DenseSmallArgs& a, long long inst, float2* sH, f
         kk[j] = slot + ctl.sk[j] * NN;
         cw[j] = 0.f;
       }
-      save_point<NP>(a, inst, ctl.save_idx, yv, kk, cw, false, red);
+      save_point<NP>(a, ctl.save_idx, yv, kk, cw, false, red);
       __syncthreads();
       if (tid == 0) ctl.save_idx += 1;
       __syncthreads();
     }
   }
   // final state when only the last state is kept (SubSaveAt(t1=True))
-  if (!o.save_states) {
+  if (!a.save_states) {
     const float2* yv = slot + ctl.sy * NN;
     for (int e = tid; e < NN; e += blockDim.x) {
       const int i = e / NP, j = e % NP;
-      if (i < n && j < n) a.states[(inst * n + i) * n + j] = yv[e];
+      if (i < n && j < n) a.states[(long long)i * n + j] = yv[e];
     }
   }
   if (tid == 0) {
-    a.status[inst] = ctl.status;
-    a.infos[inst * 3 + 0] = (int)ctl.nsteps;
-    a.infos[inst * 3 + 1] = (int)ctl.nacc;
-    a.infos[inst * 3 + 2] = (int)ctl.nrej;
+    a.status[0] = ctl.status;
+    a.infos[0] = (int)ctl.nsteps;
+    a.infos[1] = (int)ctl.nacc;
+    a.infos[2] = (int)ctl.nrej;
   }
 }
 
@@ -483,7 +522,8 @@ __global__ void __launch_bounds__(kSmallThreads) mesolve_small_kernel(DenseSmall
     __syncthreads();
     const long long inst = ctl.inst;
     if (inst >= a.batch) break;
-    solve_one<NP>(a, inst, sH, sX, sT, sL, slot, red, ctl);
+    const InstView v = view_of(a, inst);
+    solve_one<NP>(v, a.o, sH, sX, sT, sL, slot, red, ctl);
     __syncthreads();
   }
 }
@@ -535,19 +575,50 @@ static size_t smem_for(int NP, int K) {
   }
 }
 
+// Occupancy of a persistent kernel for a dynamic shared-memory size.  The kernel's
+// dynamic shared-memory limit is raised once, to the device maximum, and never lowered:
+// the attribute is per-function state shared by every host thread, so per-call values
+// could race with another thread's launch.  Results are cached per (kernel, smem).
+template <class Kern>
+static int resident_ctas(Kern kern, size_t smem) {
+  static std::mutex mu;
+  static std::vector<std::pair<const void*, size_t>> keys;  // (kernel, smem)
+  static std::vector<int> values;
+  static std::vector<const void*> raised;
+  const void* fn = (const void*)kern;
+  std::lock_guard<std::mutex> lock(mu);
+  if (std::find(raised.begin(), raised.end(), fn) == raised.end()) {
+    cudaFuncAttributes fa;
+    cudaFuncGetAttributes(&fa, kern);
+    const int limit = (int)max_optin_smem() - (int)fa.sharedSizeBytes;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+    prefer_max_shared(kern);
+    raised.push_back(fn);
+  }
+  for (size_t i = 0; i < keys.size(); ++i)
+    if (keys[i].first == fn && keys[i].second == smem) return values[i];
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSmallThreads, smem);
+  keys.emplace_back(fn, smem);
+  values.push_back(per_sm);
+  return per_sm;
+}
+
+static int sm_count() {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
 // Resident CTAs for (NP, K) on the current device; 0 if the shared memory does not fit.
 template <int NP>
 static int small_grid(int K, long long batch) {
   const size_t smem = small_smem_bytes<NP>(K);
   if (smem + 2048 > max_optin_smem()) return 0;
-  cudaFuncSetAttribute(mesolve_small_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mesolve_small_kernel<NP>, kSmallThreads, smem);
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int per_sm = resident_ctas(mesolve_small_kernel<NP>, smem);
   if (per_sm < 1) return 0;
-  long long g = (long long)per_sm * sms;
+  long long g = (long long)per_sm * sm_count();
   if (g > batch) g = batch;
   return (int)std::max<long long>(g, 1);
 }
@@ -636,7 +707,7 @@ extern "C" int dqb_mesolve_dense(const dqb_dense_problem* p, const dqb_ode_optio
   DenseSmallArgs a = make_args(p, o, out);
   a.counter = (unsigned int*)workspace;
   a.slots = (float2*)((char*)workspace + 256);
-  if (cudaMemsetAsync(workspace, 0, 256, s) != cudaSuccess) return DQB_ERR_CUDA;
+  zero_words_kernel<<<1, 64, 0, s>>>((unsigned int*)workspace, 64);
   const size_t smem = smem_for(NP, p->n_jumps);
   switch (NP) {
     case 16: mesolve_small_kernel<16><<<grid, kSmallThreads, smem, s>>>(a); break;
@@ -661,15 +732,15 @@ extern "C" int dqb_lindblad_rhs_dense(const dqb_dense_problem* p, int32_t form, 
   const unsigned grid = (unsigned)p->batch;
   switch (NP) {
     case 16:
-      cudaFuncSetAttribute(rhs_small_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      resident_ctas(rhs_small_kernel<16>, smem);
       rhs_small_kernel<16><<<grid, kSmallThreads, smem, s>>>(a, form, (const float2*)rho, (float2*)outp);
       break;
     case 32:
-      cudaFuncSetAttribute(rhs_small_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      resident_ctas(rhs_small_kernel<32>, smem);
       rhs_small_kernel<32><<<grid, kSmallThreads, smem, s>>>(a, form, (const float2*)rho, (float2*)outp);
       break;
     default:
-      cudaFuncSetAttribute(rhs_small_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      resident_ctas(rhs_small_kernel<64>, smem);
       rhs_small_kernel<64><<<grid, kSmallThreads, smem, s>>>(a, form, (const float2*)rho, (float2*)outp);
       break;
   }
@@ -724,3 +795,107 @@ int small_launch_with_scratch(const dqb_dense_problem* p, const dqb_ode_options*
 }
 
 }  // namespace dqb
+
+// ------------------------------------------------------------------------------------
+// ragged batches: every instance brings its own n, jumps, tsave and output buffers
+// ------------------------------------------------------------------------------------
+namespace dqb {
+
+template <int NP>
+__global__ void __launch_bounds__(kSmallThreads) mesolve_ragged_kernel(const dqb_ragged_instance* __restrict__ d,
+                                                                       long long count, CtrlOpts o, float2* slots,
+                                                                       unsigned int* counter) {
+  extern __shared__ float4 smem_raw[];
+  __shared__ double red[40];
+  __shared__ Ctrl ctl;
+  float2* sH = reinterpret_cast<float2*>(smem_raw);
+  float2* sX = sH + Small<NP>::MAT;
+  float2* sT = sX + Small<NP>::MAT;
+  float2* sL = sT + Small<NP>::MAT;
+  float2* slot = slots + (size_t)blockIdx.x * kSlotMats * Small<NP>::NN;
+  for (;;) {
+    if (threadIdx.x == 0) ctl.inst = (long long)atomicAdd(counter, 1u);
+    __syncthreads();
+    const long long inst = ctl.inst;
+    if (inst >= count) break;
+    const dqb_ragged_instance& r = d[inst];
+    InstView v;
+    v.n = r.n;
+    v.K = r.n_jumps;
+    v.nE = r.n_exp;
+    v.ntsave = r.n_tsave;
+    v.is_ket = r.rho0_is_ket;
+    v.save_states = r.save_states;
+    v.t0 = r.t0;
+    v.H = (const float2*)r.H;
+    v.L = (const float2*)r.L;
+    v.rho0 = (const float2*)r.rho0;
+    v.E = (const float2*)r.E;
+    v.tsave = r.tsave;
+    v.states = (float2*)r.states;
+    v.expects = (float2*)r.expects;
+    v.infos = r.infos;
+    v.status = r.status;
+    solve_one<NP>(v, o, sH, sX, sT, sL, slot, red, ctl);
+    __syncthreads();
+  }
+}
+
+template <int NP>
+static int ragged_grid(int K, long long count) {
+  const size_t smem = small_smem_bytes<NP>(K);
+  if (smem + 2048 > max_optin_smem()) return 0;
+  const int per_sm = resident_ctas(mesolve_ragged_kernel<NP>, smem);
+  if (per_sm < 1) return 0;
+  long long g = (long long)per_sm * sm_count();
+  if (g > count) g = count;
+  return (int)std::max<long long>(g, 1);
+}
+
+static int ragged_grid_for(int NP, int K, long long count) {
+  switch (NP) {
+    case 16: return ragged_grid<16>(K, count);
+    case 32: return ragged_grid<32>(K, count);
+    default: return ragged_grid<64>(K, count);
+  }
+}
+
+}  // namespace dqb
+
+extern "C" size_t dqb_mesolve_ragged_workspace_size(int32_t max_n, int32_t max_jumps, int64_t count) {
+  const int NP = pick_np(max_n);
+  if (NP == 0 || count <= 0 || max_jumps < 0) return 0;
+  const int g = ragged_grid_for(NP, max_jumps, count);
+  if (g <= 0) return 0;
+  return 256 + (size_t)g * kSlotMats * NP * NP * sizeof(float2);
+}
+
+extern "C" int dqb_mesolve_ragged(const dqb_ragged_instance* instances, int64_t count, int32_t max_n,
+                                  int32_t max_jumps, const dqb_ode_options* o, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
+  if (!o || count < 0 || max_n < 1 || max_jumps < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if (count >= (int64_t)0x7fffffff) return DQB_ERR_INVALID_ARGUMENT;
+  if (o->method != DQB_METHOD_TSIT5 && o->method != DQB_METHOD_DOPRI5) return DQB_ERR_INVALID_ARGUMENT;
+  if (o->form != DQB_FORM_HERMITIAN && o->form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
+  if (!(o->rtol >= 0) || !(o->atol >= 0) || o->max_steps < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if (count == 0) return DQB_OK;
+  if (!instances) return DQB_ERR_INVALID_ARGUMENT;
+  const int NP = pick_np(max_n);
+  if (NP == 0 || dqb_dense_small_max_n(max_jumps) < NP) return DQB_ERR_UNSUPPORTED;
+  const size_t need = dqb_mesolve_ragged_workspace_size(max_n, max_jumps, count);
+  if (need == 0) return DQB_ERR_UNSUPPORTED;
+  if (!workspace || workspace_bytes < need) return DQB_ERR_WORKSPACE_TOO_SMALL;
+  const int grid = ragged_grid_for(NP, max_jumps, count);
+  cudaStream_t s = (cudaStream_t)stream;
+  zero_words_kernel<<<1, 64, 0, s>>>((unsigned int*)workspace, 64);
+  unsigned int* counter = (unsigned int*)workspace;
+  float2* slots = (float2*)((char*)workspace + 256);
+  const CtrlOpts c = make_ctrl(*o);
+  const size_t smem = smem_for(NP, max_jumps);
+  switch (NP) {
+    case 16: mesolve_ragged_kernel<16><<<grid, kSmallThreads, smem, s>>>(instances, count, c, slots, counter); break;
+    case 32: mesolve_ragged_kernel<32><<<grid, kSmallThreads, smem, s>>>(instances, count, c, slots, counter); break;
+    default: mesolve_ragged_kernel<64><<<grid, kSmallThreads, smem, s>>>(instances, count, c, slots, counter); break;
+  }
+  return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+}

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <set>
 #include <vector>
 
@@ -244,6 +245,27 @@ struct LaunchKey {
 
 using namespace dqb;
 
+// One-time: every kernel of this file asks for the same (largest) shared-memory carveout.
+static void init_carveouts() {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    prefer_max_shared(big::setup_kernel);
+    prefer_max_shared(big::load_rho0_kernel);
+    prefer_max_shared(big::combine_kernel);
+    prefer_max_shared(big::error_kernel);
+    prefer_max_shared(big::init_norm_kernel);
+    prefer_max_shared(big::init_ctrl_kernel);
+    prefer_max_shared(big::control_kernel);
+    prefer_max_shared(big::save_kernel);
+    prefer_max_shared(big::commit_kernel);
+    prefer_max_shared(big::pre_finalize_kernel);
+    prefer_max_shared(big::finalize_kernel);
+    prefer_max_shared(zero_words_kernel);
+    prefer_max_shared(hnh_dia_kernel);
+    prefer_max_shared(rhs_dia_kernel);
+  });
+}
+
 extern "C" size_t dqb_mesolve_dia_workspace_size(const dqb_dia_problem* p) {
   if (check_problem(p)) return 0;
   DiaOps d;
@@ -265,6 +287,7 @@ extern "C" int dqb_lindblad_rhs_dia(const dqb_dia_problem* p, int32_t form, cons
   if (!workspace || workspace_bytes < need) return DQB_ERR_WORKSPACE_TOO_SMALL;
   d.hnh = (float2*)workspace;
   cudaStream_t s = (cudaStream_t)stream;
+  init_carveouts();
   hnh_dia_kernel<<<dim3((p->n + 255) / 256, (unsigned)p->batch), 256, 0, s>>>(d, (int)p->batch);
   big::Common c;
   std::memset(&c, 0, sizeof(c));
@@ -326,6 +349,7 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   const int T = big::kElemThreads;
 
   // ---- set-up and starting step (outside the graph) ----------------------------------
+  init_carveouts();
   big::setup_kernel<<<gi, 128, 0, s>>>(c);
   hnh_dia_kernel<<<dim3((p->n + 255) / 256, B), 256, 0, s>>>(d, B);
   big::load_rho0_kernel<<<ge, T, 0, s>>>(c);

@@ -11,14 +11,20 @@
 namespace dqb {
 
 // Executable graphs keyed by the bytes of the launch parameters (pointers and sizes):
-// a repeated call with the same buffers reuses its executable.  Evicted executables are
-// destroyed after the stream they were last launched on has drained.
+// a repeated call with the same buffers reuses its executable.  An evicted executable may
+// still be running, so it is parked with an event recorded on the stream it was last
+// launched on and destroyed once that event has completed (checked without blocking on
+// every later insert).
 class GraphCache {
  public:
   struct Entry {
     std::vector<unsigned char> key;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t stream = nullptr;
+  };
+  struct Parked {
+    cudaGraphExec_t exec;
+    cudaEvent_t done;
   };
 
   cudaGraphExec_t find(const void* key, size_t len) {
@@ -30,10 +36,18 @@ class GraphCache {
 
   void insert(const void* key, size_t len, cudaGraphExec_t exec, cudaStream_t s) {
     std::lock_guard<std::mutex> lock(mu_);
+    reap();
     if (entries_.size() >= kMax) {
       Entry& old = entries_.front();
-      cudaStreamSynchronize(old.stream);
-      cudaGraphExecDestroy(old.exec);
+      Parked p{old.exec, nullptr};
+      if (cudaEventCreateWithFlags(&p.done, cudaEventDisableTiming) == cudaSuccess &&
+          cudaEventRecord(p.done, old.stream) == cudaSuccess) {
+        parked_.push_back(p);
+      } else {  // no event: wait for the stream instead
+        if (p.done) cudaEventDestroy(p.done);
+        cudaStreamSynchronize(old.stream);
+        cudaGraphExecDestroy(old.exec);
+      }
       entries_.erase(entries_.begin());
     }
     Entry e;
@@ -50,9 +64,22 @@ class GraphCache {
   }
 
  private:
+  void reap() {
+    for (size_t i = 0; i < parked_.size();) {
+      if (cudaEventQuery(parked_[i].done) == cudaSuccess) {
+        cudaGraphExecDestroy(parked_[i].exec);
+        cudaEventDestroy(parked_[i].done);
+        parked_.erase(parked_.begin() + i);
+      } else {
+        ++i;
+      }
+    }
+  }
+
   static constexpr size_t kMax = 8;
   std::mutex mu_;
   std::vector<Entry> entries_;
+  std::vector<Parked> parked_;
 };
 
 // Build "WHILE (cond) { body }" where `body(stream, handle)` enqueues one loop iteration

@@ -139,6 +139,38 @@ DQB_API int dqb_lindblad_rhs_dense(const dqb_dense_problem* problem, int32_t for
 DQB_API int dqb_mesolve_dense_noalloc(const dqb_dense_problem* problem, const dqb_ode_options* options,
                                       const dqb_outputs* outputs, void* stream);
 
+/* ---- ragged batches (serving) ----------------------------------------------------- */
+/* One instance of a ragged batch: its own n (<= max_n), jump count (<= max_jumps), tsave
+ * grid, start time and output buffers; all pointers are device pointers to the
+ * instance's own data (H n x n, L n_jumps x n x n, rho0 n x n or n x 1, E n_exp x n x n,
+ * states nsave x n x n, expects n_exp x n_tsave, infos 3, status 1).  The array of
+ * descriptors itself lives in device memory. */
+typedef struct dqb_ragged_instance {
+  int32_t n, n_jumps, n_exp, n_tsave;
+  int32_t rho0_is_ket, save_states;
+  double t0;
+  const void* H;
+  const void* L;
+  const void* rho0;
+  const void* E;
+  const double* tsave;
+  void* states;
+  void* expects;
+  int32_t* infos;
+  int32_t* status;
+} dqb_ragged_instance;
+
+/* Scratch bytes for dqb_mesolve_ragged. */
+DQB_API size_t dqb_mesolve_ragged_workspace_size(int32_t max_n, int32_t max_jumps, int64_t count);
+
+/* Solve `count` independent problems of different sizes (n <= 64) in one persistent launch:
+ * the shape of a continuous-batching server's wave.  Each instance is solved exactly as a
+ * batch of one would be (same step sequence, same results); method and tolerances come
+ * from `options` (its t0 and save_states are ignored: they are per instance). */
+DQB_API int dqb_mesolve_ragged(const dqb_ragged_instance* instances, int64_t count, int32_t max_n,
+                               int32_t max_jumps, const dqb_ode_options* options, void* workspace,
+                               size_t workspace_bytes, void* stream);
+
 /* ---- dense operators, large n ---------------------------------------------------- */
 /* Scratch bytes for dqb_mesolve_dense_large (10 n x n slots per instance, Hnh, K product
  * buffers, one sum buffer, controller state, FP64 expectation accumulators). */
@@ -159,6 +191,22 @@ DQB_API int dqb_mesolve_dense_large(const dqb_dense_problem* problem, const dqb_
 DQB_API int dqb_lindblad_rhs_dense_large(const dqb_dense_problem* problem, int32_t form,
                                          const void* rho, void* out, void* workspace,
                                          size_t workspace_bytes, void* stream);
+
+/* Ragged batch for the GEMM path: every instance has this n (the caller guarantees it),
+ * its own jump count (<= max_jumps), exp_ops (<= max_exp), tsave grid (<= max_tsave
+ * points), start time and outputs, as in dqb_ragged_instance.  `count` is a capacity when
+ * `count_device` is non-NULL: the number of live instances (<= count) is then read from
+ * that device int32 when the solve starts and the rest are skipped.  Launch parameters
+ * then depend only on the capacity and the buffers, so repeated waves through the same
+ * workspace and descriptor buffers reuse one captured graph. */
+DQB_API size_t dqb_mesolve_dense_large_ragged_workspace_size(int32_t n, int32_t max_jumps,
+                                                            int32_t max_exp, int32_t max_tsave,
+                                                            int64_t count);
+DQB_API int dqb_mesolve_dense_large_ragged(const dqb_ragged_instance* instances, int64_t count,
+                                           const int32_t* count_device, int32_t n, int32_t max_jumps,
+                                           int32_t max_exp,
+                                           int32_t max_tsave, const dqb_ode_options* options,
+                                           void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- sparse-DIA operators (large n) ---------------------------------------------- */
 /* Storage of the reference's SparseDIADataArray (dynamiqs/qarrays/sparsedia_dataarray.py:

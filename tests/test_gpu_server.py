@@ -1,0 +1,78 @@
+"""Continuous-batching server: each result is the same alone (``dq.mesolve`` on that one
+request) and in the mix, within the 1e-5 relative bar; requests that arrive while others
+are on the GPU are launched before those finish (their work overlaps on the device)."""
+
+import numpy as np
+import pytest
+
+import dynamiqs_b200 as dq
+from dynamiqs_b200 import workloads
+from dynamiqs_b200.server import MESolveServer
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(num, seed, dims=(8, 16, 32, 64, 128), weights=(0.3, 0.25, 0.2, 0.15, 0.1)):
+    reqs = workloads.serving_requests(num, seed=seed, dims=dims, weights=weights)
+    for r in reqs:  # short horizons keep the test quick
+        r['tsave'] = np.linspace(0.0, min(r['tsave'][-1], 3.0), len(r['tsave']))
+    return reqs
+
+
+def _rel(x, ref):
+    x, ref = np.asarray(x), np.asarray(ref)
+    return float((np.linalg.norm(x - ref, axis=(-2, -1)) / np.linalg.norm(ref, axis=(-2, -1))).max())
+
+
+def test_results_same_alone_and_in_the_mix(cuda_device):
+    reqs = _requests(24, seed=11)
+    srv = MESolveServer(n_streams=4)
+    tickets = [srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'], exp_ops=r['exp_ops'],
+                          method=r['method']) for r in reqs]
+    results = [t.result(timeout=300) for t in tickets]
+    srv.close()
+    assert srv.stats()['solves'] == len(reqs)
+    for r, res in zip(reqs, results):
+        alone = dq.mesolve(r['H'], r['jump_ops'], r['rho0'], r['tsave'], exp_ops=r['exp_ops'],
+                           method=r['method'])
+        assert _rel(res.states.cpu().numpy(), alone.states.cpu().numpy()) < 1e-5
+        e_mix, e_alone = res.expects.cpu().numpy(), alone.expects.cpu().numpy()
+        assert np.max(np.abs(e_mix - e_alone) / np.maximum(np.abs(e_alone), 1.0)) < 1e-5
+        assert int(res.infos.nsteps) == int(alone.infos.nsteps)
+
+
+def test_late_arrivals_overlap_running_waves(cuda_device):
+    first = _requests(12, seed=3, dims=(64,), weights=(1.0,))
+    late = _requests(12, seed=4, dims=(16, 32), weights=(0.5, 0.5))
+    srv = MESolveServer(n_streams=8)
+    t1 = [srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'], method=r['method']) for r in first]
+    t2 = [srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'], method=r['method']) for r in late]
+    for t in t1 + t2:
+        t.result(timeout=300)
+    srv.close()
+    # some late request was launched before the last of the first group finished
+    assert min(t.t_launch for t in t2) < max(t.t_done for t in t1)
+    st = srv.stats()
+    assert st['errors'] == 0 and st['p99_ms'] >= st['p50_ms'] > 0
+
+
+def test_budget_admission_and_errors(cuda_device):
+    reqs = _requests(6, seed=5, dims=(16,), weights=(1.0,))
+    tiny = MESolveServer(budget_bytes=4096, n_streams=2, staging_bytes=1 << 20)
+    t = tiny.submit(reqs[0]['H'], reqs[0]['jump_ops'], reqs[0]['rho0'], reqs[0]['tsave'],
+                    method=reqs[0]['method'])
+    with pytest.raises(MemoryError, match='budget'):
+        t.result(timeout=60)
+    tiny.close()
+    srv = MESolveServer(budget_bytes=1 << 30, n_streams=2, staging_bytes=1 << 24)
+    tickets = [srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'], method=r['method'])
+               for r in reqs]
+    bad = srv.submit(reqs[0]['H'], reqs[0]['jump_ops'], reqs[0]['rho0'], reqs[0]['tsave'],
+                     method=dq.Tsit5(max_steps=2))
+    for t in tickets:
+        assert t.result(timeout=120).states.shape[-1] == 16
+        t.release()
+    with pytest.raises(RuntimeError, match='maximum number of method steps'):
+        bad.result(timeout=120)
+    srv.close()
+    assert srv._dev.used() == 0  # every wave and every released result gave its memory back

@@ -343,9 +343,10 @@ def run_b200(args):
 
     w = _workload(args.config, args, rank)
     Es = w.get('exp_ops')
+    opts = dq.Options(precision=args.precision)
     plan = make_batch_plan(w['H'], w['jump_ops'], w['rho0'], True)
     integ = MESolveB200Integrator(ts=w['tsave'], y0=w['rho0'], method=w['method'], gradient=None,
-                                  options=dq.Options(), H=w['H'], Ls=w['jump_ops'], Es=Es, plan=plan)
+                                  options=opts, H=w['H'], Ls=w['jump_ops'], Es=Es, plan=plan)
     prep = integ.prepare()
     B = plan.batch
     n = w['H'].shape[-1]
@@ -418,7 +419,7 @@ def run_b200(args):
             barrier()
             t = time.perf_counter()
             res = dq.mesolve(H_host, w['jump_ops'], w['rho0'], w['tsave'], exp_ops=Es,
-                             method=w['method'])
+                             method=w['method'], options=opts)
             ex = res.expects.cpu() if res.expects is not None else torch.zeros(0)
             inf = res.infos.nsteps.cpu()
             torch.cuda.synchronize()
@@ -478,6 +479,7 @@ def run_b200(args):
         'config': {'workload': CASES[args.config], 'batch_per_gpu': B, 'n': n, 'n_jumps': K,
                    'n_tsave': len(w['tsave']), 'method': type(w['method']).__name__,
                    'rtol': w['method'].rtol, 'atol': w['method'].atol, 'path': prep.name,
+                   'precision': args.precision,
                    'l2': 'flushed between iterations (256 MiB write)',
                    'parallelism': f'instances sharded over {world} GPU(s), no collective',
                    'avg_rk_steps': float(nsteps.mean()), 'max_rk_steps': float(nsteps.max())},
@@ -511,6 +513,8 @@ def main():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-plain', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--precision', default='fp32', choices=['fp32', 'tf32x3', 'bf16x3', 'tf32'],
+                    help='arithmetic of the GEMM path (n > 64) products')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

@@ -39,6 +39,11 @@ METHOD_TSIT5 = 0
 METHOD_DOPRI5 = 1
 FORM_HERMITIAN = 0
 FORM_STANDARD = 1
+PREC_FP32 = 0
+PREC_TF32X3 = 1
+PREC_BF16X3 = 2
+PREC_TF32 = 3
+PRECISIONS = {'fp32': PREC_FP32, 'tf32x3': PREC_TF32X3, 'bf16x3': PREC_BF16X3, 'tf32': PREC_TF32}
 
 
 class OdeOptions(ctypes.Structure):
@@ -54,6 +59,7 @@ class OdeOptions(ctypes.Structure):
         ('t0', ctypes.c_double),
         ('save_states', ctypes.c_int32),
         ('check_hermitian', ctypes.c_int32),
+        ('precision', ctypes.c_int32),
     ]
 
 
@@ -145,6 +151,8 @@ SIGNATURES = {
                                                ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
     'dqb_lindblad_rhs_dense_large': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.c_int32, _P,
                                                     _P, _P, ctypes.c_size_t, _P]),
+    'dqb_lindblad_rhs_dense_large_prec': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.c_int32,
+                                                         ctypes.c_int32, _P, _P, _P, ctypes.c_size_t, _P]),
     'dqb_mesolve_ragged_workspace_size': (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64]),
     'dqb_mesolve_ragged': (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
                                           ctypes.POINTER(OdeOptions), _P, ctypes.c_size_t, _P]),

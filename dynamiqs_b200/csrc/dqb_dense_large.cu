@@ -13,6 +13,7 @@
 // FP32 FMA; each K-slice is read from global memory into registers (coalesced along the
 // operand's rows, transposed on the way into shared memory when the operand is a ^+).
 // Any n (edges zero-filled).
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -21,6 +22,7 @@
 
 #include "dqb_big.cuh"
 #include "dqb_graph.cuh"
+#include "dqb_tc.cuh"
 
 namespace dqb {
 namespace {
@@ -43,6 +45,7 @@ struct LargeOps {
   float2* T;    // [B, K, n, n]
   float2* tmp;  // [B, n, n]
   const dqb_ragged_instance* rag;  // per-instance operators (ragged batches), or null
+  int prec;                        // DQB_PREC_*: FP32 CUDA cores or a tensor-core mode
 };
 
 __device__ __forceinline__ int jumps_of(const LargeOps& d, int b) { return d.rag ? d.rag[b].n_jumps : d.K; }
@@ -288,6 +291,354 @@ __global__ void __launch_bounds__(256) symmetrize_kernel(big::Common c, LargeOps
   }
 }
 
+// ------------------------------------------------------------------------------------
+// Tensor-core GEMM (tcgen05): C = alpha sum_t A_t M_t^+ for complex n x n matrices.
+// ------------------------------------------------------------------------------------
+// Real form.  With complex64 stored interleaved, row i of A is the real row
+// A'[i] = (Re A[i][0], Im A[i][0], Re A[i][1], ...) of length 2n, and C = A M^+ is the real
+// product C' = A' B' in which C' is C interleaved the same way and B' (2n x 2n) has, in its
+// K-major (transposed) form, the rows
+//   B'^T[2j]   = M[j]                         -> Re C[i][j] = sum_k Re A Re M + Im A Im M
+//   B'^T[2j+1] = (i M)[j] = (-Im M, Re M)     -> Im C[i][j] = sum_k Im A Re M - Re A Im M
+// so both operands are read row by row from the complex matrices with no transpose, and the
+// real GEMM does exactly the 8 n^3 flops of the complex one.  A hermitian X is its own M
+// (X = X^+), which covers every product of the hermitian-form right-hand side:
+// L_k X = L_k X^+, Hnh X = Hnh X^+ and T_k L_k^+.
+//
+// Tile: 128 rows x 128 complex columns of C (MMA M = 128, N = 256 real columns) per CTA.
+// The hi*hi products accumulate in one TMEM accumulator (256 columns) and the two small
+// cross products hi*lo + lo*hi in a second one, summed in FP32 registers at the end: the
+// tensor core's accumulation loses a fraction of an ulp of the accumulator per MMA, so
+// adding the small terms into the large accumulator would triple that loss.  The contraction runs in stages of 128 bytes of every
+// operand row (16 complex values for TF32, 32 for BF16), two stages in shared memory.
+// Eight producer warps load complex64 rows (L2-resident), split each value into hi + lo,
+// apply the (-Im, Re) map for the odd B rows and store into the swizzled tiles; one warp
+// issues the MMAs (lo*hi + hi*lo + hi*hi with FP32 accumulation in TMEM: 3xTF32 or 3xBF16;
+// hi*hi alone in the single-pass TF32 mode); the eight warps then read the accumulator out
+// of TMEM (warp w reads lanes 32 (w % 4) .. +31, column half w / 4) and write C.
+namespace tcg {
+constexpr int kProdWarps = 8;
+constexpr int kProd = kProdWarps * 32;
+constexpr int kThreads = kProd + 32;
+constexpr uint32_t kA = 128 * 128;             // one 128-row operand tile (bytes)
+constexpr uint32_t kB = 256 * 128;             // one 256-row operand tile
+constexpr uint32_t kStage = 2 * kA + 2 * kB;   // A hi, A lo, B hi, B lo
+constexpr int kStages = 2;
+constexpr int kSmem = kStages * kStage + 1024;  // + alignment slack
+constexpr uint32_t kAccCols = 256;             // one FP32 accumulator: 128 lanes x 256 columns
+}  // namespace tcg
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
+}
+
+__device__ __forceinline__ void st_split_tf32(uint32_t hi_addr, uint32_t lo_addr, float4 v, bool split) {
+  float h0, h1, h2, h3, l0, l1, l2, l3;
+  tc::split_tf32(v.x, h0, l0);
+  tc::split_tf32(v.y, h1, l1);
+  tc::split_tf32(v.z, h2, l2);
+  tc::split_tf32(v.w, h3, l3);
+  st_shared_v4(hi_addr, __float_as_uint(h0), __float_as_uint(h1), __float_as_uint(h2), __float_as_uint(h3));
+  if (split)
+    st_shared_v4(lo_addr, __float_as_uint(l0), __float_as_uint(l1), __float_as_uint(l2), __float_as_uint(l3));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+__device__ __forceinline__ void st_split_bf16(uint32_t hi_addr, uint32_t lo_addr, float4 u, float4 v) {
+  uint32_t l0, l1, l2, l3;
+  const uint32_t h0 = pack_bf16(u.x, u.y, l0);
+  const uint32_t h1 = pack_bf16(u.z, u.w, l1);
+  const uint32_t h2 = pack_bf16(v.x, v.y, l2);
+  const uint32_t h3 = pack_bf16(v.z, v.w, l3);
+  st_shared_v4(hi_addr, h0, h1, h2, h3);
+  st_shared_v4(lo_addr, l0, l1, l2, l3);
+}
+
+// The 128-byte slice [k0, k0 + KC) of this thread's four A rows and four M rows.  Job
+// e = ptid + 256 q covers row e / 8, 16-byte shared-memory chunk e % 8; a chunk is one
+// float4 (two complex values) for TF32 and two float4 (four complex values) for BF16.
+template <bool BF16>
+__device__ __forceinline__ void tc_load_stage(float4 (&v)[BF16 ? 16 : 8], const float2* __restrict__ A,
+                                              const float2* __restrict__ M, int n, int row0, int col0, int k0,
+                                              int ptid) {
+  constexpr int PER = BF16 ? 2 : 1;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int e = ptid + tcg::kProd * q;
+    const int r = e >> 3, cc = e & 7;
+    const int gr = row0 + r, gj = col0 + r;
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int k = k0 + (cc * PER + p) * 2;  // n is even, so a float4 is all in or all out
+      v[q * PER + p] = (gr < n && k < n) ? __ldg(reinterpret_cast<const float4*>(A + (long long)gr * n + k))
+                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+      v[4 * PER + q * PER + p] = (gj < n && k < n)
+                                     ? __ldg(reinterpret_cast<const float4*>(M + (long long)gj * n + k))
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+}
+
+template <bool BF16, bool SPLIT>
+__device__ __forceinline__ void tc_store_stage(const float4 (&v)[BF16 ? 16 : 8], uint32_t st, int ptid) {
+  const uint32_t Ahi = st, Alo = st + tcg::kA, Bhi = st + 2 * tcg::kA, Blo = st + 2 * tcg::kA + tcg::kB;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int e = ptid + tcg::kProd * q;
+    const uint32_t r = e >> 3, cc = e & 7;
+    const uint32_t oa = r * 128 + ((cc ^ (r & 7)) << 4);
+    const uint32_t r0 = 2 * r, r1 = 2 * r + 1;
+    const uint32_t ob0 = r0 * 128 + ((cc ^ (r0 & 7)) << 4);
+    const uint32_t ob1 = r1 * 128 + ((cc ^ (r1 & 7)) << 4);
+    if (!BF16) {
+      const float4 a = v[q], m = v[4 + q];
+      st_split_tf32(Ahi + oa, Alo + oa, a, SPLIT);
+      st_split_tf32(Bhi + ob0, Blo + ob0, m, SPLIT);
+      st_split_tf32(Bhi + ob1, Blo + ob1, make_float4(-m.y, m.x, -m.w, m.z), SPLIT);
+    } else {
+      const float4 a0 = v[2 * q], a1 = v[2 * q + 1], m0 = v[8 + 2 * q], m1 = v[8 + 2 * q + 1];
+      st_split_bf16(Ahi + oa, Alo + oa, a0, a1);
+      st_split_bf16(Bhi + ob0, Blo + ob0, m0, m1);
+      st_split_bf16(Bhi + ob1, Blo + ob1, make_float4(-m0.y, m0.x, -m0.w, m0.z),
+                    make_float4(-m1.y, m1.x, -m1.w, m1.z));
+    }
+  }
+}
+
+// grid (tiles128^2, 1, B * Kz), kThreads threads, kSmem dynamic shared bytes.  Same job
+// semantics as cgemm_kernel, restricted to terms A M^+ (opA = 0; opB = 1, or B = the
+// hermitian stage input) with one alpha; on a wait that runs out the tile is written as
+// NaN, which the error norm turns into DQB_INST_NONFINITE.
+template <int PREC>
+__global__ void __launch_bounds__(tcg::kThreads, 1)
+    tc_cgemm_kernel(big::Common c, LargeOps d, GemmJob job, const float2* ext_in, float2* ext_out) {
+  constexpr bool kBf16 = PREC == DQB_PREC_BF16X3;
+  constexpr bool kSplit = PREC != DQB_PREC_TF32;
+  constexpr int KC = kBf16 ? 32 : 16;  // complex contraction values per stage
+  constexpr int NV = kBf16 ? 16 : 8;
+  constexpr uint32_t kCols = kSplit ? 2 * tcg::kAccCols : tcg::kAccCols;
+  extern __shared__ uint8_t tc_dsm[];
+  __shared__ uint64_t bars[2 * tcg::kStages + 1];
+  __shared__ uint32_t tmem_sh;
+  __shared__ int fail_sh;
+
+  const int n = d.n;
+  const int Kz = job.kdst < 0 ? d.K : 1;
+  const int b = blockIdx.z / Kz;
+  const int kz = job.kdst < 0 ? (int)(blockIdx.z % Kz) : job.kdst;
+  if (job.need_run != 2) {
+    const big::Inst& I = c.inst[b];
+    if (job.need_run == 1 ? !I.run : I.status != DQB_INST_OK) return;
+  }
+  const int Kb = jumps_of(d, b);
+  if (job.kdst < 0 && kz >= Kb) return;
+  const int tiles = (n + 127) >> 7;
+  const int row0 = (blockIdx.x / tiles) * 128, col0 = (blockIdx.x % tiles) * 128;
+
+  const float2* Ap[4];
+  const float2* Mp[4];
+  int nt = 0;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    if (t >= job.nterms) break;
+    const Term T = job.t[t];
+    if ((T.srcA == SRC_T || T.srcA == SRC_L) && T.kA >= Kb) continue;  // missing jump
+    Ap[nt] = src_ptr(c, d, b, T.srcA, T.kA < 0 ? kz : T.kA, job.in_sel, ext_in);
+    Mp[nt] = src_ptr(c, d, b, T.srcB, T.kB < 0 ? kz : T.kB, job.in_sel, ext_in);
+    ++nt;
+  }
+  const int kchunks = (n + KC - 1) / KC;
+  const int total = nt * kchunks;
+
+  const uint32_t raw = tc::smem_u32(tc_dsm);
+  const uint32_t sbase = (raw + 1023u) & ~1023u;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t bar_full = tc::smem_u32(&bars[0]);
+  const uint32_t bar_empty = tc::smem_u32(&bars[tcg::kStages]);
+  const uint32_t bar_done = tc::smem_u32(&bars[2 * tcg::kStages]);
+  if (warp == tcg::kProdWarps) {
+    tc::tmem_alloc(tc::smem_u32(&tmem_sh), kCols);
+    tc::tmem_relinquish();
+    if (lane == 0) {
+      for (int s = 0; s < tcg::kStages; ++s) {
+        tc::mbar_init(bar_full + 8 * s, tcg::kProd);
+        tc::mbar_init(bar_empty + 8 * s, 1);
+      }
+      tc::mbar_init(bar_done, 1);
+      tc::fence_mbar_init();
+      fail_sh = 0;
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = tmem_sh;
+
+  if (warp < tcg::kProdWarps) {
+    // ---- producers ----
+    const int ptid = threadIdx.x;
+    float4 cur[NV], nxt[NV];
+    if (total > 0) tc_load_stage<kBf16>(cur, Ap[0], Mp[0], n, row0, col0, 0, ptid);
+    for (int it = 0; it < total; ++it) {
+      const int s = it % tcg::kStages;
+      if (it + 1 < total) {
+        const int term = (it + 1) / kchunks;
+        tc_load_stage<kBf16>(nxt, Ap[term], Mp[term], n, row0, col0, ((it + 1) % kchunks) * KC, ptid);
+      }
+      if (it >= tcg::kStages && !tc::mbar_wait(bar_empty + 8 * s, ((it / tcg::kStages) - 1) & 1)) {
+        fail_sh = 1;
+        break;
+      }
+      tc_store_stage<kBf16, kSplit>(cur, sbase + s * tcg::kStage, ptid);
+      tc::fence_proxy_async_smem();
+      tc::mbar_arrive(bar_full + 8 * s);
+#pragma unroll
+      for (int i = 0; i < NV; ++i) cur[i] = nxt[i];
+    }
+  } else if (lane == 0) {
+    // ---- MMA issuer ----
+    constexpr uint32_t idesc = tc::instr_desc(kBf16 ? 1u : 2u, 128, 256);
+    for (int it = 0; it < total; ++it) {
+      const int s = it % tcg::kStages;
+      if (!tc::mbar_wait(bar_full + 8 * s, (it / tcg::kStages) & 1)) {
+        fail_sh = 1;
+        break;
+      }
+      tc::tc_fence_after();
+      const uint32_t st = sbase + s * tcg::kStage;
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        const uint64_t ah = tc::smem_desc_k128(st + kk * 32);
+        const uint64_t al = tc::smem_desc_k128(st + tcg::kA + kk * 32);
+        const uint64_t bh = tc::smem_desc_k128(st + 2 * tcg::kA + kk * 32);
+        const uint64_t bl = tc::smem_desc_k128(st + 2 * tcg::kA + tcg::kB + kk * 32);
+        const uint32_t acc = (it | kk) ? 1u : 0u;
+        const uint32_t small = tmem + tcg::kAccCols;
+        if (kBf16) {
+          tc::mma_bf16(small, al, bh, idesc, acc);
+          tc::mma_bf16(small, ah, bl, idesc, 1u);
+          tc::mma_bf16(tmem, ah, bh, idesc, acc);
+        } else if (kSplit) {
+          tc::mma_tf32(small, al, bh, idesc, acc);
+          tc::mma_tf32(small, ah, bl, idesc, 1u);
+          tc::mma_tf32(tmem, ah, bh, idesc, acc);
+        } else {
+          tc::mma_tf32(tmem, ah, bh, idesc, acc);
+        }
+      }
+      tc::mma_commit(bar_empty + 8 * s);
+    }
+    tc::mma_commit(bar_done);
+  }
+
+  if (warp < tcg::kProdWarps) {
+    // ---- epilogue: TMEM -> registers -> C ----
+    __syncwarp();
+    bool got = tc::mbar_wait(bar_done, 0);
+    got = __all_sync(0xffffffffu, got);
+    tc::tc_fence_after();
+    const bool bad = __any_sync(0xffffffffu, !got || fail_sh != 0);
+    const int q = warp & 3, h = warp >> 2;
+    const int r = row0 + 32 * q + lane;
+    float2* C;
+    if (ext_out) {
+      C = ext_out + (long long)b * n * n;
+    } else if (job.dst == SRC_T) {
+      C = d.T + ((long long)b * d.K + kz) * (long long)n * n;
+    } else {
+      C = d.tmp + (long long)b * n * n;
+    }
+    const float alpha = job.t[0].alpha;
+#pragma unroll 1
+    for (int ch = 0; ch < 8; ++ch) {
+      const int fcol = h * 128 + ch * 16;
+      float v[16];
+      __syncwarp();
+      if (!bad && total > 0) {
+        const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)fcol;
+        tc::tmem_ld16(ta, v);
+        if (kSplit) {
+          float w[16];
+          tc::tmem_ld16(ta + tcg::kAccCols, w);
+          tc::tmem_ld_wait();
+#pragma unroll
+          for (int i = 0; i < 16; ++i) v[i] += w[i];
+        } else {
+          tc::tmem_ld_wait();
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = bad ? __int_as_float(0x7fc00000) : 0.f;
+      }
+      const int cc0 = col0 + (fcol >> 1);
+      if (r >= n || cc0 >= n) continue;
+      float2* row = C + (long long)r * n + cc0;
+      if (cc0 + 8 <= n) {
+#pragma unroll
+        for (int j = 0; j < 8; j += 2) {
+          float4 o = make_float4(alpha * v[2 * j], alpha * v[2 * j + 1], alpha * v[2 * j + 2], alpha * v[2 * j + 3]);
+          if (job.accumulate) {
+            const float4 p = *reinterpret_cast<const float4*>(row + j);
+            o.x += p.x;
+            o.y += p.y;
+            o.z += p.z;
+            o.w += p.w;
+          }
+          *reinterpret_cast<float4*>(row + j) = o;
+        }
+      } else {
+        for (int j = 0; j < 8 && cc0 + j < n; ++j) {
+          float2 o = make_float2(alpha * v[2 * j], alpha * v[2 * j + 1]);
+          if (job.accumulate) o = cadd(o, row[j]);
+          row[j] = o;
+        }
+      }
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == tcg::kProdWarps) {
+    __syncwarp();
+    tc::tmem_dealloc(tmem, kCols);
+  }
+}
+
+// The GEMM path's products run on the tensor cores when a precision other than FP32 is
+// asked for, the form is hermitian (every product is then A M^+) and n is even (float4
+// rows).
+bool use_tc(const LargeOps& d, int form) {
+  return d.prec != DQB_PREC_FP32 && form == DQB_FORM_HERMITIAN && (d.n % 2) == 0;
+}
+
+void launch_gemm(cudaStream_t s, const big::Common& c, const LargeOps& d, const GemmJob& j, int zdim,
+                 const float2* ext_in, float2* ext_out, bool tcp) {
+  if (tcp) {
+    const int t = (d.n + 127) / 128;
+    const dim3 g(t * t, 1, zdim);
+    switch (d.prec) {
+      case DQB_PREC_TF32X3:
+        tc_cgemm_kernel<DQB_PREC_TF32X3><<<g, tcg::kThreads, tcg::kSmem, s>>>(c, d, j, ext_in, ext_out);
+        break;
+      case DQB_PREC_BF16X3:
+        tc_cgemm_kernel<DQB_PREC_BF16X3><<<g, tcg::kThreads, tcg::kSmem, s>>>(c, d, j, ext_in, ext_out);
+        break;
+      default:
+        tc_cgemm_kernel<DQB_PREC_TF32><<<g, tcg::kThreads, tcg::kSmem, s>>>(c, d, j, ext_in, ext_out);
+        break;
+    }
+  } else {
+    const int t = (d.n + BM - 1) / BM;
+    cgemm_kernel<<<dim3(t * t, 1, zdim), NT, 0, s>>>(c, d, j, ext_in, ext_out);
+  }
+}
+
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct LargeLayout {
@@ -312,7 +663,7 @@ LargeLayout large_layout(int n, int K, int nE, int ntsave, long long B) {
 void launch_rhs(cudaStream_t s, const big::Common& c, const LargeOps& d, int B, int in_sel, int out_k,
                 int need_run, int form, const float2* ext_in, float2* ext_out) {
   const int n = d.n;
-  const int tiles = (n + BM - 1) / BM;
+  const bool tcp = use_tc(d, form);
   const float sc = form == DQB_FORM_HERMITIAN ? 0.5f : 1.0f;
   if (d.K > 0) {
     GemmJob j1;
@@ -323,7 +674,7 @@ void launch_rhs(cudaStream_t s, const big::Common& c, const LargeOps& d, int B, 
     j1.kdst = -1;
     j1.in_sel = in_sel;
     j1.need_run = need_run;
-    cgemm_kernel<<<dim3(tiles * tiles, 1, B * d.K), NT, 0, s>>>(c, d, j1, ext_in, nullptr);
+    launch_gemm(s, c, d, j1, B * d.K, ext_in, nullptr, tcp);
   }
   // tmp = Hnh X + sum_k T_k L_k^+ [+ X Hnh^+]: at most 4 summed terms per launch, the
   // rest accumulated by further launches into tmp
@@ -340,7 +691,7 @@ void launch_rhs(cudaStream_t s, const big::Common& c, const LargeOps& d, int B, 
   for (;;) {
     while (k < d.K && nt < 4) j2.t[nt++] = Term{SRC_T, k, 0, SRC_L, k, 1, 1.0f}, ++k;
     j2.nterms = nt;
-    cgemm_kernel<<<dim3(tiles * tiles, 1, B), NT, 0, s>>>(c, d, j2, ext_in, nullptr);
+    launch_gemm(s, c, d, j2, B, ext_in, nullptr, tcp);
     if (k >= d.K) break;
     j2.accumulate = 1;
     nt = 0;
@@ -356,6 +707,12 @@ int check_dense_large(const dqb_dense_problem* p) {
   if (p->batch > 65535 / std::max(1, p->n_jumps)) return DQB_ERR_UNSUPPORTED;
   if (!p->H || (p->n_jumps > 0 && !p->L)) return DQB_ERR_INVALID_ARGUMENT;
   if (p->n_jumps > 16) return DQB_ERR_UNSUPPORTED;
+  return DQB_OK;
+}
+
+int check_precision(int prec, int form, int n) {
+  if (prec < DQB_PREC_FP32 || prec > DQB_PREC_TF32) return DQB_ERR_INVALID_ARGUMENT;
+  if (prec != DQB_PREC_FP32 && (form != DQB_FORM_HERMITIAN || n % 2 != 0)) return DQB_ERR_UNSUPPORTED;
   return DQB_OK;
 }
 
@@ -424,6 +781,12 @@ static void init_carveouts() {
     prefer_max_shared(zero_words_kernel);
     prefer_max_shared(cgemm_kernel);
     prefer_max_shared(symmetrize_kernel);
+    prefer_max_shared(tc_cgemm_kernel<DQB_PREC_TF32X3>);
+    prefer_max_shared(tc_cgemm_kernel<DQB_PREC_BF16X3>);
+    prefer_max_shared(tc_cgemm_kernel<DQB_PREC_TF32>);
+    cudaFuncSetAttribute(tc_cgemm_kernel<DQB_PREC_TF32X3>, cudaFuncAttributeMaxDynamicSharedMemorySize, tcg::kSmem);
+    cudaFuncSetAttribute(tc_cgemm_kernel<DQB_PREC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize, tcg::kSmem);
+    cudaFuncSetAttribute(tc_cgemm_kernel<DQB_PREC_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, tcg::kSmem);
   });
 }
 
@@ -490,14 +853,23 @@ extern "C" size_t dqb_mesolve_dense_large_workspace_size(int32_t n, int32_t n_ju
 
 extern "C" int dqb_lindblad_rhs_dense_large(const dqb_dense_problem* p, int32_t form, const void* rho, void* outp,
                                             void* workspace, size_t workspace_bytes, void* stream) {
+  return dqb_lindblad_rhs_dense_large_prec(p, form, DQB_PREC_FP32, rho, outp, workspace, workspace_bytes, stream);
+}
+
+extern "C" int dqb_lindblad_rhs_dense_large_prec(const dqb_dense_problem* p, int32_t form, int32_t precision,
+                                                 const void* rho, void* outp, void* workspace,
+                                                 size_t workspace_bytes, void* stream) {
   int rc = check_dense_large(p);
   if (rc) return rc;
   if (!rho || !outp) return DQB_ERR_INVALID_ARGUMENT;
   if (form != DQB_FORM_HERMITIAN && form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
+  rc = check_precision(precision, form, p->n);
+  if (rc) return rc;
   if (p->batch == 0) return DQB_OK;
   const LargeLayout lay = large_layout(p->n, p->n_jumps, 0, 1, p->batch);
   if (!workspace || workspace_bytes < lay.off_mats) return DQB_ERR_WORKSPACE_TOO_SMALL;
   LargeOps d = make_ops(p, (char*)workspace, lay);
+  d.prec = precision;
   big::Common c;
   std::memset(&c, 0, sizeof(c));
   cudaStream_t s = (cudaStream_t)stream;
@@ -522,6 +894,7 @@ extern "C" int dqb_mesolve_dense_large_ragged(const dqb_ragged_instance* instanc
   if (o->method != DQB_METHOD_TSIT5 && o->method != DQB_METHOD_DOPRI5) return DQB_ERR_INVALID_ARGUMENT;
   if (o->form != DQB_FORM_HERMITIAN && o->form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
   if (!(o->rtol >= 0) || !(o->atol >= 0) || o->max_steps < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if (int prc = check_precision(o->precision, o->form, n)) return prc;
   if (count == 0) return DQB_OK;
   if (!instances) return DQB_ERR_INVALID_ARGUMENT;
   const LargeLayout lay = large_layout(n, max_jumps, max_exp, max_tsave, count);
@@ -534,6 +907,7 @@ extern "C" int dqb_mesolve_dense_large_ragged(const dqb_ragged_instance* instanc
   p.batch = count;
   LargeOps d = make_ops(&p, ws, lay);
   d.rag = instances;
+  d.prec = o->precision;
   big::Common c;
   std::memset(&c, 0, sizeof(c));
   c.n = n;
@@ -562,11 +936,13 @@ extern "C" int dqb_mesolve_dense_large(const dqb_dense_problem* p, const dqb_ode
   if (o->method != DQB_METHOD_TSIT5 && o->method != DQB_METHOD_DOPRI5) return DQB_ERR_INVALID_ARGUMENT;
   if (o->form != DQB_FORM_HERMITIAN && o->form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
   if (!(o->rtol >= 0) || !(o->atol >= 0) || o->max_steps < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if (int prc = check_precision(o->precision, o->form, p->n)) return prc;
   if (p->batch == 0) return DQB_OK;
   const LargeLayout lay = large_layout(p->n, p->n_jumps, p->n_exp, p->n_tsave, p->batch);
   if (!workspace || workspace_bytes < lay.total) return DQB_ERR_WORKSPACE_TOO_SMALL;
   char* ws = (char*)workspace;
   LargeOps d = make_ops(p, ws, lay);
+  d.prec = o->precision;
 
   big::Common c;
   std::memset(&c, 0, sizeof(c));

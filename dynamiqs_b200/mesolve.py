@@ -266,6 +266,19 @@ class PreparedSolve:
                                        b['infos'], b['status'])
 
 
+def _precision_code(o, form: int) -> int:
+    """DQB_PREC_* for ``Options.precision``; the tensor-core modes need the hermitian form."""
+    try:
+        code = _lib.PRECISIONS[o.precision]
+    except KeyError:
+        raise ValueError(f'Option `precision` must be one of {sorted(_lib.PRECISIONS)}, '
+                         f'got {o.precision!r}.') from None
+    if code != _lib.PREC_FP32 and form != _lib.FORM_HERMITIAN:
+        raise ValueError('Option `precision` other than "fp32" needs the hermitian form '
+                         '(assume_hermitian=True, vectorized=False).')
+    return code
+
+
 class MESolveB200Integrator:
     """Registry-compatible integrator: ``constructor(ts=, y0=, method=, gradient=,
     options=, H=, Ls=, Es=)`` then ``.run() -> MESolveResult``
@@ -296,7 +309,7 @@ class MESolveB200Integrator:
             form=form, rtol=float(m.rtol), atol=float(m.atol), safety=float(m.safety_factor),
             factormin=float(m.min_factor), factormax=float(m.max_factor),
             max_steps=int(m.max_steps), t0=self.t0, save_states=int(bool(o.save_states)),
-            check_hermitian=int(bool(o.assume_hermitian)))
+            check_hermitian=int(bool(o.assume_hermitian)), precision=_precision_code(o, form))
 
     def run(self) -> MESolveResult:
         return self.prepare().launch().result()

@@ -19,6 +19,11 @@ class Options:
     nmaxclick: int = 10_000
     vectorized: bool = False
     assume_hermitian: bool = True
+    # Arithmetic of the complex products on the dense GEMM path (n > 64): 'fp32' (CUDA
+    # cores, default), 'tf32x3' or 'bf16x3' (tcgen05 tensor cores on hi + lo operand
+    # splits, FP32 accumulation), 'tf32' (one TF32 pass, ~1e-3: error studies only).
+    # An addition of this library; the n <= 64 and sparse-DIA kernels always run FP32.
+    precision: str = 'fp32'
 
     def initialise(self) -> Options:
         return self
@@ -26,7 +31,7 @@ class Options:
 
 _SUPPORTED = {
     'mesolve': ('save_states', 'cartesian_batching', 'progress_meter', 't0', 'save_extra',
-                'vectorized', 'assume_hermitian'),
+                'vectorized', 'assume_hermitian', 'precision'),
 }
 
 

@@ -55,6 +55,16 @@ extern "C" {
 #define DQB_FORM_HERMITIAN 0 /* tmp = Hnh rho + 1/2 sum L rho L^+ ; out = tmp + tmp^+ */
 #define DQB_FORM_STANDARD 1  /* Hnh rho + rho Hnh^+ + sum L rho L^+                 */
 
+/* Arithmetic of the GEMM path's complex products (dqb_mesolve_dense_large and its ragged
+ * and right-hand-side entry points; the n <= 64 and DIA kernels always use FP32 CUDA
+ * cores).  The tensor-core modes run tcgen05 MMAs with FP32 accumulation in tensor
+ * memory, on each operand split into hi + lo parts (three products hi*hi + hi*lo + lo*hi);
+ * they need the hermitian form and an even n (else DQB_ERR_UNSUPPORTED). */
+#define DQB_PREC_FP32 0    /* FP32 FMA on CUDA cores (default)                         */
+#define DQB_PREC_TF32X3 1  /* 3 x TF32 tensor-core products, ~2^-21 relative per product */
+#define DQB_PREC_BF16X3 2  /* 3 x BF16 tensor-core products, ~2^-17 relative per product */
+#define DQB_PREC_TF32 3    /* 1 x TF32 (hi*hi only), ~2^-11: for error studies          */
+
 /* Mirrors dq.method.Tsit5 / Dopri5 (dynamiqs/method.py:121-127,356-476) and the
  * mesolve options that reach the integrator (dynamiqs/options.py:17-77). */
 typedef struct dqb_ode_options {
@@ -69,6 +79,7 @@ typedef struct dqb_ode_options {
   double t0;               /* start time: tsave[0] unless options.t0 is set             */
   int32_t save_states;     /* 1: state at every tsave; 0: final state only              */
   int32_t check_hermitian; /* 1: flag rho0 that fails isherm(rtol=atol=1e-5)            */
+  int32_t precision;       /* DQB_PREC_* (GEMM path only; 0 = FP32)                     */
 } dqb_ode_options;
 
 /* Outputs of a batched solve.  nsave = n_tsave if save_states else 1. */
@@ -191,6 +202,14 @@ DQB_API int dqb_mesolve_dense_large(const dqb_dense_problem* problem, const dqb_
 DQB_API int dqb_lindblad_rhs_dense_large(const dqb_dense_problem* problem, int32_t form,
                                          const void* rho, void* out, void* workspace,
                                          size_t workspace_bytes, void* stream);
+
+/* Same, with the products in `precision` (DQB_PREC_*).  The tensor-core modes read rho as
+ * hermitian (they use rho^+ in place of rho), as every stage input of the hermitian form
+ * is. */
+DQB_API int dqb_lindblad_rhs_dense_large_prec(const dqb_dense_problem* problem, int32_t form,
+                                              int32_t precision, const void* rho, void* out,
+                                              void* workspace, size_t workspace_bytes,
+                                              void* stream);
 
 /* Ragged batch for the GEMM path: every instance has this n (the caller guarantees it),
  * its own jump count (<= max_jumps), exp_ops (<= max_exp), tsave grid (<= max_tsave

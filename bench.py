@@ -191,10 +191,16 @@ def run_serving(args):
     reqs = workloads.serving_requests(N, rate=2000.0, seed=args.seed)
     warm = workloads.serving_requests(24, rate=2000.0, seed=args.seed + 999)
     srv = MESolveServer(n_streams=args.streams)
-    srv.warmup()
+
+    def opts_of(r):  # GEMM-path arithmetic for n > 64; the n <= 64 kernel is FP32
+        return dq.Options(precision=args.precision if r['n'] > 64 else 'fp32')
+
+    # every large-path graph the stream will use is captured here, before the clock starts
+    srv.warmup(method=reqs[0]['method'], options=dq.Options(precision=args.precision))
+
     for r in warm:
         srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'], exp_ops=r['exp_ops'],
-                   method=r['method'])
+                   method=r['method'], options=opts_of(r))
     while len(srv.finished) < len(warm):
         time.sleep(0.01)
     for t in srv.finished:
@@ -212,14 +218,17 @@ def run_serving(args):
             if delay > 0:
                 time.sleep(delay)
             tickets.append(srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'],
-                                      exp_ops=r['exp_ops'], method=r['method']))
+                                      exp_ops=r['exp_ops'], method=r['method'],
+                                      options=opts_of(r)))
 
     th = threading.Thread(target=feed)
     th.start()
     th.join()
     for t in tickets:
-        t.result()
+        t._event.wait()
     srv.close()
+    failed = [t for t in tickets if t._error is not None]
+    tickets = [t for t in tickets if t._error is None]
     nsteps_of = {t.id: int(t.result().infos.nsteps) for t in tickets}
     for t in tickets:
         t.release()
@@ -242,7 +251,7 @@ def run_serving(args):
         for r in sample:
             a = time.perf_counter()
             res = dq.mesolve(r['H'], r['jump_ops'], r['rho0'], r['tsave'], exp_ops=r['exp_ops'],
-                             method=r['method'])
+                             method=r['method'], options=opts_of(r))
             res.infos.nsteps.cpu()
             lat.append(time.perf_counter() - a)
         tot = time.perf_counter() - t0
@@ -251,18 +260,24 @@ def run_serving(args):
                  'p50_latency_ms': 1e3 * float(np.percentile(lat, 50)),
                  'p99_latency_ms': 1e3 * float(np.percentile(lat, 99)),
                  'served_over_plain': st['solves_per_s'] / (len(sample) / tot)}
-    by_n = {}
+    by_n, steps_n = {}, {}
     for t in tickets:
         by_n.setdefault(t.n, []).append(1e3 * t.latency)
+        steps_n.setdefault(t.n, []).append(nsteps_of[t.id])
     per_size = {str(n): {'count': len(v), 'p50_ms': float(np.percentile(v, 50)),
-                         'p99_ms': float(np.percentile(v, 99))} for n, v in sorted(by_n.items())}
+                         'p99_ms': float(np.percentile(v, 99)),
+                         'mean_rk_steps': float(np.mean(steps_n[n])),
+                         'max_rk_steps': int(np.max(steps_n[n]))}
+                for n, v in sorted(by_n.items())}
     line = {
         'metric': METRIC, 'value': st['solves_per_s'], 'unit': 'solves/s', 'n_gpus': 1,
         'steps': 1, 'warmup': 1, 'ms_per_step': 1e3 * st['makespan_s'], 'higher_is_better': True,
         'scaling': 'weak', 'vs_baseline': None, 'dtype': 'c64',
         'data': 'synthetic (seeded Poisson arrivals and Kerr problems)',
         'config': {'workload': CASES['serving'], 'requests': N, 'streams': args.streams,
+                   'precision_n_gt_64': args.precision,
                    'waves': st['waves'], 'errors': st['errors'],
+                   'error_kinds': sorted({f'n={t.n}: {t._error}' for t in failed})[:5],
                    'max_launch_s': max((x[2] for x in srv.launch_seconds), default=0.0),
                    'slow_launches': [(str(k), c, round(sec, 3)) for k, c, sec in srv.launch_seconds
                                      if sec > 0.5][:10],

@@ -416,8 +416,9 @@ static __global__ void save_kernel(Common c, int interp) {
   }
 }
 
-// One block: per-instance commit, then the WHILE-node condition.
-static __global__ void commit_kernel(Common c, cudaGraphConditionalHandle handle) {
+// One block: per-instance commit, then the WHILE-node condition (or, when the loop is
+// driven from the host, the same condition written to `flag`).
+static __global__ void commit_kernel(Common c, cudaGraphConditionalHandle handle, int* flag) {
   int any = 0;
   for (int b = threadIdx.x; b < c.B; b += blockDim.x) {
     Inst& I = c.inst[b];
@@ -443,7 +444,10 @@ static __global__ void commit_kernel(Common c, cudaGraphConditionalHandle handle
   if (threadIdx.x == 0) {
     const long long it = ++(*c.iter);
     const bool more = any && it < c.o.max_steps + 2;
-    cudaGraphSetConditional(handle, more ? 1u : 0u);
+    if (flag)
+      *flag = more ? 1 : 0;
+    else
+      cudaGraphSetConditional(handle, more ? 1u : 0u);
   }
 }
 

@@ -812,31 +812,35 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s) {
   big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 1);
   if (cudaGetLastError() != cudaSuccess) return DQB_ERR_CUDA;
 
-  LaunchKey key;
-  std::memset(&key, 0, sizeof(key));
-  key.c = c;
-  key.d = d;
-  key.form = form;
-  cudaGraphExec_t exec = g_cache.find(&key, sizeof(key));
-  if (!exec) {
-    auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
-      for (int st = 0; st < 5; ++st) {
-        big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
-        launch_rhs(cs, c, d, B, 2, st + 1, 1, form, nullptr, nullptr);
-      }
-      big::combine_kernel<<<ge, T, 0, cs>>>(c, 5);
-      launch_rhs(cs, c, d, B, 1, 6, 1, form, nullptr, nullptr);
-      big::error_kernel<<<ge, T, 0, cs>>>(c);
-      big::control_kernel<<<gi, 128, 0, cs>>>(c);
-      big::save_kernel<<<ge, T, 0, cs>>>(c, 1);
-      big::commit_kernel<<<1, 1024, 0, cs>>>(c, h);
-    };
-    if (build_while_graph(body, &exec) != cudaSuccess) return DQB_ERR_CUDA;
-    g_cache.insert(&key, sizeof(key), exec, s);
+  auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h, int* flag) {
+    for (int st = 0; st < 5; ++st) {
+      big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
+      launch_rhs(cs, c, d, B, 2, st + 1, 1, form, nullptr, nullptr);
+    }
+    big::combine_kernel<<<ge, T, 0, cs>>>(c, 5);
+    launch_rhs(cs, c, d, B, 1, 6, 1, form, nullptr, nullptr);
+    big::error_kernel<<<ge, T, 0, cs>>>(c);
+    big::control_kernel<<<gi, 128, 0, cs>>>(c);
+    big::save_kernel<<<ge, T, 0, cs>>>(c, 1);
+    big::commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
+  };
+  if (host_loop_requested()) {
+    if (run_host_loop(body, (int*)(c.iter + 1), s) != cudaSuccess) return DQB_ERR_CUDA;
   } else {
-    g_cache.touch(&key, sizeof(key), s);
+    LaunchKey key;
+    std::memset(&key, 0, sizeof(key));
+    key.c = c;
+    key.d = d;
+    key.form = form;
+    cudaGraphExec_t exec = g_cache.find(&key, sizeof(key));
+    if (!exec) {
+      if (build_while_graph(body, &exec) != cudaSuccess) return DQB_ERR_CUDA;
+      g_cache.insert(&key, sizeof(key), exec, s);
+    } else {
+      g_cache.touch(&key, sizeof(key), s);
+    }
+    if (cudaGraphLaunch(exec, s) != cudaSuccess) return DQB_ERR_CUDA;
   }
-  if (cudaGraphLaunch(exec, s) != cudaSuccess) return DQB_ERR_CUDA;
   big::pre_finalize_kernel<<<gi, 128, 0, s>>>(c);
   big::save_kernel<<<ge, T, 0, s>>>(c, 0);
   big::finalize_kernel<<<ge, T, 0, s>>>(c);

@@ -363,33 +363,37 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   if (cudaGetLastError() != cudaSuccess) return DQB_ERR_CUDA;
 
   // ---- the RK loop: graph with a WHILE node ------------------------------------------
-  LaunchKey key;
-  std::memset(&key, 0, sizeof(key));
-  key.c = c;
-  key.d = d;
-  key.grid_e = grid_e;
-  key.grid_r_x = gr.x;
-  key.grid_r_y = gr.y;
-  cudaGraphExec_t exec = g_cache.find(&key, sizeof(key));
-  if (!exec) {
-    auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
-      for (int st = 0; st < 5; ++st) {
-        big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
-        rhs_dia_kernel<<<gr, kRhsCols, 0, cs>>>(c, d, 2, st + 1, 1, nullptr, nullptr);
-      }
-      big::combine_kernel<<<ge, T, 0, cs>>>(c, 5);
-      rhs_dia_kernel<<<gr, kRhsCols, 0, cs>>>(c, d, 1, 6, 1, nullptr, nullptr);
-      big::error_kernel<<<ge, T, 0, cs>>>(c);
-      big::control_kernel<<<gi, 128, 0, cs>>>(c);
-      big::save_kernel<<<ge, T, 0, cs>>>(c, 1);
-      big::commit_kernel<<<1, 1024, 0, cs>>>(c, h);
-    };
-    if (build_while_graph(body, &exec) != cudaSuccess) return DQB_ERR_CUDA;
-    g_cache.insert(&key, sizeof(key), exec, s);
+  auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h, int* flag) {
+    for (int st = 0; st < 5; ++st) {
+      big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
+      rhs_dia_kernel<<<gr, kRhsCols, 0, cs>>>(c, d, 2, st + 1, 1, nullptr, nullptr);
+    }
+    big::combine_kernel<<<ge, T, 0, cs>>>(c, 5);
+    rhs_dia_kernel<<<gr, kRhsCols, 0, cs>>>(c, d, 1, 6, 1, nullptr, nullptr);
+    big::error_kernel<<<ge, T, 0, cs>>>(c);
+    big::control_kernel<<<gi, 128, 0, cs>>>(c);
+    big::save_kernel<<<ge, T, 0, cs>>>(c, 1);
+    big::commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
+  };
+  if (host_loop_requested()) {
+    if (run_host_loop(body, (int*)(c.iter + 1), s) != cudaSuccess) return DQB_ERR_CUDA;
   } else {
-    g_cache.touch(&key, sizeof(key), s);
+    LaunchKey key;
+    std::memset(&key, 0, sizeof(key));
+    key.c = c;
+    key.d = d;
+    key.grid_e = grid_e;
+    key.grid_r_x = gr.x;
+    key.grid_r_y = gr.y;
+    cudaGraphExec_t exec = g_cache.find(&key, sizeof(key));
+    if (!exec) {
+      if (build_while_graph(body, &exec) != cudaSuccess) return DQB_ERR_CUDA;
+      g_cache.insert(&key, sizeof(key), exec, s);
+    } else {
+      g_cache.touch(&key, sizeof(key), s);
+    }
+    if (cudaGraphLaunch(exec, s) != cudaSuccess) return DQB_ERR_CUDA;
   }
-  if (cudaGraphLaunch(exec, s) != cudaSuccess) return DQB_ERR_CUDA;
 
   // ---- leftovers and outputs -----------------------------------------------------------
   big::pre_finalize_kernel<<<gi, 128, 0, s>>>(c);

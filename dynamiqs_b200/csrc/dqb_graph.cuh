@@ -2,6 +2,8 @@
 // RK loop as a device-side WHILE node, and a small cache of its executables.
 #pragma once
 
+#include <cstdlib>
+
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -82,8 +84,35 @@ class GraphCache {
   std::vector<Parked> parked_;
 };
 
-// Build "WHILE (cond) { body }" where `body(stream, handle)` enqueues one loop iteration
-// on the capture stream and must end with a kernel that sets the condition.
+// DQB_HOST_LOOP=1 in the environment (read once): run the RK loop from the host, one
+// iteration per round trip, instead of as a graph WHILE node.  Same kernels, same
+// results; it exists for profilers that cannot see kernels inside conditional graphs.
+inline bool host_loop_requested() {
+  static const bool on = [] {
+    const char* v = std::getenv("DQB_HOST_LOOP");
+    return v != nullptr && v[0] == '1';
+  }();
+  return on;
+}
+
+// Host-driven form of "WHILE (cond) { body }": `body(stream, 0, flag)` enqueues one
+// iteration whose last kernel writes the condition to the device word `flag`; the call
+// returns when it reads 0.  Synchronises `stream` once per iteration.
+template <class Body>
+cudaError_t run_host_loop(Body body, int* flag, cudaStream_t s) {
+  for (;;) {
+    body(s, cudaGraphConditionalHandle(0), flag);
+    int more = 0;
+    cudaError_t err = cudaMemcpyAsync(&more, flag, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err == cudaSuccess) err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    if (!more) return cudaSuccess;
+  }
+}
+
+// Build "WHILE (cond) { body }" where `body(stream, handle, nullptr)` enqueues one loop
+// iteration on the capture stream and must end with a kernel that sets the condition.
 template <class Body>
 cudaError_t build_while_graph(Body body, cudaGraphExec_t* out) {
   cudaGraph_t g = nullptr;
@@ -106,7 +135,7 @@ cudaError_t build_while_graph(Body body, cudaGraphExec_t* out) {
       if (err == cudaSuccess) {
         err = cudaStreamBeginCaptureToGraph(cap, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
         if (err == cudaSuccess) {
-          body(cap, handle);
+          body(cap, handle, (int*)nullptr);
           cudaError_t e2 = cudaStreamEndCapture(cap, &bodyg);
           if (err == cudaSuccess) err = e2;
           if (err == cudaSuccess) err = cudaGetLastError();

@@ -41,8 +41,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from .mesolve import (_as_op, _check_mesolve_args, _MAX_STEPS_MSG, assert_method_supported,
-                      check_times)
+from .mesolve import (_as_op, _check_mesolve_args, _MAX_STEPS_MSG, _precision_code,
+                      assert_method_supported, check_times)
 from .method import Tsit5
 from .options import Options, check_options
 from .qarrays import to_dense
@@ -223,6 +223,10 @@ class MESolveServer:
         if len(H.shape) != 2 or any(len(L.shape) != 2 for L in Ls) or len(rho0.shape) != 2:
             raise ValueError('MESolveServer.submit takes one problem without batch dimensions.')
         n = H.shape[-1]
+        form = (_lib.FORM_STANDARD if (options.vectorized or not options.assume_hermitian)
+                else _lib.FORM_HERMITIAN)
+        if n > 64 and (_precision_code(options, form) != _lib.PREC_FP32 and n % 2):
+            raise ValueError('Option `precision` other than "fp32" needs an even n.')
         t = Ticket(id=-1, n=n, H=to_dense(H).astype(np.complex64),
                    Ls=[to_dense(L).astype(np.complex64) for L in Ls],
                    rho0=np.asarray(rho0, np.complex64), tsave=tsave,
@@ -372,7 +376,8 @@ class MESolveServer:
             rtol=float(m.rtol), atol=float(m.atol), safety=float(m.safety_factor),
             factormin=float(m.min_factor), factormax=float(m.max_factor),
             max_steps=int(m.max_steps), t0=0.0, save_states=1,
-            check_hermitian=int(bool(o.assume_hermitian)))
+            check_hermitian=int(bool(o.assume_hermitian)),
+            precision=_precision_code(o, form) if t.n > 64 else _lib.PREC_FP32)
 
     def _launch_wave(self, tickets, key, stream) -> _Wave | None:
         """Pack the wave's inputs into pinned staging (one host-to-device copy), give every
@@ -385,7 +390,7 @@ class MESolveServer:
             groups.setdefault((type(t.method), t.method.rtol, t.method.atol,
                                t.method.safety_factor, t.method.min_factor, t.method.max_factor,
                                t.method.max_steps, t.options.assume_hermitian,
-                               t.options.vectorized), []).append(t)
+                               t.options.vectorized, t.options.precision), []).append(t)
         held = []  # (arena, offset, nbytes) released when the wave retires
         outs_held = {}  # per ticket output region
         plans = []
@@ -580,10 +585,16 @@ class MESolveServer:
         slot = self._large_slots[(id(stream), n)]
         return slot[2], slot[3]
 
-    def warmup(self, large_dims=(128, 256)) -> None:
+    def warmup(self, large_dims=(128, 256), method=Tsit5(), options: Options = Options()) -> None:  # noqa: B008
         """Run a trivial request through every stream of every class, one at a time (free
         streams are used round-robin): this loads every kernel and captures every
-        large-path graph before serving starts."""
+        large-path graph before serving starts.
+
+        A large-path graph is specific to the method's tolerances and to
+        ``options.precision``: warm up with those of the requests to come.  A request with
+        other values makes its wave capture a new graph while it is being served, and graph
+        instantiation can wait for the conditional graphs already running on the device,
+        holding up every stream meanwhile."""
         torch = self._torch
         plan = [(n, len(self._free_streams['small'])) for n in (8, 24, 48)]
         plan += [(n, len(self._free_streams['large'])) for n in large_dims]
@@ -592,7 +603,8 @@ class MESolveServer:
             a = np.diag(np.sqrt(np.arange(1, n)), 1).astype(np.complex64)
             for _ in range(reps):
                 t = self.submit(np.zeros((n, n), np.complex64), [a],
-                                np.eye(n, 1, dtype=np.complex64), [0.0, 0.1])
+                                np.eye(n, 1, dtype=np.complex64), [0.0, 0.1], method=method,
+                                options=options if n > 64 else Options())
                 t.result()
                 t.release()
                 done.append(t)

@@ -419,9 +419,14 @@ def run_b200(args):
         peak = peaks.get('bf16_tflops_sustained', peaks.get('bf16_tflops'))
         roof = {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
                 'frac': achieved / peak, 'peak_source': f'bf16_tflops_sustained ({which})',
-                'traffic': None, 'algorithmic_flops_per_launch': flops,
-                'note': 'products run on the FP32 CUDA-core pipe (SIMT); FP32 nominal peak is '
-                        '148 SMs x 128 FMA x 2 x clock'}
+                'traffic': None, 'algorithmic_flops_per_launch': flops}
+        if args.precision == 'fp32':
+            roof['note'] = ('products run on the FP32 CUDA-core pipe (SIMT), not the tensor '
+                            'pipe; see roofline_fp32_simt')
+        else:
+            roof['note'] = (f'products run on tcgen05 tensor cores ({args.precision}: three '
+                            'products per complex MAC term, so the tensor pipe executes 3x the '
+                            'algorithmic flops)')
 
     # ---- e2e: public API from host inputs --------------------------------------------
     e2e = None
@@ -455,10 +460,10 @@ def run_b200(args):
         e2e = {'value': world * B / e2e_s, 'unit': 'solves/s', 'h2d_bytes_per_step': int(h2d),
                'd2h_bytes_per_step': int(d2h)}
 
-    # ---- plain path: one instance per launch -------------------------------------------
+    # ---- plain path: one instance per launch, FP32 ------------------------------------
     plain = None
-    if args.config == 'kerr' and not args.no_plain and rank == 0:
-        nplain = 16
+    if args.config in ('kerr', 'transmon') and not args.no_plain and rank == 0:
+        nplain = 16 if args.config == 'kerr' else 4
         lat = []
         for b in range(nplain):
             p1 = make_batch_plan(w['H'][b], w['jump_ops'], w['rho0'], True)
@@ -474,7 +479,8 @@ def run_b200(args):
             lat.append(e0.elapsed_time(e1))
         plain_s = float(np.sum(lat)) / 1e3
         plain = {'value': nplain / plain_s, 'unit': 'solves/s',
-                 'what': 'same kernel, one instance per launch (16 instances)',
+                 'what': f'{prep.name} with FP32 products, one instance per launch '
+                         f'({nplain} instances)',
                  'p50_latency_ms': float(np.percentile(lat, 50)),
                  'p99_latency_ms': float(np.percentile(lat, 99)),
                  'batched_over_plain': value / world / (nplain / plain_s)}
@@ -486,6 +492,15 @@ def run_b200(args):
         return
 
     clocks = _clock_summary(clk_path)
+    extra = {}
+    if roof['bound'] == 'tensor' and args.precision == 'fp32':
+        # the FP32 FMA pipe: 148 SMs x 128 lanes x 2 flop per clock, at the sampled SM clock
+        mhz = (clocks or {}).get('sm_mhz') or peaks.get('sm_max_mhz', 1965.0)
+        simt = 148 * 128 * 2 * mhz * 1e6 / 1e12
+        extra['roofline_fp32_simt'] = {'bound': 'fp32_fma', 'achieved': roof['achieved'],
+                                       'peak': simt, 'unit': 'TFLOP/s',
+                                       'frac': roof['achieved'] / simt,
+                                       'peak_source': f'nominal at the sampled {mhz:.0f} MHz'}
     line = {
         'metric': METRIC, 'value': value, 'unit': 'solves/s', 'n_gpus': world,
         'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': mean_ms,
@@ -501,6 +516,7 @@ def run_b200(args):
         'e2e': e2e,
         'gpu_launches': args.steps * _kernels_per_launch(prep.name, K, int(nsteps.max())),
         'roofline': roof,
+        **extra,
         'clocks': clocks,
         'plain_path': plain,
         'latency_ms': {'per_batch': mean_ms},

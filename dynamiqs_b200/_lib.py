@@ -60,6 +60,7 @@ class OdeOptions(ctypes.Structure):
         ('save_states', ctypes.c_int32),
         ('check_hermitian', ctypes.c_int32),
         ('precision', ctypes.c_int32),
+        ('tile', ctypes.c_int32),
     ]
 
 

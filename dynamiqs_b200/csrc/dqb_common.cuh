@@ -155,6 +155,13 @@ __device__ __forceinline__ void cmac(float2& acc, float2 a, float2 b) {
   acc.y = fmaf(a.x, b.y, acc.y);
   acc.y = fmaf(a.y, b.x, acc.y);
 }
+__device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 acc) {  // acc + a b
+  acc.x = fmaf(a.x, b.x, acc.x);
+  acc.x = fmaf(-a.y, b.y, acc.x);
+  acc.y = fmaf(a.x, b.y, acc.y);
+  acc.y = fmaf(a.y, b.x, acc.y);
+  return acc;
+}
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 caxpy(float s, float2 x, float2 y) {  // y + s x

@@ -38,6 +38,7 @@ struct DiaOps {
   int nl;                             // sum of jump diagonals
   int lstart[DQB_DIA_MAX_JUMPS + 1];
   int loff[DQB_DIA_MAX_JUMP_DIAGS];
+  int ljump[DQB_DIA_MAX_JUMP_DIAGS];  // jump operator owning each jump diagonal
   const float2* H;                    // [*, h_nd, n]
   const float2* L;                    // [*, nl, n]
   const int* Hidx;
@@ -85,11 +86,12 @@ __global__ void hnh_dia_kernel(DiaOps d, int B) {
 constexpr int kRhsCols = 128;
 constexpr int kRhsRows = 8;
 
-// f(X) for DIA operators.  grid (n / 128, n / 8, B), block 128: each thread owns one
-// column and 8 consecutive rows.
+// Generic f(X) for DIA operators (any number of diagonals).  grid (n / 128, n / 8, B),
+// block 128: each thread owns one column and 8 consecutive rows.
 // in_sel: 0 = y, 1 = y1, 2 = X.  need_run: 1 = running instances, 0 = status OK.
-__global__ void __launch_bounds__(kRhsCols) rhs_dia_kernel(big::Common c, DiaOps d, int in_sel, int out_k,
-                                                           int need_run, const float2* ext_in, float2* ext_out) {
+__global__ void __launch_bounds__(kRhsCols) rhs_dia_generic_kernel(big::Common c, DiaOps d, int in_sel, int out_k,
+                                                                   int need_run, const float2* ext_in,
+                                                                   float2* ext_out) {
   const int b = blockIdx.z;
   const float2* X;
   float2* out;
@@ -142,6 +144,125 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_kernel(big::Common c, DiaOps
   }
 }
 
+// Fast f(X) for up to kFastH Hnh diagonals and kFastL jump diagonals in total.
+// grid (n / 128, n / R, B), block 128: each thread owns one column j and R consecutive
+// rows.  Everything that depends only on the column (conj(hnh_q[j + k_q]), the column
+// factors conj(l_s[j + q_s]) and the clamped column indices) is computed once per thread
+// and kept in registers; everything that depends only on the row is computed once per CTA
+// into shared memory.  Out-of-range diagonal entries become zero coefficients on a
+// clamped (in-bounds) index, so the inner loops have no branches: per output element,
+// 2 nh + (jump pairs) coalesced loads of X and as many complex multiply-adds.
+constexpr int kFastH = 16;
+constexpr int kFastL = 8;
+
+template <int R>
+__global__ void __launch_bounds__(kRhsCols) rhs_dia_fast_kernel(big::Common c, DiaOps d, int in_sel, int out_k,
+                                                                int need_run, const float2* ext_in,
+                                                                float2* ext_out) {
+  __shared__ float2 s_hrow[kFastH][R];  // hnh_q[i + k_q] (0 outside the matrix)
+  __shared__ float2 s_lrow[kFastL][R];  // l_p[i + q_p]   (0 outside the matrix)
+  const int b = blockIdx.z;
+  const float2* X;
+  float2* out;
+  if (ext_in) {  // stand-alone evaluation (dqb_lindblad_rhs_dia)
+    X = ext_in + (long long)b * d.n * d.n;
+    out = ext_out + (long long)b * d.n * d.n;
+  } else {
+    const big::Inst& I = c.inst[b];
+    if (need_run ? !I.run : I.status != DQB_INST_OK) return;
+    X = big::slot(c, b, in_sel == 0 ? I.sy : (in_sel == 1 ? I.sy1 : big::kX));
+    out = big::slot(c, b, I.sk[out_k]);
+  }
+  const int n = d.n, nh = d.nh, nl = d.nl;
+  const long long li = d.Lidx ? d.Lidx[b] : b;
+  const float2* L = d.L + li * nl * n;
+  const float2* hnh = d.hnh + (long long)b * nh * n;
+  const int i0 = blockIdx.y * R;
+
+  // row factors of this CTA's R rows
+  for (int e = threadIdx.x; e < (kFastH + kFastL) * R; e += blockDim.x) {
+    const int q = e / R, r = e % R, i = i0 + r;
+    float2 v = make_float2(0.f, 0.f);
+    if (q < kFastH) {
+      if (q < nh) {
+        const int cidx = i + d.hoff[q];
+        if (i < n && cidx >= 0 && cidx < n) v = __ldg(&hnh[q * n + cidx]);
+      }
+      s_hrow[q][r] = v;
+    } else {
+      const int p = q - kFastH;
+      if (p < nl) {
+        const int cidx = i + d.loff[p];
+        if (i < n && cidx >= 0 && cidx < n) v = __ldg(&L[p * n + cidx]);
+      }
+      s_lrow[p][r] = v;
+    }
+  }
+  __syncthreads();
+  const int j = blockIdx.x * kRhsCols + threadIdx.x;
+  if (j >= n) return;
+
+  // column factors of this thread's column
+  float2 hcol[kFastH];
+  int jh[kFastH];
+#pragma unroll
+  for (int q = 0; q < kFastH; ++q) {
+    hcol[q] = make_float2(0.f, 0.f);
+    jh[q] = j;
+    if (q < nh) {
+      const int cidx = j + d.hoff[q];
+      const bool in = cidx >= 0 && cidx < n;
+      jh[q] = in ? cidx : j;
+      if (in) hcol[q] = cconj(__ldg(&hnh[q * n + cidx]));
+    }
+  }
+  float2 lcol[kFastL];
+  int jl[kFastL];
+#pragma unroll
+  for (int s = 0; s < kFastL; ++s) {
+    lcol[s] = make_float2(0.f, 0.f);
+    jl[s] = j;
+    if (s < nl) {
+      const int cidx = j + d.loff[s];
+      const bool in = cidx >= 0 && cidx < n;
+      jl[s] = in ? cidx : j;
+      if (in) lcol[s] = cconj(__ldg(&L[s * n + cidx]));
+    }
+  }
+
+  const int rows = min(R, n - i0);
+#pragma unroll 2
+  for (int r = 0; r < rows; ++r) {
+    const int i = i0 + r;
+    const float2* Xi = X + (long long)i * n;
+    float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < kFastH; ++q) {
+      if (q < nh) {
+        int ci = i + d.hoff[q];
+        ci = ci < 0 ? 0 : (ci >= n ? n - 1 : ci);
+        acc = cfma(s_hrow[q][r], __ldg(&X[(long long)ci * n + j]), acc);
+        acc = cfma(hcol[q], __ldg(&Xi[jh[q]]), acc);
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < kFastL; ++p) {
+      if (p < nl) {
+        const int k = d.ljump[p];
+        int ci = i + d.loff[p];
+        ci = ci < 0 ? 0 : (ci >= n ? n - 1 : ci);
+        const float2 lr = s_lrow[p][r];
+        const float2* Xc = X + (long long)ci * n;
+#pragma unroll
+        for (int s = 0; s < kFastL; ++s) {
+          if (s < nl && d.ljump[s] == k) acc = cfma(cmul(lr, lcol[s]), __ldg(&Xc[jl[s]]), acc);
+        }
+      }
+    }
+    out[(long long)i * n + j] = acc;
+  }
+}
+
 // ------------------------------------------------------------------------------------
 // host side
 // ------------------------------------------------------------------------------------
@@ -176,6 +297,8 @@ int build_ops(const dqb_dia_problem* p, DiaOps* d) {
     if (k <= -p->n || k >= p->n) return DQB_ERR_INVALID_ARGUMENT;
     offs.insert(k);
   }
+  for (int k = 0; k < p->n_jumps; ++k)
+    for (int q = d->lstart[k]; q < d->lstart[k + 1]; ++q) d->ljump[q] = k;
   for (int q = 0; q < nl; ++q) {
     d->loff[q] = p->l_offsets[q];
     if (d->loff[q] <= -p->n || d->loff[q] >= p->n) return DQB_ERR_INVALID_ARGUMENT;
@@ -232,6 +355,35 @@ int check_problem(const dqb_dia_problem* p) {
   return DQB_OK;
 }
 
+bool fast_ok(const DiaOps& d) { return d.nh <= kFastH && d.nl <= kFastL; }
+
+// Rows per thread of the fast stencil: `tile` (4, 8 or 16; 0 = 8), or the generic
+// kernel's 8 when the operators have more diagonals than the fast kernel keeps in registers.
+int rows_for(const DiaOps& d, int tile) {
+  if (!fast_ok(d)) return kRhsRows;
+  return (tile == 4 || tile == 16) ? tile : 8;
+}
+
+dim3 rhs_grid(const DiaOps& d, int rows, int B) {
+  return dim3((d.n + kRhsCols - 1) / kRhsCols, (d.n + rows - 1) / rows, B);
+}
+
+// One right-hand side of every instance: k[out_k] = f(input), through the fast stencil
+// when the operators fit it.
+void launch_rhs_dia(cudaStream_t s, const big::Common& c, const DiaOps& d, int B, int rows, int in_sel,
+                    int out_k, int need_run, const float2* ext_in, float2* ext_out) {
+  const dim3 g = rhs_grid(d, rows, B);
+  if (!fast_ok(d)) {
+    rhs_dia_generic_kernel<<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
+  } else if (rows == 4) {
+    rhs_dia_fast_kernel<4><<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
+  } else if (rows == 16) {
+    rhs_dia_fast_kernel<16><<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
+  } else {
+    rhs_dia_fast_kernel<8><<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
+  }
+}
+
 GraphCache g_cache;
 
 struct LaunchKey {
@@ -262,7 +414,10 @@ static void init_carveouts() {
     prefer_max_shared(big::finalize_kernel);
     prefer_max_shared(zero_words_kernel);
     prefer_max_shared(hnh_dia_kernel);
-    prefer_max_shared(rhs_dia_kernel);
+    prefer_max_shared(rhs_dia_generic_kernel);
+    prefer_max_shared(rhs_dia_fast_kernel<4>);
+    prefer_max_shared(rhs_dia_fast_kernel<8>);
+    prefer_max_shared(rhs_dia_fast_kernel<16>);
   });
 }
 
@@ -291,8 +446,7 @@ extern "C" int dqb_lindblad_rhs_dia(const dqb_dia_problem* p, int32_t form, cons
   hnh_dia_kernel<<<dim3((p->n + 255) / 256, (unsigned)p->batch), 256, 0, s>>>(d, (int)p->batch);
   big::Common c;
   std::memset(&c, 0, sizeof(c));
-  rhs_dia_kernel<<<dim3((p->n + kRhsCols - 1) / kRhsCols, (p->n + kRhsRows - 1) / kRhsRows, (unsigned)p->batch),
-                   kRhsCols, 0, s>>>(c, d, 2, 0, 0, (const float2*)rho, (float2*)outp);
+  launch_rhs_dia(s, c, d, (int)p->batch, rows_for(d, 0), 2, 0, 0, (const float2*)rho, (float2*)outp);
   return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
 }
 
@@ -344,7 +498,7 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   int grid_e = (int)std::min<long long>((nn + big::kElemThreads - 1) / big::kElemThreads, 1184);
   if (grid_e < 1) grid_e = 1;
   const dim3 ge(grid_e, B);
-  const dim3 gr((p->n + kRhsCols - 1) / kRhsCols, (p->n + kRhsRows - 1) / kRhsRows, B);
+  const int rows = rows_for(d, o->tile);
   const dim3 gi((B + 127) / 128);
   const int T = big::kElemThreads;
 
@@ -353,11 +507,11 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   big::setup_kernel<<<gi, 128, 0, s>>>(c);
   hnh_dia_kernel<<<dim3((p->n + 255) / 256, B), 256, 0, s>>>(d, B);
   big::load_rho0_kernel<<<ge, T, 0, s>>>(c);
-  rhs_dia_kernel<<<gr, kRhsCols, 0, s>>>(c, d, 0, 0, 0, nullptr, nullptr);
+  launch_rhs_dia(s, c, d, B, rows, 0, 0, 0, nullptr, nullptr);
   big::init_norm_kernel<<<ge, T, 0, s>>>(c, 0);
   big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 0);
   big::combine_kernel<<<ge, T, 0, s>>>(c, 6);
-  rhs_dia_kernel<<<gr, kRhsCols, 0, s>>>(c, d, 2, 1, 0, nullptr, nullptr);
+  launch_rhs_dia(s, c, d, B, rows, 2, 1, 0, nullptr, nullptr);
   big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
   big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 1);
   if (cudaGetLastError() != cudaSuccess) return DQB_ERR_CUDA;
@@ -366,10 +520,10 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h, int* flag) {
     for (int st = 0; st < 5; ++st) {
       big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
-      rhs_dia_kernel<<<gr, kRhsCols, 0, cs>>>(c, d, 2, st + 1, 1, nullptr, nullptr);
+      launch_rhs_dia(cs, c, d, B, rows, 2, st + 1, 1, nullptr, nullptr);
     }
     big::combine_kernel<<<ge, T, 0, cs>>>(c, 5);
-    rhs_dia_kernel<<<gr, kRhsCols, 0, cs>>>(c, d, 1, 6, 1, nullptr, nullptr);
+    launch_rhs_dia(cs, c, d, B, rows, 1, 6, 1, nullptr, nullptr);
     big::error_kernel<<<ge, T, 0, cs>>>(c);
     big::control_kernel<<<gi, 128, 0, cs>>>(c);
     big::save_kernel<<<ge, T, 0, cs>>>(c, 1);
@@ -383,8 +537,8 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
     key.c = c;
     key.d = d;
     key.grid_e = grid_e;
-    key.grid_r_x = gr.x;
-    key.grid_r_y = gr.y;
+    key.grid_r_x = rows;
+    key.grid_r_y = fast_ok(d);
     cudaGraphExec_t exec = g_cache.find(&key, sizeof(key));
     if (!exec) {
       if (build_while_graph(body, &exec) != cudaSuccess) return DQB_ERR_CUDA;

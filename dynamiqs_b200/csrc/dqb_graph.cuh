@@ -78,7 +78,7 @@ class GraphCache {
     }
   }
 
-  static constexpr size_t kMax = 8;
+  static constexpr size_t kMax = 64;
   std::mutex mu_;
   std::vector<Entry> entries_;
   std::vector<Parked> parked_;

@@ -80,6 +80,8 @@ typedef struct dqb_ode_options {
   int32_t save_states;     /* 1: state at every tsave; 0: final state only              */
   int32_t check_hermitian; /* 1: flag rho0 that fails isherm(rtol=atol=1e-5)            */
   int32_t precision;       /* DQB_PREC_* (GEMM path only; 0 = FP32)                     */
+  int32_t tile;            /* launch-shape choice, 0 = default: rows per thread of the
+                              sparse-DIA stencil (4, 8 or 16); ignored by other paths    */
 } dqb_ode_options;
 
 /* Outputs of a batched solve.  nsave = n_tsave if save_states else 1. */

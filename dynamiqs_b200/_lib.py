@@ -168,6 +168,8 @@ SIGNATURES = {
                                        ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
     'dqb_lindblad_rhs_dia': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.c_int32, _P, _P, _P,
                                             ctypes.c_size_t, _P]),
+    'dqb_lindblad_rhs_dia_tiled': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.c_int32,
+                                                  ctypes.c_int32, _P, _P, _P, ctypes.c_size_t, _P]),
     'dqb_dense_small_max_n': (ctypes.c_int32, [ctypes.c_int32]),
     'dqb_version': (ctypes.c_char_p, []),
 }

@@ -430,6 +430,11 @@ extern "C" size_t dqb_mesolve_dia_workspace_size(const dqb_dia_problem* p) {
 
 extern "C" int dqb_lindblad_rhs_dia(const dqb_dia_problem* p, int32_t form, const void* rho, void* outp,
                                     void* workspace, size_t workspace_bytes, void* stream) {
+  return dqb_lindblad_rhs_dia_tiled(p, form, 0, rho, outp, workspace, workspace_bytes, stream);
+}
+
+extern "C" int dqb_lindblad_rhs_dia_tiled(const dqb_dia_problem* p, int32_t form, int32_t tile, const void* rho,
+                                          void* outp, void* workspace, size_t workspace_bytes, void* stream) {
   int rc = check_ops(p);
   if (rc) return rc;
   if (!rho || !outp) return DQB_ERR_INVALID_ARGUMENT;
@@ -446,7 +451,7 @@ extern "C" int dqb_lindblad_rhs_dia(const dqb_dia_problem* p, int32_t form, cons
   hnh_dia_kernel<<<dim3((p->n + 255) / 256, (unsigned)p->batch), 256, 0, s>>>(d, (int)p->batch);
   big::Common c;
   std::memset(&c, 0, sizeof(c));
-  launch_rhs_dia(s, c, d, (int)p->batch, rows_for(d, 0), 2, 0, 0, (const float2*)rho, (float2*)outp);
+  launch_rhs_dia(s, c, d, (int)p->batch, rows_for(d, tile), 2, 0, 0, (const float2*)rho, (float2*)outp);
   return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
 }
 

@@ -267,7 +267,11 @@ class PreparedSolve:
 
 
 def _precision_code(o, form: int) -> int:
-    """DQB_PREC_* for ``Options.precision``; the tensor-core modes need the hermitian form."""
+    """DQB_PREC_* for ``Options.precision``; the tensor-core modes need the hermitian form.
+    ``'auto'`` maps to FP32 here; the GEMM path's prepare step replaces it with the
+    autotuner's choice."""
+    if o.precision == 'auto':
+        return _lib.PREC_FP32
     try:
         code = _lib.PRECISIONS[o.precision]
     except KeyError:
@@ -294,6 +298,7 @@ class MESolveB200Integrator:
         self.Ls = Ls
         self.Es = Es
         self.plan = plan
+        self._tuned: dict = {}  # launch choices made by the autotuner at prepare time
 
     @property
     def t0(self) -> float:
@@ -309,7 +314,14 @@ class MESolveB200Integrator:
             form=form, rtol=float(m.rtol), atol=float(m.atol), safety=float(m.safety_factor),
             factormin=float(m.min_factor), factormax=float(m.max_factor),
             max_steps=int(m.max_steps), t0=self.t0, save_states=int(bool(o.save_states)),
-            check_hermitian=int(bool(o.assume_hermitian)), precision=_precision_code(o, form))
+            check_hermitian=int(bool(o.assume_hermitian)),
+            precision=self._tuned.get('precision', _precision_code(o, form)),
+            tile=self._tuned.get('tile', 0))
+
+    def _form(self) -> int:
+        o = self.options
+        return (_lib.FORM_STANDARD if (o.vectorized or not o.assume_hermitian)
+                else _lib.FORM_HERMITIAN)
 
     def run(self) -> MESolveResult:
         return self.prepare().launch().result()
@@ -380,7 +392,42 @@ class MESolveB200Integrator:
             ws_bytes = lib.dqb_mesolve_dense_large_workspace_size(n, K, nE, ntsave, B)
             fn, name = lib.dqb_mesolve_dense_large, 'dqb_mesolve_dense_large'
         bufs['workspace'] = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+        if kind == 'large' and self.options.precision == 'auto':
+            self._tune_gemm_precision(lib, prob, bufs['workspace'], ws_bytes, dev)
         return PreparedSolve(self, fn, name, prob, outs, bufs, ws_bytes, dev, nE)
+
+    def _tune_gemm_precision(self, lib, prob, ws, ws_bytes, dev) -> None:
+        """``precision='auto'``: the faster of FP32 and 3xTF32 products for this (n, K,
+        batch), timed on one right-hand side of up to 256 instances."""
+        import ctypes
+
+        import torch
+
+        from . import autotune
+
+        n, K, B, form = prob.n, prob.n_jumps, prob.batch, self._form()
+        cands = [_lib.PREC_FP32]
+        if form == _lib.FORM_HERMITIAN and n % 2 == 0:
+            cands.append(_lib.PREC_TF32X3)
+        Bt = min(B, 256)
+        pt = _lib.DenseProblem.from_buffer_copy(prob)
+        pt.batch = Bt
+        g = torch.Generator(device='cpu').manual_seed(0)
+        Y = torch.randn(Bt, n, n, dtype=torch.complex64, generator=g)
+        rho = (Y @ Y.mH / n).to(dev)
+        out = torch.empty_like(rho)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+
+        def make_run(c):
+            def run():
+                _lib.check(lib.dqb_lindblad_rhs_dense_large_prec(
+                    ctypes.byref(pt), form, c, rho.data_ptr(), out.data_ptr(), ws.data_ptr(),
+                    ws_bytes, stream), 'dqb_lindblad_rhs_dense_large_prec')
+            return run
+
+        key = ('gemm_precision', torch.cuda.get_device_name(dev), n, K, 'dense',
+               autotune.batch_bucket(B), form)
+        self._tuned['precision'] = autotune.choose(key, cands, make_run, _lib.PREC_FP32)
 
     def _prepare_dia(self, lib) -> PreparedSolve:
         import ctypes
@@ -419,8 +466,38 @@ class MESolveB200Integrator:
                                       '(diagonal counts or batch size).')
         bufs['workspace'] = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
         bufs['host'] = host
+        self._tune_dia_tile(lib, prob, bufs['workspace'], ws_bytes, dev,
+                            (tuple(H.offsets), tuple(tuple(L.offsets) for L in Lsets)))
         return PreparedSolve(self, lib.dqb_mesolve_dia, 'dqb_mesolve_dia', prob, outs, bufs,
                              ws_bytes, dev, nE)
+
+    def _tune_dia_tile(self, lib, prob, ws, ws_bytes, dev, pattern) -> None:
+        """Rows per thread of the DIA stencil (4, 8 or 16) for this (n, sparsity pattern),
+        timed on one right-hand side of one instance."""
+        import ctypes
+
+        import torch
+
+        from . import autotune
+
+        n = prob.n
+        pt = _lib.DiaProblem.from_buffer_copy(prob)
+        pt.batch = 1
+        g = torch.Generator(device='cpu').manual_seed(0)
+        rho = (torch.randn(1, n, n, dtype=torch.complex64, generator=g) / n).to(dev)
+        out = torch.empty_like(rho)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+
+        def make_run(t):
+            def run():
+                _lib.check(lib.dqb_lindblad_rhs_dia_tiled(
+                    ctypes.byref(pt), _lib.FORM_HERMITIAN, t, rho.data_ptr(), out.data_ptr(),
+                    ws.data_ptr(), ws_bytes, stream), 'dqb_lindblad_rhs_dia_tiled')
+            return run
+
+        key = ('dia_tile', torch.cuda.get_device_name(dev), n, prob.n_jumps, pattern,
+               autotune.batch_bucket(prob.batch))
+        self._tuned['tile'] = autotune.choose(key, [4, 8, 16], make_run, 8)
 
     # kept for callers that select a path explicitly (tests)
     def _run_dense_small(self, lib) -> MESolveResult:

@@ -22,7 +22,9 @@ class Options:
     # Arithmetic of the complex products on the dense GEMM path (n > 64): 'fp32' (CUDA
     # cores, default), 'tf32x3' or 'bf16x3' (tcgen05 tensor cores on hi + lo operand
     # splits, FP32 accumulation), 'tf32' (one TF32 pass, ~1e-3: error studies only).
-    # An addition of this library; the n <= 64 and sparse-DIA kernels always run FP32.
+    # 'auto' lets the autotuner pick the faster of 'fp32' and 'tf32x3' for the problem's
+    # (n, jumps, batch).  An addition of this library; the n <= 64 and sparse-DIA kernels
+    # always run FP32.
     precision: str = 'fp32'
 
     def initialise(self) -> Options:

@@ -275,6 +275,13 @@ DQB_API int dqb_mesolve_dia(const dqb_dia_problem* problem, const dqb_ode_option
 DQB_API int dqb_lindblad_rhs_dia(const dqb_dia_problem* problem, int32_t form, const void* rho,
                                  void* out, void* workspace, size_t workspace_bytes, void* stream);
 
+/* Same, with the stencil's launch shape `tile` (rows per thread: 4, 8 or 16; 0 = default),
+ * as dqb_ode_options.tile selects it for dqb_mesolve_dia; the autotuner times the choices
+ * through this entry point. */
+DQB_API int dqb_lindblad_rhs_dia_tiled(const dqb_dia_problem* problem, int32_t form, int32_t tile,
+                                       const void* rho, void* out, void* workspace,
+                                       size_t workspace_bytes, void* stream);
+
 /* ---- library info ------------------------------------------------------------- */
 /* Largest n handled by the shared-memory persistent kernel for a jump count. */
 DQB_API int32_t dqb_dense_small_max_n(int32_t n_jumps);

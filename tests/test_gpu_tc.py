@@ -134,3 +134,26 @@ def test_solve_tc_full_dim_short_horizon(cuda_device):
     fp = dq.mesolve(w['H'], w['jump_ops'], w['rho0'], ts, **kw)
     assert rel_frob(tc.states.cpu().numpy(), fp.states.cpu().numpy()).max() < 1e-5
     assert np.abs(tc.infos.nsteps.cpu().numpy() - fp.infos.nsteps.cpu().numpy()).max() <= 1
+
+
+def test_solve_auto_precision_picks_a_qualified_mode(cuda_device, tmp_path, monkeypatch):
+    """precision='auto': the autotuner picks FP32 or 3xTF32 (the modes that meet 1e-5) for
+    this (n, K, batch), caches it, and the solve matches the FP32 path within 1e-5."""
+    from dynamiqs_b200 import autotune
+    from dynamiqs_b200.mesolve import MESolveB200Integrator, make_batch_plan
+
+    monkeypatch.setenv('DQB_AUTOTUNE_CACHE', str(tmp_path / 'tune.json'))
+    autotune.clear_memory_cache()
+    w = workloads.transmon_cavity(batch=4, nq=2, nc=64, seed=7)
+    ts = np.linspace(0.0, 1.0, 3)
+    opts = dq.Options(precision='auto')
+    plan = make_batch_plan(w['H'], w['jump_ops'], w['rho0'], True)
+    integ = MESolveB200Integrator(ts=ts, y0=w['rho0'], method=w['method'], gradient=None,
+                                  options=opts, H=w['H'], Ls=w['jump_ops'], Es=w['exp_ops'],
+                                  plan=plan)
+    res = integ.prepare().launch().result()
+    assert integ._tuned['precision'] in (_lib.PREC_FP32, _lib.PREC_TF32X3)
+    assert (tmp_path / 'tune.json').exists()
+    fp = dq.mesolve(w['H'], w['jump_ops'], w['rho0'], ts, exp_ops=w['exp_ops'], method=w['method'])
+    assert rel_frob(res.states.cpu().numpy(), fp.states.cpu().numpy()).max() < 1e-5
+    autotune.clear_memory_cache()

@@ -301,7 +301,7 @@ def _workload(name, args, rank):
 
     seed = args.seed + rank
     if name == 'kerr':
-        w = workloads.batched_kerr(batch=args.batch or 4096, seed=seed)
+        w = workloads.batched_kerr(batch=args.batch or 4096, n=args.n or 64, seed=seed)
         if args.tend != 10.0:
             w['tsave'] = np.linspace(0.0, args.tend, 51)
     elif name == 'oscillator':
@@ -506,7 +506,8 @@ def run_b200(args):
         'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': mean_ms,
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'c64',
         'data': 'synthetic (seeded numpy generator; no dataset)',
-        'config': {'workload': CASES[args.config], 'batch_per_gpu': B, 'n': n, 'n_jumps': K,
+        'config': {'workload': CASES[args.config] if n == 64 or args.config != 'kerr' else
+                   CASES['kerr'].replace('n=64', f'n={n}'), 'batch_per_gpu': B, 'n': n, 'n_jumps': K,
                    'n_tsave': len(w['tsave']), 'method': type(w['method']).__name__,
                    'rtol': w['method'].rtol, 'atol': w['method'].atol, 'path': prep.name,
                    'precision': args.precision,
@@ -535,6 +536,7 @@ def main():
     ap.add_argument('--config', default='kerr', choices=sorted(CASES))
     ap.add_argument('--batch', type=int, default=0, help='instances (0: the workload default)')
     ap.add_argument('--seed', type=int, default=0)
+    ap.add_argument('--n', type=int, default=0, help='kerr: Hilbert dimension (0: 64, the workload)')
     ap.add_argument('--tend', type=float, default=10.0, help='end time (10 in the workload; '
                     'shorter only for profiling captures)')
     ap.add_argument('--e2e-steps', type=int, default=1)

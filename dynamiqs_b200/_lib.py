@@ -89,6 +89,7 @@ class DenseProblem(ctypes.Structure):
         ('H_index', ctypes.c_void_p),
         ('L_index', ctypes.c_void_p),
         ('rho0_index', ctypes.c_void_p),
+        ('start_order', ctypes.c_void_p),
     ]
 
 

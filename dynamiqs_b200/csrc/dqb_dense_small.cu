@@ -56,6 +56,7 @@ struct DenseSmallArgs {
   int* status;
   float2* slots;
   unsigned int* counter;
+  const int* order;  // start order of the instances, or null (0, 1, 2, ...)
   CtrlOpts o;
 };
 
@@ -520,8 +521,13 @@ __global__ void __launch_bounds__(kSmallThreads) mesolve_small_kernel(DenseSmall
   for (;;) {
     if (threadIdx.x == 0) ctl.inst = (long long)atomicAdd(a.counter, 1u);
     __syncthreads();
-    const long long inst = ctl.inst;
-    if (inst >= a.batch) break;
+    const long long pos = ctl.inst;
+    if (pos >= a.batch) break;
+    const long long inst = a.order ? (long long)a.order[pos] : pos;
+    if (inst < 0 || inst >= a.batch) {  // not a valid instance: skip it
+      __syncthreads();                    // every thread has read ctl.inst
+      continue;
+    }
     const InstView v = view_of(a, inst);
     solve_one<NP>(v, a.o, sH, sX, sT, sL, slot, red, ctl);
     __syncthreads();
@@ -680,6 +686,7 @@ static DenseSmallArgs make_args(const dqb_dense_problem* p, const dqb_ode_option
   a.Hidx = p->H_index;
   a.Lidx = p->L_index;
   a.ridx = p->rho0_index;
+  a.order = p->start_order;
   a.states = out ? (float2*)out->states : nullptr;
   a.expects = out ? (float2*)out->expects : nullptr;
   a.infos = out ? out->infos : nullptr;

@@ -38,7 +38,11 @@ struct DiaOps {
   int nl;                             // sum of jump diagonals
   int lstart[DQB_DIA_MAX_JUMPS + 1];
   int loff[DQB_DIA_MAX_JUMP_DIAGS];
-  int ljump[DQB_DIA_MAX_JUMP_DIAGS];  // jump operator owning each jump diagonal
+  // (p, s) pairs of diagonals of the same jump operator: the terms
+  // l_p[i + q_p] conj(l_s[j + q_s]) X[i + q_p][j + q_s] of L X L^+ (up to 64 recorded)
+  int npair;
+  int pair_p[64];
+  int pair_s[64];
   const float2* H;                    // [*, h_nd, n]
   const float2* L;                    // [*, nl, n]
   const int* Hidx;
@@ -144,23 +148,24 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_generic_kernel(big::Common c
   }
 }
 
-// Fast f(X) for up to kFastH Hnh diagonals and kFastL jump diagonals in total.
+// Fast f(X) for up to kFastH Hnh diagonals and kFastP (p, s) jump-diagonal pairs.
 // grid (n / 128, n / R, B), block 128: each thread owns one column j and R consecutive
 // rows.  Everything that depends only on the column (conj(hnh_q[j + k_q]), the column
-// factors conj(l_s[j + q_s]) and the clamped column indices) is computed once per thread
-// and kept in registers; everything that depends only on the row is computed once per CTA
-// into shared memory.  Out-of-range diagonal entries become zero coefficients on a
-// clamped (in-bounds) index, so the inner loops have no branches: per output element,
-// 2 nh + (jump pairs) coalesced loads of X and as many complex multiply-adds.
-constexpr int kFastH = 16;
-constexpr int kFastL = 8;
+// factors conj(l_s[j + q_s]) of the pairs and the clamped column indices) is computed once
+// per thread and kept in registers; everything that depends only on the row (hnh_q[i + k_q],
+// l_p[i + q_p]) once per CTA into shared memory.  Out-of-range diagonal entries become zero
+// coefficients on a clamped (in-bounds) index, so the inner loops have no data-dependent
+// branches: per output element, 2 nh + npair coalesced loads of X and as many complex
+// multiply-adds.
+constexpr int kFastH = 8;
+constexpr int kFastP = 8;
 
 template <int R>
-__global__ void __launch_bounds__(kRhsCols) rhs_dia_fast_kernel(big::Common c, DiaOps d, int in_sel, int out_k,
-                                                                int need_run, const float2* ext_in,
-                                                                float2* ext_out) {
-  __shared__ float2 s_hrow[kFastH][R];  // hnh_q[i + k_q] (0 outside the matrix)
-  __shared__ float2 s_lrow[kFastL][R];  // l_p[i + q_p]   (0 outside the matrix)
+__global__ void __launch_bounds__(kRhsCols, 6) rhs_dia_fast_kernel(big::Common c, DiaOps d, int in_sel, int out_k,
+                                                                   int need_run, const float2* ext_in,
+                                                                   float2* ext_out) {
+  __shared__ float2 s_hrow[kFastH][R];  // hnh_q[i + k_q]       (0 outside the matrix)
+  __shared__ float2 s_prow[kFastP][R];  // l_{p(t)}[i + q_p(t)] (0 outside the matrix)
   const int b = blockIdx.z;
   const float2* X;
   float2* out;
@@ -173,14 +178,14 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_fast_kernel(big::Common c, D
     X = big::slot(c, b, in_sel == 0 ? I.sy : (in_sel == 1 ? I.sy1 : big::kX));
     out = big::slot(c, b, I.sk[out_k]);
   }
-  const int n = d.n, nh = d.nh, nl = d.nl;
+  const int n = d.n, nh = d.nh, np = d.npair;
   const long long li = d.Lidx ? d.Lidx[b] : b;
-  const float2* L = d.L + li * nl * n;
+  const float2* L = d.L + li * d.nl * n;
   const float2* hnh = d.hnh + (long long)b * nh * n;
   const int i0 = blockIdx.y * R;
 
   // row factors of this CTA's R rows
-  for (int e = threadIdx.x; e < (kFastH + kFastL) * R; e += blockDim.x) {
+  for (int e = threadIdx.x; e < (kFastH + kFastP) * R; e += blockDim.x) {
     const int q = e / R, r = e % R, i = i0 + r;
     float2 v = make_float2(0.f, 0.f);
     if (q < kFastH) {
@@ -190,12 +195,13 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_fast_kernel(big::Common c, D
       }
       s_hrow[q][r] = v;
     } else {
-      const int p = q - kFastH;
-      if (p < nl) {
+      const int t = q - kFastH;
+      if (t < np) {
+        const int p = d.pair_p[t];
         const int cidx = i + d.loff[p];
         if (i < n && cidx >= 0 && cidx < n) v = __ldg(&L[p * n + cidx]);
       }
-      s_lrow[p][r] = v;
+      s_prow[t][r] = v;
     }
   }
   __syncthreads();
@@ -216,22 +222,22 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_fast_kernel(big::Common c, D
       if (in) hcol[q] = cconj(__ldg(&hnh[q * n + cidx]));
     }
   }
-  float2 lcol[kFastL];
-  int jl[kFastL];
+  float2 pcol[kFastP];
+  int jp[kFastP];
 #pragma unroll
-  for (int s = 0; s < kFastL; ++s) {
-    lcol[s] = make_float2(0.f, 0.f);
-    jl[s] = j;
-    if (s < nl) {
+  for (int t = 0; t < kFastP; ++t) {
+    pcol[t] = make_float2(0.f, 0.f);
+    jp[t] = j;
+    if (t < np) {
+      const int s = d.pair_s[t];
       const int cidx = j + d.loff[s];
       const bool in = cidx >= 0 && cidx < n;
-      jl[s] = in ? cidx : j;
-      if (in) lcol[s] = cconj(__ldg(&L[s * n + cidx]));
+      jp[t] = in ? cidx : j;
+      if (in) pcol[t] = cconj(__ldg(&L[s * n + cidx]));
     }
   }
 
   const int rows = min(R, n - i0);
-#pragma unroll 2
   for (int r = 0; r < rows; ++r) {
     const int i = i0 + r;
     const float2* Xi = X + (long long)i * n;
@@ -246,17 +252,11 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_fast_kernel(big::Common c, D
       }
     }
 #pragma unroll
-    for (int p = 0; p < kFastL; ++p) {
-      if (p < nl) {
-        const int k = d.ljump[p];
-        int ci = i + d.loff[p];
+    for (int t = 0; t < kFastP; ++t) {
+      if (t < np) {
+        int ci = i + d.loff[d.pair_p[t]];
         ci = ci < 0 ? 0 : (ci >= n ? n - 1 : ci);
-        const float2 lr = s_lrow[p][r];
-        const float2* Xc = X + (long long)ci * n;
-#pragma unroll
-        for (int s = 0; s < kFastL; ++s) {
-          if (s < nl && d.ljump[s] == k) acc = cfma(cmul(lr, lcol[s]), __ldg(&Xc[jl[s]]), acc);
-        }
+        acc = cfma(cmul(s_prow[t][r], pcol[t]), __ldg(&X[(long long)ci * n + jp[t]]), acc);
       }
     }
     out[(long long)i * n + j] = acc;
@@ -297,8 +297,16 @@ int build_ops(const dqb_dia_problem* p, DiaOps* d) {
     if (k <= -p->n || k >= p->n) return DQB_ERR_INVALID_ARGUMENT;
     offs.insert(k);
   }
+  d->npair = 0;
   for (int k = 0; k < p->n_jumps; ++k)
-    for (int q = d->lstart[k]; q < d->lstart[k + 1]; ++q) d->ljump[q] = k;
+    for (int a = d->lstart[k]; a < d->lstart[k + 1]; ++a)
+      for (int b = d->lstart[k]; b < d->lstart[k + 1]; ++b) {
+        if (d->npair < 64) {
+          d->pair_p[d->npair] = a;
+          d->pair_s[d->npair] = b;
+        }
+        d->npair++;  // counts past 64 too: the fast kernel is then not used
+      }
   for (int q = 0; q < nl; ++q) {
     d->loff[q] = p->l_offsets[q];
     if (d->loff[q] <= -p->n || d->loff[q] >= p->n) return DQB_ERR_INVALID_ARGUMENT;
@@ -355,7 +363,7 @@ int check_problem(const dqb_dia_problem* p) {
   return DQB_OK;
 }
 
-bool fast_ok(const DiaOps& d) { return d.nh <= kFastH && d.nl <= kFastL; }
+bool fast_ok(const DiaOps& d) { return d.nh <= kFastH && d.npair <= kFastP; }
 
 // Rows per thread of the fast stencil: `tile` (4, 8 or 16; 0 = 8), or the generic
 // kernel's 8 when the operators have more diagonals than the fast kernel keeps in registers.

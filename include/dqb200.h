@@ -112,6 +112,11 @@ typedef struct dqb_dense_problem {
   const int32_t* H_index;    /* int32 [batch] or NULL */
   const int32_t* L_index;    /* int32 [batch] or NULL */
   const int32_t* rho0_index; /* int32 [batch] or NULL */
+  const int32_t* start_order; /* int32 [batch] or NULL: a permutation of 0..batch-1, the
+                                 order in which the n <= 64 kernel starts instances (e.g.
+                                 stiffest first, so that short solves fill the tail);
+                                 entries outside [0, batch) are skipped.  Results do not
+                                 depend on it. */
 } dqb_dense_problem;
 
 /* Scratch bytes needed by dqb_mesolve_dense on the current device. */

@@ -206,3 +206,26 @@ def test_capi_rejects_bad_arguments(cuda_device):
     assert lib.dqb_mesolve_dense(None, opts, outs, None, 0, None) == _lib.DQB_ERR_INVALID_ARGUMENT
     assert lib.dqb_dense_small_max_n(2) == 64
     assert lib.dqb_mesolve_dense_workspace_size(64, 2, 4096) > 0
+
+
+def test_start_order_changes_no_result(cuda_device):
+    """With more instances than resident CTAs the host starts the stiffest first
+    (start_order); every result is bitwise the one of the natural order."""
+    from dynamiqs_b200.mesolve import MESolveB200Integrator, make_batch_plan
+
+    w = workloads.batched_kerr(batch=400, n=16, seed=2)
+    ts = np.linspace(0.0, 1.0, 5)
+    plan = make_batch_plan(w['H'], w['jump_ops'], w['rho0'], True)
+    integ = MESolveB200Integrator(ts=ts, y0=w['rho0'], method=w['method'], gradient=None,
+                                  options=dq.Options(), H=w['H'], Ls=w['jump_ops'],
+                                  Es=w['exp_ops'], plan=plan)
+    prep = integ.prepare()
+    assert prep.prob.start_order
+    order = prep.bufs['start_order'].cpu().numpy()
+    assert sorted(order.tolist()) == list(range(400)) and order.tolist() != list(range(400))
+    a = prep.launch().result()
+    sa, ia = a.states.cpu().numpy().copy(), a.infos.nsteps.cpu().numpy().copy()
+    prep.prob.start_order = None
+    b = prep.launch().result()
+    assert np.array_equal(sa, b.states.cpu().numpy())
+    assert np.array_equal(ia, b.infos.nsteps.cpu().numpy())

@@ -10,7 +10,8 @@ signature, batch bucket, form).  Later solves with the same key reuse the choice
 
 Choices tuned:
 
-* sparse DIA (``dqb_mesolve_dia``): rows per thread of the stencil, 4, 8 or 16
+* sparse DIA (``dqb_mesolve_dia``): the stencil kernel and its rows per thread -- the
+  generic kernel, or the register-blocked one with 4, 8 or 16 rows per thread
   (``dqb_ode_options.tile``).
 * dense GEMM path (n > 64) with ``Options(precision='auto')``: FP32 CUDA-core products or
   3xTF32 tensor-core products, the two arithmetic modes that meet the 1e-5 relative error
@@ -18,7 +19,8 @@ Choices tuned:
 
 The cache lives in memory and in a JSON file, ``$DQB_AUTOTUNE_CACHE`` or
 ``~/.cache/dynamiqs_b200/autotune.json`` (not written when the location is read-only).
-``DQB_AUTOTUNE=0`` turns tuning off: every choice is then its default (8 rows, FP32).
+``DQB_AUTOTUNE=0`` turns tuning off: every choice is then its default (generic DIA
+stencil, FP32 products).
 """
 
 from __future__ import annotations

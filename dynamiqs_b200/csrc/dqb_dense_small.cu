@@ -124,10 +124,22 @@ __device__ __forceinline__ void gemm(float2 (&acc)[NP / 16][NP / 16], const floa
     for (int r = 0; r < R; ++r) a[r] = CA ? cconj(A[k * LD + ty + 16 * r]) : A[(ty + 16 * r) * LD + k];
 #pragma unroll
     for (int c = 0; c < R; ++c) b[c] = CB ? cconj(B[(tx + 16 * c) * LD + k]) : B[k * LD + tx + 16 * c];
+    // the two FMAs of a real or imaginary part that depend on each other are R*R
+    // instructions apart
 #pragma unroll
     for (int r = 0; r < R; ++r)
 #pragma unroll
-      for (int c = 0; c < R; ++c) cmac(acc[r][c], a[r], b[c]);
+      for (int c = 0; c < R; ++c) {
+        acc[r][c].x = fmaf(a[r].x, b[c].x, acc[r][c].x);
+        acc[r][c].y = fmaf(a[r].x, b[c].y, acc[r][c].y);
+      }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int c = 0; c < R; ++c) {
+        acc[r][c].x = fmaf(-a[r].y, b[c].y, acc[r][c].x);
+        acc[r][c].y = fmaf(a[r].y, b[c].x, acc[r][c].y);
+      }
   }
 }
 
@@ -509,7 +521,7 @@ __device__ void solve_one(const InstView& a, const CtrlOpts& o, float2* sH, floa
 }
 
 template <int NP>
-__global__ void __launch_bounds__(kSmallThreads) mesolve_small_kernel(DenseSmallArgs a) {
+__global__ void __launch_bounds__(kSmallThreads, NP == 64 ? 1 : (NP == 32 ? 3 : 4)) mesolve_small_kernel(DenseSmallArgs a) {
   extern __shared__ float4 smem_raw[];
   __shared__ double red[40];
   __shared__ Ctrl ctl;
@@ -809,7 +821,7 @@ int small_launch_with_scratch(const dqb_dense_problem* p, const dqb_ode_options*
 namespace dqb {
 
 template <int NP>
-__global__ void __launch_bounds__(kSmallThreads) mesolve_ragged_kernel(const dqb_ragged_instance* __restrict__ d,
+__global__ void __launch_bounds__(kSmallThreads, NP == 64 ? 1 : (NP == 32 ? 3 : 4)) mesolve_ragged_kernel(const dqb_ragged_instance* __restrict__ d,
                                                                        long long count, CtrlOpts o, float2* slots,
                                                                        unsigned int* counter) {
   extern __shared__ float4 smem_raw[];

@@ -238,6 +238,7 @@ __global__ void __launch_bounds__(kRhsCols, 6) rhs_dia_fast_kernel(big::Common c
   }
 
   const int rows = min(R, n - i0);
+#pragma unroll 2
   for (int r = 0; r < rows; ++r) {
     const int i = i0 + r;
     const float2* Xi = X + (long long)i * n;
@@ -365,30 +366,34 @@ int check_problem(const dqb_dia_problem* p) {
 
 bool fast_ok(const DiaOps& d) { return d.nh <= kFastH && d.npair <= kFastP; }
 
-// Rows per thread of the fast stencil: `tile` (4, 8 or 16; 0 = 8), or the generic
-// kernel's 8 when the operators have more diagonals than the fast kernel keeps in registers.
+// Launch shape of the stencil from `tile`: 4, 8 or 16 = the fast kernel with that many rows
+// per thread (when the operators fit it); anything else (0 = default, 1) = the generic
+// kernel, which keeps every thread's work in a few registers (full occupancy) and so hides
+// load latency best when the fast kernel's register arrays cost it occupancy.  The
+// autotuner picks among them per problem shape.  Returns the shape code (1 = generic).
 int rows_for(const DiaOps& d, int tile) {
-  if (!fast_ok(d)) return kRhsRows;
-  return (tile == 4 || tile == 16) ? tile : 8;
+  if (!fast_ok(d)) return 1;
+  return (tile == 4 || tile == 8 || tile == 16) ? tile : 1;
 }
 
 dim3 rhs_grid(const DiaOps& d, int rows, int B) {
-  return dim3((d.n + kRhsCols - 1) / kRhsCols, (d.n + rows - 1) / rows, B);
+  const int r = rows == 1 ? kRhsRows : rows;
+  return dim3((d.n + kRhsCols - 1) / kRhsCols, (d.n + r - 1) / r, B);
 }
 
-// One right-hand side of every instance: k[out_k] = f(input), through the fast stencil
-// when the operators fit it.
+// One right-hand side of every instance: k[out_k] = f(input), through the kernel the shape
+// code `rows` selects (rows_for).
 void launch_rhs_dia(cudaStream_t s, const big::Common& c, const DiaOps& d, int B, int rows, int in_sel,
                     int out_k, int need_run, const float2* ext_in, float2* ext_out) {
   const dim3 g = rhs_grid(d, rows, B);
-  if (!fast_ok(d)) {
-    rhs_dia_generic_kernel<<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
-  } else if (rows == 4) {
+  if (rows == 4) {
     rhs_dia_fast_kernel<4><<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
+  } else if (rows == 8) {
+    rhs_dia_fast_kernel<8><<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
   } else if (rows == 16) {
     rhs_dia_fast_kernel<16><<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
   } else {
-    rhs_dia_fast_kernel<8><<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
+    rhs_dia_generic_kernel<<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
   }
 }
 

@@ -80,8 +80,9 @@ typedef struct dqb_ode_options {
   int32_t save_states;     /* 1: state at every tsave; 0: final state only              */
   int32_t check_hermitian; /* 1: flag rho0 that fails isherm(rtol=atol=1e-5)            */
   int32_t precision;       /* DQB_PREC_* (GEMM path only; 0 = FP32)                     */
-  int32_t tile;            /* launch-shape choice, 0 = default: rows per thread of the
-                              sparse-DIA stencil (4, 8 or 16); ignored by other paths    */
+  int32_t tile;            /* launch-shape choice of the sparse-DIA stencil: 4, 8 or 16 =
+                              register-blocked kernel with that many rows per thread;
+                              0 (default) or 1 = generic kernel; ignored by other paths  */
 } dqb_ode_options;
 
 /* Outputs of a batched solve.  nsave = n_tsave if save_states else 1. */
@@ -280,7 +281,8 @@ DQB_API int dqb_mesolve_dia(const dqb_dia_problem* problem, const dqb_ode_option
 DQB_API int dqb_lindblad_rhs_dia(const dqb_dia_problem* problem, int32_t form, const void* rho,
                                  void* out, void* workspace, size_t workspace_bytes, void* stream);
 
-/* Same, with the stencil's launch shape `tile` (rows per thread: 4, 8 or 16; 0 = default),
+/* Same, with the stencil's launch shape `tile` (as dqb_ode_options.tile: 4, 8, 16 or the
+ * generic kernel),
  * as dqb_ode_options.tile selects it for dqb_mesolve_dia; the autotuner times the choices
  * through this entry point. */
 DQB_API int dqb_lindblad_rhs_dia_tiled(const dqb_dia_problem* problem, int32_t form, int32_t tile,

@@ -1,5 +1,6 @@
 """Autotuner cache logic (CPU) and, on a GPU, that every tuned launch shape of the DIA
-stencil gives bitwise the same right-hand side and that the choice is cached."""
+stencil gives the same right-hand side (bitwise among the register-blocked shapes, to
+rounding against the generic kernel) and that the choice is cached."""
 
 import ctypes
 import json
@@ -40,7 +41,7 @@ def test_disabled_returns_default(monkeypatch):
 
 
 @pytest.mark.gpu
-def test_dia_tiles_bitwise_equal_and_cached(cuda_device, tmp_path, monkeypatch):
+def test_dia_tiles_equal_and_cached(cuda_device, tmp_path, monkeypatch):
     import torch
 
     from dynamiqs_b200 import _lib, workloads
@@ -54,7 +55,7 @@ def test_dia_tiles_bitwise_equal_and_cached(cuda_device, tmp_path, monkeypatch):
                                   options=__import__('dynamiqs_b200').Options(), H=w['H'],
                                   Ls=w['jump_ops'], Es=None, plan=plan)
     prep = integ.prepare()
-    assert integ._tuned['tile'] in (4, 8, 16)
+    assert integ._tuned['tile'] in (1, 4, 8, 16)
     assert (tmp_path / 'tune.json').exists()
     lib = _lib.load()
     n = w['H'].diags.shape[-1]
@@ -62,12 +63,15 @@ def test_dia_tiles_bitwise_equal_and_cached(cuda_device, tmp_path, monkeypatch):
     Y = rng.normal(size=(2, n, n)) + 1j * rng.normal(size=(2, n, n))
     rho = torch.from_numpy((Y @ np.conj(np.swapaxes(Y, -1, -2)) / n).astype(np.complex64)).cuda()
     outs = []
-    for tile in (4, 8, 16):
+    for tile in (1, 4, 8, 16):
         out = torch.empty_like(rho)
         _lib.check(lib.dqb_lindblad_rhs_dia_tiled(
             ctypes.byref(prep.prob), _lib.FORM_HERMITIAN, tile, rho.data_ptr(), out.data_ptr(),
             prep.bufs['workspace'].data_ptr(), prep.ws_bytes,
             torch.cuda.current_stream().cuda_stream), 'rhs_dia_tiled')
         outs.append(out.cpu().numpy())
-    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[1], outs[2])
+    # the generic and the register-blocked kernels sum the same terms in different
+    # orders: equal to rounding; the blocked shapes among themselves: bitwise
+    assert np.array_equal(outs[1], outs[2]) and np.array_equal(outs[2], outs[3])
+    assert np.abs(outs[0] - outs[1]).max() <= 1e-6 * np.abs(outs[1]).max()
     autotune.clear_memory_cache()

@@ -31,7 +31,7 @@ constexpr int kElemThreads = 256;
 struct Inst {
   double t, tnext, h, dtnew, t1, h0;
   double acc[3];  // error / starting-step norm accumulators
-  int status, run, keep, save_idx, save_lo, save_hi, herm_bad, pad;
+  int status, run, keep, save_idx, save_lo, save_hi, herm_bad, retired;
   long long nsteps, nacc, nrej;
   int sy, sy1, sk[7];
   // the instance's own problem data and outputs (shared arrays or a ragged descriptor)
@@ -89,6 +89,7 @@ static __global__ void setup_kernel(Common c) {
   Inst& I = c.inst[b];
   if (c.count_dev && b >= *c.count_dev) {  // unused capacity: every kernel skips it
     I.status = kInactive;
+    I.retired = 0;
     I.run = 0;
     I.nts = I.nE = 0;
     I.save_idx = I.save_lo = I.save_hi = 0;
@@ -136,6 +137,7 @@ static __global__ void setup_kernel(Common c) {
   I.keep = 0;
   I.save_idx = I.save_lo = I.save_hi = 0;
   I.herm_bad = 0;
+  I.retired = 0;
   I.nsteps = I.nacc = I.nrej = 0;
   I.sy = 0;
   I.sy1 = 1;
@@ -466,6 +468,35 @@ static __global__ void pre_finalize_kernel(Common c) {
   }
 }
 
+// grid (B), inside the RK loop of ragged launches, after the commit: hands out each
+// instance that finished normally in this iteration (every save written) without waiting
+// for the rest of the batch -- final state (when only it is kept), expectation values,
+// infos, then, after a system-scope fence, the status word, which a serving loop may poll
+// in host-mapped memory.  finalize_kernel later writes the same values again.
+static __global__ void retire_kernel(Common c) {
+  const int b = blockIdx.x;
+  Inst& I = c.inst[b];
+  if (I.retired || I.run || I.status != DQB_INST_OK || I.save_idx < I.nts) return;
+  if (!I.save_states) {
+    const float2* y = slot(c, b, I.sy);
+    for (long long e = threadIdx.x; e < c.nn; e += blockDim.x) I.states[e] = y[e];
+  }
+  for (int e = threadIdx.x; e < I.nE * I.nts; e += blockDim.x) {
+    const double2 v = I.eacc[e];
+    I.expects[e] = make_float2((float)v.x, (float)v.y);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    I.infos[0] = (int)I.nsteps;
+    I.infos[1] = (int)I.nacc;
+    I.infos[2] = (int)I.nrej;
+    __threadfence_system();
+    I.status_out[0] = I.status;
+    I.retired = 1;
+  }
+}
+
 static __global__ void finalize_kernel(Common c) {
   const int b = blockIdx.y;
   Inst& I = c.inst[b];
@@ -481,11 +512,14 @@ static __global__ void finalize_kernel(Common c) {
       const double2 v = I.eacc[e];
       I.expects[e] = make_float2((float)v.x, (float)v.y);
     }
+    __threadfence();
+    __syncthreads();
     if (threadIdx.x == 0) {
-      I.status_out[0] = I.status;
       I.infos[0] = (int)I.nsteps;
       I.infos[1] = (int)I.nacc;
       I.infos[2] = (int)I.nrej;
+      __threadfence_system();
+      I.status_out[0] = I.status;
     }
   }
 }

@@ -776,6 +776,7 @@ static void init_carveouts() {
     prefer_max_shared(big::control_kernel);
     prefer_max_shared(big::save_kernel);
     prefer_max_shared(big::commit_kernel);
+    prefer_max_shared(big::retire_kernel);
     prefer_max_shared(big::pre_finalize_kernel);
     prefer_max_shared(big::finalize_kernel);
     prefer_max_shared(zero_words_kernel);
@@ -823,6 +824,7 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s) {
     big::control_kernel<<<gi, 128, 0, cs>>>(c);
     big::save_kernel<<<ge, T, 0, cs>>>(c, 1);
     big::commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
+    if (c.rag) big::retire_kernel<<<B, 256, 0, cs>>>(c);
   };
   if (host_loop_requested()) {
     if (run_host_loop(body, (int*)(c.iter + 1), s) != cudaSuccess) return DQB_ERR_CUDA;

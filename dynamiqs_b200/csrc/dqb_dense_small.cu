@@ -311,8 +311,9 @@ __device__ void solve_one(const InstView& a, const CtrlOpts& o, float2* sH, floa
   bad = __syncthreads_or(bad);
   if (bad) {
     if (tid == 0) {
-      a.status[0] = DQB_INST_NOT_HERMITIAN;
       a.infos[0] = a.infos[1] = a.infos[2] = 0;
+      __threadfence_system();  // status last: a caller may poll it from the host
+      a.status[0] = DQB_INST_NOT_HERMITIAN;
     }
     return;
   }
@@ -512,11 +513,17 @@ __device__ void solve_one(const InstView& a, const CtrlOpts& o, float2* sH, floa
       if (i < n && j < n) a.states[(long long)i * n + j] = yv[e];
     }
   }
+  // Every output of the instance is written before its status, with a system-scope fence
+  // in between, so that a caller polling the status word in host-mapped memory (the
+  // serving loop) can hand the result out as soon as the word changes.
+  __threadfence();
+  __syncthreads();
   if (tid == 0) {
-    a.status[0] = ctl.status;
     a.infos[0] = (int)ctl.nsteps;
     a.infos[1] = (int)ctl.nacc;
     a.infos[2] = (int)ctl.nrej;
+    __threadfence_system();
+    a.status[0] = ctl.status;
   }
 }
 

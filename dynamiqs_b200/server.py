@@ -17,8 +17,10 @@ Waves run on a pool of CUDA streams, so requests that arrive while others are on
 start right away on another stream and their work overlaps on the device.  Admission is
 bounded by a byte budget for the device memory a wave holds (inputs, outputs and
 scratch), 150 GB by default; a finished wave releases its budget.  Results stay on the
-device (as ``dq.mesolve`` returns them); the server copies back only status and step
-counts.
+device (as ``dq.mesolve`` returns them).  The kernels write each request's step counts and
+then, after a system-scope fence, its status word straight into page-locked host memory;
+the dispatcher hands a request out as soon as its status word appears, without waiting for
+the rest of its wave (a quick request does not wait for a slow one launched with it).
 
 Tickets record submit, launch and completion times, from which :meth:`stats` reports
 solves/s and p50 / p99 latency.
@@ -176,8 +178,10 @@ class MESolveServer:
         # the memory budget is a device arena allocated once; waves and results live in it
         self._dev_buf = torch.empty(self.budget, dtype=torch.uint8, device=self.dev)
         self._dev = _Arena(self.budget)
-        self._host_buf = torch.empty(int(staging_bytes), dtype=torch.uint8, pin_memory=True)
-        self._host = _Arena(int(staging_bytes))
+        staging = int(staging_bytes) // 256 * 256
+        self._host_buf = torch.empty(staging, dtype=torch.uint8, pin_memory=True)
+        self._host_i32 = self._host_buf.numpy().view(np.int32)
+        self._host = _Arena(staging)
         self.max_wave = max_wave
         self.poll_s = poll_s
         # separate stream pools, so that long GEMM-path waves never hold up small requests;
@@ -292,13 +296,34 @@ class MESolveServer:
     def _retire(self) -> bool:
         with self._lock:
             inflight = list(self._inflight)
+        progressed = False
+        for w in inflight:  # requests whose status word is written: hand them out now
+            progressed |= self._retire_early(w)
         done = [w for w in inflight if w.event.query()]
         for w in done:
             self._finish(w)
             with self._lock:
                 self._inflight.remove(w)
                 self._free_streams[w.kind].append(w.stream)
-        return bool(done)
+        return bool(done) or progressed
+
+    def _retire_early(self, w: _Wave) -> bool:
+        """Finish the tickets of a running wave whose status word the kernel has written
+        (it writes it last, after the request's outputs and a system-scope fence), without
+        waiting for the rest of the wave."""
+        if not w.pending:
+            return False
+        words = self._host_i32[w.status_words]
+        ready = np.nonzero(words != -1)[0]
+        if ready.size == 0:
+            return False
+        keep = np.ones(len(w.pending), bool)
+        keep[ready] = False
+        for i in ready:
+            self._finish_ticket(w, w.pending[i])
+        w.pending = [t for t, k in zip(w.pending, keep) if k]
+        w.status_words = w.status_words[keep]
+        return True
 
     def _admit(self) -> bool:
         launched = False
@@ -458,6 +483,7 @@ class MESolveServer:
             return None
 
         dev_base = self._dev_buf.data_ptr()
+        host_base = self._host_buf.data_ptr()
         host_np = self._host_buf.numpy()
         now = time.perf_counter()
         outputs, infos_host = {}, {}
@@ -473,6 +499,7 @@ class MESolveServer:
                  maxE, maxT) in plans:
                 sv = host_np[h_in:h_in + in_bytes]
                 base_in = dev_base + d_in
+                host_in = host_base + h_in
                 descs = (_lib.RaggedInstance * len(group))()
                 for i, t in enumerate(group):
                     ent = layout[i]
@@ -500,11 +527,15 @@ class MESolveServer:
                     d.H, d.L = base_in + ent['H'], base_in + ent['L']
                     d.rho0, d.E, d.tsave = base_in + ent['rho0'], base_in + ent['E'], base_in + ent['tsave']
                     d.states, d.expects = dev_base + o, dev_base + o + sb
-                    d.infos = base_in + info_off + 16 * i
-                    d.status = base_in + info_off + 16 * i + 12
+                    # step counts and status go straight to page-locked host memory, which
+                    # the device reaches through unified addressing: the dispatcher polls
+                    # the status word and hands a result out as soon as it is written
+                    d.infos = host_in + info_off + 16 * i
+                    d.status = host_in + info_off + 16 * i + 12
                     t.t_launch = now
                 raw = np.frombuffer(bytes(descs), dtype=np.uint8)
                 sv[desc_off:desc_off + raw.size] = raw
+                sv[info_off:info_off + 16 * len(group)].view(np.int32).reshape(-1, 4)[:, 3] = -1
                 count = len(group)
                 if key[0] == 'large':  # descriptors and live count go to the stream's slot
                     sv[info_off:info_off + 4] = np.array([count], np.int32).view(np.uint8)
@@ -531,10 +562,6 @@ class MESolveServer:
                     _lib.check(rc, 'dqb_mesolve_dense_large_ragged')
                 mark('launch', t1)
                 t1 = time.perf_counter()
-                # status and step counts back to the staging buffer, on this stream
-                self._host_buf[h_in + info_off:h_in + info_off + 16 * count].copy_(
-                    self._dev_buf[d_in + info_off:d_in + info_off + 16 * count], non_blocking=True)
-                mark('d2h', t1)
                 for i, t in enumerate(group):
                     o, nb, sb = outs_held[t.id]
                     nE = len(t.Es) if t.Es else 0
@@ -552,6 +579,8 @@ class MESolveServer:
         t1 = time.perf_counter()
         w = _Wave(key[0], tickets, stream, ev, held, 0, outputs)
         w.infos_host = infos_host
+        w.pending = list(tickets)
+        w.status_words = np.array([(infos_host[t.id] + 12) // 4 for t in tickets], np.int64)
         mark('exit', t1)
         self.launch_profile.append((key, prof))
         return w
@@ -613,31 +642,37 @@ class MESolveServer:
             for t in done:
                 self.finished.remove(t)
 
-    def _finish(self, w: _Wave) -> None:
+    def _finish_ticket(self, w: _Wave, t: Ticket) -> None:
         torch = self._torch
-        now = time.perf_counter()
-        host = self._host_buf.numpy()
-        for t in w.tickets:
-            st, ex = w.outputs[t.id]
-            o = w.infos_host[t.id]
-            nsteps, nacc, nrej, status = host[o:o + 16].view(np.int32).tolist()
-            t.t_done = now
-            if status == _lib.INST_MAX_STEPS:
-                t._error = RuntimeError(_MAX_STEPS_MSG)
-            elif status == _lib.INST_NONFINITE:
-                t._error = RuntimeError('The solution became non-finite (NaN or inf) during '
-                                        'the integration.')
-            elif status == _lib.INST_NOT_HERMITIAN:
-                t._error = RuntimeError('Argument y0 is not hermitian.')
-            if t._error is not None:
-                t.release()
-            else:
-                t._result = MESolveResult(
-                    tsave=t.tsave, method=t.method, gradient=None, options=t.options,
-                    states=st, expects=ex,
-                    infos=AdaptiveStepInfos(torch.tensor(nsteps), torch.tensor(nacc),
-                                            torch.tensor(nrej)))
-            self.finished.append(t)
-            t._event.set()
+        st, ex = w.outputs[t.id]
+        o = w.infos_host[t.id]
+        # status first, then the step counts (written before it on the device)
+        status = int(self._host_i32[(o + 12) // 4])
+        nsteps, nacc, nrej = (int(v) for v in self._host_i32[o // 4:o // 4 + 3])
+        t.t_done = time.perf_counter()
+        if status == _lib.INST_MAX_STEPS:
+            t._error = RuntimeError(_MAX_STEPS_MSG)
+        elif status == _lib.INST_NONFINITE:
+            t._error = RuntimeError('The solution became non-finite (NaN or inf) during '
+                                    'the integration.')
+        elif status == _lib.INST_NOT_HERMITIAN:
+            t._error = RuntimeError('Argument y0 is not hermitian.')
+        elif status != _lib.INST_OK:
+            t._error = RuntimeError(f'request ended with status {status}')
+        if t._error is not None:
+            t.release()
+        else:
+            t._result = MESolveResult(
+                tsave=t.tsave, method=t.method, gradient=None, options=t.options,
+                states=st, expects=ex,
+                infos=AdaptiveStepInfos(torch.tensor(nsteps), torch.tensor(nacc),
+                                        torch.tensor(nrej)))
+        self.finished.append(t)
+        t._event.set()
+
+    def _finish(self, w: _Wave) -> None:
+        for t in w.pending:  # the whole wave is done: every status word is final
+            self._finish_ticket(w, t)
+        w.pending = []
         for arena, off, nb in w.keep:
             arena.release(off, nb)

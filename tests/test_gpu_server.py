@@ -76,3 +76,32 @@ def test_budget_admission_and_errors(cuda_device):
         bad.result(timeout=120)
     srv.close()
     assert srv._dev.used() == 0  # every wave and every released result gave its memory back
+
+
+def test_quick_request_leaves_before_slow_one_of_its_wave(cuda_device):
+    """A quick and a slow request launched in the same GEMM-path wave: the quick one is
+    handed out when its own status word is written, long before the wave ends, and both
+    results equal the request solved alone."""
+    from dynamiqs_b200 import operators as ops
+
+    n = 80
+
+    def kerr(kerr_, t_end):
+        H = workloads.kerr_hamiltonians(n, [0.3], [kerr_], [1.0])[0]
+        a = ops.destroy(n, layout='dense')
+        return dict(H=H, jump_ops=[np.float32(np.sqrt(0.1)) * a], rho0=ops.fock(n, 0),
+                    tsave=np.linspace(0.0, t_end, 5), method=dq.Tsit5(rtol=1e-6, atol=1e-6))
+
+    blocker, quick, slow = kerr(0.1, 0.5), kerr(0.1, 0.05), kerr(0.5, 8.0)
+    srv = MESolveServer(n_streams=2)  # one stream per class: quick and slow share a wave
+    sub = [srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'], method=r['method'])
+           for r in (blocker, quick, slow)]
+    res = [t.result(timeout=600) for t in sub]
+    srv.close()
+    t_b, t_q, t_s = sub
+    assert t_q.t_launch == t_s.t_launch  # the same wave
+    assert t_s.t_done - t_q.t_done > 0.05, (t_q.t_done, t_s.t_done)
+    for r, got in zip((quick, slow), res[1:]):
+        alone = dq.mesolve(r['H'], r['jump_ops'], r['rho0'], r['tsave'], method=r['method'])
+        assert _rel(got.states.cpu().numpy(), alone.states.cpu().numpy()) < 1e-5
+        assert int(got.infos.nsteps) == int(alone.infos.nsteps)

@@ -143,6 +143,44 @@ __device__ __forceinline__ void gemm(float2 (&acc)[NP / 16][NP / 16], const floa
   }
 }
 
+// The hermitian product S = T L^+ (T = L X with X hermitian, so S = L X L^+ is hermitian)
+// computed on the tile pairs r >= c only: acc[r][r] += S blocks on the diagonal,
+// low[r (r - 1) / 2 + c] += S blocks strictly below it.  The strictly-upper blocks are
+// conj(S^T) of these, so the right-hand side only needs S on and below the diagonal blocks:
+// (R + 1) R / 2 of the R^2 block pairs (10 of 16 at NP = 64).
+template <int NP>
+__device__ __forceinline__ void gemm_herm(float2 (&acc)[NP / 16][NP / 16],
+                                          float2 (&low)[(NP / 16) * (NP / 16 - 1) / 2 + 1],
+                                          const float2* __restrict__ A, const float2* __restrict__ B,
+                                          int kn) {
+  constexpr int R = NP / 16, LD = NP + 1;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll 4
+  for (int k = 0; k < kn; ++k) {
+    float2 a[R], b[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) a[r] = A[(ty + 16 * r) * LD + k];
+#pragma unroll
+    for (int c = 0; c < R; ++c) b[c] = cconj(B[(tx + 16 * c) * LD + k]);
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int c = 0; c <= r; ++c) {
+        float2& d = r == c ? acc[r][r] : low[r * (r - 1) / 2 + c];
+        d.x = fmaf(a[r].x, b[c].x, d.x);
+        d.y = fmaf(a[r].x, b[c].y, d.y);
+      }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int c = 0; c <= r; ++c) {
+        float2& d = r == c ? acc[r][r] : low[r * (r - 1) / 2 + c];
+        d.x = fmaf(-a[r].y, b[c].y, d.x);
+        d.y = fmaf(a[r].y, b[c].x, d.y);
+      }
+  }
+}
+
 template <int NP>
 __device__ __forceinline__ void zero_tile(float2 (&t)[NP / 16][NP / 16]) {
 #pragma unroll
@@ -198,16 +236,36 @@ __device__ void rhs(const float2* sH, const float2* sL, const float2* sX, float2
   zero_tile<NP>(acc);
   gemm<NP, false, false>(acc, sH, sX, n);
   if (form == DQB_FORM_STANDARD) gemm<NP, false, true>(acc, sX, sH, n);
-  const float sc = form == DQB_FORM_HERMITIAN ? 0.5f : 1.0f;
+  const bool hermf = form == DQB_FORM_HERMITIAN;
+  constexpr int R = NP / 16, NLOW = R * (R - 1) / 2 + 1;
+  float2 low[NLOW];
+#pragma unroll
+  for (int q = 0; q < NLOW; ++q) low[q] = make_float2(0.f, 0.f);
   for (int k = 0; k < K; ++k) {
     const float2* Lk = sL + k * Small<NP>::MAT;
     float2 t[NP / 16][NP / 16];
     zero_tile<NP>(t);
     gemm<NP, false, false>(t, Lk, sX, n);
     __syncthreads();  // readers of the previous T are done
-    store_tile<NP>(sT, t, sc);
+    store_tile<NP>(sT, t, hermf ? 0.5f : 1.0f);
     __syncthreads();
-    gemm<NP, false, true>(acc, sT, Lk, n);
+    if (hermf)
+      gemm_herm<NP>(acc, low, sT, Lk, n);
+    else
+      gemm<NP, false, true>(acc, sT, Lk, n);
+  }
+  if (hermf) {
+    // tmp = Hnh X + 1/2 S with S's strictly-upper blocks left out and its strictly-lower
+    // blocks doubled: tmp + tmp^+ is then Hnh X + (Hnh X)^+ + S, the reference's
+    // hermitian form (S hermitian), from 10 of the 16 block products of T L^+
+#pragma unroll
+    for (int r = 1; r < R; ++r)
+#pragma unroll
+      for (int c = 0; c < r; ++c) {
+        const float2 v = low[r * (r - 1) / 2 + c];
+        acc[r][c].x = fmaf(2.f, v.x, acc[r][c].x);
+        acc[r][c].y = fmaf(2.f, v.y, acc[r][c].y);
+      }
   }
   __syncthreads();
   store_tile<NP>(sT, acc, 1.0f);

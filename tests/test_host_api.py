@@ -100,3 +100,20 @@ def test_operator_constructors_match_reference_examples():
     np.testing.assert_allclose(ops.position(3).to_dense(),
                                [[0, .5, 0], [.5, 0, .70710678], [0, .70710678, 0]], atol=1e-6)
     np.testing.assert_allclose(ops.displace(4, 0.5)[:, 0], [0.882, 0.441, 0.156, 0.047], atol=1e-3)
+
+
+def test_start_order_is_stiffest_first_permutation():
+    """The host's start order for the persistent kernel: a permutation of the instances,
+    largest stiffness bound (row-sum norm of H plus 1/2 sum ||L||^2) first."""
+    from dynamiqs_b200 import workloads
+    from dynamiqs_b200.mesolve import MESolveB200Integrator
+
+    w = workloads.batched_kerr(batch=300, n=16, seed=4)
+    plan = make_batch_plan(w['H'], w['jump_ops'], w['rho0'], True)
+    integ = MESolveB200Integrator(ts=w['tsave'], y0=w['rho0'], method=w['method'], gradient=None,
+                                  options=dq.Options(), H=w['H'], Ls=w['jump_ops'], Es=None,
+                                  plan=plan)
+    order = integ._start_order()
+    assert order.dtype == np.int32 and sorted(order.tolist()) == list(range(300))
+    h = np.abs(w['H']).sum(-1).max(-1)
+    assert np.all(np.diff(h[order]) <= 1e-6)  # the jump operators are shared: H decides

@@ -424,10 +424,12 @@ def run_b200(args):
             roof['note'] = ('products run on the FP32 CUDA-core pipe (SIMT), not the tensor '
                             'pipe; see roofline_fp32_simt')
             if n <= 64 and K > 0:
+                R = (16 if n <= 16 else (32 if n <= 32 else 64)) // 16
+                part = (R + 1) * R / 2 / (R * R)
                 roof['note'] += ('. Algorithmic flops count (1+2K) complex products per RHS; '
-                                 'the hermitian form computes (L X) L^+ on 10 of 16 tile '
-                                 f'pairs, so the kernel executes {(1 + K + K * 10 / 16) / (1 + 2 * K):.3f}'
-                                 ' of them')
+                                 f'the hermitian form computes (L X) L^+ on {part:.3f} of the '
+                                 'tile pairs, so the kernel executes '
+                                 f'{(1 + K + K * part) / (1 + 2 * K):.3f} of them')
         else:
             roof['note'] = (f'products run on tcgen05 tensor cores ({args.precision}: three '
                             'products per complex MAC term, so the tensor pipe executes 3x the '

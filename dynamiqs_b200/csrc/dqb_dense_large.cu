@@ -397,17 +397,37 @@ __device__ __forceinline__ void tc_store_stage(const float4 (&v)[BF16 ? 16 : 8],
     const uint32_t r0 = 2 * r, r1 = 2 * r + 1;
     const uint32_t ob0 = r0 * 128 + ((cc ^ (r0 & 7)) << 4);
     const uint32_t ob1 = r1 * 128 + ((cc ^ (r1 & 7)) << 4);
+    // The (-Im, Re) row of M is the (Re, Im) row's split with its pairs swapped and the
+    // first element negated: the hi/lo split commutes with negation, so each value of M is
+    // split once.
     if (!BF16) {
       const float4 a = v[q], m = v[4 + q];
       st_split_tf32(Ahi + oa, Alo + oa, a, SPLIT);
-      st_split_tf32(Bhi + ob0, Blo + ob0, m, SPLIT);
-      st_split_tf32(Bhi + ob1, Blo + ob1, make_float4(-m.y, m.x, -m.w, m.z), SPLIT);
+      float h0, h1, h2, h3, l0, l1, l2, l3;
+      tc::split_tf32(m.x, h0, l0);
+      tc::split_tf32(m.y, h1, l1);
+      tc::split_tf32(m.z, h2, l2);
+      tc::split_tf32(m.w, h3, l3);
+      st_shared_v4(Bhi + ob0, __float_as_uint(h0), __float_as_uint(h1), __float_as_uint(h2), __float_as_uint(h3));
+      st_shared_v4(Bhi + ob1, __float_as_uint(-h1), __float_as_uint(h0), __float_as_uint(-h3), __float_as_uint(h2));
+      if (SPLIT) {
+        st_shared_v4(Blo + ob0, __float_as_uint(l0), __float_as_uint(l1), __float_as_uint(l2), __float_as_uint(l3));
+        st_shared_v4(Blo + ob1, __float_as_uint(-l1), __float_as_uint(l0), __float_as_uint(-l3), __float_as_uint(l2));
+      }
     } else {
       const float4 a0 = v[2 * q], a1 = v[2 * q + 1], m0 = v[8 + 2 * q], m1 = v[8 + 2 * q + 1];
       st_split_bf16(Ahi + oa, Alo + oa, a0, a1);
-      st_split_bf16(Bhi + ob0, Blo + ob0, m0, m1);
-      st_split_bf16(Bhi + ob1, Blo + ob1, make_float4(-m0.y, m0.x, -m0.w, m0.z),
-                    make_float4(-m1.y, m1.x, -m1.w, m1.z));
+      uint32_t l0, l1, l2, l3;
+      const uint32_t h0 = pack_bf16(m0.x, m0.y, l0);
+      const uint32_t h1 = pack_bf16(m0.z, m0.w, l1);
+      const uint32_t h2 = pack_bf16(m1.x, m1.y, l2);
+      const uint32_t h3 = pack_bf16(m1.z, m1.w, l3);
+      st_shared_v4(Bhi + ob0, h0, h1, h2, h3);
+      st_shared_v4(Blo + ob0, l0, l1, l2, l3);
+      // (re, im) in the low / high halves -> (-im, re)
+      auto rot = [](uint32_t x) { return ((x >> 16) ^ 0x8000u) | (x << 16); };
+      st_shared_v4(Bhi + ob1, rot(h0), rot(h1), rot(h2), rot(h3));
+      st_shared_v4(Blo + ob1, rot(l0), rot(l1), rot(l2), rot(l3));
     }
   }
 }
@@ -483,24 +503,32 @@ __global__ void __launch_bounds__(tcg::kThreads, 1)
 
   if (warp < tcg::kProdWarps) {
     // ---- producers ----
+    // Global loads run PRE stages ahead of the shared-memory stores (two for TF32, whose
+    // stage fits twice more in registers; one for BF16).
+    constexpr int PRE = kBf16 ? 1 : 2;
     const int ptid = threadIdx.x;
-    float4 cur[NV], nxt[NV];
-    if (total > 0) tc_load_stage<kBf16>(cur, Ap[0], Mp[0], n, row0, col0, 0, ptid);
+    float4 buf[PRE + 1][NV];
+#pragma unroll
+    for (int p = 0; p < PRE; ++p)
+      if (p < total)
+        tc_load_stage<kBf16>(buf[p], Ap[p / kchunks], Mp[p / kchunks], n, row0, col0, (p % kchunks) * KC, ptid);
     for (int it = 0; it < total; ++it) {
       const int s = it % tcg::kStages;
-      if (it + 1 < total) {
-        const int term = (it + 1) / kchunks;
-        tc_load_stage<kBf16>(nxt, Ap[term], Mp[term], n, row0, col0, ((it + 1) % kchunks) * KC, ptid);
+      if (it + PRE < total) {
+        const int term = (it + PRE) / kchunks;
+        tc_load_stage<kBf16>(buf[PRE], Ap[term], Mp[term], n, row0, col0, ((it + PRE) % kchunks) * KC, ptid);
       }
       if (it >= tcg::kStages && !tc::mbar_wait(bar_empty + 8 * s, ((it / tcg::kStages) - 1) & 1)) {
         fail_sh = 1;
         break;
       }
-      tc_store_stage<kBf16, kSplit>(cur, sbase + s * tcg::kStage, ptid);
+      tc_store_stage<kBf16, kSplit>(buf[0], sbase + s * tcg::kStage, ptid);
       tc::fence_proxy_async_smem();
       tc::mbar_arrive(bar_full + 8 * s);
 #pragma unroll
-      for (int i = 0; i < NV; ++i) cur[i] = nxt[i];
+      for (int p = 0; p < PRE; ++p)
+#pragma unroll
+        for (int i = 0; i < NV; ++i) buf[p][i] = buf[p + 1][i];
     }
   } else if (lane == 0) {
     // ---- MMA issuer ----

@@ -148,24 +148,30 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_generic_kernel(big::Common c
   }
 }
 
-// Fast f(X) for up to kFastH Hnh diagonals and kFastP (p, s) jump-diagonal pairs.
-// grid (n / 128, n / R, B), block 128: each thread owns one column j and R consecutive
-// rows.  Everything that depends only on the column (conj(hnh_q[j + k_q]), the column
-// factors conj(l_s[j + q_s]) of the pairs and the clamped column indices) is computed once
-// per thread and kept in registers; everything that depends only on the row (hnh_q[i + k_q],
-// l_p[i + q_p]) once per CTA into shared memory.  Out-of-range diagonal entries become zero
-// coefficients on a clamped (in-bounds) index, so the inner loops have no data-dependent
-// branches: per output element, 2 nh + npair coalesced loads of X and as many complex
-// multiply-adds.
-constexpr int kFastH = 8;
-constexpr int kFastP = 8;
+// Tiled f(X): every coefficient in shared memory, the inner loops over the diagonals read
+// one 16-byte table entry per term.  grid (n / 128, n / R, B), block 128: each thread owns
+// one column j and R consecutive rows.  Per CTA, for the diagonal terms t (the nh diagonals
+// of Hnh, then the npair (p, s) jump-diagonal pairs):
+//   row table  [t][r]:   the row factor (hnh_q[i + k_q] or l_p[i + q_p], 0 outside the
+//                        matrix) and the clamped source row of that term for row i0 + r;
+//   col table  [t][tid]: the column factor (conj(hnh_q[j + k_q]) or conj(l_s[j + q_s])) and
+//                        the clamped source column for this thread's column.
+// Then out[i][j] = sum_q (hrow_q(i) X[ri_q(i)][j] + hcol_q(j) X[i][cj_q(j)])
+//                + sum_pairs prow_t(i) pcol_t(j) X[ri_t(i)][cj_t(j)],
+// the same terms as the generic kernel.  Occupancy stays high (few registers; the tables
+// are (nh + npair) (R + 128) 16 bytes), which the load latency of the shifted reads needs.
+struct __align__(16) DiaCoef {
+  float2 f;  // factor
+  int idx;   // clamped source row (row table) or column (column table)
+  int pad;
+};
+constexpr int kTiledMaxTerms = 20;
 
 template <int R>
-__global__ void __launch_bounds__(kRhsCols, 6) rhs_dia_fast_kernel(big::Common c, DiaOps d, int in_sel, int out_k,
-                                                                   int need_run, const float2* ext_in,
-                                                                   float2* ext_out) {
-  __shared__ float2 s_hrow[kFastH][R];  // hnh_q[i + k_q]       (0 outside the matrix)
-  __shared__ float2 s_prow[kFastP][R];  // l_{p(t)}[i + q_p(t)] (0 outside the matrix)
+__global__ void __launch_bounds__(kRhsCols) rhs_dia_tiled_kernel(big::Common c, DiaOps d, int in_sel, int out_k,
+                                                                int need_run, const float2* ext_in,
+                                                                float2* ext_out) {
+  extern __shared__ DiaCoef dia_tab[];
   const int b = blockIdx.z;
   const float2* X;
   float2* out;
@@ -178,87 +184,75 @@ __global__ void __launch_bounds__(kRhsCols, 6) rhs_dia_fast_kernel(big::Common c
     X = big::slot(c, b, in_sel == 0 ? I.sy : (in_sel == 1 ? I.sy1 : big::kX));
     out = big::slot(c, b, I.sk[out_k]);
   }
-  const int n = d.n, nh = d.nh, np = d.npair;
+  const int n = d.n, nh = d.nh, np = d.npair, nt = nh + np;
   const long long li = d.Lidx ? d.Lidx[b] : b;
   const float2* L = d.L + li * d.nl * n;
   const float2* hnh = d.hnh + (long long)b * nh * n;
   const int i0 = blockIdx.y * R;
+  const int j0 = blockIdx.x * kRhsCols;
+  DiaCoef* rowt = dia_tab;          // [nt][R]
+  DiaCoef* colt = dia_tab + nt * R;  // [nt][kRhsCols]
 
-  // row factors of this CTA's R rows
-  for (int e = threadIdx.x; e < (kFastH + kFastP) * R; e += blockDim.x) {
-    const int q = e / R, r = e % R, i = i0 + r;
-    float2 v = make_float2(0.f, 0.f);
-    if (q < kFastH) {
-      if (q < nh) {
-        const int cidx = i + d.hoff[q];
-        if (i < n && cidx >= 0 && cidx < n) v = __ldg(&hnh[q * n + cidx]);
-      }
-      s_hrow[q][r] = v;
+  for (int e = threadIdx.x; e < nt * R; e += blockDim.x) {
+    const int t = e / R, r = e % R, i = i0 + r;
+    int off;
+    const float2* diag;
+    if (t < nh) {
+      off = d.hoff[t];
+      diag = hnh + t * n;
     } else {
-      const int t = q - kFastH;
-      if (t < np) {
-        const int p = d.pair_p[t];
-        const int cidx = i + d.loff[p];
-        if (i < n && cidx >= 0 && cidx < n) v = __ldg(&L[p * n + cidx]);
+      const int p = d.pair_p[t - nh];
+      off = d.loff[p];
+      diag = L + p * n;
+    }
+    const int src = i + off;
+    const bool in = i < n && src >= 0 && src < n;
+    DiaCoef v;
+    v.f = in ? __ldg(&diag[src]) : make_float2(0.f, 0.f);
+    v.idx = src < 0 ? 0 : (src >= n ? n - 1 : src);
+    v.pad = 0;
+    rowt[e] = v;
+  }
+  {
+    const int j = j0 + threadIdx.x;
+    for (int t = 0; t < nt; ++t) {
+      int off;
+      const float2* diag;
+      if (t < nh) {
+        off = d.hoff[t];
+        diag = hnh + t * n;
+      } else {
+        const int sd = d.pair_s[t - nh];
+        off = d.loff[sd];
+        diag = L + sd * n;
       }
-      s_prow[t][r] = v;
+      const int src = j + off;
+      const bool in = j < n && src >= 0 && src < n;
+      DiaCoef v;
+      v.f = in ? cconj(__ldg(&diag[src])) : make_float2(0.f, 0.f);
+      v.idx = src < 0 ? 0 : (src >= n ? n - 1 : src);
+      v.pad = 0;
+      colt[t * kRhsCols + threadIdx.x] = v;
     }
   }
   __syncthreads();
-  const int j = blockIdx.x * kRhsCols + threadIdx.x;
+  const int j = j0 + threadIdx.x;
   if (j >= n) return;
-
-  // column factors of this thread's column
-  float2 hcol[kFastH];
-  int jh[kFastH];
-#pragma unroll
-  for (int q = 0; q < kFastH; ++q) {
-    hcol[q] = make_float2(0.f, 0.f);
-    jh[q] = j;
-    if (q < nh) {
-      const int cidx = j + d.hoff[q];
-      const bool in = cidx >= 0 && cidx < n;
-      jh[q] = in ? cidx : j;
-      if (in) hcol[q] = cconj(__ldg(&hnh[q * n + cidx]));
-    }
-  }
-  float2 pcol[kFastP];
-  int jp[kFastP];
-#pragma unroll
-  for (int t = 0; t < kFastP; ++t) {
-    pcol[t] = make_float2(0.f, 0.f);
-    jp[t] = j;
-    if (t < np) {
-      const int s = d.pair_s[t];
-      const int cidx = j + d.loff[s];
-      const bool in = cidx >= 0 && cidx < n;
-      jp[t] = in ? cidx : j;
-      if (in) pcol[t] = cconj(__ldg(&L[s * n + cidx]));
-    }
-  }
-
   const int rows = min(R, n - i0);
-#pragma unroll 2
   for (int r = 0; r < rows; ++r) {
     const int i = i0 + r;
     const float2* Xi = X + (long long)i * n;
     float2 acc = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int q = 0; q < kFastH; ++q) {
-      if (q < nh) {
-        int ci = i + d.hoff[q];
-        ci = ci < 0 ? 0 : (ci >= n ? n - 1 : ci);
-        acc = cfma(s_hrow[q][r], __ldg(&X[(long long)ci * n + j]), acc);
-        acc = cfma(hcol[q], __ldg(&Xi[jh[q]]), acc);
-      }
+    for (int q = 0; q < nh; ++q) {
+      const DiaCoef rc = rowt[q * R + r];
+      const DiaCoef cc = colt[q * kRhsCols + threadIdx.x];
+      acc = cfma(rc.f, __ldg(&X[(long long)rc.idx * n + j]), acc);
+      acc = cfma(cc.f, __ldg(&Xi[cc.idx]), acc);
     }
-#pragma unroll
-    for (int t = 0; t < kFastP; ++t) {
-      if (t < np) {
-        int ci = i + d.loff[d.pair_p[t]];
-        ci = ci < 0 ? 0 : (ci >= n ? n - 1 : ci);
-        acc = cfma(cmul(s_prow[t][r], pcol[t]), __ldg(&X[(long long)ci * n + jp[t]]), acc);
-      }
+    for (int t = nh; t < nt; ++t) {
+      const DiaCoef rc = rowt[t * R + r];
+      const DiaCoef cc = colt[t * kRhsCols + threadIdx.x];
+      acc = cfma(cmul(rc.f, cc.f), __ldg(&X[(long long)rc.idx * n + cc.idx]), acc);
     }
     out[(long long)i * n + j] = acc;
   }
@@ -364,13 +358,16 @@ int check_problem(const dqb_dia_problem* p) {
   return DQB_OK;
 }
 
-bool fast_ok(const DiaOps& d) { return d.nh <= kFastH && d.npair <= kFastP; }
+bool fast_ok(const DiaOps& d) { return d.npair <= 64 && d.nh + d.npair <= kTiledMaxTerms; }
 
-// Launch shape of the stencil from `tile`: 4, 8 or 16 = the fast kernel with that many rows
-// per thread (when the operators fit it); anything else (0 = default, 1) = the generic
-// kernel, which keeps every thread's work in a few registers (full occupancy) and so hides
-// load latency best when the fast kernel's register arrays cost it occupancy.  The
-// autotuner picks among them per problem shape.  Returns the shape code (1 = generic).
+size_t tiled_smem(const DiaOps& d, int rows) {
+  return (size_t)(d.nh + d.npair) * (rows + kRhsCols) * sizeof(DiaCoef);
+}
+
+// Launch shape of the stencil from `tile`: 4, 8 or 16 = the tiled kernel with that many rows
+// per thread (when the operators have at most kTiledMaxTerms diagonal terms); anything else
+// (0 = default, 1) = the generic kernel.  The autotuner picks among them per problem shape.
+// Returns the shape code (1 = generic).
 int rows_for(const DiaOps& d, int tile) {
   if (!fast_ok(d)) return 1;
   return (tile == 4 || tile == 8 || tile == 16) ? tile : 1;
@@ -386,12 +383,13 @@ dim3 rhs_grid(const DiaOps& d, int rows, int B) {
 void launch_rhs_dia(cudaStream_t s, const big::Common& c, const DiaOps& d, int B, int rows, int in_sel,
                     int out_k, int need_run, const float2* ext_in, float2* ext_out) {
   const dim3 g = rhs_grid(d, rows, B);
+  const size_t sm = tiled_smem(d, rows);
   if (rows == 4) {
-    rhs_dia_fast_kernel<4><<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
+    rhs_dia_tiled_kernel<4><<<g, kRhsCols, sm, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
   } else if (rows == 8) {
-    rhs_dia_fast_kernel<8><<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
+    rhs_dia_tiled_kernel<8><<<g, kRhsCols, sm, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
   } else if (rows == 16) {
-    rhs_dia_fast_kernel<16><<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
+    rhs_dia_tiled_kernel<16><<<g, kRhsCols, sm, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
   } else {
     rhs_dia_generic_kernel<<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
   }
@@ -428,9 +426,9 @@ static void init_carveouts() {
     prefer_max_shared(zero_words_kernel);
     prefer_max_shared(hnh_dia_kernel);
     prefer_max_shared(rhs_dia_generic_kernel);
-    prefer_max_shared(rhs_dia_fast_kernel<4>);
-    prefer_max_shared(rhs_dia_fast_kernel<8>);
-    prefer_max_shared(rhs_dia_fast_kernel<16>);
+    prefer_max_shared(rhs_dia_tiled_kernel<4>);
+    prefer_max_shared(rhs_dia_tiled_kernel<8>);
+    prefer_max_shared(rhs_dia_tiled_kernel<16>);
   });
 }
 

@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_generic_kernel(big::Common c
 // are (nh + npair) (R + 128) 16 bytes), which the load latency of the shifted reads needs.
 struct __align__(16) DiaCoef {
   float2 f;  // factor
-  int idx;   // clamped source row (row table) or column (column table)
+  int idx;   // clamped source row times n (row table) or clamped source column (column table)
   int pad;
 };
 constexpr int kTiledMaxTerms = 20;
@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_tiled_kernel(big::Common c, 
     const bool in = i < n && src >= 0 && src < n;
     DiaCoef v;
     v.f = in ? __ldg(&diag[src]) : make_float2(0.f, 0.f);
-    v.idx = src < 0 ? 0 : (src >= n ? n - 1 : src);
+    v.idx = (src < 0 ? 0 : (src >= n ? n - 1 : src)) * n;  // element offset of the source row
     v.pad = 0;
     rowt[e] = v;
   }
@@ -243,16 +243,19 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_tiled_kernel(big::Common c, 
     const int i = i0 + r;
     const float2* Xi = X + (long long)i * n;
     float2 acc = make_float2(0.f, 0.f);
+    // unrolled so that several terms' loads are in flight at once
+#pragma unroll 4
     for (int q = 0; q < nh; ++q) {
       const DiaCoef rc = rowt[q * R + r];
       const DiaCoef cc = colt[q * kRhsCols + threadIdx.x];
-      acc = cfma(rc.f, __ldg(&X[(long long)rc.idx * n + j]), acc);
+      acc = cfma(rc.f, __ldg(&X[rc.idx + j]), acc);
       acc = cfma(cc.f, __ldg(&Xi[cc.idx]), acc);
     }
+#pragma unroll 2
     for (int t = nh; t < nt; ++t) {
       const DiaCoef rc = rowt[t * R + r];
       const DiaCoef cc = colt[t * kRhsCols + threadIdx.x];
-      acc = cfma(cmul(rc.f, cc.f), __ldg(&X[(long long)rc.idx * n + cc.idx]), acc);
+      acc = cfma(cmul(rc.f, cc.f), __ldg(&X[rc.idx + cc.idx]), acc);
     }
     out[(long long)i * n + j] = acc;
   }
@@ -358,7 +361,9 @@ int check_problem(const dqb_dia_problem* p) {
   return DQB_OK;
 }
 
-bool fast_ok(const DiaOps& d) { return d.npair <= 64 && d.nh + d.npair <= kTiledMaxTerms; }
+bool fast_ok(const DiaOps& d) {  // row offsets i * n held in int32
+  return d.npair <= 64 && d.nh + d.npair <= kTiledMaxTerms && d.n <= 46340;
+}
 
 size_t tiled_smem(const DiaOps& d, int rows) {
   return (size_t)(d.nh + d.npair) * (rows + kRhsCols) * sizeof(DiaCoef);

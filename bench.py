@@ -553,7 +553,7 @@ def main():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-plain', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--precision', default='fp32', choices=['fp32', 'tf32x3', 'bf16x3', 'tf32'],
+    ap.add_argument('--precision', default='fp32', choices=['fp32', 'tf32x3', 'bf16x3', 'tf32', 'auto'],
                     help='arithmetic of the GEMM path (n > 64) products')
     args = ap.parse_args()
     if args.impl == 'reference':

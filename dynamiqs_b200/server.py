@@ -34,6 +34,7 @@ wait behind an unrelated long wave on the same queue.
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 import threading
 import time
 from collections import deque
@@ -157,6 +158,8 @@ class MESolveServer:
     LARGE_MAX_JUMPS = 8
     LARGE_MAX_EXP = 8
     LARGE_MAX_TSAVE = 1024
+    # precision='auto': GEMM-path waves with at least this many requests use 3xTF32
+    AUTO_TC_MIN_WAVE = 8
 
     def __init__(self, budget_bytes: float = 150e9, max_wave: int = 4096, n_streams: int = 16,
                  poll_s: float = 50e-6, max_large_wave: int = 64, staging_bytes: float = 2e9):
@@ -392,7 +395,20 @@ class MESolveServer:
             t._event.set()
 
     # ---- waves --------------------------------------------------------------------------
-    def _ode_options(self, t: Ticket) -> _lib.OdeOptions:
+    def _precision_of(self, t: Ticket, form: int, count: int) -> int:
+        """GEMM-path arithmetic of a wave.  ``precision='auto'``: 3xTF32 tensor cores for
+        waves of at least AUTO_TC_MIN_WAVE requests, FP32 CUDA cores for smaller ones, whose
+        few 128x128 tensor-core tiles per product would leave most SMs idle (the FP32 path's
+        64x64 tiles give 4x more CTAs per instance): a lone stiff request then steps faster."""
+        o = t.options
+        if t.n <= 64:
+            return _lib.PREC_FP32
+        if o.precision == 'auto':
+            ok = form == _lib.FORM_HERMITIAN and t.n % 2 == 0 and count >= self.AUTO_TC_MIN_WAVE
+            return _lib.PREC_TF32X3 if ok else _lib.PREC_FP32
+        return _precision_code(o, form)
+
+    def _ode_options(self, t: Ticket, count: int = 1) -> _lib.OdeOptions:
         m, o = t.method, t.options
         form = (_lib.FORM_STANDARD if (o.vectorized or not o.assume_hermitian)
                 else _lib.FORM_HERMITIAN)
@@ -402,7 +418,7 @@ class MESolveServer:
             factormin=float(m.min_factor), factormax=float(m.max_factor),
             max_steps=int(m.max_steps), t0=0.0, save_states=1,
             check_hermitian=int(bool(o.assume_hermitian)),
-            precision=_precision_code(o, form) if t.n > 64 else _lib.PREC_FP32)
+            precision=self._precision_of(t, form, count))
 
     def _launch_wave(self, tickets, key, stream) -> _Wave | None:
         """Pack the wave's inputs into pinned staging (one host-to-device copy), give every
@@ -543,7 +559,7 @@ class MESolveServer:
                 self._dev_buf[d_in:d_in + in_bytes].copy_(self._host_buf[h_in:h_in + in_bytes],
                                                          non_blocking=True)
                 mark('h2d', t1)
-                opts = self._ode_options(group[0])
+                opts = self._ode_options(group[0], len(group))
                 t1 = time.perf_counter()
                 if key[0] == 'small':
                     rc = self.lib.dqb_mesolve_ragged(base_in + desc_off, count, key[1], maxK, opts,
@@ -625,15 +641,18 @@ class MESolveServer:
         instantiation can wait for the conditional graphs already running on the device,
         holding up every stream meanwhile."""
         torch = self._torch
-        plan = [(n, len(self._free_streams['small'])) for n in (8, 24, 48)]
-        plan += [(n, len(self._free_streams['large'])) for n in large_dims]
+        # 'auto' serves large waves in either arithmetic: capture both
+        large_opts = ([dataclasses.replace(options, precision=p) for p in ('fp32', 'tf32x3')]
+                      if options.precision == 'auto' else [options])
+        plan = [(n, len(self._free_streams['small']), Options()) for n in (8, 24, 48)]
+        plan += [(n, len(self._free_streams['large']), o) for n in large_dims for o in large_opts]
         done = []
-        for n, reps in plan:
+        for n, reps, opt in plan:
             a = np.diag(np.sqrt(np.arange(1, n)), 1).astype(np.complex64)
             for _ in range(reps):
                 t = self.submit(np.zeros((n, n), np.complex64), [a],
                                 np.eye(n, 1, dtype=np.complex64), [0.0, 0.1], method=method,
-                                options=options if n > 64 else Options())
+                                options=opt)
                 t.result()
                 t.release()
                 done.append(t)

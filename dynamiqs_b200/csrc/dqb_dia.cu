@@ -261,6 +261,127 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_tiled_kernel(big::Common c, 
   }
 }
 
+// Staged f(X): the few groups of rows of X that the diagonals touch, with their column
+// halos, are copied into shared memory once per CTA; every term then reads shared memory.
+// Every read of the stencil is X[i + ro][j + co] for a (row offset, column offset) pair of
+// its term: (k_q, 0) for the row term of Hnh diagonal q, (0, k_q) for its column term, and
+// (q_p, q_s) for a jump-diagonal pair.  The host groups the distinct row offsets that lie
+// within R of each other (DiaStage): group g stages rows i0 + rlo_g .. i0 + R - 1 + rhi_g and
+// columns j0 + clo_g .. j0 + 127 + chi_g of X (zeros outside the matrix).  For the coupled
+// Kerr operators (row offsets -64, -63, 0, 1, 63, 64) that is three groups of R + 1 rows, so
+// each element of X leaves L2 about 5 times per right-hand side instead of ~12.
+constexpr int kStageMaxGroups = 8;
+constexpr int kStageMaxTerms = 24;
+constexpr size_t kStageMaxSmem = 200 * 1024;  // dynamic shared memory of one CTA
+
+struct DiaStage {
+  int ngroup;
+  int g_rlo[kStageMaxGroups];   // smallest row offset of the group
+  int g_rows[kStageMaxGroups];  // staged rows: R + (rhi - rlo)
+  int g_clo[kStageMaxGroups];   // smallest column offset of the group's reads
+  int g_cols[kStageMaxGroups];  // staged columns: 128 + (chi - clo)
+  int g_off[kStageMaxGroups];   // start of the group in the staged array (complex values)
+  int n0, n1, n2;               // row terms, column terms, pair terms, in this order
+  int t_diag[kStageMaxTerms];   // Hnh diagonal (row / column terms) or pair index (pairs)
+  int t_base[kStageMaxTerms];   // staged index of (row 0 of the tile, column 0 of the tile)
+  int t_stride[kStageMaxTerms]; // row stride of the term's group
+  int staged;                   // complex values staged per CTA
+};
+
+template <int R>
+__global__ void __launch_bounds__(kRhsCols) rhs_dia_staged_kernel(big::Common c, DiaOps d, DiaStage st, int in_sel,
+                                                                 int out_k, int need_run, const float2* ext_in,
+                                                                 float2* ext_out) {
+  extern __shared__ float4 dia_stage_raw[];
+  const int b = blockIdx.z;
+  const float2* X;
+  float2* out;
+  if (ext_in) {  // stand-alone evaluation (dqb_lindblad_rhs_dia)
+    X = ext_in + (long long)b * d.n * d.n;
+    out = ext_out + (long long)b * d.n * d.n;
+  } else {
+    const big::Inst& I = c.inst[b];
+    if (need_run ? !I.run : I.status != DQB_INST_OK) return;
+    X = big::slot(c, b, in_sel == 0 ? I.sy : (in_sel == 1 ? I.sy1 : big::kX));
+    out = big::slot(c, b, I.sk[out_k]);
+  }
+  const int n = d.n, nt = st.n0 + st.n1 + st.n2, tid = threadIdx.x;
+  const long long li = d.Lidx ? d.Lidx[b] : b;
+  const float2* L = d.L + li * d.nl * n;
+  const float2* hnh = d.hnh + (long long)b * d.nh * n;
+  const int i0 = blockIdx.y * R, j0 = blockIdx.x * kRhsCols;
+  float2* S = reinterpret_cast<float2*>(dia_stage_raw);
+  float2* rowc = S + st.staged;    // [nt][R]
+  float2* colc = rowc + nt * R;    // [nt][128]
+
+  for (int g = 0; g < st.ngroup; ++g) {
+    const int gr0 = i0 + st.g_rlo[g], gc0 = j0 + st.g_clo[g], cols = st.g_cols[g];
+    float2* dst = S + st.g_off[g];
+    for (int rr = 0; rr < st.g_rows[g]; ++rr) {
+      const int gr = gr0 + rr;
+      const bool rin = gr >= 0 && gr < n;
+      const float2* src = X + (long long)(rin ? gr : 0) * n;
+      for (int cc = tid; cc < cols; cc += kRhsCols) {
+        const int gc = gc0 + cc;
+        dst[rr * cols + cc] = (rin && gc >= 0 && gc < n) ? __ldg(&src[gc]) : make_float2(0.f, 0.f);
+      }
+    }
+  }
+  for (int e = tid; e < nt * R; e += kRhsCols) {
+    const int t = e / R, i = i0 + e % R;
+    float2 v = make_float2(0.f, 0.f);
+    if (i < n) {
+      if (t < st.n0) {
+        const int q = st.t_diag[t], src = i + d.hoff[q];
+        if (src >= 0 && src < n) v = __ldg(&hnh[q * n + src]);
+      } else if (t < st.n0 + st.n1) {
+        v = make_float2(1.f, 0.f);
+      } else {
+        const int p = d.pair_p[st.t_diag[t]], src = i + d.loff[p];
+        if (src >= 0 && src < n) v = __ldg(&L[p * n + src]);
+      }
+    }
+    rowc[e] = v;
+  }
+  {
+    const int j = j0 + tid;
+    for (int t = 0; t < nt; ++t) {
+      float2 v = make_float2(0.f, 0.f);
+      if (j < n) {
+        if (t < st.n0) {
+          v = make_float2(1.f, 0.f);
+        } else if (t < st.n0 + st.n1) {
+          const int q = st.t_diag[t], src = j + d.hoff[q];
+          if (src >= 0 && src < n) v = cconj(__ldg(&hnh[q * n + src]));
+        } else {
+          const int sd = d.pair_s[st.t_diag[t]], src = j + d.loff[sd];
+          if (src >= 0 && src < n) v = cconj(__ldg(&L[sd * n + src]));
+        }
+      }
+      colc[t * kRhsCols + tid] = v;
+    }
+  }
+  __syncthreads();
+  const int j = j0 + tid;
+  if (j >= n) return;
+  const int rows = min(R, n - i0);
+  const int e0 = st.n0, e1 = st.n0 + st.n1;
+  for (int r = 0; r < rows; ++r) {
+    float2 acc = make_float2(0.f, 0.f);
+#pragma unroll 4
+    for (int t = 0; t < e0; ++t)
+      acc = cfma(rowc[t * R + r], S[st.t_base[t] + r * st.t_stride[t] + tid], acc);
+#pragma unroll 4
+    for (int t = e0; t < e1; ++t)
+      acc = cfma(colc[t * kRhsCols + tid], S[st.t_base[t] + r * st.t_stride[t] + tid], acc);
+#pragma unroll 2
+    for (int t = e1; t < nt; ++t)
+      acc = cfma(cmul(rowc[t * R + r], colc[t * kRhsCols + tid]), S[st.t_base[t] + r * st.t_stride[t] + tid],
+                 acc);
+    out[(long long)(i0 + r) * n + j] = acc;
+  }
+}
+
 // ------------------------------------------------------------------------------------
 // host side
 // ------------------------------------------------------------------------------------
@@ -369,17 +490,76 @@ size_t tiled_smem(const DiaOps& d, int rows) {
   return (size_t)(d.nh + d.npair) * (rows + kRhsCols) * sizeof(DiaCoef);
 }
 
+// Staging plan of rhs_dia_staged_kernel<R> (see DiaStage); false when the operators need
+// more groups, terms or shared memory than it allows.
+bool plan_stage(const DiaOps& d, int R, DiaStage* st, size_t* smem) {
+  std::memset(st, 0, sizeof(*st));
+  if (d.n > 46340 || d.npair > 64) return false;
+  const int nt = 2 * d.nh + d.npair;
+  if (nt > kStageMaxTerms) return false;
+  int ro[kStageMaxTerms], co[kStageMaxTerms], diag[kStageMaxTerms];
+  int t = 0;
+  for (int q = 0; q < d.nh; ++q, ++t) ro[t] = d.hoff[q], co[t] = 0, diag[t] = q;
+  for (int q = 0; q < d.nh; ++q, ++t) ro[t] = 0, co[t] = d.hoff[q], diag[t] = q;
+  for (int k = 0; k < d.npair; ++k, ++t) ro[t] = d.loff[d.pair_p[k]], co[t] = d.loff[d.pair_s[k]], diag[t] = k;
+  std::vector<int> rs(ro, ro + nt);
+  std::sort(rs.begin(), rs.end());
+  rs.erase(std::unique(rs.begin(), rs.end()), rs.end());
+  int glo[kStageMaxGroups], ghi[kStageMaxGroups], ng = 0;
+  for (int v : rs) {
+    if (ng > 0 && v - ghi[ng - 1] <= R) {
+      ghi[ng - 1] = v;
+    } else {
+      if (ng == kStageMaxGroups) return false;
+      glo[ng] = ghi[ng] = v;
+      ++ng;
+    }
+  }
+  st->ngroup = ng;
+  int total = 0;
+  for (int g = 0; g < ng; ++g) {
+    int clo = 1 << 30, chi = -(1 << 30);
+    for (int k = 0; k < nt; ++k)
+      if (ro[k] >= glo[g] && ro[k] <= ghi[g]) clo = std::min(clo, co[k]), chi = std::max(chi, co[k]);
+    st->g_rlo[g] = glo[g];
+    st->g_rows[g] = R + ghi[g] - glo[g];
+    st->g_clo[g] = clo;
+    st->g_cols[g] = kRhsCols + chi - clo;
+    st->g_off[g] = total;
+    total += st->g_rows[g] * st->g_cols[g];
+  }
+  st->staged = total;
+  st->n0 = d.nh;
+  st->n1 = d.nh;
+  st->n2 = d.npair;
+  for (int k = 0; k < nt; ++k) {
+    int g = 0;
+    while (!(ro[k] >= glo[g] && ro[k] <= ghi[g])) ++g;
+    st->t_diag[k] = diag[k];
+    st->t_stride[k] = st->g_cols[g];
+    st->t_base[k] = st->g_off[g] + (ro[k] - glo[g]) * st->g_cols[g] + (co[k] - st->g_clo[g]);
+  }
+  *smem = ((size_t)total + (size_t)nt * (R + kRhsCols)) * sizeof(float2);
+  return *smem <= kStageMaxSmem;
+}
+
 // Launch shape of the stencil from `tile`: 4, 8 or 16 = the tiled kernel with that many rows
-// per thread (when the operators have at most kTiledMaxTerms diagonal terms); anything else
-// (0 = default, 1) = the generic kernel.  The autotuner picks among them per problem shape.
+// per thread (when the operators have at most kTiledMaxTerms diagonal terms); 108 or 116 =
+// the staged kernel with 8 or 16 rows per CTA (when its plan fits); anything else (0 =
+// default, 1) = the generic kernel.  The autotuner picks among them per problem shape.
 // Returns the shape code (1 = generic).
 int rows_for(const DiaOps& d, int tile) {
+  if (tile == 108 || tile == 116) {
+    DiaStage st;
+    size_t sm;
+    if (plan_stage(d, tile - 100, &st, &sm)) return tile;
+  }
   if (!fast_ok(d)) return 1;
   return (tile == 4 || tile == 8 || tile == 16) ? tile : 1;
 }
 
 dim3 rhs_grid(const DiaOps& d, int rows, int B) {
-  const int r = rows == 1 ? kRhsRows : rows;
+  const int r = rows == 1 ? kRhsRows : (rows > 100 ? rows - 100 : rows);
   return dim3((d.n + kRhsCols - 1) / kRhsCols, (d.n + r - 1) / r, B);
 }
 
@@ -388,6 +568,16 @@ dim3 rhs_grid(const DiaOps& d, int rows, int B) {
 void launch_rhs_dia(cudaStream_t s, const big::Common& c, const DiaOps& d, int B, int rows, int in_sel,
                     int out_k, int need_run, const float2* ext_in, float2* ext_out) {
   const dim3 g = rhs_grid(d, rows, B);
+  if (rows > 100) {
+    DiaStage st;
+    size_t sm = 0;
+    plan_stage(d, rows - 100, &st, &sm);  // rows_for checked that it fits
+    if (rows == 116)
+      rhs_dia_staged_kernel<16><<<g, kRhsCols, sm, s>>>(c, d, st, in_sel, out_k, need_run, ext_in, ext_out);
+    else
+      rhs_dia_staged_kernel<8><<<g, kRhsCols, sm, s>>>(c, d, st, in_sel, out_k, need_run, ext_in, ext_out);
+    return;
+  }
   const size_t sm = tiled_smem(d, rows);
   if (rows == 4) {
     rhs_dia_tiled_kernel<4><<<g, kRhsCols, sm, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
@@ -434,6 +624,10 @@ static void init_carveouts() {
     prefer_max_shared(rhs_dia_tiled_kernel<4>);
     prefer_max_shared(rhs_dia_tiled_kernel<8>);
     prefer_max_shared(rhs_dia_tiled_kernel<16>);
+    prefer_max_shared(rhs_dia_staged_kernel<8>);
+    prefer_max_shared(rhs_dia_staged_kernel<16>);
+    cudaFuncSetAttribute(rhs_dia_staged_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageMaxSmem);
+    cudaFuncSetAttribute(rhs_dia_staged_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageMaxSmem);
   });
 }
 

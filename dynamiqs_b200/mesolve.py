@@ -494,8 +494,8 @@ class MESolveB200Integrator:
 
     def _tune_dia_tile(self, lib, prob, ws, ws_bytes, dev, pattern) -> None:
         """Launch shape of the DIA stencil for this (n, sparsity pattern): the generic
-        kernel (1) or the register-blocked one with 4, 8 or 16 rows per thread, timed on one
-        right-hand side of one instance."""
+        kernel (1), the tiled one with 4, 8 or 16 rows per thread, or the staged one with 8
+        or 16 rows per CTA (108, 116), timed on one right-hand side of one instance."""
         import ctypes
 
         import torch
@@ -519,7 +519,7 @@ class MESolveB200Integrator:
 
         key = ('dia_tile', torch.cuda.get_device_name(dev), n, prob.n_jumps, pattern,
                autotune.batch_bucket(prob.batch))
-        self._tuned['tile'] = autotune.choose(key, [1, 4, 8, 16], make_run, 1)
+        self._tuned['tile'] = autotune.choose(key, [1, 4, 8, 16, 108, 116], make_run, 1)
 
     # kept for callers that select a path explicitly (tests)
     def _run_dense_small(self, lib) -> MESolveResult:

@@ -81,8 +81,10 @@ typedef struct dqb_ode_options {
   int32_t check_hermitian; /* 1: flag rho0 that fails isherm(rtol=atol=1e-5)            */
   int32_t precision;       /* DQB_PREC_* (GEMM path only; 0 = FP32)                     */
   int32_t tile;            /* launch-shape choice of the sparse-DIA stencil: 4, 8 or 16 =
-                              register-blocked kernel with that many rows per thread;
-                              0 (default) or 1 = generic kernel; ignored by other paths  */
+                              tiled kernel with that many rows per thread; 108 or 116 =
+                              staged kernel with 8 or 16 rows per CTA; 0 (default) or 1 =
+                              generic kernel; shapes that do not fit the operators fall
+                              back to the generic kernel; ignored by other paths          */
 } dqb_ode_options;
 
 /* Outputs of a batched solve.  nsave = n_tsave if save_states else 1. */

@@ -51,9 +51,12 @@ def _problem_struct(H, Ls, n, batch):
     return p, [h_off, l_nd, l_off, H_d, L_d]
 
 
+@pytest.mark.parametrize('tile', [0, 8, 108, 116])
 @pytest.mark.parametrize('form', [_lib.FORM_HERMITIAN, _lib.FORM_STANDARD])
 @pytest.mark.parametrize('n', [10, 77, 300])
-def test_rhs_dia_matches_oracle(cuda_device, form, n):
+def test_rhs_dia_matches_oracle(cuda_device, form, n, tile):
+    """Every stencil kernel (generic; tiled, 8 rows; staged, 8 and 16 rows) against the
+    oracle, on operators whose offsets make the edges and the shared-memory groups ragged."""
     rng = np.random.default_rng(n)
     B = 2
     Hs = [_rand_dia(n, (-2, 0, 2), rng) for _ in range(B)]
@@ -71,8 +74,9 @@ def test_rhs_dia_matches_oracle(cuda_device, form, n):
     out = torch.empty_like(r_d)
     ws = torch.empty(1 << 20, dtype=torch.uint8, device='cuda')
     lib = _lib.load()
-    _lib.check(lib.dqb_lindblad_rhs_dia(p, form, r_d.data_ptr(), out.data_ptr(), ws.data_ptr(),
-                                        ws.numel(), torch.cuda.current_stream().cuda_stream), 'rhs_dia')
+    _lib.check(lib.dqb_lindblad_rhs_dia_tiled(p, form, tile, r_d.data_ptr(), out.data_ptr(),
+                                              ws.data_ptr(), ws.numel(),
+                                              torch.cuda.current_stream().cuda_stream), 'rhs_dia')
     got = out.cpu().numpy()
     for b in range(B):
         Hb = (H.offsets, H.diags[b].astype(complex))

@@ -158,8 +158,6 @@ class MESolveServer:
     LARGE_MAX_JUMPS = 8
     LARGE_MAX_EXP = 8
     LARGE_MAX_TSAVE = 1024
-    # precision='auto': GEMM-path waves with at least this many requests use 3xTF32
-    AUTO_TC_MIN_WAVE = 8
 
     def __init__(self, budget_bytes: float = 150e9, max_wave: int = 4096, n_streams: int = 16,
                  poll_s: float = 50e-6, max_large_wave: int = 64, staging_bytes: float = 2e9):
@@ -396,15 +394,15 @@ class MESolveServer:
 
     # ---- waves --------------------------------------------------------------------------
     def _precision_of(self, t: Ticket, form: int, count: int) -> int:
-        """GEMM-path arithmetic of a wave.  ``precision='auto'``: 3xTF32 tensor cores for
-        waves of at least AUTO_TC_MIN_WAVE requests, FP32 CUDA cores for smaller ones, whose
-        few 128x128 tensor-core tiles per product would leave most SMs idle (the FP32 path's
-        64x64 tiles give 4x more CTAs per instance): a lone stiff request then steps faster."""
+        """GEMM-path arithmetic of a wave.  ``precision='auto'``: 3xTF32 tensor cores
+        whenever the form and n allow them (hermitian form, even n), else FP32 CUDA cores.
+        Measured on the serving workload, the tensor cores were also the faster choice for
+        waves of one or two stiff requests, where their 128x128 tiles leave most SMs idle."""
         o = t.options
         if t.n <= 64:
             return _lib.PREC_FP32
         if o.precision == 'auto':
-            ok = form == _lib.FORM_HERMITIAN and t.n % 2 == 0 and count >= self.AUTO_TC_MIN_WAVE
+            ok = form == _lib.FORM_HERMITIAN and t.n % 2 == 0
             return _lib.PREC_TF32X3 if ok else _lib.PREC_FP32
         return _precision_code(o, form)
 

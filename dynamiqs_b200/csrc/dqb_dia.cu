@@ -314,6 +314,8 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_staged_kernel(big::Common c,
   float2* rowc = S + st.staged;    // [nt][R]
   float2* colc = rowc + nt * R;    // [nt][128]
 
+  // stage with asynchronous 8-byte copies (zero-filled outside the matrix), all in flight
+  // while the coefficient tables are computed
   for (int g = 0; g < st.ngroup; ++g) {
     const int gr0 = i0 + st.g_rlo[g], gc0 = j0 + st.g_clo[g], cols = st.g_cols[g];
     float2* dst = S + st.g_off[g];
@@ -323,10 +325,15 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_staged_kernel(big::Common c,
       const float2* src = X + (long long)(rin ? gr : 0) * n;
       for (int cc = tid; cc < cols; cc += kRhsCols) {
         const int gc = gc0 + cc;
-        dst[rr * cols + cc] = (rin && gc >= 0 && gc < n) ? __ldg(&src[gc]) : make_float2(0.f, 0.f);
+        const bool in = rin && gc >= 0 && gc < n;
+        const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(dst + rr * cols + cc));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(sa), "l"(in ? src + gc : X),
+                     "r"(in ? 8 : 0)
+                     : "memory");
       }
     }
   }
+  asm volatile("cp.async.commit_group;" ::: "memory");
   for (int e = tid; e < nt * R; e += kRhsCols) {
     const int t = e / R, i = i0 + e % R;
     float2 v = make_float2(0.f, 0.f);
@@ -361,6 +368,7 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_staged_kernel(big::Common c,
       colc[t * kRhsCols + tid] = v;
     }
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
   const int j = j0 + tid;
   if (j >= n) return;

@@ -11,7 +11,9 @@
 // bank-conflict free.  The seven RK stages, y and y1 live in a per-CTA scratch slot in
 // global memory (9 * NP^2 complex64 = 288 KiB at NP = 64; 148 slots = 43 MB, resident
 // in the 126 MB L2).  The products run on the FP32 pipes: 256 threads, each owning an
-// (NP/16) x (NP/16) tile of the output, complex multiply-accumulate as 4 FFMA.
+// (NP/16) x (NP/16) tile of the output, complex multiply-accumulate as 4 FFMA.  In the
+// hermitian form the hermitian product (L_k X) L_k^+ is computed only on the tile pairs on
+// and below the block diagonal (gemm_herm), which tmp + tmp^+ completes exactly.
 //
 // Right-hand sides (dynamiqs/integrators/core/diffrax_integrator.py:312-323):
 //   hermitian: tmp = Hnh X + 1/2 sum_k (L_k X) L_k^+ ;  out = tmp + tmp^+

@@ -8,8 +8,11 @@
 // and f(X) = Hnh X + X Hnh^+ + sum_k L_k X L_k^+.  For a hermitian X this equals the
 // reference's hermitian form tmp + tmp^+ with tmp = Hnh X + 1/2 sum L X L^+
 // (diffrax_integrator.py:319-323) and it is the standard form (:312-317) for any X, so
-// one stencil serves both.  Every term is a shifted, coalesced read of X; the kernel is
-// HBM/L2-bandwidth bound (algorithmic traffic: read X once, write f(X) once).
+// one stencil serves both.  Every term is a shifted, coalesced read of X (algorithmic
+// traffic: read X once, write f(X) once; the shifted re-reads come from L1/L2 or shared
+// memory).  Three kernels compute it -- generic, tiled (coefficient tables in shared
+// memory) and staged (the rows of X the offsets touch in shared memory) -- and the
+// autotuner keeps the fastest per problem shape (dqb_ode_options.tile).
 //
 // Hnh's diagonals are built once per instance on the device (the reference rebuilds
 // them with matmul_sparsedia_sparsedia + add_sparsedia_sparsedia on every RHS,

@@ -119,7 +119,7 @@ __device__ __forceinline__ void gemm(float2 (&acc)[NP / 16][NP / 16], const floa
                                      const float2* __restrict__ B, int kn) {
   constexpr int R = NP / 16, LD = NP + 1;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-#pragma unroll 4
+#pragma unroll 8
   for (int k = 0; k < kn; ++k) {
     float2 a[R], b[R];
 #pragma unroll
@@ -157,7 +157,7 @@ __device__ __forceinline__ void gemm_herm(float2 (&acc)[NP / 16][NP / 16],
                                           int kn) {
   constexpr int R = NP / 16, LD = NP + 1;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-#pragma unroll 4
+#pragma unroll 8
   for (int k = 0; k < kn; ++k) {
     float2 a[R], b[R];
 #pragma unroll
@@ -446,6 +446,7 @@ __device__ void solve_one(const InstView& a, const CtrlOpts& o, float2* sH, floa
       float cf[6];
 #pragma unroll
       for (int j = 0; j < 6; ++j) cf[j] = (float)(h * T.a[s][j]);
+#pragma unroll 4
       for (int e = tid; e < NN; e += blockDim.x) {
         float2 x = yv[e];
 #pragma unroll
@@ -462,6 +463,7 @@ __device__ void solve_one(const InstView& a, const CtrlOpts& o, float2* sH, floa
       float cf[6];
 #pragma unroll
       for (int j = 0; j < 6; ++j) cf[j] = (float)(h * T.b[j]);
+#pragma unroll 4
       for (int e = tid; e < NN; e += blockDim.x) {
         float2 x = yv[e];
 #pragma unroll
@@ -479,6 +481,7 @@ __device__ void solve_one(const InstView& a, const CtrlOpts& o, float2* sH, floa
       double cb[7];
 #pragma unroll
       for (int j = 0; j < 7; ++j) cb[j] = h * T.btilde[j];
+#pragma unroll 4
       for (int e = tid; e < NN; e += blockDim.x) {
         double ex = 0.0, ey = 0.0;
 #pragma unroll

@@ -56,7 +56,7 @@ def test_rhs_large_matches_oracle(cuda_device, n, K, form):
 
 
 def _check_vs_oracle(res, H, Ls, rho0, ts, Es, method, b=None):
-    kw = dict(exp_ops=Es, rtol=method.rtol, atol=method.atol)
+    kw = dict(exp_ops=Es, rtol=method.rtol, atol=method.atol, method=type(method).__name__)
     r = oracle_mesolve(H, Ls, rho0, ts, **kw)
     r64 = oracle_mesolve(H, Ls, rho0, ts, dtype=np.complex64, **kw)
     st = res.states if b is None else res.states[b]
@@ -110,3 +110,14 @@ def test_large_standard_form_and_save_states_false(cuda_device):
     last = dq.mesolve(H, Ls, rho, ts, options=dq.Options(assume_hermitian=False, save_states=False))
     assert last.states.shape == (1, 90, 90)
     assert rel_frob(last.states[0].cpu().numpy(), r.states[-1]) < 1e-5
+
+
+def test_large_path_dopri5_vs_oracle(cuda_device):
+    """Dopri5 (its tableau, embedded error and Shampine dense output) through the GEMM
+    path: transmon(2) x cavity(40), n = 80, 2 instances."""
+    w = workloads.transmon_cavity(batch=2, nq=2, nc=40, seed=4)
+    ts = np.linspace(0.0, 3.0, 7)
+    m = dq.Dopri5(rtol=1e-6, atol=1e-8)
+    res = dq.mesolve(w['H'], w['jump_ops'], w['rho0'], ts, exp_ops=w['exp_ops'], method=m)
+    for b in range(2):
+        _check_vs_oracle(res, w['H'][b], w['jump_ops'], w['rho0'], ts, w['exp_ops'], m, b)

@@ -159,3 +159,13 @@ def test_dia_full_size_properties(cuda_device):
     assert herm < 1e-6
     assert float(torch.diagonal(st, dim1=-2, dim2=-1).real.min()) > -1e-6
     assert int(res.infos.nrejected[0]) >= 0 and int(res.infos.nsteps[0]) > 0
+
+
+def test_dia_path_dopri5_vs_oracle(cuda_device):
+    """Dopri5 through the DIA stepper: two coupled Kerr modes of 10 levels (n = 100)."""
+    w = workloads.coupled_kerr_dia(batch=2, m=10, seed=6)
+    w['method'] = dq.Dopri5(rtol=1e-5, atol=1e-7)
+    res = dq.mesolve(w['H'], w['jump_ops'], w['rho0'], w['tsave'], method=w['method'])
+    assert int((res.infos.nsteps > 0).sum()) == 2
+    for b in range(2):
+        _oracle_compare(res, w, b, method='Dopri5')

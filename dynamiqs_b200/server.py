@@ -160,7 +160,8 @@ class MESolveServer:
     LARGE_MAX_TSAVE = 1024
 
     def __init__(self, budget_bytes: float = 150e9, max_wave: int = 4096, n_streams: int = 16,
-                 poll_s: float = 50e-6, max_large_wave: int = 64, staging_bytes: float = 2e9):
+                 poll_s: float = 50e-6, max_large_wave: int = 64, staging_bytes: float = 2e9,
+                 history: int = 100_000):
         import torch
 
         if not torch.cuda.is_available():
@@ -202,10 +203,12 @@ class MESolveServer:
         self._wake = threading.Condition(self._lock)
         self._closing = False
         self._next_id = 0
-        self.finished: list[Ticket] = []
+        # finished tickets and per-wave launch records, the latest `history` of each (a
+        # long-running server keeps a bounded window for stats())
+        self.finished: deque[Ticket] = deque(maxlen=history)
         self.waves_launched = 0
-        self.launch_seconds: list[tuple] = []  # (class, instances, host seconds in the launch)
-        self.launch_profile: list[tuple] = []  # (class, {step: host seconds}) per wave
+        self.launch_seconds: deque = deque(maxlen=history)  # (class, instances, host s in the launch)
+        self.launch_profile: deque = deque(maxlen=history)  # (class, {step: host seconds}) per wave
         # waves are launched from worker threads: a driver call that waits (for instance a
         # graph instantiation while another conditional graph runs) holds up only its class
         self._launcher = ThreadPoolExecutor(max_workers=n_streams, thread_name_prefix='mesolve-launch')

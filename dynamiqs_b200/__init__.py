@@ -9,7 +9,8 @@ from .method import Dopri5, Tsit5
 from .options import Options
 from .qarrays import SparseDIA, dense, dia
 from .result import AdaptiveStepInfos, MESolveResult
+from .time_qarray import pwc
 
 __all__ = ['mesolve', 'MESolveB200Integrator', 'Options', 'Tsit5', 'Dopri5',
            'MESolveResult', 'AdaptiveStepInfos', 'SparseDIA', 'dense', 'dia', 'method',
-           'operators']
+           'operators', 'pwc']

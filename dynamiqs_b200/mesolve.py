@@ -583,9 +583,17 @@ def mesolve(H, jump_ops, rho0, tsave, *, exp_ops=None, method: Method = Tsit5(),
     :class:`~dynamiqs_b200.qarrays.SparseDIA`.  ``method`` is ``Tsit5`` (default) or
     ``Dopri5``.
     """
+    from .time_qarray import PWCTimeQArray, SummedTimeQArray
+
+    if isinstance(H, (PWCTimeQArray, SummedTimeQArray)):
+        return _mesolve_piecewise(H, jump_ops, rho0, tsave, exp_ops=exp_ops, method=method,
+                                  gradient=gradient, options=options, solve=mesolve)
     if getattr(H, '__class__', None).__name__.endswith('TimeQArray'):
-        raise NotImplementedError('Time-dependent operators are not supported on the B200 '
-                                  'mesolve path yet.')
+        raise NotImplementedError('Only piecewise-constant time-dependent operators (dq.pwc and '
+                                  'sums with constant operators) are supported on the B200 path.')
+    if any(isinstance(L, (PWCTimeQArray, SummedTimeQArray)) for L in jump_ops):
+        raise NotImplementedError('Time-dependent jump operators are not supported on the B200 '
+                                  'path.')
     H = _as_op(H)
     Ls = [_as_op(L) for L in jump_ops]
     rho0 = _as_op(rho0)
@@ -612,6 +620,49 @@ def mesolve(H, jump_ops, rho0, tsave, *, exp_ops=None, method: Method = Tsit5(),
     integrator = MESolveB200Integrator(ts=tsave, y0=rho0, method=method, gradient=gradient,
                                        options=options, H=H, Ls=Ls, Es=exp_ops, plan=plan)
     return integrator.run()
+
+
+def _mesolve_piecewise(H, jump_ops, rho0, tsave, *, exp_ops, method, gradient, options, solve):
+    """Solve with a piecewise-constant H (``time_qarray``): one constant-operator ``solve``
+    per piece between consecutive discontinuities, each started from the previous piece's
+    final state; saved states, expectation values and step counts are stitched together
+    into one result over ``tsave``.  ``solve`` has ``mesolve``'s signature (the oracle's
+    stand-in in the CPU tests)."""
+    import dataclasses
+
+    from .time_qarray import as_summed, piecewise_plan
+
+    Hs = as_summed(H)
+    tsave = check_times(np.asarray(tsave.detach().cpu().numpy() if hasattr(tsave, 'detach')
+                                   else tsave, dtype=np.float64), 'tsave')
+    t0 = float(tsave[0] if options.t0 is None else options.t0)
+    piece_opts = dataclasses.replace(options, t0=None)
+    states, expects, infos = [], [], None
+    state = rho0
+    for _a, _b, Hc, ts, keep in piecewise_plan(Hs, tsave, t0):
+        r = solve(Hc, jump_ops, state, ts, exp_ops=exp_ops, method=method, gradient=gradient,
+                  options=piece_opts)
+        if options.save_states:
+            states.append(r.states[..., keep, :, :])
+        if r.expects is not None:
+            expects.append(r.expects[..., keep])
+        state = r.states[..., -1, :, :]
+        i = (r.infos.nsteps, r.infos.naccepted, r.infos.nrejected)
+        infos = i if infos is None else tuple(x + y for x, y in zip(infos, i))
+    cat = _concatenate_like(state)
+    out_states = cat(states, -3) if options.save_states else state[..., None, :, :]
+    out_expects = cat(expects, -1) if expects else None
+    return MESolveResult(tsave=tsave, method=method, gradient=gradient, options=options,
+                         states=out_states, expects=out_expects,
+                         infos=AdaptiveStepInfos(*infos))
+
+
+def _concatenate_like(x):
+    if hasattr(x, 'detach'):
+        import torch
+
+        return lambda xs, axis: torch.cat(list(xs), dim=axis)
+    return lambda xs, axis: np.concatenate(list(xs), axis=axis)
 
 
 def _prod(shape) -> int:

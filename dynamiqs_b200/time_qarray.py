@@ -1,0 +1,152 @@
+"""Piecewise-constant time-dependent operators for ``mesolve``.
+
+Mirrors the reference's ``dq.pwc`` / ``PWCTimeQArray`` (``dynamiqs/time_qarray.py:53-120,
+572-640``): ``pwc(times, values, qarray)`` is the operator
+``O(t) = c_k O_0`` for ``t`` in ``[t_k, t_{k+1})`` and ``0`` outside ``[t_0, t_N)``, and a
+constant operator plus PWC terms (``H0 + pwc(...) + ...``) is a summed time-dependent
+operator.  The reference integrates such a Hamiltonian with its discontinuity times passed
+to the step-size controller as ``jump_ts`` (``dynamiqs/integrators/core/
+diffrax_integrator.py:64-72``), so that no step crosses a discontinuity.  Here the solve is
+split at the discontinuities instead: each piece is a constant-operator solve on the GPU
+(one batched kernel launch), started from the previous piece's final state.  Every step
+therefore also stays inside one constant piece; what differs from the reference is the
+first step of each piece, which comes from the starting-step heuristic rather than from the
+controller's last proposal, so step counts differ slightly while the accuracy (rtol, atol)
+is the same.
+
+Scope: the PWC values are one-dimensional (no batch over values) and ``H0``'s constant
+part and the jump operators are unbatched; ``rho0`` may be batched.  Modulated (callable)
+prefactors are not supported: a Python callable cannot be evaluated inside the kernels.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from .qarrays import SparseDIA
+
+__all__ = ['PWCTimeQArray', 'SummedTimeQArray', 'pwc']
+
+
+def _dense_op(x) -> np.ndarray:
+    if isinstance(x, SparseDIA):
+        return np.asarray(x.to_dense(), dtype=np.complex64)
+    if hasattr(x, 'detach'):
+        x = x.detach().cpu().numpy()
+    return np.asarray(x, dtype=np.complex64)
+
+
+class PWCTimeQArray:
+    """``O(t) = values[k] * qarray`` for ``times[k] <= t < times[k+1]``, ``0`` elsewhere."""
+
+    __array_ufunc__ = None  # ``ndarray + PWCTimeQArray`` defers to __radd__
+
+    def __init__(self, times, values, qarray):
+        times = np.asarray(times, dtype=np.float64)
+        values = np.asarray(values)
+        if times.ndim != 1 or times.size < 2:
+            raise ValueError('Argument `times` must be a 1-D array of at least 2 time points.')
+        if np.any(np.diff(times) < 0):
+            raise ValueError('Argument `times` must be sorted in ascending order.')
+        if values.shape[-1:] != (times.size - 1,):
+            raise ValueError(f'Argument `values` must have shape (..., {times.size - 1}), got '
+                             f'{values.shape}.')
+        if values.ndim != 1:
+            raise NotImplementedError('Batched PWC values are not supported on the B200 path.')
+        self.times = times
+        self.values = values.astype(np.complex128)
+        self.qarray = _dense_op(qarray)
+        if self.qarray.ndim != 2 or self.qarray.shape[0] != self.qarray.shape[1]:
+            raise ValueError('Argument `qarray` must be a square (n, n) operator.')
+
+    @property
+    def shape(self) -> tuple[int, ...]:
+        return self.qarray.shape
+
+    @property
+    def discontinuity_ts(self) -> np.ndarray:
+        return self.times
+
+    def prefactor(self, t: float) -> complex:
+        k = int(np.searchsorted(self.times, t, side='right')) - 1
+        return complex(self.values[k]) if 0 <= k < self.values.size else 0.0
+
+    def __call__(self, t: float) -> np.ndarray:
+        return (self.prefactor(t) * self.qarray).astype(np.complex64)
+
+    def __add__(self, other) -> SummedTimeQArray:
+        return SummedTimeQArray([self, other])
+
+    __radd__ = __add__
+
+
+class SummedTimeQArray:
+    """A sum of constant operators and :class:`PWCTimeQArray` terms."""
+
+    __array_ufunc__ = None
+
+    def __init__(self, terms):
+        flat = []
+        for t in terms:
+            flat.extend(t.terms if isinstance(t, SummedTimeQArray) else [t])
+        self.pwc_terms = [t for t in flat if isinstance(t, PWCTimeQArray)]
+        const = [_dense_op(t) for t in flat if not isinstance(t, PWCTimeQArray)]
+        n = (self.pwc_terms[0].shape if self.pwc_terms else const[0].shape)[-1]
+        for c in const:
+            if c.ndim != 2:
+                raise NotImplementedError('A batched constant part of a time-dependent H is not '
+                                          'supported on the B200 path.')
+        self.constant = sum(const) if const else np.zeros((n, n), np.complex64)
+        self.terms = flat
+        for t in self.pwc_terms:
+            if t.shape != self.constant.shape:
+                raise ValueError('All terms of a time-dependent operator must have the same shape.')
+
+    @property
+    def shape(self) -> tuple[int, ...]:
+        return self.constant.shape
+
+    @property
+    def discontinuity_ts(self) -> np.ndarray:
+        ts = [t.times for t in self.pwc_terms]
+        return np.unique(np.concatenate(ts)) if ts else np.zeros(0)
+
+    def __call__(self, t: float) -> np.ndarray:
+        out = self.constant.astype(np.complex128)
+        for term in self.pwc_terms:
+            out = out + term.prefactor(t) * term.qarray
+        return out.astype(np.complex64)
+
+    def __add__(self, other) -> SummedTimeQArray:
+        return SummedTimeQArray([self, other])
+
+    __radd__ = __add__
+
+
+def pwc(times, values, qarray) -> PWCTimeQArray:
+    """Piecewise-constant operator ``O(t) = sum_k c_k 1_[t_k, t_{k+1})(t) O_0``
+    (``dq.pwc``, ``dynamiqs/time_qarray.py:53-120``)."""
+    return PWCTimeQArray(times, values, qarray)
+
+
+def as_summed(H) -> SummedTimeQArray:
+    return H if isinstance(H, SummedTimeQArray) else SummedTimeQArray([H])
+
+
+def piecewise_plan(H: SummedTimeQArray, tsave: np.ndarray, t0: float):
+    """The constant pieces of a solve from ``t0`` to ``tsave[-1]``: a list of
+    ``(a, b, H_piece, ts_piece, keep)`` where ``ts_piece`` is the save grid handed to the
+    constant-operator solve of ``[a, b]`` (it starts at ``a`` and ends at ``b``) and
+    ``keep`` the indices of ``ts_piece`` that are points of ``tsave``, in order.  Every
+    point of ``tsave`` is kept exactly once (a point on a discontinuity belongs to the piece
+    that ends there; ``tsave[0] == t0`` to the first piece)."""
+    t1 = float(tsave[-1])
+    bps = [float(t) for t in H.discontinuity_ts if t0 < t < t1]
+    edges = [t0] + sorted(set(bps)) + [t1]
+    plan = []
+    for i, (a, b) in enumerate(zip(edges[:-1], edges[1:])):
+        inside = [float(t) for t in tsave if (a < t <= b) or (i == 0 and t == a)]
+        ts = sorted(set([a, b] + inside))
+        keep = [ts.index(t) for t in inside]
+        plan.append((a, b, H(0.5 * (a + b)), np.asarray(ts), keep))
+    return plan

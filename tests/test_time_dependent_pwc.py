@@ -1,0 +1,124 @@
+"""Piecewise-constant Hamiltonians (``dq.pwc``, ``dynamiqs/time_qarray.py:53-120,572-640``).
+
+CPU: the split-at-discontinuities driver, run with the oracle as the constant-operator
+solver, against the exact solution (matrix exponential of the Lindbladian on each constant
+piece); the piece plan's save bookkeeping; the reference's PWC semantics (value c_k on
+[t_k, t_{k+1}), 0 outside).  GPU: the same problem through ``dq.mesolve`` on the kernels."""
+
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+from scipy.linalg import expm
+
+import dynamiqs_b200 as dq
+from dynamiqs_b200 import operators as ops
+from dynamiqs_b200.mesolve import _mesolve_piecewise
+from dynamiqs_b200.time_qarray import as_summed, piecewise_plan
+from oracle.mesolve import mesolve as oracle_mesolve
+
+N = 5
+TIMES = [0.3, 0.8, 1.5, 2.2]
+VALUES = [1.0, -0.5, 2.0]
+TSAVE = np.linspace(0.0, 3.0, 13)  # 1.5 is both a save time and a discontinuity
+
+
+def _system():
+    a = ops.destroy(N, layout='dense')
+    H0 = 0.7 * (ops.dag(a) @ a)
+    drive = a + ops.dag(a)
+    H = H0 + dq.pwc(TIMES, VALUES, drive)
+    L = [np.float32(np.sqrt(0.2)) * a]
+    rho0 = ops.fock(N, 0)
+    return H, H0, drive, L, rho0, [ops.dag(a) @ a]
+
+
+def _lindbladian(H, Ls):
+    n = H.shape[0]
+    I = np.eye(n)
+    # column-stacking vec: vec(A X B) = (B^T kron A) vec(X)
+    out = -1j * (np.kron(I, H) - np.kron(H.T, I))
+    for L in Ls:
+        LdL = L.conj().T @ L
+        out += np.kron(L.conj(), L) - 0.5 * (np.kron(I, LdL) + np.kron(LdL.T, I))
+    return out
+
+
+def _exact(H0, drive, Ls, rho0, tsave):
+    psi = np.asarray(rho0, complex).reshape(-1)
+    rho = np.outer(psi, psi.conj())
+    Ls = [np.asarray(L, complex) for L in Ls]
+    edges = [0.0] + [t for t in TIMES if 0.0 < t < tsave[-1]] + [tsave[-1]]
+    out, t, vec = [], 0.0, rho.reshape(-1, order='F')
+    for a, b in zip(edges[:-1], edges[1:]):
+        k = np.searchsorted(TIMES, 0.5 * (a + b), side='right') - 1
+        c = VALUES[k] if 0 <= k < len(VALUES) else 0.0
+        Lv = _lindbladian(np.asarray(H0, complex) + c * np.asarray(drive, complex), Ls)
+        for ts in tsave:
+            if (a < ts <= b) or (a == ts == 0.0):
+                out.append((expm(Lv * (ts - a)) @ vec).reshape(N, N, order='F'))
+        vec = expm(Lv * (b - a)) @ vec
+    return np.stack(out)
+
+
+def _oracle_solve(H, Ls, rho0, ts, *, exp_ops, method, gradient, options):
+    r = oracle_mesolve(np.asarray(H), [np.asarray(L) for L in Ls], np.asarray(rho0), ts,
+                       exp_ops=exp_ops, method=type(method).__name__, rtol=method.rtol,
+                       atol=method.atol)
+    return SimpleNamespace(states=r.states, expects=r.expects,
+                           infos=SimpleNamespace(nsteps=np.array(r.nsteps),
+                                                 naccepted=np.array(r.naccepted),
+                                                 nrejected=np.array(r.nrejected)))
+
+
+def test_pwc_semantics():
+    P = dq.pwc(TIMES, VALUES, np.eye(2))
+    assert P.prefactor(0.0) == 0.0 and P.prefactor(0.3) == 1.0 and P.prefactor(0.79) == 1.0
+    assert P.prefactor(0.8) == -0.5 and P.prefactor(2.2) == 0.0 and P.prefactor(5.0) == 0.0
+    with pytest.raises(ValueError, match='sorted'):
+        dq.pwc([1.0, 0.0], [1.0], np.eye(2))
+    with pytest.raises(ValueError, match='values'):
+        dq.pwc([0.0, 1.0], [1.0, 2.0], np.eye(2))
+
+
+def test_piece_plan_keeps_every_save_once():
+    H, *_ = _system()
+    plan = piecewise_plan(as_summed(H), TSAVE, 0.0)
+    kept = np.concatenate([ts[keep] for _a, _b, _H, ts, keep in plan])
+    assert np.array_equal(kept, TSAVE)
+    edges = [(a, b) for a, b, *_ in plan]
+    assert edges[0][0] == 0.0 and edges[-1][1] == 3.0
+    assert [b for _a, b in edges[:-1]] == TIMES  # pieces end on every discontinuity in range
+    for a, b, _H, ts, _keep in plan:
+        assert ts[0] == a and ts[-1] == b
+
+
+def test_piecewise_driver_with_oracle_matches_exact():
+    H, H0, drive, L, rho0, E = _system()
+    m = dq.Tsit5(rtol=1e-9, atol=1e-11)
+    r = _mesolve_piecewise(H, L, rho0, TSAVE, exp_ops=E, method=m, gradient=None,
+                           options=dq.Options(), solve=_oracle_solve)
+    ref = _exact(H0, drive, L, rho0, TSAVE)
+    assert r.states.shape == (len(TSAVE), N, N)
+    err = np.linalg.norm(r.states - ref, axis=(-2, -1)) / np.linalg.norm(ref, axis=(-2, -1))
+    assert err.max() < 1e-7
+    n_ref = np.real(np.einsum('ij,tji->t', np.asarray(E[0]), ref))
+    assert np.abs(r.expects[0] - n_ref).max() < 1e-7
+    assert int(r.infos.nsteps) > 0
+
+
+@pytest.mark.gpu
+def test_pwc_mesolve_on_gpu_matches_exact(cuda_device):
+    H, H0, drive, L, rho0, E = _system()
+    m = dq.Tsit5(rtol=1e-6, atol=1e-8)
+    res = dq.mesolve(H, L, rho0, TSAVE, exp_ops=E, method=m)
+    ref = _exact(H0, drive, L, rho0, TSAVE)
+    got = res.states.cpu().numpy()
+    err = np.linalg.norm(got - ref, axis=(-2, -1)) / np.linalg.norm(ref, axis=(-2, -1))
+    assert err.max() < 1e-5
+    n_ref = np.real(np.einsum('ij,tji->t', np.asarray(E[0]), ref))
+    assert np.abs(res.expects.cpu().numpy()[0] - n_ref).max() < 1e-5
+    # same piecewise algorithm on the CPU oracle: the same steps within one per piece
+    o = _mesolve_piecewise(H, L, rho0, TSAVE, exp_ops=E, method=m, gradient=None,
+                           options=dq.Options(), solve=_oracle_solve)
+    assert abs(int(res.infos.nsteps) - int(o.infos.nsteps)) <= 5

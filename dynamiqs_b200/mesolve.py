@@ -633,6 +633,28 @@ def _mesolve_piecewise(H, jump_ops, rho0, tsave, *, exp_ops, method, gradient, o
     from .time_qarray import as_summed, piecewise_plan
 
     Hs = as_summed(H)
+    if Hs.batch_shape:
+        if not options.cartesian_batching:
+            raise NotImplementedError('Batched PWC values need cartesian batching on the B200 '
+                                      'path.')
+        rs = [_mesolve_piecewise(Hs.item(idx), jump_ops, rho0, tsave, exp_ops=exp_ops,
+                                 method=method, gradient=gradient, options=options, solve=solve)
+              for idx in np.ndindex(*Hs.batch_shape)]
+        stack = _stack_like(rs[0].states)
+        shape = Hs.batch_shape
+
+        def stacked(xs):
+            out = stack(xs)
+            return out.reshape(*shape, *out.shape[1:])
+
+        r0 = rs[0]
+        return MESolveResult(
+            tsave=r0.tsave, method=method, gradient=gradient, options=options,
+            states=stacked([r.states for r in rs]),
+            expects=stacked([r.expects for r in rs]) if r0.expects is not None else None,
+            infos=AdaptiveStepInfos(stacked([r.infos.nsteps for r in rs]),
+                                    stacked([r.infos.naccepted for r in rs]),
+                                    stacked([r.infos.nrejected for r in rs])))
     tsave = check_times(np.asarray(tsave.detach().cpu().numpy() if hasattr(tsave, 'detach')
                                    else tsave, dtype=np.float64), 'tsave')
     t0 = float(tsave[0] if options.t0 is None else options.t0)
@@ -655,6 +677,14 @@ def _mesolve_piecewise(H, jump_ops, rho0, tsave, *, exp_ops, method, gradient, o
     return MESolveResult(tsave=tsave, method=method, gradient=gradient, options=options,
                          states=out_states, expects=out_expects,
                          infos=AdaptiveStepInfos(*infos))
+
+
+def _stack_like(x):
+    if hasattr(x, 'detach'):
+        import torch
+
+        return lambda xs: torch.stack([torch.as_tensor(v) for v in xs])
+    return lambda xs: np.stack([np.asarray(v) for v in xs])
 
 
 def _concatenate_like(x):

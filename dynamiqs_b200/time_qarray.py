@@ -14,8 +14,10 @@ first step of each piece, which comes from the starting-step heuristic rather th
 controller's last proposal, so step counts differ slightly while the accuracy (rtol, atol)
 is the same.
 
-Scope: the PWC values are one-dimensional (no batch over values) and ``H0``'s constant
-part and the jump operators are unbatched; ``rho0`` may be batched.  Modulated (callable)
+Scope: ``H0``'s constant part and the jump operators are unbatched; ``rho0`` may be
+batched; PWC values may carry batch dimensions ``(..., N)`` (broadcast together across the
+terms), solved one value-batch item at a time with cartesian batching (H's batch dimensions
+first, as the reference orders them).  Modulated (callable)
 prefactors are not supported: a Python callable cannot be evaluated inside the kernels.
 """
 
@@ -51,8 +53,6 @@ class PWCTimeQArray:
         if values.shape[-1:] != (times.size - 1,):
             raise ValueError(f'Argument `values` must have shape (..., {times.size - 1}), got '
                              f'{values.shape}.')
-        if values.ndim != 1:
-            raise NotImplementedError('Batched PWC values are not supported on the B200 path.')
         self.times = times
         self.values = values.astype(np.complex128)
         self.qarray = _dense_op(qarray)
@@ -61,7 +61,21 @@ class PWCTimeQArray:
 
     @property
     def shape(self) -> tuple[int, ...]:
-        return self.qarray.shape
+        return (*self.values.shape[:-1], *self.qarray.shape)
+
+    @property
+    def batch_shape(self) -> tuple[int, ...]:
+        return self.values.shape[:-1]
+
+    def item(self, idx: tuple) -> PWCTimeQArray:
+        """The unbatched term at index ``idx`` of a batch shape that this term's value batch
+        broadcasts to (dimensions aligned on the right, size-1 dimensions broadcast)."""
+        bs = self.batch_shape
+        if not bs:
+            return self
+        tail = idx[len(idx) - len(bs):]
+        sub = self.values[tuple(0 if size == 1 else i for i, size in zip(tail, bs))]
+        return PWCTimeQArray(self.times, sub, self.qarray)
 
     @property
     def discontinuity_ts(self) -> np.ndarray:
@@ -99,12 +113,24 @@ class SummedTimeQArray:
         self.constant = sum(const) if const else np.zeros((n, n), np.complex64)
         self.terms = flat
         for t in self.pwc_terms:
-            if t.shape != self.constant.shape:
+            if t.qarray.shape != self.constant.shape:
                 raise ValueError('All terms of a time-dependent operator must have the same shape.')
+        try:
+            self.batch_shape
+        except ValueError:
+            raise ValueError('The batch shapes of the PWC values do not broadcast together.') from None
 
     @property
     def shape(self) -> tuple[int, ...]:
-        return self.constant.shape
+        return (*self.batch_shape, *self.constant.shape)
+
+    @property
+    def batch_shape(self) -> tuple[int, ...]:
+        return np.broadcast_shapes(*[t.batch_shape for t in self.pwc_terms]) if self.pwc_terms else ()
+
+    def item(self, idx: tuple) -> SummedTimeQArray:
+        """The unbatched operator at index ``idx`` of :attr:`batch_shape`."""
+        return SummedTimeQArray([self.constant] + [t.item(idx) for t in self.pwc_terms])
 
     @property
     def discontinuity_ts(self) -> np.ndarray:

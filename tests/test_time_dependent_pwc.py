@@ -44,7 +44,7 @@ def _lindbladian(H, Ls):
     return out
 
 
-def _exact(H0, drive, Ls, rho0, tsave):
+def _exact(H0, drive, Ls, rho0, tsave, values=VALUES):
     psi = np.asarray(rho0, complex).reshape(-1)
     rho = np.outer(psi, psi.conj())
     Ls = [np.asarray(L, complex) for L in Ls]
@@ -52,7 +52,7 @@ def _exact(H0, drive, Ls, rho0, tsave):
     out, t, vec = [], 0.0, rho.reshape(-1, order='F')
     for a, b in zip(edges[:-1], edges[1:]):
         k = np.searchsorted(TIMES, 0.5 * (a + b), side='right') - 1
-        c = VALUES[k] if 0 <= k < len(VALUES) else 0.0
+        c = values[k] if 0 <= k < len(values) else 0.0
         Lv = _lindbladian(np.asarray(H0, complex) + c * np.asarray(drive, complex), Ls)
         for ts in tsave:
             if (a < ts <= b) or (a == ts == 0.0):
@@ -122,3 +122,41 @@ def test_pwc_mesolve_on_gpu_matches_exact(cuda_device):
     o = _mesolve_piecewise(H, L, rho0, TSAVE, exp_ops=E, method=m, gradient=None,
                            options=dq.Options(), solve=_oracle_solve)
     assert abs(int(res.infos.nsteps) - int(o.infos.nsteps)) <= 5
+
+
+VALUES2 = [[1.0, -0.5, 2.0], [0.2, 0.7, -1.0]]
+
+
+def test_batched_pwc_values_with_oracle():
+    """values of shape (2, N): the result has H's batch dimension first, and each item is
+    the unbatched solve with that row of values."""
+    a = ops.destroy(N, layout='dense')
+    H0 = 0.7 * (ops.dag(a) @ a)
+    H = H0 + dq.pwc(TIMES, VALUES2, a + ops.dag(a))
+    L = [np.float32(np.sqrt(0.2)) * a]
+    m = dq.Tsit5(rtol=1e-9, atol=1e-11)
+    r = _mesolve_piecewise(H, L, ops.fock(N, 0), TSAVE, exp_ops=None, method=m, gradient=None,
+                           options=dq.Options(), solve=_oracle_solve)
+    assert r.states.shape == (2, len(TSAVE), N, N) and r.infos.nsteps.shape == (2,)
+    for i, vals in enumerate(VALUES2):
+        ref = _exact(H0, a + ops.dag(a), L, ops.fock(N, 0), TSAVE, values=vals)
+        err = np.linalg.norm(r.states[i] - ref, axis=(-2, -1)) / np.linalg.norm(ref, axis=(-2, -1))
+        assert err.max() < 1e-7
+
+
+@pytest.mark.gpu
+def test_batched_pwc_values_and_rho0_on_gpu(cuda_device):
+    a = ops.destroy(N, layout='dense')
+    H0 = 0.7 * (ops.dag(a) @ a)
+    drive = a + ops.dag(a)
+    H = H0 + dq.pwc(TIMES, VALUES2, drive)
+    L = [np.float32(np.sqrt(0.2)) * a]
+    rho0 = np.stack([ops.fock(N, 0), ops.fock(N, 1)])
+    res = dq.mesolve(H, L, rho0, TSAVE, method=dq.Tsit5(rtol=1e-6, atol=1e-8))
+    got = res.states.cpu().numpy()
+    assert got.shape == (2, 2, len(TSAVE), N, N)
+    for i, vals in enumerate(VALUES2):
+        for j in range(2):
+            ref = _exact(H0, drive, L, rho0[j], TSAVE, values=vals)
+            err = np.linalg.norm(got[i, j] - ref, axis=(-2, -1)) / np.linalg.norm(ref, axis=(-2, -1))
+            assert err.max() < 1e-5

@@ -27,6 +27,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 # The oracle legs run numpy; its OpenBLAS is built with MAX_THREADS=64, whose threaded
@@ -206,7 +207,7 @@ def run_serving(args):
     for t in srv.finished:
         t.release()
     srv.finished.clear()
-    clk_path = os.path.join(ROOT, 'gpurun_out', 'clocks_rank0.csv')
+    clk_path = os.path.join(tempfile.gettempdir(), 'dqb_bench_clocks_rank0.csv')
     os.makedirs(os.path.dirname(clk_path), exist_ok=True)
     sampler = _clock_sampler(clk_path)
     tickets = []
@@ -376,7 +377,7 @@ def run_b200(args):
     assert int((status != 0).sum()) == 0, 'solver status not OK'
 
     # ---- timed region: device-resident inputs --------------------------------------
-    clk_path = os.path.join(ROOT, 'gpurun_out', f'clocks_rank{rank}.csv')
+    clk_path = os.path.join(tempfile.gettempdir(), f'dqb_bench_clocks_rank{rank}.csv')
     os.makedirs(os.path.dirname(clk_path), exist_ok=True)
     sampler = _clock_sampler(clk_path)
     time.sleep(0.3)

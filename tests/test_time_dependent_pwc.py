@@ -160,3 +160,22 @@ def test_batched_pwc_values_and_rho0_on_gpu(cuda_device):
             ref = _exact(H0, drive, L, rho0[j], TSAVE, values=vals)
             err = np.linalg.norm(got[i, j] - ref, axis=(-2, -1)) / np.linalg.norm(ref, axis=(-2, -1))
             assert err.max() < 1e-5
+
+
+def test_piece_plan_edge_cases():
+    """Discontinuities outside the solve interval or repeated across terms add no piece; a
+    start time before tsave[0] saves nothing at the start; a PWC-only H is zero outside its
+    times."""
+    P1 = dq.pwc([-1.0, 0.5, 9.0], [1.0, 2.0], np.eye(2))
+    P2 = dq.pwc([0.5, 1.0], [3.0], np.eye(2))
+    H = np.zeros((2, 2)) + P1 + P2
+    ts = np.array([0.2, 0.5, 1.5])
+    plan = piecewise_plan(as_summed(H), ts, 0.0)
+    assert [(a, b) for a, b, *_ in plan] == [(0.0, 0.5), (0.5, 1.0), (1.0, 1.5)]
+    kept = np.concatenate([t[k] for *_, t, k in plan])
+    assert np.array_equal(kept, ts)
+    assert plan[0][3][0] == 0.0 and 0 not in plan[0][4]  # t0 = 0 is not a save time
+    assert np.allclose(plan[0][2], np.eye(2)) and np.allclose(plan[1][2], 5 * np.eye(2))
+    assert np.allclose(plan[2][2], 2 * np.eye(2))
+    only = dq.pwc([1.0, 2.0], [4.0], np.eye(2))
+    assert np.allclose(as_summed(only)(0.5), 0) and np.allclose(as_summed(only)(1.5), 4 * np.eye(2))

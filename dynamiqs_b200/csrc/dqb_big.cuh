@@ -351,7 +351,7 @@ static __global__ void init_ctrl_kernel(Common c, int phase) {
     const double d1 = I.acc[1];
     const double d2 = sqrt(I.acc[2] * inv_nn) / I.h0;
     const double md = d1 > d2 ? d1 : d2;
-    const double h1 = md <= 1e-15 ? fmax(1e-6, I.h0 * 1e-3) : pow(0.01 / md, 0.2);
+    const double h1 = md <= 1e-15 ? fmax(1e-6, I.h0 * 1e-3) : pow(0.01 / md, 0.25);
     const double dt = fmin(100.0 * I.h0, h1);
     double tn = I.t + dt;
     if (tn > I.t1 - 1e-10) tn = I.t1;

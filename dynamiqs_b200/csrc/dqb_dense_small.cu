@@ -414,7 +414,7 @@ __device__ void solve_one(const InstView& a, const CtrlOpts& o, float2* sH, floa
   if (tid == 0) {
     const double d2 = sqrt(s2 * inv_nn) / h0;
     const double md = d1 > d2 ? d1 : d2;
-    const double h1 = md <= 1e-15 ? fmax(1e-6, h0 * 1e-3) : pow(0.01 / md, 0.2);
+    const double h1 = md <= 1e-15 ? fmax(1e-6, h0 * 1e-3) : pow(0.01 / md, 0.25);
     const double dt = fmin(100.0 * h0, h1);
     ctl.t = a.t0;
     ctl.t1 = t1;

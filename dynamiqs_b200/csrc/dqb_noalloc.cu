@@ -18,7 +18,11 @@
 //
 // Set-up: the first call on each device looks up the array's device address with
 // cudaGetSymbolAddress (with that device current) and caches it; make that first call
-// before any stream capture.  Every call shares the one array, and a call leaves its
+// before any stream capture.  With lazy module loading (CUDA's default since 12.2) that
+// lookup is also when the driver loads this file's module and reserves the array, so the
+// first call should precede a framework's preallocation (or set
+// CUDA_MODULE_LOADING=EAGER to reserve it at load).  The cache assumes the context of a
+// device is never reset; after cudaDeviceReset the cached address would be stale.  Every call shares the one array, and a call leaves its
 // contents behind: the work counter is cleared (cudaMemsetAsync on the caller's stream)
 // at the start of every call, and the slots need no clearing because every value in them
 // is written before it is read.  Calls whose work overlaps on the GPU -- on different

@@ -154,8 +154,13 @@ DQB_API int dqb_lindblad_rhs_dense(const dqb_dense_problem* problem, int32_t for
  * throughput is lower.  n > 64 returns DQB_ERR_UNSUPPORTED; a problem whose single-instance
  * scratch exceeds the array returns DQB_ERR_SCRATCH_TOO_SMALL.  The first call on each
  * device looks up the array's address (cudaGetSymbolAddress) and should come before any
- * stream capture.  All calls share the array: each clears its work counter first; calls
- * that overlap on the GPU race and must be serialised by the caller. */
+ * stream capture.  Under CUDA's lazy module loading (the default since CUDA 12.2) the
+ * driver reserves the array at that first call, not when the library loads
+ * (CUDA_MODULE_LOADING=EAGER reserves it at load): make the first call before a
+ * framework preallocates its pool.  The address is cached per device index and assumes
+ * the device's context is never reset (after cudaDeviceReset it would be stale).  All
+ * calls share the array: each clears its work counter first; calls that overlap on the
+ * GPU race and must be serialised by the caller. */
 #define DQB_NOALLOC_SCRATCH_BYTES (8u << 20)
 DQB_API int dqb_mesolve_dense_noalloc(const dqb_dense_problem* problem, const dqb_ode_options* options,
                                       const dqb_outputs* outputs, void* stream);

@@ -1,9 +1,9 @@
 """Extract the known answers for the mesolve hot path from the reference's own docs.
 
-Run from the repository root with the reference checked out (read-only) at
-``/root/reference``::
+Run from the repository root with the path of a read-only checkout of the reference
+as the only argument::
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 
 It reads printed outputs (step counts, final states, expectation values) from the
 reference's README, docstrings and docs pages, and writes ``known_answers.json`` next to
@@ -103,4 +103,6 @@ def main(ref: str) -> None:
 
 
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    if len(sys.argv) != 2:
+        sys.exit('usage: python tests/golden/make_golden.py <reference checkout>')
+    main(sys.argv[1])

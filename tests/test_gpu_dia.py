@@ -2,9 +2,8 @@
 against the oracle's DIA restatement (``oracle.lindblad``, following
 dynamiqs/qarrays/sparsedia_primitives.py) and against the dense kernel.
 
-Bars as in test_gpu_dense: 1e-5 relative Frobenius per saved state / on expectation
-values (widened to twice the oracle's own complex64 error on stiff problems); single
-right-hand sides 2e-6 relative."""
+Solves are held to the bar of tests/parity.py; single right-hand sides are compared at
+2e-6 relative."""
 
 import ctypes
 
@@ -17,6 +16,7 @@ from dynamiqs_b200 import _lib, workloads
 from dynamiqs_b200.qarrays import SparseDIA
 from oracle import lindblad as lb
 from oracle.mesolve import mesolve as oracle_mesolve
+from tests.parity import assert_solve_parity
 
 pytestmark = pytest.mark.gpu
 
@@ -89,17 +89,12 @@ def test_rhs_dia_matches_oracle(cuda_device, form, n, tile):
         assert rel_frob(got[b], ref) < 2e-6
 
 
-def _oracle_compare(res, w, b, **kw):
+def _oracle_compare(res, w, b, method='Tsit5'):
     H = (w['H'].offsets, w['H'].diags[b])
     Ls = [(L.offsets, L.diags) for L in w['jump_ops']]
     m = w['method']
-    r = oracle_mesolve(H, Ls, w['rho0'], w['tsave'], rtol=m.rtol, atol=m.atol, **kw)
-    r64 = oracle_mesolve(H, Ls, w['rho0'], w['tsave'], rtol=m.rtol, atol=m.atol,
-                         dtype=np.complex64, **kw)
-    got = res.states[b].cpu().numpy()
-    tol = max(1e-5, 2 * rel_frob(r64.states, r.states).max())
-    assert rel_frob(got, r.states).max() < tol
-    assert abs(int(res.infos.nsteps[b]) - r.nsteps) <= max(1, int(0.002 * r.nsteps))
+    return assert_solve_parity(res.states[b].cpu().numpy(), None, int(res.infos.nsteps[b]), H,
+                               Ls, w['rho0'], w['tsave'], None, method, m.rtol, m.atol)
 
 
 def test_coupled_kerr_dia_small_vs_oracle(cuda_device):
@@ -143,6 +138,55 @@ def test_dia_expects_save_states_false_and_standard_form(cuda_device):
     np.testing.assert_allclose(full.expects[0, 0].cpu().numpy(), ref_e, rtol=1e-5, atol=1e-5)
     assert rel_frob(std.states.cpu().numpy(), full.states.cpu().numpy()).max() < 1e-5
     np.testing.assert_allclose(std.expects.cpu().numpy(), full.expects.cpu().numpy(), rtol=1e-5, atol=1e-5)
+
+
+@pytest.fixture(scope='module')
+def coupled_kerr_4096_rhs():
+    """Coupled-Kerr operators at their full size (two 64-level modes, n = 4096; H offsets
+    {-64, -63, 0, 63, 64}, jumps {+64} and {+1}), a random hermitian X and the oracle's
+    hermitian right-hand side of it in complex128."""
+    w = workloads.coupled_kerr_dia(batch=1, m=64, seed=0)
+    n = 4096
+    rng = np.random.default_rng(4096)
+    Y = (rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))) / (2 * n)
+    X = (Y + np.conj(Y.T)).astype(np.complex64)
+    Hb = (w['H'].offsets, w['H'].diags[0].astype(complex))
+    Lb = [(L.offsets, L.diags.astype(complex)) for L in w['jump_ops']]
+    ref = lb.vf_hermitian_dia(Hb, Lb, X.astype(complex))
+    return w, X, ref
+
+
+@pytest.mark.parametrize('tile', [0, 4, 8, 16, 108, 116])
+def test_rhs_dia_full_size_every_stencil(cuda_device, coupled_kerr_4096_rhs, tile):
+    """One right-hand side at n = 4096 with the workload's own offsets (+-63/+-64 select
+    other row groups in the staged kernel and other halos in the tiled one than the small
+    cases above) through every stencil shape, against the oracle at 2e-6."""
+    w, X, ref = coupled_kerr_4096_rhs
+    n = 4096
+    Ls = [SparseDIA(L.offsets, L.diags[None]) for L in w['jump_ops']]
+    p, keep = _problem_struct(w['H'], Ls, n, 1)
+    r_d = torch.from_numpy(np.ascontiguousarray(X[None])).to('cuda')
+    out = torch.empty_like(r_d)
+    ws = torch.empty(1 << 20, dtype=torch.uint8, device='cuda')
+    lib = _lib.load()
+    _lib.check(lib.dqb_lindblad_rhs_dia_tiled(p, _lib.FORM_HERMITIAN, tile, r_d.data_ptr(),
+                                              out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                              torch.cuda.current_stream().cuda_stream), 'rhs_dia')
+    assert rel_frob(out[0].cpu().numpy(), ref) < 2e-6
+
+
+def test_dia_full_size_short_solve_vs_oracle(cuda_device):
+    """The n = 4096 coupled-Kerr solve (Tsit5 1e-5/1e-7) over t in [0, 0.05] against the
+    oracle (complex128 state) at 1e-5 on every saved state, with equal step counts."""
+    w = workloads.coupled_kerr_dia(batch=1, m=64, seed=0)
+    ts = np.linspace(0.0, 0.05, 3)
+    m = w['method']
+    res = dq.mesolve(w['H'], w['jump_ops'], w['rho0'], ts, method=m)
+    H = (w['H'].offsets, w['H'].diags[0])
+    Ls = [(L.offsets, L.diags) for L in w['jump_ops']]
+    r = oracle_mesolve(H, Ls, w['rho0'], ts, rtol=m.rtol, atol=m.atol)
+    assert rel_frob(res.states[0].cpu().numpy(), r.states).max() < 1e-5
+    assert (int(res.infos.nsteps[0]), int(res.infos.nrejected[0])) == (r.nsteps, r.nrejected)
 
 
 def test_dia_full_size_properties(cuda_device):

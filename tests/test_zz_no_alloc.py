@@ -21,6 +21,7 @@ from dynamiqs_b200 import _lib, workloads
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-5
+NOALLOC_SCRATCH_BYTES = 8 << 20  # DQB_NOALLOC_SCRATCH_BYTES in include/dqb200.h
 
 
 def _problem(batch, seed):
@@ -77,21 +78,30 @@ def test_noalloc_matches_workspace_entry_point(cuda_device):
     torch.cuda.synchronize()
     assert int((ref['status'] != 0).sum()) == 0
 
-    for call in range(2):
+    drops = []
+    for call in range(4):
         got, got_s = _outputs(batch, nt)
         torch.cuda.synchronize()
         free_before = torch.cuda.mem_get_info()[0]
         _lib.check(lib.dqb_mesolve_dense_noalloc(prob, opts, got_s, stream),
                    'dqb_mesolve_dense_noalloc')
         torch.cuda.synchronize()
-        if call == 1:  # after the first call's one-time set-up, nothing is allocated
-            assert torch.cuda.mem_get_info()[0] == free_before
+        drops.append(free_before - torch.cuda.mem_get_info()[0])
+        if call >= 2:
+            continue  # calls 2 and 3 only add samples of free memory
         assert int((got['status'] != 0).sum()) == 0
         assert _rel(got['states'], ref['states']) < TOL
         e_err = ((got['expects'] - ref['expects']).abs()
                  / ref['expects'].abs().clamp(min=1.0)).max().item()
         assert e_err < TOL
         assert torch.equal(got['infos'], ref['infos'])
+    # Free device memory is a device-wide figure (other processes can move it), so the
+    # check is coarse: the first call may reserve the static array when the driver loads
+    # its module lazily (at most the array plus page rounding); no later call takes as
+    # much as one instance slot (288 KiB at n = 64), so none allocates scratch.
+    slot = 9 * 64 * 64 * 8
+    assert drops[0] <= NOALLOC_SCRATCH_BYTES + (4 << 20), drops
+    assert all(d < slot for d in drops[1:]), drops
 
 
 def test_noalloc_rejects_sizes_beyond_its_kernel(cuda_device):

@@ -29,6 +29,7 @@ class OracleResult:
     nrejected: int
     status: int
     final_state: np.ndarray
+    errors: list  # (t, h, scaled error) of every attempted step
 
 
 def _as_dense(op, n):
@@ -106,7 +107,7 @@ def mesolve(H, Ls, rho0, tsave, exp_ops=None, *, method='Tsit5', rtol=1e-6, atol
     if not save_states:
         states = final[None]
     return OracleResult(states, expects, out.nsteps, out.naccepted, out.nrejected,
-                        out.status, final)
+                        out.status, final, out.errors)
 
 
 def sesolve(H, psi0, tsave, *, method='Tsit5', rtol=1e-6, atol=1e-6, dtype=np.complex128,

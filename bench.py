@@ -98,8 +98,14 @@ def _peaks():
 # CPU legs (oracle)
 # --------------------------------------------------------------------------------------
 
+def _kerr_config(batch):
+    return {'workload': CASES['kerr'], 'batch_per_gpu': batch, 'n': 64, 'n_jumps': 2,
+            'n_tsave': 51, 'method': 'Tsit5', 'rtol': 1e-6, 'atol': 1e-8}
+
+
 def _oracle_solve(args):
-    """One oracle solve of instance `b` of the workload (complex64 state)."""
+    """One oracle solve of instance `b` of the workload (complex64 state); returns its
+    number of attempted steps."""
     b, seed = args
     from dynamiqs_b200 import workloads
     from oracle.mesolve import mesolve as om
@@ -120,38 +126,52 @@ def cpu_baseline(sample: int = 3, seed: int = 0) -> dict:
                       f'(complex64 state, 1 thread), {dt:.1f} s'}
 
 
+def _host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
 def run_reference(args):
+    """The reference's loop restated on the CPU (the oracle: numpy, complex64 state, one
+    thread per process) on every host core, through one continuous work queue: each step is
+    a sample of 2 x cores distinct instances of the workload's batch, all steps' instances
+    are queued at once (imap_unordered, chunksize 1), so no core idles at a step boundary
+    and the timed throughput is load-balanced; the only tail is the last few instances."""
     import multiprocessing as mp
 
     rank = int(os.environ.get('RANK', 0))
     if rank != 0:
         return
-    cores = os.cpu_count() or 1
-    per_step = cores  # one instance per core per step
+    cores = _host_cores()
+    per_step = 2 * cores
     ctx = mp.get_context('spawn')
     os.environ.setdefault('OMP_NUM_THREADS', '1')
     os.environ.setdefault('OPENBLAS_NUM_THREADS', '1')
     os.environ.setdefault('MKL_NUM_THREADS', '1')
+    B = 4096
+    tasks = [(i % B, i // B) for i in range(args.steps * per_step)]
     with ctx.Pool(cores) as pool:
-        for w in range(args.warmup):
-            pool.map(_oracle_solve, [(b, 1000 + w) for b in range(per_step)])
-        times = []
-        for s in range(args.steps):
-            t = time.perf_counter()
-            pool.map(_oracle_solve, [(b, s) for b in range(per_step)])
-            times.append(time.perf_counter() - t)
-    total = sum(times)
-    value = per_step * args.steps / total
+        warm = [(B - 1 - i, 1000 + w) for w in range(args.warmup) for i in range(cores)]
+        for _ in pool.imap_unordered(_oracle_solve, warm, chunksize=1):
+            pass
+        t = time.perf_counter()
+        steps_done = sum(pool.imap_unordered(_oracle_solve, tasks, chunksize=1))
+        total = time.perf_counter() - t
+    value = len(tasks) / total
     line = {
         'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'solves/s',
         'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': 1e3 * total / args.steps, 'higher_is_better': True, 'scaling': 'weak',
-        'vs_baseline': None, 'dtype': 'c64', 'data': 'synthetic (seeded)',
-        'config': {'workload': CASES['kerr'], 'sample_per_step': per_step},
+        'vs_baseline': None, 'dtype': 'c64', 'data': 'synthetic (seeded numpy generator; no dataset)',
+        'config': dict(_kerr_config(B), sample_per_step=per_step,
+                       avg_rk_steps_of_sample=steps_done / len(tasks)),
         'cpu_baseline': {'value': value, 'unit': 'solves/s', 'cores': cores, 'kind': 'port',
-                         'sample': f'{per_step} instances per step (one per core) through '
-                                   'the numpy oracle; the reference (JAX + diffrax) is not '
-                                   'installed on this image'},
+                         'sample': f'{args.steps} steps x {per_step} distinct instances of the '
+                                   'workload (instances 0.. of its seed-0 batch) through the numpy '
+                                   'oracle, one process per core, one work queue; the reference '
+                                   '(JAX + diffrax) is not installed on this image'},
         'e2e': {'value': value, 'unit': 'solves/s', 'h2d_bytes_per_step': 0,
                 'd2h_bytes_per_step': 0},
     }
@@ -332,6 +352,67 @@ def _kernels_per_launch(path: str, K: int, iterations: int) -> int:
     return init + body * iterations + 3
 
 
+def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which):
+    """Roofline record of the dominant kernel of a solve launch: `nsteps` (tensor) is the
+    attempted RK steps of every instance, `mean_ms` the launch's mean duration."""
+    import torch
+
+    if config == 'dia':
+        # algorithmic HBM bytes per attempted step and instance (a fully fused Tsit5 step
+        # touches 34 n x n complex64 matrices: stages 2-6 read y and k_1..k_{i-1} and write
+        # k_i, 25 passes; y1, k7 and the error estimate 9 more)
+        nbytes = float((34 * 8.0 * n * n * nsteps).sum())
+        achieved = nbytes / (mean_ms / 1e3) / 1e9
+        return {'bound': 'hbm', 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
+                'frac': achieved / peaks['hbm_gbs'], 'peak_source': f'hbm_gbs ({which})',
+                'traffic': _traffic(config, precision, B, nsteps),
+                'algorithmic_bytes_per_launch': nbytes,
+                'note': 'bytes = 34 n^2 complex64 matrix passes per attempted RK step per '
+                        'instance (the fused-step minimum); the kernels today make 54'}
+    rhs_evals = float((6 * nsteps + 2).sum())
+    flops = rhs_evals * _flops_per_rhs(n, K)
+    achieved = flops / (mean_ms / 1e3) / 1e12
+    peak = peaks.get('bf16_tflops_sustained', peaks.get('bf16_tflops'))
+    roof = {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
+            'frac': achieved / peak, 'peak_source': f'bf16_tflops_sustained ({which})',
+            'traffic': _traffic(config, precision, B, nsteps), 'algorithmic_flops_per_launch': flops}
+    if precision == 'fp32' or (precision in ('tf32x3', 'bf16x3', 'tf32') and n <= 64):
+        roof['note'] = ('products run on the FP32 CUDA-core pipe (SIMT), not the tensor '
+                        'pipe; see roofline_fp32_simt')
+        if n <= 64 and K > 0:
+            R = (16 if n <= 16 else (32 if n <= 32 else 64)) // 16
+            part = (R + 1) * R / 2 / (R * R)
+            roof['note'] += ('. Algorithmic flops count (1+2K) complex products per RHS; '
+                             f'the hermitian form computes (L X) L^+ on {part:.3f} of the '
+                             'tile pairs, so the kernel executes '
+                             f'{(1 + K + K * part) / (1 + 2 * K):.3f} of them')
+    elif precision in ('f16x3', 'auto') and n <= 64:
+        roof['note'] = ('products run on tcgen05 tensor cores (f16x3: a complex 64^3 product is '
+                        'one 128x128x64 real MMA, the same real work, taken three times on the hi '
+                        'and lo FP16 parts, so the tensor pipe executes 3x the algorithmic flops)')
+    else:
+        roof['note'] = (f'products run on tcgen05 tensor cores ({precision}: three products '
+                        'per complex MAC term, so the tensor pipe executes 3x the algorithmic '
+                        'flops)')
+    return roof
+
+
+# DRAM bytes (read + write) per unit of work of each solve kernel, from one ncu capture of
+# dram__bytes_read.sum + dram__bytes_write.sum on a smaller launch of the same workload,
+# scaled to the launch by the units it processes (profiles/ names each capture):
+#   per instance for the n <= 64 kernels (inputs, states and expectation values out; the RK
+#   slots stay in L2), per instance-step for the DIA stepper.
+TRAFFIC_PER_UNIT = {}
+
+
+def _traffic(config, precision, B, nsteps):
+    key = (config, precision)
+    if key not in TRAFFIC_PER_UNIT:
+        return None
+    unit, per = TRAFFIC_PER_UNIT[key]
+    return float(per * (B if unit == 'instance' else float(nsteps.sum())))
+
+
 def run_b200(args):
     import torch
 
@@ -404,37 +485,7 @@ def run_b200(args):
     value = world * B * args.steps / (kern / 1e3)
     mean_ms = kern / args.steps
     peaks, which = _peaks()
-    if args.config == 'dia':
-        # algorithmic HBM bytes per attempted step and instance: stage inputs (25 matrix
-        # passes), y1 (8), six right-hand sides (read X, write k: 12), error (9)
-        nbytes = float((54 * 8.0 * n * n * nsteps).sum())
-        achieved = nbytes / (mean_ms / 1e3) / 1e9
-        roof = {'bound': 'hbm', 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
-                'frac': achieved / peaks['hbm_gbs'], 'peak_source': f'hbm_gbs ({which})',
-                'traffic': None, 'algorithmic_bytes_per_launch': nbytes,
-                'note': 'bytes = 54 n^2 complex64 matrix passes per attempted RK step per instance'}
-    else:
-        rhs_evals = float((6 * nsteps + 2).sum())
-        flops = rhs_evals * _flops_per_rhs(n, K)
-        achieved = flops / (mean_ms / 1e3) / 1e12
-        peak = peaks.get('bf16_tflops_sustained', peaks.get('bf16_tflops'))
-        roof = {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
-                'frac': achieved / peak, 'peak_source': f'bf16_tflops_sustained ({which})',
-                'traffic': None, 'algorithmic_flops_per_launch': flops}
-        if args.precision == 'fp32':
-            roof['note'] = ('products run on the FP32 CUDA-core pipe (SIMT), not the tensor '
-                            'pipe; see roofline_fp32_simt')
-            if n <= 64 and K > 0:
-                R = (16 if n <= 16 else (32 if n <= 32 else 64)) // 16
-                part = (R + 1) * R / 2 / (R * R)
-                roof['note'] += ('. Algorithmic flops count (1+2K) complex products per RHS; '
-                                 f'the hermitian form computes (L X) L^+ on {part:.3f} of the '
-                                 'tile pairs, so the kernel executes '
-                                 f'{(1 + K + K * part) / (1 + 2 * K):.3f} of them')
-        else:
-            roof['note'] = (f'products run on tcgen05 tensor cores ({args.precision}: three '
-                            'products per complex MAC term, so the tensor pipe executes 3x the '
-                            'algorithmic flops)')
+    roof = _roofline(args.config, args.precision, n, K, nsteps, mean_ms, B, peaks, which)
 
     # ---- e2e: public API from host inputs --------------------------------------------
     e2e = None
@@ -532,7 +583,56 @@ def run_b200(args):
     }
     if args.config == 'kerr' and not args.no_cpu_baseline:
         line['cpu_baseline'] = cpu_baseline(sample=args.cpu_sample)
+    if args.config == 'kerr' and world == 1 and not args.no_extra:
+        line['extra_configs'] = _extra_configs(args, dev, stream, flush, peaks, which)
     print(json.dumps(line), flush=True)
+
+
+def _extra_configs(args, dev, stream, flush, peaks, which):
+    """The tensor-core GEMM path (transmon x cavity, n = 256, 3xTF32) and the sparse-DIA
+    path (coupled Kerr modes, n = 4096) measured in the same run as the headline, on
+    device-resident inputs with the headline's timing rules (CUDA events on the launching
+    stream, L2 flushed between launches), 3 warm-up and 2 timed launches each."""
+    import torch
+
+    import dynamiqs_b200 as dq
+    from dynamiqs_b200.mesolve import MESolveB200Integrator, make_batch_plan
+
+    out = {}
+    for key, cfg, prec in (('transmon_tf32x3', 'transmon', 'tf32x3'), ('coupled_kerr_dia', 'dia', 'fp32')):
+        sub = argparse.Namespace(**vars(args))
+        sub.batch, sub.n, sub.tend = 0, 0, 10.0
+        w = _workload(cfg, sub, 0)
+        plan = make_batch_plan(w['H'], w['jump_ops'], w['rho0'], True)
+        prep = MESolveB200Integrator(ts=w['tsave'], y0=w['rho0'], method=w['method'], gradient=None,
+                                     options=dq.Options(precision=prec), H=w['H'], Ls=w['jump_ops'],
+                                     Es=w.get('exp_ops'), plan=plan).prepare()
+        for _ in range(3):
+            prep.launch(stream.cuda_stream)
+        torch.cuda.synchronize()
+        assert int((prep.bufs['status'] != 0).sum()) == 0, f'{key}: solver status not OK'
+        ms = []
+        for _ in range(2):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            prep.launch(stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        nsteps = prep.bufs['infos'][:, 0].to(torch.float64)
+        B = plan.batch
+        n = int(w['H'].shape[-1])
+        mean_ms = float(np.mean(ms))
+        out[key] = {'workload': CASES[cfg], 'path': prep.name, 'precision': prec,
+                    'value': B / (mean_ms / 1e3), 'unit': 'solves/s', 'ms_per_step': mean_ms,
+                    'steps': 2, 'warmup': 3, 'batch': B, 'avg_rk_steps': float(nsteps.mean()),
+                    'max_rk_steps': float(nsteps.max()),
+                    'roofline': _roofline(cfg, prec, n, len(w['jump_ops']), nsteps, mean_ms, B,
+                                          peaks, which)}
+        del prep
+        torch.cuda.empty_cache()
+    return out
 
 
 def main():
@@ -554,8 +654,12 @@ def main():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-plain', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--precision', default='fp32', choices=['fp32', 'tf32x3', 'bf16x3', 'tf32', 'auto'],
-                    help='arithmetic of the GEMM path (n > 64) products')
+    ap.add_argument('--no-extra', action='store_true',
+                    help='skip the GEMM-path and DIA lines the kerr run adds (extra_configs)')
+    ap.add_argument('--precision', default='fp32',
+                    choices=['fp32', 'tf32x3', 'bf16x3', 'tf32', 'f16x3', 'auto'],
+                    help='arithmetic of the complex products (tf32x3 / bf16x3 / tf32: GEMM '
+                         'path, n > 64; f16x3: the n <= 64 kernel)')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

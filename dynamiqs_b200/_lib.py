@@ -43,7 +43,9 @@ PREC_FP32 = 0
 PREC_TF32X3 = 1
 PREC_BF16X3 = 2
 PREC_TF32 = 3
-PRECISIONS = {'fp32': PREC_FP32, 'tf32x3': PREC_TF32X3, 'bf16x3': PREC_BF16X3, 'tf32': PREC_TF32}
+PREC_F16X3 = 4
+PRECISIONS = {'fp32': PREC_FP32, 'tf32x3': PREC_TF32X3, 'bf16x3': PREC_BF16X3, 'tf32': PREC_TF32,
+              'f16x3': PREC_F16X3}
 
 
 class OdeOptions(ctypes.Structure):
@@ -146,6 +148,8 @@ SIGNATURES = {
     'dqb_mesolve_dense_noalloc': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
                                                  ctypes.POINTER(Outputs), _P]),
     'dqb_lindblad_rhs_dense': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.c_int32, _P, _P, _P]),
+    'dqb_lindblad_rhs_dense_prec': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.c_int32,
+                                                   ctypes.c_int32, _P, _P, _P, ctypes.c_size_t, _P]),
     'dqb_mesolve_dense_large_workspace_size': (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32,
                                                                  ctypes.c_int32, ctypes.c_int32,
                                                                  ctypes.c_int64]),

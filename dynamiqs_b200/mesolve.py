@@ -266,10 +266,13 @@ class PreparedSolve:
                                        b['infos'], b['status'])
 
 
-def _precision_code(o, form: int) -> int:
-    """DQB_PREC_* for ``Options.precision``; the tensor-core modes need the hermitian form.
-    ``'auto'`` maps to FP32 here; the GEMM path's prepare step replaces it with the
-    autotuner's choice."""
+def _precision_code(o, form: int, path: str = 'large') -> int:
+    """DQB_PREC_* for ``Options.precision`` on `path` ('small': the n <= 64 kernel,
+    'large': the GEMM path, 'dia'); the tensor-core modes need the hermitian form.
+    'f16x3' applies to the n <= 64 kernel only and the TF32/BF16 modes to the GEMM path
+    only: elsewhere they mean FP32.  ``'auto'`` maps to FP32 here (the n <= 64 kernel keeps
+    the reference's error control only in FP32: see Options.precision); the GEMM path's
+    prepare step replaces it with the autotuner's choice."""
     if o.precision == 'auto':
         return _lib.PREC_FP32
     try:
@@ -280,6 +283,8 @@ def _precision_code(o, form: int) -> int:
     if code != _lib.PREC_FP32 and form != _lib.FORM_HERMITIAN:
         raise ValueError('Option `precision` other than "fp32" needs the hermitian form '
                          '(assume_hermitian=True, vectorized=False).')
+    if (code == _lib.PREC_F16X3) != (path == 'small'):
+        return _lib.PREC_FP32
     return code
 
 
@@ -299,6 +304,7 @@ class MESolveB200Integrator:
         self.Es = Es
         self.plan = plan
         self._tuned: dict = {}  # launch choices made by the autotuner at prepare time
+        self._path = 'large'  # 'small', 'large' or 'dia': set by prepare()
 
     @property
     def t0(self) -> float:
@@ -315,7 +321,7 @@ class MESolveB200Integrator:
             factormin=float(m.min_factor), factormax=float(m.max_factor),
             max_steps=int(m.max_steps), t0=self.t0, save_states=int(bool(o.save_states)),
             check_hermitian=int(bool(o.assume_hermitian)),
-            precision=self._tuned.get('precision', _precision_code(o, form)),
+            precision=self._tuned.get('precision', _precision_code(o, form, self._path)),
             tile=self._tuned.get('tile', 0))
 
     def _form(self) -> int:
@@ -338,6 +344,7 @@ class MESolveB200Integrator:
         if dia_ops:
             return self._prepare_dia(lib)
         return self._prepare_dense(lib, 'large')
+
 
     def _common_buffers(self, dev, n, ntsave, nE, B, nsave):
         import torch
@@ -373,6 +380,7 @@ class MESolveB200Integrator:
     def _prepare_dense(self, lib, kind) -> PreparedSolve:
         import torch
 
+        self._path = kind
         dev = _device()
         n, K, ntsave, B, nE, nsave = self._sizes()
         c64 = torch.complex64
@@ -455,6 +463,7 @@ class MESolveB200Integrator:
 
         import torch
 
+        self._path = 'dia'
         dev = _device()
         n, K, ntsave, B, nE, nsave = self._sizes()
         plan = self.plan

@@ -19,12 +19,17 @@ class Options:
     nmaxclick: int = 10_000
     vectorized: bool = False
     assume_hermitian: bool = True
-    # Arithmetic of the complex products on the dense GEMM path (n > 64): 'fp32' (CUDA
-    # cores, default), 'tf32x3' or 'bf16x3' (tcgen05 tensor cores on hi + lo operand
-    # splits, FP32 accumulation), 'tf32' (one TF32 pass, ~1e-3: error studies only).
-    # 'auto' lets the autotuner pick the faster of 'fp32' and 'tf32x3' for the problem's
-    # (n, jumps, batch).  An addition of this library; the n <= 64 and sparse-DIA kernels
-    # always run FP32.
+    # Arithmetic of the complex products (an addition of this library): 'fp32' (CUDA
+    # cores, default); on the dense GEMM path (n > 64) 'tf32x3' or 'bf16x3' (tcgen05
+    # tensor cores on hi + lo operand splits, FP32 accumulation) or 'tf32' (one TF32 pass,
+    # ~1e-3: error studies only); on the n <= 64 kernel 'f16x3' (tcgen05 on FP16 hi + lo
+    # splits of power-of-two-scaled operands, for 32 < n <= 64, at most two jumps; other
+    # problems run FP32), ~1.4x faster on the batched-Kerr workload but with ~38 bits of
+    # dynamic range: entries below ~2^-38 of a matrix's largest are flushed, so the error
+    # control no longer sees a density matrix's far tail and takes fewer, larger steps
+    # than the reference (states stay as accurate against an FP64 solution).  'auto' lets
+    # the autotuner pick the faster of 'fp32' and 'tf32x3' on the GEMM path and means
+    # 'fp32' elsewhere.  The sparse-DIA kernels always run FP32.
     precision: str = 'fp32'
 
     def initialise(self) -> Options:

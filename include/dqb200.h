@@ -55,15 +55,20 @@ extern "C" {
 #define DQB_FORM_HERMITIAN 0 /* tmp = Hnh rho + 1/2 sum L rho L^+ ; out = tmp + tmp^+ */
 #define DQB_FORM_STANDARD 1  /* Hnh rho + rho Hnh^+ + sum L rho L^+                 */
 
-/* Arithmetic of the GEMM path's complex products (dqb_mesolve_dense_large and its ragged
- * and right-hand-side entry points; the n <= 64 and DIA kernels always use FP32 CUDA
- * cores).  The tensor-core modes run tcgen05 MMAs with FP32 accumulation in tensor
- * memory, on each operand split into hi + lo parts (three products hi*hi + hi*lo + lo*hi);
- * they need the hermitian form and an even n (else DQB_ERR_UNSUPPORTED). */
+/* Arithmetic of the complex products.  The tensor-core modes run tcgen05 MMAs with FP32
+ * accumulation in tensor memory, on each operand split into hi + lo parts (three products
+ * hi*hi + hi*lo + lo*hi).  TF32X3, BF16X3 and TF32 apply to the GEMM path
+ * (dqb_mesolve_dense_large and its ragged and right-hand-side entry points), where they
+ * need the hermitian form and an even n (else DQB_ERR_UNSUPPORTED).  F16X3 applies to the
+ * n <= 64 persistent kernel (dqb_mesolve_dense) for 32 < n <= 64, at most two jump
+ * operators and the hermitian form; other problems given F16X3 run on FP32 CUDA cores.
+ * The sparse-DIA kernels always use FP32 CUDA cores. */
 #define DQB_PREC_FP32 0    /* FP32 FMA on CUDA cores (default)                         */
 #define DQB_PREC_TF32X3 1  /* 3 x TF32 tensor-core products, ~2^-21 relative per product */
 #define DQB_PREC_BF16X3 2  /* 3 x BF16 tensor-core products, ~2^-17 relative per product */
 #define DQB_PREC_TF32 3    /* 1 x TF32 (hi*hi only), ~2^-11: for error studies          */
+#define DQB_PREC_F16X3 4   /* 3 x FP16 tensor-core products of operands scaled by powers
+                              of two, ~2^-22 relative per product                        */
 
 /* Mirrors dq.method.Tsit5 / Dopri5 (dynamiqs/method.py:121-127,356-476) and the
  * mesolve options that reach the integrator (dynamiqs/options.py:17-77). */
@@ -79,7 +84,7 @@ typedef struct dqb_ode_options {
   double t0;               /* start time: tsave[0] unless options.t0 is set             */
   int32_t save_states;     /* 1: state at every tsave; 0: final state only              */
   int32_t check_hermitian; /* 1: flag rho0 that fails isherm(rtol=atol=1e-5)            */
-  int32_t precision;       /* DQB_PREC_* (GEMM path only; 0 = FP32)                     */
+  int32_t precision;       /* DQB_PREC_* (0 = FP32; see above for the paths of each)   */
   int32_t tile;            /* launch-shape choice of the sparse-DIA stencil: 4, 8 or 16 =
                               tiled kernel with that many rows per thread; 108 or 116 =
                               staged kernel with 8 or 16 rows per CTA; 0 (default) or 1 =
@@ -140,6 +145,14 @@ DQB_API int dqb_mesolve_dense(const dqb_dense_problem* problem, const dqb_ode_op
  * diffrax_integrator.py:312-323).  rho, out: complex64 [batch, n, n]. n <= 64. */
 DQB_API int dqb_lindblad_rhs_dense(const dqb_dense_problem* problem, int32_t form,
                            const void* rho, void* out, void* stream);
+
+/* Same, with the products in `precision`: DQB_PREC_F16X3 runs the tensor-core
+ * right-hand side of dqb_mesolve_dense (32 < n <= 64, n_jumps <= 2, hermitian form; else
+ * DQB_ERR_UNSUPPORTED) and needs a `workspace` of batch * 32768 bytes; DQB_PREC_FP32 is
+ * dqb_lindblad_rhs_dense (no workspace). */
+DQB_API int dqb_lindblad_rhs_dense_prec(const dqb_dense_problem* problem, int32_t form,
+                                        int32_t precision, const void* rho, void* out,
+                                        void* workspace, size_t workspace_bytes, void* stream);
 
 /* Same solve as dqb_mesolve_dense, for callers that cannot allocate device memory.
  * No counterpart in the reference (it is an addition of this library).  Who needs it:

@@ -18,6 +18,9 @@
    smaller, complex128) must be at most twice the oracle's own error at the same
    tolerances (and at most 1e-5 where the oracle's is smaller), and the oracle's run
    must show an error estimate within 0.1 of the acceptance threshold.
+
+Step counts: within max(1, 0.2 %) of the oracle's; within max(2, 1 %) when the oracle's
+run has such borderline decisions (one decision taken the other way costs up to two).
 """
 
 from __future__ import annotations
@@ -50,10 +53,14 @@ def assert_solve_parity(states, expects, nsteps, H, Ls, rho0, tsave, exp_ops, me
     states = np.asarray(states)
     s_err = rel_frob(states, r.states).max()
     e_err = expect_err(expects, r.expects).max() if exp_ops else 0.0
+    borderline = any(abs(e - 1.0) < 0.1 for (_, _, e) in r.errors)
     if s_err <= STATE_RTOL and e_err <= EXPECT_TOL:
-        assert abs(int(nsteps) - r.nsteps) <= max(1, int(0.002 * r.nsteps)), (nsteps, r.nsteps)
+        # one accept/reject decision taken the other way near the threshold adds an attempt
+        # and shifts the later step sizes: up to two steps per such decision
+        slack = max(2, int(0.01 * r.nsteps)) if borderline else max(1, int(0.002 * r.nsteps))
+        assert abs(int(nsteps) - r.nsteps) <= slack, (nsteps, r.nsteps)
         return 'trajectory'
-    assert any(abs(e - 1.0) < 0.1 for (_, _, e) in r.errors), \
+    assert borderline, \
         f'trajectory parity failed ({s_err:.2e}) without a borderline controller decision'
     tight = oracle_mesolve(H, Ls, rho0, tsave, rtol=rtol * 1e-3, atol=atol * 1e-3, **kw)
     gpu_s = rel_frob(states, tight.states).max()
@@ -65,3 +72,16 @@ def assert_solve_parity(states, expects, nsteps, H, Ls, rho0, tsave, exp_ops, me
         assert gpu_e <= max(EXPECT_TOL, 2 * ref_e), (gpu_e, ref_e)
     assert abs(int(nsteps) - r.nsteps) <= max(1, int(0.01 * r.nsteps)), (nsteps, r.nsteps)
     return 'accuracy'
+
+
+def assert_accuracy(states, H, Ls, rho0, tsave, method_name, rtol, atol, **okw) -> None:
+    """The accuracy bar alone (for arithmetic whose error control is not the reference's,
+    such as the FP16-split tensor-core mode): every saved state's error against a tight
+    FP64 solution is at most twice the oracle's own error at the same tolerances, or 1e-5."""
+    kw = dict(method=method_name, **okw)
+    r = oracle_mesolve(H, Ls, rho0, tsave, rtol=rtol, atol=atol, **kw)
+    tight = oracle_mesolve(H, Ls, rho0, tsave, rtol=rtol * 1e-3, atol=atol * 1e-3, **kw)
+    gpu_s = rel_frob(states, tight.states).max()
+    ref_s = rel_frob(r.states, tight.states).max()
+    assert gpu_s <= max(STATE_RTOL, 2 * ref_s), (gpu_s, ref_s)
+

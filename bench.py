@@ -352,7 +352,7 @@ def _kernels_per_launch(path: str, K: int, iterations: int) -> int:
     return init + body * iterations + 3
 
 
-def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which):
+def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which, nsave=0):
     """Roofline record of the dominant kernel of a solve launch: `nsteps` (tensor) is the
     attempted RK steps of every instance, `mean_ms` the launch's mean duration."""
     import torch
@@ -365,7 +365,7 @@ def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which):
         achieved = nbytes / (mean_ms / 1e3) / 1e9
         return {'bound': 'hbm', 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
                 'frac': achieved / peaks['hbm_gbs'], 'peak_source': f'hbm_gbs ({which})',
-                'traffic': _traffic(config, precision, B, nsteps),
+                'traffic': _traffic(config, precision, B, nsteps, nsave),
                 'algorithmic_bytes_per_launch': nbytes,
                 'note': 'bytes = 34 n^2 complex64 matrix passes per attempted RK step per '
                         'instance (the fused-step minimum); the kernels today make 54'}
@@ -397,20 +397,28 @@ def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which):
     return roof
 
 
-# DRAM bytes (read + write) per unit of work of each solve kernel, from one ncu capture of
+# DRAM bytes (read + write) per unit of work of each solve, from one ncu capture of
 # dram__bytes_read.sum + dram__bytes_write.sum on a smaller launch of the same workload,
-# scaled to the launch by the units it processes (profiles/ names each capture):
-#   per instance for the n <= 64 kernels (inputs, states and expectation values out; the RK
-#   slots stay in L2), per instance-step for the DIA stepper.
-TRAFFIC_PER_UNIT = {}
+# scaled to the benchmark launch by the units it processes:
+#   kerr / fp32: per instance (148 instances, the full t in [0, 10] and 51 saves: 419.9 MB
+#     for 148 = 2.837 MB; inputs, states and expectation values, the RK slots stay in L2);
+#     profiles/mesolve_small_kernel_n64_kerr.md.
+#   dia / fp32: per attempted RK step of one instance (every kernel of the stepper, host
+#     loop: 7.19 GB = 54 passes over the 134 MB matrix) plus 1.22 GB per save point;
+#     profiles/dia_stepper_n4096_coupled_kerr_traffic.md.
+TRAFFIC_PER_UNIT = {
+    ('kerr', 'fp32'): ('instance', 2.837e6, 0.0),
+    ('dia', 'fp32'): ('instance_step', 7.19e9, 1.22e9),
+}
 
 
-def _traffic(config, precision, B, nsteps):
+def _traffic(config, precision, B, nsteps, nsave=0):
     key = (config, precision)
     if key not in TRAFFIC_PER_UNIT:
         return None
-    unit, per = TRAFFIC_PER_UNIT[key]
-    return float(per * (B if unit == 'instance' else float(nsteps.sum())))
+    unit, per, per_save = TRAFFIC_PER_UNIT[key]
+    units = B if unit == 'instance' else float(nsteps.sum())
+    return float(per * units + per_save * nsave * B)
 
 
 def run_b200(args):
@@ -485,7 +493,8 @@ def run_b200(args):
     value = world * B * args.steps / (kern / 1e3)
     mean_ms = kern / args.steps
     peaks, which = _peaks()
-    roof = _roofline(args.config, args.precision, n, K, nsteps, mean_ms, B, peaks, which)
+    roof = _roofline(args.config, args.precision, n, K, nsteps, mean_ms, B, peaks, which,
+                     len(w['tsave']))
 
     # ---- e2e: public API from host inputs --------------------------------------------
     e2e = None
@@ -629,7 +638,7 @@ def _extra_configs(args, dev, stream, flush, peaks, which):
                     'steps': 2, 'warmup': 3, 'batch': B, 'avg_rk_steps': float(nsteps.mean()),
                     'max_rk_steps': float(nsteps.max()),
                     'roofline': _roofline(cfg, prec, n, len(w['jump_ops']), nsteps, mean_ms, B,
-                                          peaks, which)}
+                                          peaks, which, len(w['tsave']))}
         del prep
         torch.cuda.empty_cache()
     return out

@@ -9,8 +9,9 @@ from .method import Dopri5, Tsit5
 from .options import Options
 from .qarrays import SparseDIA, dense, dia
 from .result import AdaptiveStepInfos, MESolveResult
+from .sesolve import SESolveResult, sesolve
 from .time_qarray import pwc
 
-__all__ = ['mesolve', 'MESolveB200Integrator', 'Options', 'Tsit5', 'Dopri5',
-           'MESolveResult', 'AdaptiveStepInfos', 'SparseDIA', 'dense', 'dia', 'method',
-           'operators', 'pwc']
+__all__ = ['mesolve', 'sesolve', 'MESolveB200Integrator', 'Options', 'Tsit5', 'Dopri5',
+           'MESolveResult', 'SESolveResult', 'AdaptiveStepInfos', 'SparseDIA', 'dense', 'dia',
+           'method', 'operators', 'pwc']

@@ -176,6 +176,12 @@ SIGNATURES = {
     'dqb_lindblad_rhs_dia_tiled': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.c_int32,
                                                   ctypes.c_int32, _P, _P, _P, ctypes.c_size_t, _P]),
     'dqb_dense_small_max_n': (ctypes.c_int32, [ctypes.c_int32]),
+    'dqb_sesolve_dense_workspace_size': (ctypes.c_size_t, []),
+    'dqb_sesolve_dense': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
+                                         ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
+    'dqb_schrodinger_rhs_dense': (ctypes.c_int, [ctypes.POINTER(DenseProblem), _P, _P, _P]),
+    'dqb_mesolve_vectorized': (ctypes.c_int, [ctypes.POINTER(DenseProblem), _P, ctypes.POINTER(OdeOptions),
+                                              ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
     'dqb_version': (ctypes.c_char_p, []),
 }
 

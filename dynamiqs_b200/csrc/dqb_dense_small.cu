@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 #include <utility>
 #include <vector>
@@ -214,29 +215,62 @@ __device__ void rhs(const float2* sH, const float2* sL, const float2* sX, float2
 
 // The right-hand side on CUDA cores (the engine of solve_one, dqb_small.cuh): Hnh, the
 // jump operators, the stage input X and the product buffer T in padded shared memory.
+// With a time-dependent H (td->M > 0) the constant part Hnh0 = -iH0 - 1/2 sum L^+L is kept
+// in one more padded matrix, and every right-hand side first forms
+// Hnh(t) = Hnh0 - i sum_m c_m(t) H_m in sH from the terms' operators in global memory.
 template <int NP>
 struct SimtEngine {
   float2 *sH, *sX, *sT, *sL;
   int n, K, form;
+  const TdArgs* td;
+  float2* sH0;
+  long long inst;
 
   __device__ void load(const InstView& a) {
     n = a.n;
     K = a.K;
+    inst = a.inst;
     load_padded<NP>(sH, a.H, n);
     for (int k = 0; k < K; ++k) load_padded<NP>(sL + k * Small<NP>::MAT, a.L + (long long)k * n * n, n);
     __syncthreads();
     build_hnh<NP>(sH, sL, n, K);
     __syncthreads();
+    if (td && td->M > 0) {
+      for (int e = threadIdx.x; e < Small<NP>::MAT; e += blockDim.x) sH0[e] = sH[e];
+      __syncthreads();
+    }
   }
 
   template <class F>
-  __device__ void rhs(F x_of, float2* also, float2* out) {
+  __device__ void rhs(F x_of, float2* also, float2* out, double t) {
     constexpr int LD = NP + 1;
+    const int M = td ? td->M : 0;
+    float2 c[DQB_TD_MAX_TERMS];
+#pragma unroll
+    for (int m = 0; m < DQB_TD_MAX_TERMS; ++m) {
+      c[m] = make_float2(0.f, 0.f);
+      if (m < M) {
+        const double2 v = td_coef(td->term[m], inst, t);
+        c[m] = make_float2((float)v.x, (float)v.y);
+      }
+    }
 #pragma unroll 4
     for (int e = threadIdx.x; e < NP * NP; e += blockDim.x) {
+      const int i = e / NP, j = e % NP;
       const float2 x = x_of(e);
-      sX[(e / NP) * LD + (e % NP)] = x;
+      sX[i * LD + j] = x;
       if (also) also[e] = x;
+      if (M > 0) {
+        float2 h = sH0[i * LD + j];
+        if (i < n && j < n) {
+          float2 acc = make_float2(0.f, 0.f);  // sum_m c_m(t) H_m[i][j]
+#pragma unroll
+          for (int m = 0; m < DQB_TD_MAX_TERMS; ++m)
+            if (m < M) cmac(acc, c[m], td->ops[((long long)m * n + i) * n + j]);
+          h = make_float2(h.x + acc.y, h.y - acc.x);  // - i acc
+        }
+        sH[i * LD + j] = h;
+      }
     }
     __syncthreads();
     dqb::rhs<NP>(sH, sL, sX, sT, n, K, form, out, NP, NP);
@@ -267,7 +301,7 @@ __global__ void __launch_bounds__(kSmallThreads, NP == 64 ? 1 : (NP == 32 ? 3 : 
       continue;
     }
     const InstView v = view_of(a, inst);
-    SimtEngine<NP> eng{sH, sX, sT, sL, a.n, a.K, a.o.form};
+    SimtEngine<NP> eng{sH, sX, sT, sL, a.n, a.K, a.o.form, &a.td, sL + a.K * Small<NP>::MAT, inst};
     solve_one<NP>(eng, v, a.o, slot, red, ctl);
     __syncthreads();
   }
@@ -433,6 +467,7 @@ static DenseSmallArgs make_args(const dqb_dense_problem* p, const dqb_ode_option
   a.slots = nullptr;
   a.counter = nullptr;
   if (o) a.o = make_ctrl(*o);
+  std::memset(&a.td, 0, sizeof(a.td));
   return a;
 }
 
@@ -457,6 +492,67 @@ extern "C" int dqb_mesolve_dense(const dqb_dense_problem* p, const dqb_ode_optio
   if (o->precision == DQB_PREC_F16X3 && small_tc_applies(p->n, p->n_jumps, o->form))
     return small_tc_launch(a, grid, s);
   const size_t smem = smem_for(NP, p->n_jumps);
+  switch (NP) {
+    case 16: mesolve_small_kernel<16><<<grid, kSmallThreads, smem, s>>>(a); break;
+    case 32: mesolve_small_kernel<32><<<grid, kSmallThreads, smem, s>>>(a); break;
+    default: mesolve_small_kernel<64><<<grid, kSmallThreads, smem, s>>>(a); break;
+  }
+  return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+}
+
+extern "C" int dqb_mesolve_dense_td(const dqb_dense_problem* p, const dqb_td_hamiltonian* td,
+                                    const dqb_ode_options* o, const dqb_outputs* out, void* workspace,
+                                    size_t workspace_bytes, void* stream) {
+  int rc = validate_dense(p, o);
+  if (rc) return rc;
+  if (!out || !out->states || !out->infos || !out->status || (p->n_exp > 0 && !out->expects))
+    return DQB_ERR_INVALID_ARGUMENT;
+  if (!td || td->n_terms < 0 || td->n_terms > DQB_TD_MAX_TERMS || td->n_jump_ts < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if ((td->n_terms > 0 && (!td->ops || !td->terms)) || (td->n_jump_ts > 0 && !td->jump_ts))
+    return DQB_ERR_INVALID_ARGUMENT;
+  for (int m = 0; m < td->n_terms; ++m) {
+    const dqb_td_term& T = td->terms[m];
+    if (T.kind == DQB_TD_PWC) {
+      if (T.n_times < 2 || !T.times || !T.values) return DQB_ERR_INVALID_ARGUMENT;
+    } else if (T.kind != DQB_TD_WAVE) {
+      return DQB_ERR_INVALID_ARGUMENT;
+    }
+  }
+  if (p->batch == 0) return DQB_OK;
+  const int NP = pick_np(p->n);
+  const int Keff = p->n_jumps + 1;  // one more shared-memory matrix: the constant Hnh0
+  if (NP == 0 || dqb_dense_small_max_n(Keff) < NP) return DQB_ERR_UNSUPPORTED;
+  const size_t need = dqb_mesolve_dense_workspace_size(p->n, Keff, p->batch);
+  if (need == 0) return DQB_ERR_UNSUPPORTED;
+  if (!workspace || workspace_bytes < need) return DQB_ERR_WORKSPACE_TOO_SMALL;
+  const int grid = grid_for(NP, Keff, p->batch);
+  cudaStream_t s = (cudaStream_t)stream;
+  DenseSmallArgs a = make_args(p, o, out);
+  a.counter = (unsigned int*)workspace;
+  a.slots = (float2*)((char*)workspace + 256);
+  a.td.M = td->n_terms;
+  a.td.ops = (const float2*)td->ops;
+  for (int m = 0; m < td->n_terms; ++m) {
+    const dqb_td_term& T = td->terms[m];
+    TdTerm& d = a.td.term[m];
+    d.kind = T.kind;
+    d.n_times = T.n_times;
+    d.times = T.times;
+    d.values = (const double2*)T.values;
+    d.vidx = T.value_index;
+    d.amp_re = T.amp_re;
+    d.amp_im = T.amp_im;
+    d.omega = T.omega;
+    d.phase = T.phase;
+    d.t_center = T.t_center;
+    d.sigma = T.sigma;
+    d.t_start = T.t_start;
+    d.t_end = T.t_end;
+  }
+  a.td.n_jump = td->n_jump_ts;
+  a.td.jump_ts = td->jump_ts;
+  zero_words_kernel<<<1, 64, 0, s>>>((unsigned int*)workspace, 64);
+  const size_t smem = smem_for(NP, Keff);
   switch (NP) {
     case 16: mesolve_small_kernel<16><<<grid, kSmallThreads, smem, s>>>(a); break;
     case 32: mesolve_small_kernel<32><<<grid, kSmallThreads, smem, s>>>(a); break;
@@ -601,7 +697,10 @@ __global__ void __launch_bounds__(kSmallThreads, NP == 64 ? 1 : (NP == 32 ? 3 : 
     v.expects = (float2*)r.expects;
     v.infos = r.infos;
     v.status = r.status;
-    SimtEngine<NP> eng{sH, sX, sT, sL, v.n, v.K, o.form};
+    v.inst = inst;
+    v.n_jump = 0;
+    v.jump_ts = nullptr;
+    SimtEngine<NP> eng{sH, sX, sT, sL, v.n, v.K, o.form, nullptr, nullptr, inst};
     solve_one<NP>(eng, v, o, slot, red, ctl);
     __syncthreads();
   }

@@ -249,7 +249,7 @@ struct TcEngine {
   }
 
   template <class F>
-  __device__ void rhs(F x_of, float2* also, float2* out) {
+  __device__ void rhs(F x_of, float2* also, float2* out, double /*t: constant operators*/) {
     const int tid = threadIdx.x, warp = tid >> 5;
     const int q = warp & 3;
     constexpr uint32_t idesc = tc::instr_desc(0u, 128, 128);  // FP16 x FP16 -> FP32
@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) rhs_small_tc_kernel(DenseSma
             const int i = e >> 6, j = e & 63;
             return (i < n && j < n) ? r[i * n + j] : make_float2(0.f, 0.f);
           },
-          nullptr, full);
+          nullptr, full, 0.0);
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) o[e] = full[(e / n) * 64 + e % n];
   tc::tc_fence_before();
   __syncthreads();

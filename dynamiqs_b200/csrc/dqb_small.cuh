@@ -8,9 +8,9 @@
 //     // there); ends with a barrier.
 //     __device__ void load(const InstView& a);
 //     // X[e] = x_of(e) for every e = i * NP + j (i, j < NP); when `also` is not null,
-//     // also[e] = X[e]; then out[e] = f(X)[e] for every e (zero outside n x n).  Every
-//     // thread of the block calls it; it ends with a barrier.
-//     template <class F> __device__ void rhs(F x_of, float2* also, float2* out);
+//     // also[e] = X[e]; then out[e] = f(t, X)[e] for every e (zero outside n x n).
+//     // Every thread of the block calls it; it ends with a barrier.
+//     template <class F> __device__ void rhs(F x_of, float2* also, float2* out, double t);
 //     // True once a bounded wait has run out (the tensor-core engine); the instance then
 //     // ends with DQB_INST_NONFINITE and the kernel stops taking new instances.
 //     __device__ bool failed() const;
@@ -28,6 +28,71 @@ namespace dqb {
 
 constexpr int kSmallThreads = 256;
 constexpr int kSlotMats = 9;  // y, y1, k1..k7
+
+// Time-dependent part of H (dqb_td_hamiltonian), by value in the kernel arguments.
+struct TdTerm {
+  int kind, n_times;
+  const double* times;
+  const double2* values;
+  const int* vidx;
+  double amp_re, amp_im, omega, phase, t_center, sigma, t_start, t_end;
+};
+struct TdArgs {
+  int M;                 // number of terms (0: constant H)
+  const float2* ops;     // [M, n, n]
+  TdTerm term[DQB_TD_MAX_TERMS];
+  int n_jump;
+  const double* jump_ts;
+};
+
+// c_m(t) of term T for instance `inst`.
+__device__ __forceinline__ double2 td_coef(const TdTerm& T, long long inst, double t) {
+  if (T.kind == DQB_TD_PWC) {
+    const int nt = T.n_times;
+    if (!(t >= T.times[0]) || !(t < T.times[nt - 1])) return make_double2(0.0, 0.0);
+    int lo = 0, hi = nt - 1;  // times[lo] <= t < times[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (T.times[mid] <= t) lo = mid; else hi = mid;
+    }
+    const long long set = T.vidx ? T.vidx[inst] : 0;
+    return T.values[set * (nt - 1) + lo];
+  }
+  if (!(t >= T.t_start) || !(t < T.t_end)) return make_double2(0.0, 0.0);
+  double f = cos(T.omega * t + T.phase);
+  if (T.sigma > 0.0) {
+    const double d = (t - T.t_center) / T.sigma;
+    f *= exp(-0.5 * d * d);
+  }
+  return make_double2(T.amp_re * f, T.amp_im * f);
+}
+
+// First discontinuity strictly after t (or +inf).
+__device__ __forceinline__ double next_jump(const double* jts, int nj, double t) {
+  int lo = 0, hi = nj;  // first index with jts[idx] > t
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (jts[mid] <= t) lo = mid + 1; else hi = mid;
+  }
+  return lo < nj ? jts[lo] : INFINITY;
+}
+
+// Next trial end time from t for a step dt: clipped just before the next discontinuity
+// (made_jump), then clipped to t1 as next_tend does.
+__device__ __forceinline__ double next_trial(const double* jts, int nj, double t, double dt, double t1, bool keep,
+                                             int& made_jump) {
+  double tn = t + dt;
+  made_jump = 0;
+  if (nj > 0) {
+    const double J = next_jump(jts, nj, t);
+    if (tn >= J) {
+      tn = nextafter(J, -INFINITY);
+      made_jump = 1;
+    }
+  }
+  if (tn > t1 - 1e-10) tn = keep ? t1 : t + 0.5 * (t1 - t);
+  return tn < t1 ? tn : t1;
+}
 
 struct DenseSmallArgs {
   int n, K, nE, ntsave;
@@ -49,10 +114,12 @@ struct DenseSmallArgs {
   unsigned int* counter;
   const int* order;  // start order of the instances, or null (0, 1, 2, ...)
   CtrlOpts o;
+  TdArgs td;
 };
 
 struct Ctrl {
-  double t, tnext, h, t1, dtnew;
+  double t, tnext, h, t1, dtnew, dt_prop;
+  int made_jump;
   float w[7];
   int keep, run, status, save_idx;
   long long nsteps, nacc, nrej;
@@ -73,10 +140,16 @@ struct InstView {
   float2* expects;     // nE x ntsave
   int* infos;          // 3
   int* status;         // 1
+  long long inst;      // index of the instance in its batch
+  int n_jump;          // discontinuity times (the controller's jump_ts)
+  const double* jump_ts;
 };
 
 __device__ __forceinline__ InstView view_of(const DenseSmallArgs& a, long long inst) {
   InstView v;
+  v.inst = inst;
+  v.n_jump = a.td.n_jump;
+  v.jump_ts = a.td.jump_ts;
   const int n = a.n;
   const long long nn = (long long)n * n;
   const long long hi = a.Hidx ? a.Hidx[inst] : inst;
@@ -197,7 +270,7 @@ __device__ void solve_one(Engine& eng, const InstView& a, const CtrlOpts& o, flo
   const double t1 = a.tsave[a.ntsave - 1];
   float2* k1 = slot + ctl.sk[0] * NN;
   float2* kscr = slot + ctl.sk[1] * NN;
-  eng.rhs([&](int e) { return y[e]; }, nullptr, k1);
+  eng.rhs([&](int e) { return y[e]; }, nullptr, k1, a.t0);
   double s0 = 0.0, s1 = 0.0;
   for (int e = tid; e < NN; e += blockDim.x) {
     const float2 yv = y[e], fv = k1[e];
@@ -210,7 +283,7 @@ __device__ void solve_one(Engine& eng, const InstView& a, const CtrlOpts& o, flo
   const double d0 = sqrt(s0 * inv_nn), d1 = sqrt(s1 * inv_nn);
   const double h0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : 0.01 * d0 / d1;
   const float h0f = (float)h0;
-  eng.rhs([&](int e) { return caxpy(h0f, k1[e], y[e]); }, nullptr, kscr);
+  eng.rhs([&](int e) { return caxpy(h0f, k1[e], y[e]); }, nullptr, kscr, a.t0 + h0);
   double s2 = 0.0;
   for (int e = tid; e < NN; e += blockDim.x) {
     const float2 yv = y[e], f0 = k1[e], f1 = kscr[e];
@@ -226,9 +299,8 @@ __device__ void solve_one(Engine& eng, const InstView& a, const CtrlOpts& o, flo
     const double dt = fmin(100.0 * h0, h1);
     ctl.t = a.t0;
     ctl.t1 = t1;
-    double tn = a.t0 + dt;
-    if (tn > t1 - 1e-10) tn = t1;
-    ctl.tnext = tn < t1 ? tn : t1;
+    ctl.dt_prop = dt;
+    ctl.tnext = next_trial(a.jump_ts, a.n_jump, a.t0, dt, t1, true, ctl.made_jump);
     ctl.run = a.t0 < t1;
     if (eng.failed()) {
       ctl.status = DQB_INST_NONFINITE;
@@ -265,7 +337,7 @@ __device__ void solve_one(Engine& eng, const InstView& a, const CtrlOpts& o, flo
               if (j < s) x = caxpy(cf[j], kk[j][e], x);
             return x;
           },
-          nullptr, kk[s]);
+          nullptr, kk[s], ctl.t + T.c[s] * h);
     }
     // y1 (FSAL stage input) and k7
     {
@@ -279,7 +351,7 @@ __device__ void solve_one(Engine& eng, const InstView& a, const CtrlOpts& o, flo
             for (int j = 0; j < 6; ++j) x = caxpy(cf[j], kk[j][e], x);
             return x;
           },
-          y1, kk[6]);
+          y1, kk[6], ctl.tnext);
     }
     // embedded error, FP64 accumulation
     double se = 0.0;
@@ -314,7 +386,8 @@ __device__ void solve_one(Engine& eng, const InstView& a, const CtrlOpts& o, flo
         const bool keep = err < 1.0;
         ctl.keep = keep;
         if (keep) ctl.nacc += 1; else ctl.nrej += 1;
-        ctl.dtnew = h * step_factor(o, err, keep);
+        // after a step clipped at a discontinuity the controller scales its proposal
+        ctl.dtnew = (ctl.made_jump ? ctl.dt_prop : h) * step_factor(o, err, keep);
       }
     }
     __syncthreads();
@@ -345,12 +418,19 @@ __device__ void solve_one(Engine& eng, const InstView& a, const CtrlOpts& o, flo
         tmp = ctl.sk[0];
         ctl.sk[0] = ctl.sk[6];
         ctl.sk[6] = tmp;
-        ctl.t = ctl.tnext;
+        // a step that ended just before a discontinuity: the next starts on it
+        ctl.t = ctl.made_jump ? nextafter(ctl.tnext, INFINITY) : ctl.tnext;
+      }
+      __syncthreads();
+      if (ctl.made_jump && ctl.t < ctl.t1) {  // first stage re-evaluated across the jump
+        const float2* yn = slot + ctl.sy * NN;
+        eng.rhs([&](int e) { return yn[e]; }, nullptr, slot + ctl.sk[0] * NN, ctl.t);
       }
     }
     __syncthreads();
     if (tid == 0) {
-      ctl.tnext = next_tend(ctl.t, ctl.dtnew, ctl.t1, ctl.keep);
+      ctl.dt_prop = ctl.dtnew;
+      ctl.tnext = next_trial(a.jump_ts, a.n_jump, ctl.t, ctl.dtnew, ctl.t1, ctl.keep, ctl.made_jump);
       ctl.run = ctl.t < ctl.t1;
     }
     __syncthreads();

@@ -33,6 +33,10 @@ from .result import AdaptiveStepInfos, MESolveResult
 
 __all__ = ['mesolve', 'MESolveB200Integrator']
 
+# Largest n^2 of the vectorized master-equation kernel (n <= 16); beyond it
+# options.vectorized=True solves the standard form, the same ODE with the same RMS norm.
+VECTORIZED_MAX_N2 = 256
+
 _MAX_STEPS_MSG = (
     'The maximum number of method steps has been reached (the default value is '
     '`max_steps=100_000`). Try increasing `max_steps` with the `method` argument, e.g. '
@@ -339,12 +343,70 @@ class MESolveB200Integrator:
         n = _shape(self.H)[-1]
         K = len(self.Ls)
         dia_ops = isinstance(self.H, SparseDIA) or any(isinstance(L, SparseDIA) for L in self.Ls)
+        if self.options.vectorized and n * n <= VECTORIZED_MAX_N2:
+            return self._prepare_vectorized(lib)
         if n <= lib.dqb_dense_small_max_n(K):
             return self._prepare_dense(lib, 'small')
         if dia_ops:
             return self._prepare_dia(lib)
         return self._prepare_dense(lib, 'large')
 
+
+    def _prepare_vectorized(self, lib) -> PreparedSolve:
+        """``options.vectorized=True`` (``diffrax_integrator.py:325-345``): the ODE
+        d vec(rho)/dt = S vec(rho) with S = slindbladian(H, jump_ops), one superoperator
+        per distinct (H item, jump set) pair of the batch, solved by dqb_mesolve_vectorized
+        on vec(rho) (n^2 entries: the error norm runs over them, as in the reference)."""
+        import torch
+
+        from .vectorization import slindbladian, vectorize
+
+        self._path = 'vectorized'
+        dev = _device()
+        n, K, ntsave, B, nE, nsave = self._sizes()
+        N = n * n
+        plan = self.plan
+        c64 = torch.complex64
+        Hs = plan.H_items_dense()
+        Lsets = plan.L_sets_dense()
+        pairs = np.stack([plan.H_index, plan.L_index], axis=1)
+        uniq, inverse = np.unique(pairs, axis=0, return_inverse=True)
+        S_T = np.stack([np.ascontiguousarray(
+            slindbladian(Hs[h], [Lsets[l, k] for k in range(K)]).T) for h, l in uniq])
+        rho = plan.rho_items
+        if rho.shape[-1] == 1 and n > 1:
+            rho = rho @ np.conj(np.swapaxes(rho, -1, -2))  # todm
+        if self.options.assume_hermitian:
+            herm = np.abs(rho - np.conj(np.swapaxes(rho, -1, -2))) <= 1e-5 + 1e-5 * np.abs(rho)
+            if not herm.all():
+                raise RuntimeError('Argument y0 is not hermitian.')
+        bufs = {
+            'superop_t': _to_dev(S_T, c64, dev),
+            'rho0': _to_dev(vectorize(rho)[..., 0], c64, dev),
+            'E': (_to_dev(np.stack([to_dense(E).reshape(-1) for E in self.Es]), c64, dev) if nE
+                  else torch.zeros(1, dtype=c64, device=dev)),
+            'tsave': _to_dev(np.asarray(self.ts, dtype=np.float64), torch.float64, dev),
+            'S_index': _to_dev(inverse.reshape(-1).astype(np.int32), torch.int32, dev),
+            'rho0_index': _to_dev(plan.rho_index, torch.int32, dev),
+            'states': torch.empty((B, nsave, N), dtype=c64, device=dev),
+            'expects': torch.empty((B, max(nE, 1), ntsave), dtype=c64, device=dev),
+            'infos': torch.empty((B, 3), dtype=torch.int32, device=dev),
+            'status': torch.empty((B,), dtype=torch.int32, device=dev),
+            'workspace': torch.empty(256, dtype=torch.uint8, device=dev),
+        }
+        prob = _lib.DenseProblem(
+            n=N, n_jumps=0, n_exp=nE, n_tsave=ntsave, batch=B, H=bufs['superop_t'].data_ptr(),
+            rho0=bufs['rho0'].data_ptr(), rho0_is_ket=1, E=bufs['E'].data_ptr(),
+            tsave=bufs['tsave'].data_ptr(), H_index=bufs['S_index'].data_ptr(),
+            rho0_index=bufs['rho0_index'].data_ptr())
+        outs = _lib.Outputs(states=bufs['states'].data_ptr(), expects=bufs['expects'].data_ptr(),
+                            infos=bufs['infos'].data_ptr(), status=bufs['status'].data_ptr())
+        S_ptr = bufs['superop_t'].data_ptr()
+
+        def fn(prob_, opts, outs_, ws, wsb, stream):
+            return lib.dqb_mesolve_vectorized(prob_, S_ptr, opts, outs_, ws, wsb, stream)
+
+        return PreparedSolve(self, fn, 'dqb_mesolve_vectorized', prob, outs, bufs, 256, dev, nE)
 
     def _common_buffers(self, dev, n, ntsave, nE, B, nsave):
         import torch
@@ -552,6 +614,9 @@ class MESolveB200Integrator:
             raise RuntimeError('The solution became non-finite (NaN or inf) during the '
                                'integration.')
         bshape = self.plan.bshape
+        if self._path == 'vectorized':  # vec(rho) -> rho (unvectorize, columns stacked)
+            m = int(round(states.shape[-1] ** 0.5))
+            states = states.reshape(*states.shape[:-1], m, m).transpose(-1, -2)
         n = states.shape[-1]
         states = states.reshape(*bshape, states.shape[1], n, n)
         if expects is not None:

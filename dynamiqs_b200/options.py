@@ -37,6 +37,7 @@ class Options:
 
 
 _SUPPORTED = {
+    'sesolve': ('save_states', 'cartesian_batching', 'progress_meter', 't0', 'save_extra'),
     'mesolve': ('save_states', 'cartesian_batching', 'progress_meter', 't0', 'save_extra',
                 'vectorized', 'assume_hermitian', 'precision'),
 }

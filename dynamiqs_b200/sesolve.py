@@ -1,0 +1,194 @@
+"""``dq.sesolve`` on the GPU: the Schroedinger equation d psi/dt = -i H psi on the same
+Runge-Kutta engine as ``mesolve`` (``dynamiqs/integrators/apis/sesolve.py:35-330``;
+vector field ``dynamiqs/integrators/core/diffrax_integrator.py:221-228``), through one
+C-ABI call (``dqb_sesolve_dense``, ``include/dqb200.h``) for the whole batch.
+
+Same signature, argument checks and batching semantics as the reference: ``H`` of shape
+``(...H, n, n)``, ``psi0`` ``(...psi0, n, 1)``, ``tsave`` ``(ntsave,)``, ``exp_ops`` a
+list of ``(n, n)``; cartesian batching gives results of shape ``(...H, ...psi0, ...)``,
+flat batching broadcasts ``...H`` against ``...psi0``.  ``method`` is ``Tsit5`` (default)
+or ``Dopri5``.  Dense ``H`` with n <= 128 (sparse-DIA operators are densified).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .mesolve import (_as_op, _check_shape, _device, _MAX_STEPS_MSG, _shape, _to_dev,
+                      assert_method_supported, check_times, make_batch_plan)
+from .method import Method, Tsit5
+from .options import Options, check_options
+from .qarrays import to_dense
+from .result import AdaptiveStepInfos, MESolveResult
+
+__all__ = ['sesolve', 'SESolveResult', 'SESolveB200Integrator']
+
+
+class SESolveResult(MESolveResult):
+    """``dynamiqs/result.py`` SESolveResult: ``states`` ``(..., nsave, n, 1)``,
+    ``final_state`` ``(..., n, 1)``, ``expects`` ``(..., nE, ntsave)``, ``infos``."""
+
+
+def _check_sesolve_args(H, psi0, exp_ops) -> None:
+    """``_check_sesolve_args`` (``sesolve.py:318-330``)."""
+    _check_shape(H, 'H', '(..., n, n)', subs={'...': '...H'})
+    _check_shape(psi0, 'psi0', '(..., n, 1)', subs={'...': '...psi0'})
+    if exp_ops is not None:
+        for i, E in enumerate(exp_ops):
+            _check_shape(E, f'exp_ops[{i}]', '(n, n)')
+
+
+@dataclass
+class _Prepared:
+    integ: 'SESolveB200Integrator'
+    prob: object
+    outs: object
+    bufs: dict
+
+    def launch(self, stream=None):
+        import torch
+
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        lib = _lib.load()
+        rc = lib.dqb_sesolve_dense(self.prob, self.integ._ode_options(), self.outs,
+                                   self.bufs['workspace'].data_ptr(), self.bufs['workspace'].numel(), s)
+        _lib.check(rc, 'dqb_sesolve_dense')
+        return self
+
+    def result(self) -> SESolveResult:
+        return self.integ._result(self.bufs)
+
+
+class SESolveB200Integrator:
+    """Registry-compatible integrator: ``constructor(ts=, y0=, method=, gradient=,
+    options=, H=, Es=)`` then ``.run() -> SESolveResult`` (``sesolve.py:289-304``)."""
+
+    def __init__(self, *, ts, y0, method, gradient, options, H, Es, plan):
+        self.ts = ts
+        self.y0 = y0
+        self.method = method
+        self.gradient = gradient
+        self.options = options
+        self.H = H
+        self.Es = Es
+        self.plan = plan
+
+    @property
+    def t0(self) -> float:
+        return float(self.ts[0] if self.options.t0 is None else self.options.t0)
+
+    def _ode_options(self) -> _lib.OdeOptions:
+        m = self.method
+        return _lib.OdeOptions(
+            method=_lib.METHOD_TSIT5 if isinstance(m, Tsit5) else _lib.METHOD_DOPRI5,
+            form=_lib.FORM_STANDARD, rtol=float(m.rtol), atol=float(m.atol),
+            safety=float(m.safety_factor), factormin=float(m.min_factor),
+            factormax=float(m.max_factor), max_steps=int(m.max_steps), t0=self.t0,
+            save_states=int(bool(self.options.save_states)), check_hermitian=0)
+
+    def prepare(self) -> _Prepared:
+        import torch
+
+        dev = _device()
+        plan = self.plan
+        n = _shape(self.H)[-1]
+        ntsave = len(self.ts)
+        nE = len(self.Es) if self.Es else 0
+        nsave = ntsave if self.options.save_states else 1
+        B = plan.batch
+        c64 = torch.complex64
+        bufs = {
+            'H': _to_dev(plan.H_items_dense(), c64, dev),
+            'psi0': _to_dev(plan.rho_items, c64, dev),
+            'E': (_to_dev(np.stack([to_dense(E) for E in self.Es]), c64, dev) if nE
+                  else torch.zeros(1, dtype=c64, device=dev)),
+            'tsave': _to_dev(np.asarray(self.ts, dtype=np.float64), torch.float64, dev),
+            'H_index': _to_dev(plan.H_index, torch.int32, dev),
+            'psi0_index': _to_dev(plan.rho_index, torch.int32, dev),
+            'states': torch.empty((B, nsave, n, 1), dtype=c64, device=dev),
+            'expects': torch.empty((B, max(nE, 1), ntsave), dtype=c64, device=dev),
+            'infos': torch.empty((B, 3), dtype=torch.int32, device=dev),
+            'status': torch.empty((B,), dtype=torch.int32, device=dev),
+            'workspace': torch.empty(_lib.load().dqb_sesolve_dense_workspace_size(),
+                                     dtype=torch.uint8, device=dev),
+        }
+        prob = _lib.DenseProblem(
+            n=n, n_jumps=0, n_exp=nE, n_tsave=ntsave, batch=B, H=bufs['H'].data_ptr(), L=None,
+            rho0=bufs['psi0'].data_ptr(), rho0_is_ket=1, E=bufs['E'].data_ptr(),
+            tsave=bufs['tsave'].data_ptr(), H_index=bufs['H_index'].data_ptr(), L_index=None,
+            rho0_index=bufs['psi0_index'].data_ptr())
+        outs = _lib.Outputs(states=bufs['states'].data_ptr(), expects=bufs['expects'].data_ptr(),
+                            infos=bufs['infos'].data_ptr(), status=bufs['status'].data_ptr())
+        self._nE = nE
+        return _Prepared(self, prob, outs, bufs)
+
+    def run(self) -> SESolveResult:
+        return self.prepare().launch().result()
+
+    def _result(self, b) -> SESolveResult:
+        st = b['status'].cpu()
+        if bool((st == _lib.INST_MAX_STEPS).any()):
+            raise RuntimeError(_MAX_STEPS_MSG)
+        if bool((st == _lib.INST_NONFINITE).any()):
+            raise RuntimeError('The solution became non-finite (NaN or inf) during the '
+                               'integration.')
+        bshape = self.plan.bshape
+        states = b['states'].reshape(*bshape, *b['states'].shape[1:])
+        expects = None
+        if self._nE:
+            expects = b['expects'].reshape(*bshape, *b['expects'].shape[1:])
+        infos = b['infos'].reshape(*bshape, 3)
+        info = AdaptiveStepInfos(infos[..., 0], infos[..., 1], infos[..., 2])
+        extra = None
+        if self.options.save_extra is not None:  # applied to every saved state
+            import torch
+
+            if not self.options.save_states:
+                raise NotImplementedError('`save_extra` needs `save_states=True` on the '
+                                          'B200 path (it is applied to the saved states).')
+            vals = [self.options.save_extra(x) for x in states.reshape(-1, *states.shape[-2:])]
+            try:
+                extra = torch.stack([torch.as_tensor(v) for v in vals]).reshape(
+                    *states.shape[:-2], *torch.as_tensor(vals[0]).shape)
+            except (TypeError, RuntimeError):
+                extra = vals
+        return SESolveResult(tsave=self.ts, method=self.method, gradient=self.gradient,
+                             options=self.options, states=states, expects=expects, infos=info,
+                             extra=extra)
+
+
+def sesolve(H, psi0, tsave, *, exp_ops=None, method: Method = Tsit5(),  # noqa: B008
+            gradient=None, options: Options = Options()) -> SESolveResult:  # noqa: B008
+    r"""Solve the Schroedinger equation d psi/dt = -i H psi on the GPU (``dq.sesolve``,
+    ``dynamiqs/integrators/apis/sesolve.py:35-224``).  Returns a :class:`SESolveResult`
+    with ``states`` ``(..., nsave, n, 1)`` and ``expects`` ``(..., nE, ntsave)``."""
+    if getattr(H, '__class__', None).__name__.endswith('TimeQArray'):
+        raise NotImplementedError('Time-dependent Hamiltonians are not supported by sesolve '
+                                  'on the B200 path.')
+    H = _as_op(H)
+    psi0 = _as_op(psi0)
+    tsave = np.asarray(tsave.detach().cpu().numpy() if hasattr(tsave, 'detach') else tsave,
+                       dtype=np.float64)
+    if exp_ops is not None:
+        exp_ops = [_as_op(E) for E in exp_ops] if len(exp_ops) > 0 else None
+
+    _check_sesolve_args(H, psi0, exp_ops)
+    tsave = check_times(tsave, 'tsave')
+    check_options(options, 'sesolve')
+    options = options.initialise()
+    assert_method_supported(method)
+    method.assert_supports_gradient(gradient)
+
+    n = _shape(H)[-1]
+    if _shape(psi0)[-2] != n:
+        raise ValueError(f'Argument `psi0` must have shape (..., {n}, 1).')
+    if n > 128:
+        raise NotImplementedError('sesolve on the B200 path supports n <= 128.')
+    H = to_dense(H) if not isinstance(H, np.ndarray) else H
+    plan = make_batch_plan(H, [], psi0, options.cartesian_batching)
+    integ = SESolveB200Integrator(ts=tsave, y0=psi0, method=method, gradient=gradient,
+                                  options=options, H=H, Es=exp_ops, plan=plan)
+    return integ.run()

@@ -178,6 +178,85 @@ DQB_API int dqb_lindblad_rhs_dense_prec(const dqb_dense_problem* problem, int32_
 DQB_API int dqb_mesolve_dense_noalloc(const dqb_dense_problem* problem, const dqb_ode_options* options,
                                       const dqb_outputs* outputs, void* stream);
 
+/* ---- time-dependent Hamiltonians (n <= 64 kernel) ------------------------------------ */
+/* H(t) = H + sum_m c_m(t) ops[m] (the reference's ConstantTimeQArray + PWCTimeQArray /
+ * ModulatedTimeQArray sums, dynamiqs/time_qarray.py:497-754), with prefactors the device
+ * evaluates at every stage time: */
+#define DQB_TD_PWC 0  /* c(t) = values[v][k] for times[k] <= t < times[k+1]; 0 outside
+                         [times[0], times[n_times-1]) (PWCTimeQArray._prefactor, :631-641) */
+#define DQB_TD_WAVE 1 /* c(t) = (amp_re + i amp_im) cos(omega t + phase) env(t) for
+                         t_start <= t < t_end, else 0; env(t) = exp(-(t - t_center)^2 /
+                         (2 sigma^2)) when sigma > 0, else 1 (a ModulatedTimeQArray whose
+                         prefactor is one of these closed forms) */
+#define DQB_TD_MAX_TERMS 4
+
+typedef struct dqb_td_term {
+  int32_t kind;                /* DQB_TD_*                                                 */
+  int32_t n_times;             /* PWC: number of time points (n_times - 1 values per set)  */
+  const double* times;         /* PWC: device float64 [n_times], ascending                 */
+  const void* values;          /* PWC: device complex128 [n_sets, n_times - 1]             */
+  const int32_t* value_index;  /* PWC: device int32 [batch]: instance b uses set
+                                  value_index[b]; NULL: set 0 for every instance          */
+  double amp_re, amp_im, omega, phase, t_center, sigma, t_start, t_end; /* WAVE           */
+} dqb_td_term;
+
+typedef struct dqb_td_hamiltonian {
+  int32_t n_terms;             /* M <= DQB_TD_MAX_TERMS                                    */
+  const void* ops;             /* device complex64 [M, n, n]                               */
+  const dqb_td_term* terms;    /* host array [M]                                           */
+  int32_t n_jump_ts;           /* discontinuity times handed to the controller            */
+  const double* jump_ts;       /* device float64 [n_jump_ts], ascending (PIDController
+                                  jump_ts, diffrax_integrator.py:59-72): a step never
+                                  crosses one; it ends just before it, the next starts on
+                                  it with its first stage re-evaluated, and the next step
+                                  size scales the proposal, not the clipped step          */
+} dqb_td_hamiltonian;
+
+/* dqb_mesolve_dense with a time-dependent Hamiltonian: problem->H is the constant part;
+ * jump operators stay constant.  n <= 64 on CUDA cores (the workspace of
+ * dqb_mesolve_dense_workspace_size(n, n_jumps + 1, batch) suffices). */
+DQB_API int dqb_mesolve_dense_td(const dqb_dense_problem* problem, const dqb_td_hamiltonian* td,
+                                 const dqb_ode_options* options, const dqb_outputs* outputs,
+                                 void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- Schroedinger equation on the same Runge-Kutta engine ---------------------------- */
+/* Scratch bytes of dqb_sesolve_dense (a work counter). */
+DQB_API size_t dqb_sesolve_dense_workspace_size(void);
+
+/* Batched adaptive solve of d psi/dt = -i H psi with dense H, n <= 128.  Replaces
+ * DiffraxIntegrator.run for SESolveDiffraxIntegrator with Tsit5 / Dopri5
+ * (dynamiqs/integrators/core/diffrax_integrator.py:221-228,265-280; sesolve.py:240-330):
+ * the same tableaux, starting step, controller, error norm (RMS over the n entries of
+ * psi) and dense output as dqb_mesolve_dense.  The problem is a dqb_dense_problem with
+ * n_jumps = 0 and rho0 = psi0 as kets [*, n, 1] (rho0_is_ket and L are ignored); states
+ * are kets: complex64 [batch, nsave, n, 1]; expects[b, m, s] = <psi|E_m|psi>
+ * (utils/general.py:467-474).  One warp per in-flight instance, H in shared memory, psi
+ * and the stages in registers.  n > 128 returns DQB_ERR_UNSUPPORTED. */
+DQB_API int dqb_sesolve_dense(const dqb_dense_problem* problem, const dqb_ode_options* options,
+                              const dqb_outputs* outputs, void* workspace, size_t workspace_bytes,
+                              void* stream);
+
+/* Batched adaptive solve of the vectorized master equation d vec(rho)/dt = S vec(rho)
+ * (MESolveDiffraxIntegrator.vector_field_vec with options.vectorized=True,
+ * diffrax_integrator.py:325-327; S = slindbladian(H, jump_ops), utils/vectorization.py:
+ * 213-259), on the engine of dqb_sesolve_dense: the state is vec(rho), the columns of rho
+ * stacked (vectorize, utils/vectorization.py:25-59), N = n^2 <= 256 entries, and the error
+ * norm is the RMS over those N entries, as in the reference.  `problem` describes the
+ * vectorized system: problem->n = N, problem->rho0 = vec(rho0) complex64 [*, N],
+ * problem->E = exp_ops read row by row complex64 [n_exp, N] (expects = sum_k E_k y_k =
+ * tr(E rho)), problem->H ignored except as a non-NULL check, H_index selecting the
+ * instance's superoperator in `superop_t`: complex64 [*, N, N] holding S TRANSPOSED
+ * (S[k][l] at superop_t[l * N + k]).  states: vec(rho) complex64 [batch, nsave, N].
+ * N <= 128: S in shared memory; 128 < N <= 256: S read from global memory (L2). */
+DQB_API int dqb_mesolve_vectorized(const dqb_dense_problem* problem, const void* superop_t,
+                                   const dqb_ode_options* options, const dqb_outputs* outputs,
+                                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* One Schroedinger right-hand side per instance, out[b] = -i H[H_index[b]] psi[b]
+ * (diffrax_integrator.py:225-227); psi, out: complex64 [batch, n]. */
+DQB_API int dqb_schrodinger_rhs_dense(const dqb_dense_problem* problem, const void* psi, void* out,
+                                      void* stream);
+
 /* ---- ragged batches (serving) ----------------------------------------------------- */
 /* One instance of a ragged batch: its own n (<= max_n), jump count (<= max_jumps), tsave
  * grid, start time and output buffers; all pointers are device pointers to the

@@ -241,13 +241,22 @@ def solve(f: Callable, y0: np.ndarray, tsave: np.ndarray, *, method: str = 'Tsit
           rtol: float = 1e-6, atol: float = 1e-6, safety: float = 0.9,
           factormin: float = 0.2, factormax: float = 5.0, max_steps: int = 100_000,
           t0: float | None = None, time_dtype=np.float64,
-          save_fn: Callable | None = None, dt0: float | None = None) -> SolveOutput:
+          save_fn: Callable | None = None, dt0: float | None = None,
+          jump_ts=None) -> SolveOutput:
     """Adaptive explicit RK (Tsit5 or Dopri5) from t0 to tsave[-1].
 
     ``f(t, y)`` is the vector field; ``y`` keeps its dtype (complex64 to mimic the
     reference's default precision, complex128 for the FP64 oracle).  Time arithmetic is
     done in ``time_dtype`` (float32 mimics JAX's default, float64 is the GPU design).
     ``save_fn(y)`` is applied to every interpolated save.
+
+    ``jump_ts``: discontinuity times of the vector field, handled as the reference's
+    ``PIDController(jump_ts=...)`` does (``dynamiqs/integrators/core/
+    diffrax_integrator.py:59-72``): a trial step that would cross the next discontinuity J
+    is clipped to end just before it (the largest time below J), the step after it starts
+    at J itself with its first stage re-evaluated (no first-same-as-last across the jump),
+    and the controller scales the step it had proposed -- not the clipped one -- to
+    propose the next.
     """
     tab = TSIT5 if method == 'Tsit5' else DOPRI5
     td = np.dtype(time_dtype).type
@@ -262,13 +271,24 @@ def solve(f: Callable, y0: np.ndarray, tsave: np.ndarray, *, method: str = 'Tsit
     def fe(t, y):
         return np.asarray(f(t, y), dtype=ydt)
 
+    jumps = np.unique(np.asarray([] if jump_ts is None else jump_ts, dtype=time_dtype))
+
+    def clip_jump(ta, tb):
+        """(tb clipped before the first discontinuity after ta, whether it was)."""
+        k = int(np.searchsorted(jumps, ta, side='right'))
+        if k < jumps.size and tb >= jumps[k]:
+            return np.nextafter(jumps[k], td(-np.inf)), True
+        return tb, False
+
     y = y0.copy()
     t = t_start
     if dt0 is None:
         dt = td(select_initial_step(fe, float(t), y, rtol, atol, tab.start_exponent))
     else:
         dt = td(dt0)
-    tnext = min(td(t + dt), t_end)
+    dt_prop = dt  # the controller's last proposal (before any clipping)
+    tnext, made_jump = clip_jump(t, td(t + dt))
+    tnext = min(tnext, t_end)
     if tnext > t_end - clip_tol:
         tnext = t_end
     k1 = fe(t, y)
@@ -321,7 +341,7 @@ def solve(f: Callable, y0: np.ndarray, tsave: np.ndarray, *, method: str = 'Tsit
         fmin = 1.0 if keep else factormin
         factor = safety * (inv ** (1.0 / tab.error_order)) if np.isfinite(inv) else np.inf
         factor = float(np.clip(factor, fmin, factormax))
-        dt_new = td(h * td(factor))
+        dt_new = td((dt_prop if made_jump else h) * td(factor))
         if keep:
             out.naccepted += 1
             out.accepted_times.append(float(tnext))
@@ -336,15 +356,20 @@ def solve(f: Callable, y0: np.ndarray, tsave: np.ndarray, *, method: str = 'Tsit
                         ys = ys + (hf * w[j]) * ks[j]
                 out.ysave.append(save_fn(ys.astype(ydt)))
                 save_idx += 1
-            t = tnext
             y = y1
-            k1 = ks[6]
+            if made_jump:  # step ended just before a discontinuity: restart at it
+                t = np.nextafter(tnext, td(np.inf))
+                k1 = fe(float(t), y)
+            else:
+                t = tnext
+                k1 = ks[6]
             if not np.all(np.isfinite(y)):
                 out.status = STATUS_NONFINITE
                 break
         else:
             out.nrejected += 1
-        tn = td(t + dt_new)
+        dt_prop = dt_new
+        tn, made_jump = clip_jump(t, td(t + dt_new))
         if tn > t_end - clip_tol:
             # close to the end: an accepted step lands on t1, a rejected one retries
             # with half of what is left

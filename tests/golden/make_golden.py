@@ -64,6 +64,15 @@ def main(ref: str) -> None:
         'nsteps': int(m[1]), 'naccepted': int(m[2]), 'nrejected': int(m[3]),
     }
 
+    m, ln = _find(ref / 'dynamiqs/integrators/apis/sesolve.py', steps_rx)
+    out['sesolve_docstring'] = {
+        'source': f'dynamiqs/integrators/apis/sesolve.py:{ln}',
+        'system': {'n': 16, 'H': 'a^+ a', 'psi0': 'coherent(n, 1.0)',
+                   'tsave': 'linspace(0, 1, 11)', 'method': 'Tsit5', 'rtol': 1e-6,
+                   'atol': 1e-6, 'equation': 'Schroedinger'},
+        'nsteps': int(m[1]), 'naccepted': int(m[2]), 'nrejected': int(m[3]),
+    }
+
     p = ref / 'docs/documentation/basics/open-systems.md'
     m0, ln0 = _find(p, r'^\s*\[\[([-\d.]+)\+0\.j\s+0\.\s*\+0\.j\]')
     m1, _ = _find(p, r'^\s*\[\s*0\.\s*\+0\.j\s+([-\d.]+)\+0\.j\]\]')

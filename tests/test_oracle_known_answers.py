@@ -82,3 +82,15 @@ def test_ocavity_analytic(layout, form):
     errs = np.linalg.norm(r.states - p['true_states'], axis=(-2, -1))
     assert np.all(errs <= 1e-3)
     np.testing.assert_allclose(r.expects, p['true_expects'], rtol=1e-3, atol=1e-4)
+
+
+@pytest.mark.parametrize('dtype', [np.complex128, np.complex64])
+def test_sesolve_docstring(dtype):
+    """``dq.sesolve`` docstring (dynamiqs/integrators/apis/sesolve.py): 11 steps, none
+    rejected -- a fourth printed count, reproduced by the controller pinned on the other
+    three."""
+    g = GOLDEN['sesolve_docstring']
+    a = ops.destroy(16, layout='dense')
+    out = sesolve(ops.dag(a) @ a, ops.coherent(16, 1.0), np.linspace(0, 1.0, 11), dtype=dtype)
+    assert (out.nsteps, out.naccepted, out.nrejected) == (g['nsteps'], g['naccepted'],
+                                                          g['nrejected'])

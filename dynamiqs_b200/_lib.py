@@ -139,12 +139,61 @@ class RaggedInstance(ctypes.Structure):
     ]
 
 
+TD_PWC = 0
+TD_WAVE = 1
+TD_MAX_TERMS = 4
+
+
+class TdTerm(ctypes.Structure):
+    _fields_ = [
+        ('kind', ctypes.c_int32),
+        ('n_times', ctypes.c_int32),
+        ('times', ctypes.c_void_p),
+        ('values', ctypes.c_void_p),
+        ('value_index', ctypes.c_void_p),
+        ('amp_re', ctypes.c_double),
+        ('amp_im', ctypes.c_double),
+        ('omega', ctypes.c_double),
+        ('phase', ctypes.c_double),
+        ('t_center', ctypes.c_double),
+        ('sigma', ctypes.c_double),
+        ('t_start', ctypes.c_double),
+        ('t_end', ctypes.c_double),
+    ]
+
+
+class TdHamiltonian(ctypes.Structure):
+    _fields_ = [
+        ('n_terms', ctypes.c_int32),
+        ('ops', ctypes.c_void_p),
+        ('terms', ctypes.POINTER(TdTerm)),
+        ('n_jump_ts', ctypes.c_int32),
+        ('jump_ts', ctypes.c_void_p),
+    ]
+
+
+class Tape(ctypes.Structure):
+    _fields_ = [('t', ctypes.c_void_p), ('h', ctypes.c_void_p), ('y', ctypes.c_void_p),
+                ('capacity', ctypes.c_int32)]
+
+
+class Cotangents(ctypes.Structure):
+    _fields_ = [('states', ctypes.c_void_p), ('expects', ctypes.c_void_p)]
+
+
+class Gradients(ctypes.Structure):
+    _fields_ = [('rho0', ctypes.c_void_p), ('H', ctypes.c_void_p), ('L', ctypes.c_void_p)]
+
+
 # Every symbol include/dqb200.h declares, with (restype, argtypes).
 _P = ctypes.c_void_p
 SIGNATURES = {
     'dqb_mesolve_dense_workspace_size': (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64]),
     'dqb_mesolve_dense': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
                                          ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
+    'dqb_mesolve_dense_td': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(TdHamiltonian),
+                                            ctypes.POINTER(OdeOptions), ctypes.POINTER(Outputs), _P,
+                                            ctypes.c_size_t, _P]),
     'dqb_mesolve_dense_noalloc': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
                                                  ctypes.POINTER(Outputs), _P]),
     'dqb_lindblad_rhs_dense': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.c_int32, _P, _P, _P]),
@@ -176,6 +225,17 @@ SIGNATURES = {
     'dqb_lindblad_rhs_dia_tiled': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.c_int32,
                                                   ctypes.c_int32, _P, _P, _P, ctypes.c_size_t, _P]),
     'dqb_dense_small_max_n': (ctypes.c_int32, [ctypes.c_int32]),
+    'dqb_set_tc_wait_limit_ns': (None, [ctypes.c_uint64]),
+    'dqb_mesolve_dense_tape_bytes': (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64]),
+    'dqb_mesolve_dense_taped': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
+                                               ctypes.POINTER(Outputs), ctypes.POINTER(Tape), _P,
+                                               ctypes.c_size_t, _P]),
+    'dqb_mesolve_dense_adjoint_workspace_size': (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32,
+                                                                   ctypes.c_int64]),
+    'dqb_mesolve_dense_adjoint': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
+                                                 ctypes.POINTER(Tape), _P, ctypes.POINTER(Cotangents),
+                                                 ctypes.POINTER(Gradients), _P, ctypes.c_size_t, _P]),
+    'dqb_probe_bounded_wait': (ctypes.c_int, [ctypes.c_uint64, _P, _P]),
     'dqb_sesolve_dense_workspace_size': (ctypes.c_size_t, []),
     'dqb_sesolve_dense': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
                                          ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),

@@ -218,8 +218,9 @@ __device__ void rhs(const float2* sH, const float2* sL, const float2* sX, float2
 // With a time-dependent H (td->M > 0) the constant part Hnh0 = -iH0 - 1/2 sum L^+L is kept
 // in one more padded matrix, and every right-hand side first forms
 // Hnh(t) = Hnh0 - i sum_m c_m(t) H_m in sH from the terms' operators in global memory.
-template <int NP>
+template <int NP, int FEAT>
 struct SimtEngine {
+  static constexpr bool kJumps = (FEAT & 1) != 0, kTape = (FEAT & 2) != 0;
   float2 *sH, *sX, *sT, *sL;
   int n, K, form;
   const TdArgs* td;
@@ -235,7 +236,7 @@ struct SimtEngine {
     __syncthreads();
     build_hnh<NP>(sH, sL, n, K);
     __syncthreads();
-    if (td && td->M > 0) {
+    if constexpr (kJumps) {
       for (int e = threadIdx.x; e < Small<NP>::MAT; e += blockDim.x) sH0[e] = sH[e];
       __syncthreads();
     }
@@ -244,12 +245,12 @@ struct SimtEngine {
   template <class F>
   __device__ void rhs(F x_of, float2* also, float2* out, double t) {
     constexpr int LD = NP + 1;
-    const int M = td ? td->M : 0;
+    const int M = kJumps ? td->M : 0;
     float2 c[DQB_TD_MAX_TERMS];
 #pragma unroll
     for (int m = 0; m < DQB_TD_MAX_TERMS; ++m) {
       c[m] = make_float2(0.f, 0.f);
-      if (m < M) {
+      if (kJumps && m < M) {
         const double2 v = td_coef(td->term[m], inst, t);
         c[m] = make_float2((float)v.x, (float)v.y);
       }
@@ -260,7 +261,7 @@ struct SimtEngine {
       const float2 x = x_of(e);
       sX[i * LD + j] = x;
       if (also) also[e] = x;
-      if (M > 0) {
+      if (kJumps) {
         float2 h = sH0[i * LD + j];
         if (i < n && j < n) {
           float2 acc = make_float2(0.f, 0.f);  // sum_m c_m(t) H_m[i][j]
@@ -280,7 +281,8 @@ struct SimtEngine {
   __device__ bool failed() const { return false; }
 };
 
-template <int NP>
+// FEAT: 0 = constant operators, 1 = time-dependent H (discontinuity times), 2 = gradient tape.
+template <int NP, int FEAT = 0>
 __global__ void __launch_bounds__(kSmallThreads, NP == 64 ? 1 : (NP == 32 ? 3 : 4)) mesolve_small_kernel(DenseSmallArgs a) {
   extern __shared__ float4 smem_raw[];
   __shared__ double red[40];
@@ -301,7 +303,7 @@ __global__ void __launch_bounds__(kSmallThreads, NP == 64 ? 1 : (NP == 32 ? 3 : 
       continue;
     }
     const InstView v = view_of(a, inst);
-    SimtEngine<NP> eng{sH, sX, sT, sL, a.n, a.K, a.o.form, &a.td, sL + a.K * Small<NP>::MAT, inst};
+    SimtEngine<NP, FEAT> eng{sH, sX, sT, sL, a.n, a.K, a.o.form, &a.td, sL + a.K * Small<NP>::MAT, inst};
     solve_one<NP>(eng, v, a.o, slot, red, ctl);
     __syncthreads();
   }
@@ -390,23 +392,25 @@ static int sm_count() {
   return sms;
 }
 
-// Resident CTAs for (NP, K) on the current device; 0 if the shared memory does not fit.
-template <int NP>
+// Resident CTAs for (NP, K) of the kernel variant FEAT on the current device (raising
+// that variant's shared-memory limit); 0 if the shared memory does not fit.
+template <int NP, int FEAT = 0>
 static int small_grid(int K, long long batch) {
   const size_t smem = small_smem_bytes<NP>(K);
   if (smem + 2048 > max_optin_smem()) return 0;
-  const int per_sm = resident_ctas(mesolve_small_kernel<NP>, smem);
+  const int per_sm = resident_ctas(mesolve_small_kernel<NP, FEAT>, smem);
   if (per_sm < 1) return 0;
   long long g = (long long)per_sm * sm_count();
   if (g > batch) g = batch;
   return (int)std::max<long long>(g, 1);
 }
 
+template <int FEAT = 0>
 static int grid_for(int NP, int K, long long batch) {
   switch (NP) {
-    case 16: return small_grid<16>(K, batch);
-    case 32: return small_grid<32>(K, batch);
-    default: return small_grid<64>(K, batch);
+    case 16: return small_grid<16, FEAT>(K, batch);
+    case 32: return small_grid<32, FEAT>(K, batch);
+    default: return small_grid<64, FEAT>(K, batch);
   }
 }
 
@@ -468,6 +472,9 @@ static DenseSmallArgs make_args(const dqb_dense_problem* p, const dqb_ode_option
   a.counter = nullptr;
   if (o) a.o = make_ctrl(*o);
   std::memset(&a.td, 0, sizeof(a.td));
+  a.tape_t = a.tape_h = nullptr;
+  a.tape_y = nullptr;
+  a.tape_cap = 0;
   return a;
 }
 
@@ -525,7 +532,7 @@ extern "C" int dqb_mesolve_dense_td(const dqb_dense_problem* p, const dqb_td_ham
   const size_t need = dqb_mesolve_dense_workspace_size(p->n, Keff, p->batch);
   if (need == 0) return DQB_ERR_UNSUPPORTED;
   if (!workspace || workspace_bytes < need) return DQB_ERR_WORKSPACE_TOO_SMALL;
-  const int grid = grid_for(NP, Keff, p->batch);
+  const int grid = grid_for<1>(NP, Keff, p->batch);
   cudaStream_t s = (cudaStream_t)stream;
   DenseSmallArgs a = make_args(p, o, out);
   a.counter = (unsigned int*)workspace;
@@ -554,9 +561,9 @@ extern "C" int dqb_mesolve_dense_td(const dqb_dense_problem* p, const dqb_td_ham
   zero_words_kernel<<<1, 64, 0, s>>>((unsigned int*)workspace, 64);
   const size_t smem = smem_for(NP, Keff);
   switch (NP) {
-    case 16: mesolve_small_kernel<16><<<grid, kSmallThreads, smem, s>>>(a); break;
-    case 32: mesolve_small_kernel<32><<<grid, kSmallThreads, smem, s>>>(a); break;
-    default: mesolve_small_kernel<64><<<grid, kSmallThreads, smem, s>>>(a); break;
+    case 16: mesolve_small_kernel<16, 1><<<grid, kSmallThreads, smem, s>>>(a); break;
+    case 32: mesolve_small_kernel<32, 1><<<grid, kSmallThreads, smem, s>>>(a); break;
+    default: mesolve_small_kernel<64, 1><<<grid, kSmallThreads, smem, s>>>(a); break;
   }
   return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
 }
@@ -606,6 +613,374 @@ extern "C" int dqb_lindblad_rhs_dense_prec(const dqb_dense_problem* p, int32_t f
   if (!workspace || workspace_bytes < (size_t)p->batch * 32768) return DQB_ERR_WORKSPACE_TOO_SMALL;
   DenseSmallArgs a = make_args(p, nullptr, nullptr);
   return small_tc_rhs(a, (const float2*)rho, (float2*)outp, (float2*)workspace, (cudaStream_t)stream);
+}
+
+namespace dqb {
+
+// ------------------------------------------------------------------------------------
+// gradients: the discrete adjoint of the recorded Runge-Kutta steps
+// ------------------------------------------------------------------------------------
+//
+// Reverse-mode differentiation of the whole solve -- what JAX does through diffrax for the
+// reference's Direct / BackwardCheckpointed gradients (dynamiqs/gradient.py:10-110,
+// diffrax_integrator.py:88-99): the step sizes are constants (the controller is not
+// differentiated), and every accepted step is differentiated exactly.  For a linear
+// right-hand side k = S(X) = Hnh X + X Hnh^+ + sum_k L_k X L_k^+ the reverse pass of one
+// step, given the cotangent lambda of its end state and the cotangents G_s of the saves it
+// made (y_s = y + h sum_j w_j(theta_s) k_j), is
+//   kappa_j = h b_j lambda + sum_s h w_j(theta_s) G_s,
+//   for j = 7 .. 1: xi_j = S^+(kappa_j),  kappa_l += h a_jl xi_j (l < j),
+//   lambda <- lambda + sum_s G_s + sum_j xi_j,
+// with S^+(Z) = Hnh^+ Z + Z Hnh + sum_k L_k^+ Z L_k (the same product structure with Hnh
+// and L_k replaced by their adjoints, applied in place in shared memory), and the
+// operator gradients accumulate, with Zs = kappa_j + kappa_j^+ and X_j hermitian,
+//   dH += i Zs X_j,   dL_k += Zs L_k X_j - 1/2 L_k (X_j Zs + Zs X_j)
+// (complex gradients in the convention dLoss = Re tr(G^+ dA)).  The stage inputs X_j are
+// recomputed from the recorded start state of each step.
+
+constexpr int kAdjMats = 23;  // X_1..7, k_1..6 (+1 spare), kappa_1..7, xi, lambda
+
+struct AdjArgs {
+  DenseSmallArgs p;              // operators, indices, E, tsave, method, form, t0
+  const int* nacc;               // [batch] accepted steps of each instance (forward infos)
+  const float2* gstates;         // [batch, nsave, n, n] cotangents of the saved states, or null
+  const float2* gexpects;        // [batch, nE, ntsave] cotangents of the expectation values, or null
+  float2* grad_rho0;             // [batch, n, n] (or [batch, n] for kets)
+  float2* grad_H;                // [batch, n, n]
+  float2* grad_L;                // [batch, K, n, n]
+};
+
+// Conjugate-transpose a padded NP x NP matrix in shared memory, in place.
+template <int NP>
+__device__ void dagger_inplace(float2* S) {
+  constexpr int LD = NP + 1;
+  for (int e = threadIdx.x; e < NP * NP; e += blockDim.x) {
+    const int i = e / NP, j = e % NP;
+    if (i < j) {
+      const float2 a = S[i * LD + j], b = S[j * LD + i];
+      S[i * LD + j] = cconj(b);
+      S[j * LD + i] = cconj(a);
+    } else if (i == j) {
+      S[i * LD + i] = cconj(S[i * LD + i]);
+    }
+  }
+}
+
+// Global NP x NP matrix into a padded shared buffer (all NP^2 entries).
+template <int NP>
+__device__ __forceinline__ void to_smem(float2* S, const float2* __restrict__ g) {
+  for (int e = threadIdx.x; e < NP * NP; e += blockDim.x) S[(e / NP) * (NP + 1) + e % NP] = g[e];
+}
+
+// g[e] (+)= s * tile (the 4x4 register tile layout of gemm) for the n x n block.
+template <int NP>
+__device__ __forceinline__ void add_tile(float2* g, const float2 (&t)[NP / 16][NP / 16], float2 s, int n) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int r = 0; r < NP / 16; ++r)
+#pragma unroll
+    for (int c = 0; c < NP / 16; ++c) {
+      const int i = ty + 16 * r, j = tx + 16 * c;
+      if (i < n && j < n) {
+        float2& d = g[i * n + j];
+        d = cadd(d, cmul(s, t[r][c]));
+      }
+    }
+}
+
+template <int NP>
+__global__ void __launch_bounds__(kSmallThreads, 1) mesolve_adjoint_kernel(AdjArgs A) {
+  extern __shared__ float4 smem_raw[];
+  __shared__ long long inst_sh;
+  constexpr int NN = NP * NP, LD = NP + 1, MAT = Small<NP>::MAT;
+  const DenseSmallArgs& a = A.p;
+  const int tid = threadIdx.x, n = a.n, K = a.K;
+  float2* sH = reinterpret_cast<float2*>(smem_raw);
+  float2* sX = sH + MAT;
+  float2* sT = sX + MAT;
+  float2* sL = sT + MAT;
+  float2* sU = sL + K * MAT;  // one more product buffer
+  float2* slot = a.slots + (size_t)blockIdx.x * kAdjMats * NN;
+  float2* Xs = slot;             // X_1..7
+  float2* ks = slot + 7 * NN;    // k_1..6
+  float2* kap = slot + 14 * NN;  // kappa_1..7
+  float2* xi = slot + 21 * NN;
+  float2* lam = slot + 22 * NN;
+  const Tableau& T = c_tab[a.o.method];
+  for (;;) {
+    if (tid == 0) inst_sh = (long long)atomicAdd(a.counter, 1u);
+    __syncthreads();
+    const long long b = inst_sh;
+    if (b >= a.batch) break;
+    const InstView v = view_of(a, b);
+    const long long nn = (long long)n * n;
+    float2* gH = A.grad_H + b * nn;
+    float2* gL = A.grad_L + b * K * nn;
+    for (long long e = tid; e < nn; e += blockDim.x) gH[e] = make_float2(0.f, 0.f);
+    for (long long e = tid; e < K * nn; e += blockDim.x) gL[e] = make_float2(0.f, 0.f);
+    load_padded<NP>(sH, v.H, n);
+    for (int k = 0; k < K; ++k) load_padded<NP>(sL + k * MAT, v.L + (long long)k * nn, n);
+    __syncthreads();
+    build_hnh<NP>(sH, sL, n, K);
+    __syncthreads();
+    const int nsave = a.o.save_states ? a.ntsave : 1;
+    // lambda: the final state's cotangent when only it is saved, else zero
+    for (int e = tid; e < NN; e += blockDim.x) {
+      const int i = e / NP, j = e % NP;
+      float2 g = make_float2(0.f, 0.f);
+      if (!a.o.save_states && A.gstates && i < n && j < n) g = A.gstates[b * nn + i * n + j];
+      lam[e] = g;
+    }
+    int sp = a.ntsave - 1;  // saves are taken from the last one backwards
+    const int N = A.nacc[b];
+    for (int st = N - 1; st >= 0; --st) {
+      const double t = v.tape_t[st], h = v.tape_h[st];
+      const float2* y = a.tape_y + (b * (long long)a.tape_cap + st) * NN;
+      // (a) direct cotangents of the stages: the step's end state and its saves
+      for (int e = tid; e < NN; e += blockDim.x) {
+        const float2 l = lam[e];
+#pragma unroll
+        for (int j = 0; j < 7; ++j) kap[j * NN + e] = make_float2((float)(h * T.b[j]) * l.x, (float)(h * T.b[j]) * l.y);
+      }
+      __syncthreads();
+      while (sp >= 0 && (st == 0 || a.tsave[sp] > t)) {
+        double w[7];
+        dense_weights(a.o.method, h > 0.0 ? (a.tsave[sp] - t) / h : 1.0, w);
+        for (int e = tid; e < NN; e += blockDim.x) {
+          const int i = e / NP, j = e % NP;
+          if (i >= n || j >= n) continue;
+          float2 g = make_float2(0.f, 0.f);
+          if (a.o.save_states && A.gstates) g = A.gstates[(b * nsave + sp) * nn + i * n + j];
+          if (A.gexpects)
+            for (int m = 0; m < a.nE; ++m) {  // d tr(E rho) / d rho: cotangent ebar E^+
+              const float2 eb = A.gexpects[(b * a.nE + m) * a.ntsave + sp];
+              g = cfma(eb, cconj(a.E[((long long)m * n + j) * n + i]), g);
+            }
+#pragma unroll
+          for (int q = 0; q < 7; ++q) kap[q * NN + e] = caxpy((float)(h * w[q]), g, kap[q * NN + e]);
+          lam[e] = cadd(lam[e], g);
+        }
+        __syncthreads();
+        --sp;
+      }
+      // (b) the forward stages again: X_1 = y, X_j = y + h sum_{l<j} a_jl k_l, k_j = S(X_j)
+      for (int j = 0; j < 7; ++j) {
+        float cf[6];
+#pragma unroll
+        for (int l = 0; l < 6; ++l) cf[l] = (float)(h * T.a[j][l]);
+        for (int e = tid; e < NN; e += blockDim.x) {
+          float2 x = y[e];
+          for (int l = 0; l < j; ++l) x = caxpy(cf[l], ks[l * NN + e], x);
+          Xs[j * NN + e] = x;
+          sX[(e / NP) * LD + e % NP] = x;
+        }
+        __syncthreads();
+        if (j < 6) dqb::rhs<NP>(sH, sL, sX, sT, n, K, DQB_FORM_STANDARD, ks + j * NN, NP, NP);
+        __syncthreads();
+      }
+      // (c) adjoint operators in place: Hnh -> Hnh^+, L_k -> L_k^+
+      dagger_inplace<NP>(sH);
+      for (int k = 0; k < K; ++k) dagger_inplace<NP>(sL + k * MAT);
+      __syncthreads();
+      // (d) stages backwards
+      for (int j = 6; j >= 0; --j) {
+        to_smem<NP>(sX, kap + j * NN);
+        __syncthreads();
+        dqb::rhs<NP>(sH, sL, sX, sT, n, K, DQB_FORM_STANDARD, xi, NP, NP);  // xi = S^+(kappa_j)
+        __syncthreads();
+        for (int e = tid; e < NN; e += blockDim.x) {
+          const float2 x = xi[e];
+          lam[e] = cadd(lam[e], x);
+          for (int l = 0; l < j; ++l) kap[l * NN + e] = caxpy((float)(h * T.a[j][l]), x, kap[l * NN + e]);
+        }
+        // operator gradients: sT <- Zs = kappa_j + kappa_j^+, sX <- X_j
+        for (int e = tid; e < NN; e += blockDim.x) {
+          const int i = e / NP, c = e % NP;
+          sT[i * LD + c] = cadd(kap[j * NN + e], cconj(kap[j * NN + c * NP + i]));
+          sX[i * LD + c] = Xs[j * NN + e];
+        }
+        __syncthreads();
+        float2 acc[NP / 16][NP / 16];
+        zero_tile<NP>(acc);
+        gemm<NP, false, false>(acc, sT, sX, NP);  // Zs X
+        add_tile<NP>(gH, acc, make_float2(0.f, 1.f), n);
+        store_tile<NP>(sU, acc, 1.0f);              // sU = Zs X
+        __syncthreads();
+        for (int k = 0; k < K; ++k) {
+          const float2* Lk = sL + k * MAT;  // holds L_k^+; op = ^+ reads L_k back
+          // - 1/2 L (Zs X)
+          zero_tile<NP>(acc);
+          gemm<NP, true, false>(acc, Lk, sU, NP);
+          add_tile<NP>(gL + k * nn, acc, make_float2(-0.5f, 0.f), n);
+        }
+        __syncthreads();
+        zero_tile<NP>(acc);
+        gemm<NP, false, false>(acc, sX, sT, NP);  // X Zs
+        store_tile<NP>(sU, acc, 1.0f);
+        __syncthreads();
+        for (int k = 0; k < K; ++k) {
+          const float2* Lk = sL + k * MAT;
+          zero_tile<NP>(acc);
+          gemm<NP, true, false>(acc, Lk, sU, NP);  // - 1/2 L (X Zs)
+          add_tile<NP>(gL + k * nn, acc, make_float2(-0.5f, 0.f), n);
+        }
+        for (int k = 0; k < K; ++k) {
+          const float2* Lk = sL + k * MAT;
+          zero_tile<NP>(acc);
+          gemm<NP, false, true>(acc, sT, Lk, NP);  // Zs L
+          __syncthreads();
+          store_tile<NP>(sU, acc, 1.0f);
+          __syncthreads();
+          zero_tile<NP>(acc);
+          gemm<NP, false, false>(acc, sU, sX, NP);  // (Zs L) X
+          add_tile<NP>(gL + k * nn, acc, make_float2(1.f, 0.f), n);
+          __syncthreads();
+        }
+        __syncthreads();
+      }
+      // (e) operators back
+      dagger_inplace<NP>(sH);
+      for (int k = 0; k < K; ++k) dagger_inplace<NP>(sL + k * MAT);
+      __syncthreads();
+    }
+    // saves at or before t0 (no step reached them): they read y0 itself
+    while (sp >= 0) {
+      for (int e = tid; e < NN; e += blockDim.x) {
+        const int i = e / NP, j = e % NP;
+        if (i >= n || j >= n) continue;
+        float2 g = make_float2(0.f, 0.f);
+        if (a.o.save_states && A.gstates) g = A.gstates[(b * nsave + sp) * nn + i * n + j];
+        if (A.gexpects)
+          for (int m = 0; m < a.nE; ++m)
+            g = cfma(A.gexpects[(b * a.nE + m) * a.ntsave + sp], cconj(a.E[((long long)m * n + j) * n + i]), g);
+        lam[e] = cadd(lam[e], g);
+      }
+      __syncthreads();
+      --sp;
+    }
+    // rho0 = psi psi^+ for a ket: psibar = (lambda + lambda^+) psi
+    __syncthreads();
+    if (v.is_ket) {
+      for (int i = tid; i < n; i += blockDim.x) {
+        float2 acc = make_float2(0.f, 0.f);
+        for (int j = 0; j < n; ++j)
+          acc = cfma(cadd(lam[i * NP + j], cconj(lam[j * NP + i])), v.rho0[j], acc);
+        A.grad_rho0[b * n + i] = acc;
+      }
+    } else {
+      for (long long e = tid; e < nn; e += blockDim.x) A.grad_rho0[b * nn + e] = lam[(e / n) * NP + e % n];
+    }
+    __syncthreads();
+  }
+}
+
+template <int NP>
+static size_t adjoint_smem_bytes(int K) {
+  return (size_t)(4 + K) * Small<NP>::MAT * sizeof(float2);
+}
+
+template <int NP>
+static int adjoint_launch(const AdjArgs& A, cudaStream_t s, long long max_grid) {
+  const size_t smem = adjoint_smem_bytes<NP>(A.p.K);
+  if (smem + 2048 > max_optin_smem()) return DQB_ERR_UNSUPPORTED;
+  const int per_sm = resident_ctas(mesolve_adjoint_kernel<NP>, smem);
+  if (per_sm < 1) return DQB_ERR_UNSUPPORTED;
+  long long g = std::min<long long>((long long)per_sm * sm_count(), A.p.batch);
+  g = std::min<long long>(g, max_grid);
+  mesolve_adjoint_kernel<NP><<<(unsigned)std::max<long long>(g, 1), kSmallThreads, smem, s>>>(A);
+  return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+}
+
+}  // namespace dqb
+
+extern "C" size_t dqb_mesolve_dense_tape_bytes(int32_t n, int32_t tape_cap, int64_t batch) {
+  const int NP = dqb::pick_np(n);
+  if (NP == 0 || tape_cap < 0 || batch < 0) return 0;
+  return (size_t)batch * tape_cap * NP * NP * sizeof(float2);
+}
+
+extern "C" int dqb_mesolve_dense_taped(const dqb_dense_problem* p, const dqb_ode_options* o,
+                                       const dqb_outputs* out, const dqb_tape* tape, void* workspace,
+                                       size_t workspace_bytes, void* stream) {
+  using namespace dqb;
+  int rc = validate_dense(p, o);
+  if (rc) return rc;
+  if (!out || !out->states || !out->infos || !out->status || (p->n_exp > 0 && !out->expects))
+    return DQB_ERR_INVALID_ARGUMENT;
+  if (!tape || !tape->t || !tape->h || !tape->y || tape->capacity < 1) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->batch == 0) return DQB_OK;
+  const int NP = pick_np(p->n);
+  if (NP == 0 || dqb_dense_small_max_n(p->n_jumps) < NP) return DQB_ERR_UNSUPPORTED;
+  const size_t need = dqb_mesolve_dense_workspace_size(p->n, p->n_jumps, p->batch);
+  if (need == 0) return DQB_ERR_UNSUPPORTED;
+  if (!workspace || workspace_bytes < need) return DQB_ERR_WORKSPACE_TOO_SMALL;
+  const int grid = grid_for<2>(NP, p->n_jumps, p->batch);
+  cudaStream_t s = (cudaStream_t)stream;
+  DenseSmallArgs a = make_args(p, o, out);
+  a.counter = (unsigned int*)workspace;
+  a.slots = (float2*)((char*)workspace + 256);
+  a.tape_t = tape->t;
+  a.tape_h = tape->h;
+  a.tape_y = (float2*)tape->y;
+  a.tape_cap = tape->capacity;
+  zero_words_kernel<<<1, 64, 0, s>>>((unsigned int*)workspace, 64);
+  const size_t smem = smem_for(NP, p->n_jumps);
+  switch (NP) {
+    case 16: mesolve_small_kernel<16, 2><<<grid, kSmallThreads, smem, s>>>(a); break;
+    case 32: mesolve_small_kernel<32, 2><<<grid, kSmallThreads, smem, s>>>(a); break;
+    default: mesolve_small_kernel<64, 2><<<grid, kSmallThreads, smem, s>>>(a); break;
+  }
+  return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+}
+
+extern "C" size_t dqb_mesolve_dense_adjoint_workspace_size(int32_t n, int32_t n_jumps, int64_t batch) {
+  using namespace dqb;
+  const int NP = pick_np(n);
+  if (NP == 0 || batch <= 0 || n_jumps < 0) return 0;
+  const size_t smem = (size_t)(4 + n_jumps) * (NP + 1) * NP * sizeof(float2);
+  if (smem + 2048 > max_optin_smem()) return 0;
+  const long long g = std::min<long long>((long long)sm_count(), batch);
+  return 256 + (size_t)g * kAdjMats * NP * NP * sizeof(float2);
+}
+
+extern "C" int dqb_mesolve_dense_adjoint(const dqb_dense_problem* p, const dqb_ode_options* o,
+                                         const dqb_tape* tape, const int32_t* naccepted,
+                                         const dqb_cotangents* cot, const dqb_gradients* grads,
+                                         void* workspace, size_t workspace_bytes, void* stream) {
+  using namespace dqb;
+  int rc = validate_dense(p, o);
+  if (rc) return rc;
+  if (!tape || !tape->t || !tape->h || !tape->y || !naccepted || !cot || !grads) return DQB_ERR_INVALID_ARGUMENT;
+  if (!grads->rho0 || !grads->H || (p->n_jumps > 0 && !grads->L)) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->n_exp > 0 && cot->expects && !p->E) return DQB_ERR_INVALID_ARGUMENT;
+  if (p->batch == 0) return DQB_OK;
+  const int NP = pick_np(p->n);
+  if (NP == 0) return DQB_ERR_UNSUPPORTED;
+  const size_t need = dqb_mesolve_dense_adjoint_workspace_size(p->n, p->n_jumps, p->batch);
+  if (need == 0) return DQB_ERR_UNSUPPORTED;
+  if (!workspace || workspace_bytes < need) return DQB_ERR_WORKSPACE_TOO_SMALL;
+  cudaStream_t s = (cudaStream_t)stream;
+  AdjArgs A;
+  A.p = make_args(p, o, nullptr);
+  A.p.counter = (unsigned int*)workspace;
+  A.p.slots = (float2*)((char*)workspace + 256);
+  A.p.tape_t = tape->t;
+  A.p.tape_h = tape->h;
+  A.p.tape_y = (float2*)tape->y;
+  A.p.tape_cap = tape->capacity;
+  A.nacc = naccepted;
+  A.gstates = (const float2*)cot->states;
+  A.gexpects = (const float2*)cot->expects;
+  A.grad_rho0 = (float2*)grads->rho0;
+  A.grad_H = (float2*)grads->H;
+  A.grad_L = (float2*)grads->L;
+  zero_words_kernel<<<1, 64, 0, s>>>((unsigned int*)workspace, 64);
+  const long long max_grid = (long long)((workspace_bytes - 256) / ((size_t)kAdjMats * NP * NP * sizeof(float2)));
+  switch (NP) {
+    case 16: return adjoint_launch<16>(A, s, max_grid);
+    case 32: return adjoint_launch<32>(A, s, max_grid);
+    default: return adjoint_launch<64>(A, s, max_grid);
+  }
 }
 
 extern "C" const char* dqb_version(void) { return "dqb200 0.2 sm_100a"; }
@@ -700,7 +1075,10 @@ __global__ void __launch_bounds__(kSmallThreads, NP == 64 ? 1 : (NP == 32 ? 3 : 
     v.inst = inst;
     v.n_jump = 0;
     v.jump_ts = nullptr;
-    SimtEngine<NP> eng{sH, sX, sT, sL, v.n, v.K, o.form, nullptr, nullptr, inst};
+    v.tape_t = v.tape_h = nullptr;
+    v.tape_y = nullptr;
+    v.tape_cap = 0;
+    SimtEngine<NP, 0> eng{sH, sX, sT, sL, v.n, v.K, o.form, nullptr, nullptr, inst};
     solve_one<NP>(eng, v, o, slot, red, ctl);
     __syncthreads();
   }

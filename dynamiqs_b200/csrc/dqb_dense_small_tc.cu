@@ -34,6 +34,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "dqb_small.cuh"
@@ -118,6 +119,7 @@ __device__ __forceinline__ void mma3(uint32_t d, uint32_t a_hi, uint32_t b_hi, u
 }  // namespace stc
 
 struct TcEngine {
+  static constexpr bool kJumps = false, kTape = false;
   uint8_t* g;        // tile area (generic address, 1024-aligned)
   uint32_t s;        // its shared-window address
   uint32_t tmem;     // tensor-memory base (512 columns)
@@ -127,6 +129,7 @@ struct TcEngine {
   int eL[2], eH;     // scale exponents of the operators
   float* redf;       // >= 9 floats of shared scratch
   int* fail;         // shared failure flag
+  unsigned long long wait_ns;  // limit of every mbarrier wait
 
   __device__ uint8_t* x_hi() const { return g; }
   __device__ uint8_t* h_hi() const { return g + 2 * stc::kTile; }
@@ -138,7 +141,8 @@ struct TcEngine {
   __device__ bool failed() const { return *fail != 0; }
 
   __device__ bool wait(uint32_t bar, uint32_t& ph) {
-    bool ok = !failed() && tc::mbar_wait(bar, ph & 1u);
+    // a limit of 1 ns gives up at once (how a test drives this path deterministically)
+    bool ok = !failed() && wait_ns > 1 && tc::mbar_wait_for(bar, ph & 1u, wait_ns);
     ok = __syncthreads_and(ok);
     ++ph;
     if (!ok && threadIdx.x == 0) *fail = 1;
@@ -381,12 +385,24 @@ struct TcEngine {
   }
 };
 
-__global__ void __launch_bounds__(kSmallThreads, 1) mesolve_small_tc_kernel(DenseSmallArgs a) {
+// After a wait has run out, MMAs issued before it may still be in flight: commit them to
+// a fresh barrier and wait for them (the default limit) before the tensor memory they write
+// is freed.
+__device__ void drain_after_failure(uint64_t* bar_exit, int failed) {
+  if (failed && threadIdx.x == 0) {
+    const uint32_t b = tc::smem_u32(bar_exit);
+    tc::mma_commit(b);
+    tc::mbar_wait_for(b, 0, tc::kWaitLimitNs);
+  }
+}
+
+__global__ void __launch_bounds__(kSmallThreads, 1) mesolve_small_tc_kernel(DenseSmallArgs a,
+                                                                            unsigned long long wait_ns) {
   extern __shared__ uint8_t stc_dsm[];
   __shared__ double red[40];
   __shared__ float redf[16];
   __shared__ Ctrl ctl;
-  __shared__ uint64_t bars[2];
+  __shared__ uint64_t bars[3];
   __shared__ uint32_t tmem_sh;
   __shared__ int fail_sh;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -396,6 +412,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) mesolve_small_tc_kernel(Dens
     if (lane == 0) {
       tc::mbar_init(tc::smem_u32(&bars[0]), 1);
       tc::mbar_init(tc::smem_u32(&bars[1]), 1);
+      tc::mbar_init(tc::smem_u32(&bars[2]), 1);
       tc::fence_mbar_init();
       fail_sh = 0;
     }
@@ -416,6 +433,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) mesolve_small_tc_kernel(Dens
   eng.K = a.K;
   eng.redf = redf;
   eng.fail = &fail_sh;
+  eng.wait_ns = wait_ns;
   float2* slot = a.slots + (size_t)blockIdx.x * kSlotMats * 4096;
   for (;;) {
     if (threadIdx.x == 0) ctl.inst = (long long)atomicAdd(a.counter, 1u);
@@ -431,6 +449,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) mesolve_small_tc_kernel(Dens
     solve_one<64>(eng, v, a.o, slot, red, ctl);
     __syncthreads();
   }
+  drain_after_failure(&bars[2], fail_sh);
   tc::tc_fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -472,6 +491,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) rhs_small_tc_kernel(DenseSma
   eng.ph1 = eng.ph2 = 0;
   eng.redf = redf;
   eng.fail = &fail_sh;
+  eng.wait_ns = tc::kWaitLimitNs;
   const long long b = blockIdx.x;
   const int n = a.n;
   InstView v{};
@@ -496,6 +516,24 @@ __global__ void __launch_bounds__(kSmallThreads, 1) rhs_small_tc_kernel(DenseSma
     __syncwarp();
     tc::tmem_dealloc(eng.tmem, stc::kTmemCols);
   }
+}
+
+// Limit of the tensor-core kernels' mbarrier waits (dqb_set_tc_wait_limit_ns).
+std::atomic<unsigned long long> g_wait_limit_ns{tc::kWaitLimitNs};
+unsigned long long tc_wait_limit_ns() { return g_wait_limit_ns.load(); }
+
+// One mbarrier wait that nothing completes, bounded by `limit_ns`: out[0] = 1 if it gave
+// up, out[1] = microseconds it waited.
+__global__ void bounded_wait_probe_kernel(unsigned long long limit_ns, int* out) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x != 0) return;
+  const uint32_t b = tc::smem_u32(&bar);
+  tc::mbar_init(b, 1);
+  tc::fence_mbar_init();
+  const unsigned long long t0 = tc::globaltimer_ns();
+  const bool done = tc::mbar_wait_for(b, 0, limit_ns);
+  out[0] = done ? 0 : 1;
+  out[1] = (int)((tc::globaltimer_ns() - t0) / 1000ull);
 }
 
 static void raise_smem_limit_once() {
@@ -524,7 +562,7 @@ int small_tc_launch(const DenseSmallArgs& a, int max_grid, cudaStream_t s) {
   long long g = std::min<long long>(sms, a.batch);
   g = std::min<long long>(g, max_grid);
   if (g < 1) g = 1;
-  mesolve_small_tc_kernel<<<(unsigned)g, kSmallThreads, stc::smem_bytes(a.K), s>>>(a);
+  mesolve_small_tc_kernel<<<(unsigned)g, kSmallThreads, stc::smem_bytes(a.K), s>>>(a, tc_wait_limit_ns());
   return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
 }
 
@@ -539,3 +577,13 @@ int small_tc_rhs(const DenseSmallArgs& a, const float2* rho, float2* out, float2
 }
 
 }  // namespace dqb
+
+extern "C" void dqb_set_tc_wait_limit_ns(uint64_t ns) {
+  dqb::g_wait_limit_ns.store(ns ? (unsigned long long)ns : dqb::tc::kWaitLimitNs);
+}
+
+extern "C" int dqb_probe_bounded_wait(uint64_t limit_ns, int32_t* result, void* stream) {
+  if (!result || limit_ns > 1000000000ull) return DQB_ERR_INVALID_ARGUMENT;
+  dqb::bounded_wait_probe_kernel<<<1, 32, 0, (cudaStream_t)stream>>>((unsigned long long)limit_ns, result);
+  return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+}

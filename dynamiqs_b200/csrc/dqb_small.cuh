@@ -14,6 +14,9 @@
 //     // True once a bounded wait has run out (the tensor-core engine); the instance then
 //     // ends with DQB_INST_NONFINITE and the kernel stops taking new instances.
 //     __device__ bool failed() const;
+//     // Compile-time features: discontinuity times in the controller (time-dependent H),
+//     // and the gradient tape; solves without them carry none of their code.
+//     static constexpr bool kJumps, kTape;
 //   };
 //
 // The loop follows what dynamiqs obtains from diffrax (dynamiqs/integrators/core/
@@ -115,6 +118,12 @@ struct DenseSmallArgs {
   const int* order;  // start order of the instances, or null (0, 1, 2, ...)
   CtrlOpts o;
   TdArgs td;
+  // gradient tape (or null): per instance, the start time, size and starting state of
+  // every accepted step, at most tape_cap of them
+  double* tape_t;
+  double* tape_h;
+  float2* tape_y;
+  int tape_cap;
 };
 
 struct Ctrl {
@@ -143,6 +152,10 @@ struct InstView {
   long long inst;      // index of the instance in its batch
   int n_jump;          // discontinuity times (the controller's jump_ts)
   const double* jump_ts;
+  double* tape_t;      // gradient tape of the instance (null: none)
+  double* tape_h;
+  float2* tape_y;      // the batch's tape states: [batch, tape_cap, NP, NP]
+  int tape_cap;
 };
 
 __device__ __forceinline__ InstView view_of(const DenseSmallArgs& a, long long inst) {
@@ -150,6 +163,10 @@ __device__ __forceinline__ InstView view_of(const DenseSmallArgs& a, long long i
   v.inst = inst;
   v.n_jump = a.td.n_jump;
   v.jump_ts = a.td.jump_ts;
+  v.tape_cap = a.tape_cap;
+  v.tape_t = a.tape_t ? a.tape_t + inst * a.tape_cap : nullptr;
+  v.tape_h = a.tape_h ? a.tape_h + inst * a.tape_cap : nullptr;
+  v.tape_y = a.tape_y;  // the whole tape: solve_one offsets it by inst * tape_cap * NP^2
   const int n = a.n;
   const long long nn = (long long)n * n;
   const long long hi = a.Hidx ? a.Hidx[inst] : inst;
@@ -300,7 +317,14 @@ __device__ void solve_one(Engine& eng, const InstView& a, const CtrlOpts& o, flo
     ctl.t = a.t0;
     ctl.t1 = t1;
     ctl.dt_prop = dt;
-    ctl.tnext = next_trial(a.jump_ts, a.n_jump, a.t0, dt, t1, true, ctl.made_jump);
+    ctl.made_jump = 0;
+    if constexpr (Engine::kJumps) {
+      ctl.tnext = next_trial(a.jump_ts, a.n_jump, a.t0, dt, t1, true, ctl.made_jump);
+    } else {
+      double tn = a.t0 + dt;
+      if (tn > t1 - 1e-10) tn = t1;
+      ctl.tnext = tn < t1 ? tn : t1;
+    }
     ctl.run = a.t0 < t1;
     if (eng.failed()) {
       ctl.status = DQB_INST_NONFINITE;
@@ -387,13 +411,24 @@ __device__ void solve_one(Engine& eng, const InstView& a, const CtrlOpts& o, flo
         ctl.keep = keep;
         if (keep) ctl.nacc += 1; else ctl.nrej += 1;
         // after a step clipped at a discontinuity the controller scales its proposal
-        ctl.dtnew = (ctl.made_jump ? ctl.dt_prop : h) * step_factor(o, err, keep);
+        const double base = (Engine::kJumps && ctl.made_jump) ? ctl.dt_prop : h;
+        ctl.dtnew = base * step_factor(o, err, keep);
       }
     }
     __syncthreads();
     if (ctl.status != DQB_INST_OK) break;
 
     if (ctl.keep) {
+      // gradient tape: the accepted step's start time, size and starting state
+      if (Engine::kTape && a.tape_y && ctl.nacc <= a.tape_cap) {
+        const long long idx = ctl.nacc - 1;
+        if (tid == 0) {
+          a.tape_t[idx] = ctl.t;
+          a.tape_h[idx] = h;
+        }
+        float2* dst = a.tape_y + (a.inst * (long long)a.tape_cap + idx) * NN;
+        for (int e = tid; e < NN; e += blockDim.x) dst[e] = yv[e];
+      }
       // dense output at every save time in (t, tnext]
       while (ctl.save_idx < a.ntsave && a.tsave[ctl.save_idx] <= ctl.tnext) {
         if (tid == 0) {
@@ -419,18 +454,24 @@ __device__ void solve_one(Engine& eng, const InstView& a, const CtrlOpts& o, flo
         ctl.sk[0] = ctl.sk[6];
         ctl.sk[6] = tmp;
         // a step that ended just before a discontinuity: the next starts on it
-        ctl.t = ctl.made_jump ? nextafter(ctl.tnext, INFINITY) : ctl.tnext;
+        ctl.t = (Engine::kJumps && ctl.made_jump) ? nextafter(ctl.tnext, INFINITY) : ctl.tnext;
       }
-      __syncthreads();
-      if (ctl.made_jump && ctl.t < ctl.t1) {  // first stage re-evaluated across the jump
-        const float2* yn = slot + ctl.sy * NN;
-        eng.rhs([&](int e) { return yn[e]; }, nullptr, slot + ctl.sk[0] * NN, ctl.t);
+      if constexpr (Engine::kJumps) {
+        __syncthreads();
+        if (ctl.made_jump && ctl.t < ctl.t1) {  // first stage re-evaluated across the jump
+          const float2* yn = slot + ctl.sy * NN;
+          eng.rhs([&](int e) { return yn[e]; }, nullptr, slot + ctl.sk[0] * NN, ctl.t);
+        }
       }
     }
     __syncthreads();
     if (tid == 0) {
-      ctl.dt_prop = ctl.dtnew;
-      ctl.tnext = next_trial(a.jump_ts, a.n_jump, ctl.t, ctl.dtnew, ctl.t1, ctl.keep, ctl.made_jump);
+      if constexpr (Engine::kJumps) {
+        ctl.dt_prop = ctl.dtnew;
+        ctl.tnext = next_trial(a.jump_ts, a.n_jump, ctl.t, ctl.dtnew, ctl.t1, ctl.keep, ctl.made_jump);
+      } else {
+        ctl.tnext = next_tend(ctl.t, ctl.dtnew, ctl.t1, ctl.keep);
+      }
       ctl.run = ctl.t < ctl.t1;
     }
     __syncthreads();

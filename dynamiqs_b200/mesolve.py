@@ -305,7 +305,10 @@ class MESolveB200Integrator:
         self.options = options
         self.H = H
         self.Ls = Ls
-        self.Es = Es
+        # The identity is appended to the expectation operators: its FP64-summed expectation
+        # value at every save point is the trace check of the saved states (result.checks).
+        self._n_user_E = len(Es) if Es else 0
+        self.Es = list(Es or []) + [np.eye(_shape(H)[-1], dtype=np.complex64)]
         self.plan = plan
         self._tuned: dict = {}  # launch choices made by the autotuner at prepare time
         self._path = 'large'  # 'small', 'large' or 'dia': set by prepare()
@@ -439,7 +442,9 @@ class MESolveB200Integrator:
         nsave = ntsave if self.options.save_states else 1
         return n, len(self.Ls), ntsave, self.plan.batch, nE, nsave
 
-    def _prepare_dense(self, lib, kind) -> PreparedSolve:
+    def _prepare_dense(self, lib, kind, extra_mats: int = 0) -> PreparedSolve:
+        """`extra_mats`: shared-memory matrices the kernel needs beyond the jump operators
+        (1 for a time-dependent H: its constant part)."""
         import torch
 
         self._path = kind
@@ -456,7 +461,7 @@ class MESolveB200Integrator:
             H_index=bufs['H_index'].data_ptr(), L_index=bufs['L_index'].data_ptr(),
             rho0_index=bufs['rho0_index'].data_ptr())
         if kind == 'small':
-            ws_bytes = lib.dqb_mesolve_dense_workspace_size(n, K, B)
+            ws_bytes = lib.dqb_mesolve_dense_workspace_size(n, K + extra_mats, B)
             fn, name = lib.dqb_mesolve_dense, 'dqb_mesolve_dense'
             if B > 256:  # more instances than resident CTAs: start the stiffest first
                 bufs['start_order'] = _to_dev(self._start_order(), torch.int32, dev)
@@ -602,6 +607,17 @@ class MESolveB200Integrator:
     def _run_dia(self, lib) -> MESolveResult:
         return self._prepare_dia(lib).launch().result()
 
+    def _checks(self, states, trace):
+        """FP64 checks of the saved states: tr(rho) at every save point (the identity's
+        expectation value, summed in FP64 by the kernels) and the hermiticity defect
+        ||rho - rho^+||_F / ||rho||_F of every saved state (FP64, on the device)."""
+        import torch
+
+        st = states.to(torch.complex128)
+        den = torch.linalg.norm(st.reshape(*st.shape[:-2], -1), dim=-1)
+        num = torch.linalg.norm((st - st.mH).reshape(*st.shape[:-2], -1), dim=-1)
+        return {'trace': trace, 'hermiticity': num / torch.clamp(den, min=1e-300)}
+
     def _result(self, states, expects, infos, status) -> MESolveResult:
         import torch
 
@@ -614,6 +630,11 @@ class MESolveB200Integrator:
             raise RuntimeError('The solution became non-finite (NaN or inf) during the '
                                'integration.')
         bshape = self.plan.bshape
+        trace = None
+        if expects is not None:  # the last row is the identity's: the trace check
+            trace = expects[:, self._n_user_E].to(torch.complex128)
+            trace = trace.reshape(*bshape, trace.shape[-1])
+            expects = expects[:, :self._n_user_E] if self._n_user_E else None
         if self._path == 'vectorized':  # vec(rho) -> rho (unvectorize, columns stacked)
             m = int(round(states.shape[-1] ** 0.5))
             states = states.reshape(*states.shape[:-1], m, m).transpose(-1, -2)
@@ -637,7 +658,7 @@ class MESolveB200Integrator:
                 extra = vals
         return MESolveResult(tsave=self.ts, method=self.method, gradient=self.gradient,
                              options=self.options, states=states, expects=expects,
-                             infos=info, extra=extra)
+                             infos=info, extra=extra, checks=self._checks(states, trace))
 
 
 # --------------------------------------------------------------------------------------
@@ -657,14 +678,40 @@ def mesolve(H, jump_ops, rho0, tsave, *, exp_ops=None, method: Method = Tsit5(),
     :class:`~dynamiqs_b200.qarrays.SparseDIA`.  ``method`` is ``Tsit5`` (default) or
     ``Dopri5``.
     """
-    from .time_qarray import PWCTimeQArray, SummedTimeQArray
+    from .time_qarray import ModulatedTimeQArray, PWCTimeQArray, SummedTimeQArray, as_summed
 
-    if isinstance(H, (PWCTimeQArray, SummedTimeQArray)):
+    td_types = (PWCTimeQArray, ModulatedTimeQArray, SummedTimeQArray)
+    if any(isinstance(L, td_types) for L in jump_ops):
+        raise NotImplementedError('Time-dependent jump operators are not supported on the B200 '
+                                  'path.')
+    if isinstance(H, td_types):
+        Hs = as_summed(H)
+        if _td_on_device(Hs, jump_ops, options):
+            return _mesolve_td(Hs, jump_ops, rho0, tsave, exp_ops=exp_ops, method=method,
+                               gradient=gradient, options=options)
+        if not Hs.only_pwc:
+            raise NotImplementedError('Modulated Hamiltonians run on the n <= 64 kernel only '
+                                      '(at most four time-dependent terms, dense jump '
+                                      'operators, options.vectorized=False).')
         return _mesolve_piecewise(H, jump_ops, rho0, tsave, exp_ops=exp_ops, method=method,
                                   gradient=gradient, options=options, solve=mesolve)
     if getattr(H, '__class__', None).__name__.endswith('TimeQArray'):
-        raise NotImplementedError('Only piecewise-constant time-dependent operators (dq.pwc and '
-                                  'sums with constant operators) are supported on the B200 path.')
+        raise NotImplementedError('Callable time-dependent operators cannot run inside the B200 '
+                                  'kernels: use dq.pwc or dq.modulated with a Wave prefactor.')
+    from .autodiff import mesolve_autograd, needs_autograd
+
+    if needs_autograd(H, jump_ops, rho0):
+        tsave_np = np.asarray(tsave.detach().cpu().numpy() if hasattr(tsave, 'detach') else tsave,
+                              dtype=np.float64)
+        tsave_np = check_times(tsave_np, 'tsave')
+        check_options(options, 'mesolve')
+        options = options.initialise()
+        assert_method_supported(method)
+        method.assert_supports_gradient(gradient)
+        return mesolve_autograd(H, jump_ops, rho0, tsave_np, exp_ops=exp_ops, method=method,
+                                gradient=gradient, options=options,
+                                integ_cls=MESolveB200Integrator, make_plan=make_batch_plan,
+                                check=_check_mesolve_args)
     if any(isinstance(L, (PWCTimeQArray, SummedTimeQArray)) for L in jump_ops):
         raise NotImplementedError('Time-dependent jump operators are not supported on the B200 '
                                   'path.')
@@ -694,6 +741,86 @@ def mesolve(H, jump_ops, rho0, tsave, *, exp_ops=None, method: Method = Tsit5(),
     integrator = MESolveB200Integrator(ts=tsave, y0=rho0, method=method, gradient=gradient,
                                        options=options, H=H, Ls=Ls, Es=exp_ops, plan=plan)
     return integrator.run()
+
+
+def _td_on_device(Hs, jump_ops, options) -> bool:
+    """Whether a time-dependent H runs as one launch of the n <= 64 kernel."""
+    n = Hs.constant.shape[-1]
+    if options.vectorized or len(Hs.td_terms) > _lib.TD_MAX_TERMS:
+        return False
+    if any(isinstance(L, SparseDIA) or np.ndim(L) != 2 for L in jump_ops):
+        return False
+    return n <= _lib.load().dqb_dense_small_max_n(len(jump_ops) + 1)
+
+
+def _mesolve_td(Hs, jump_ops, rho0, tsave, *, exp_ops, method, gradient, options):
+    """``H(t) = H0 + sum_m c_m(t) H_m`` in one launch (``dqb_mesolve_dense_td``): the
+    kernels evaluate the PWC and Wave prefactors at every stage time, and the controller
+    clips its steps at the discontinuity times as the reference's ``jump_ts`` does.
+    Batched PWC values ``(..., N)`` are the leading result dimensions (cartesian batching)
+    and run as instances of the same launch."""
+    import ctypes
+
+    import torch
+
+    from .time_qarray import PWCTimeQArray
+
+    Ls = [_as_op(L) for L in jump_ops]
+    rho0 = _as_op(rho0)
+    tsave = np.asarray(tsave.detach().cpu().numpy() if hasattr(tsave, 'detach') else tsave,
+                       dtype=np.float64)
+    if exp_ops is not None:
+        exp_ops = [_as_op(E) for E in exp_ops] if len(exp_ops) > 0 else None
+    n = Hs.constant.shape[-1]
+    bs = tuple(Hs.batch_shape)
+    if bs and not options.cartesian_batching:
+        raise NotImplementedError('Batched PWC values need cartesian batching on the B200 path.')
+    Hb = np.broadcast_to(Hs.constant.astype(np.complex64), (*bs, n, n))
+    _check_mesolve_args(Hb, Ls, rho0, exp_ops)
+    tsave = check_times(tsave, 'tsave')
+    check_options(options, 'mesolve')
+    options = options.initialise()
+    assert_method_supported(method)
+    method.assert_supports_gradient(gradient)
+    plan = make_batch_plan(Hb, Ls, rho0, True)
+    integ = MESolveB200Integrator(ts=tsave, y0=rho0, method=method, gradient=gradient,
+                                  options=options, H=Hb, Ls=Ls, Es=exp_ops, plan=plan)
+    lib = _lib.load()
+    prep = integ._prepare_dense(lib, 'small', extra_mats=1)
+    dev = prep.dev
+    nsets = int(np.prod(bs, dtype=np.int64)) if bs else 1
+    terms = (_lib.TdTerm * _lib.TD_MAX_TERMS)()
+    keep = []
+    for m, term in enumerate(Hs.td_terms):
+        T = terms[m]
+        if isinstance(term, PWCTimeQArray):
+            vals = np.broadcast_to(term.values, (*bs, term.values.shape[-1])).reshape(nsets, -1)
+            tt = _to_dev(term.times, torch.float64, dev)
+            vv = _to_dev(np.ascontiguousarray(vals, dtype=np.complex128), torch.complex128, dev)
+            keep += [tt, vv]
+            T.kind, T.n_times = _lib.TD_PWC, term.times.size
+            T.times, T.values = tt.data_ptr(), vv.data_ptr()
+            T.value_index = prep.bufs['H_index'].data_ptr() if bs else None
+        else:
+            f = term.f
+            T.kind = _lib.TD_WAVE
+            T.amp_re, T.amp_im = f.amplitude.real, f.amplitude.imag
+            T.omega, T.phase, T.t_center, T.sigma = f.omega, f.phase, f.t_center, f.sigma
+            T.t_start, T.t_end = f.t_start, f.t_end
+    ops_d = _to_dev(np.stack([t.qarray for t in Hs.td_terms]), torch.complex64, dev)
+    jts = np.asarray(Hs.discontinuity_ts, dtype=np.float64)
+    jts_d = _to_dev(jts if jts.size else np.zeros(1), torch.float64, dev)
+    keep += [ops_d, jts_d]
+    td = _lib.TdHamiltonian(n_terms=len(Hs.td_terms), ops=ops_d.data_ptr(),
+                            terms=ctypes.cast(terms, ctypes.POINTER(_lib.TdTerm)),
+                            n_jump_ts=int(jts.size), jump_ts=jts_d.data_ptr())
+    prep.bufs['td'] = (td, terms, keep)
+
+    def fn(prob, opts, outs, ws, wsb, stream):
+        return lib.dqb_mesolve_dense_td(prob, td, opts, outs, ws, wsb, stream)
+
+    prep.fn, prep.name = fn, 'dqb_mesolve_dense_td'
+    return prep.launch().result()
 
 
 def _mesolve_piecewise(H, jump_ops, rho0, tsave, *, exp_ops, method, gradient, options, solve):

@@ -29,10 +29,16 @@ class _DEAdaptiveStep(Method):
     max_steps: int = 100_000
 
     def assert_supports_gradient(self, gradient) -> None:
-        if gradient is not None:
-            raise NotImplementedError(
-                'Gradients are not available on the B200 mesolve path (forward solve '
-                'only); pass `gradient=None`.')
+        """``Method.assert_supports_gradient`` (``dynamiqs/method.py:44-60``): Tsit5 and
+        Dopri5 take ``Direct``, ``BackwardCheckpointed`` and ``Forward``."""
+        from .gradient import BackwardCheckpointed, Direct, Forward
+
+        supported = (Direct, BackwardCheckpointed, Forward)
+        if gradient is not None and not isinstance(gradient, supported):
+            support_str = ', '.join(f'`{x.__name__}`' for x in supported)
+            raise ValueError(f'Method `{type(self).__name__}` does not support gradient '
+                             f'`{type(gradient).__name__}` (supported gradient types: '
+                             f'{support_str}).')
 
 
 @dataclass(frozen=True)

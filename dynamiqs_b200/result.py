@@ -47,6 +47,10 @@ class MESolveResult:
     expects: Any
     infos: AdaptiveStepInfos
     extra: Any = None
+    # FP64 checks of the saved states (an addition of this library): 'trace' tr(rho) at
+    # every save point (..., ntsave) and 'hermiticity' ||rho - rho^+||_F / ||rho||_F of
+    # every saved state (..., nsave)
+    checks: Any = None
 
     @property
     def final_state(self):

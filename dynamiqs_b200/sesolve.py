@@ -73,7 +73,9 @@ class SESolveB200Integrator:
         self.gradient = gradient
         self.options = options
         self.H = H
-        self.Es = Es
+        # the identity's expectation value <psi|psi> (FP64 sums) is the norm check
+        self._n_user_E = len(Es) if Es else 0
+        self.Es = list(Es or []) + [np.eye(_shape(H)[-1], dtype=np.complex64)]
         self.plan = plan
 
     @property
@@ -137,9 +139,11 @@ class SESolveB200Integrator:
                                'integration.')
         bshape = self.plan.bshape
         states = b['states'].reshape(*bshape, *b['states'].shape[1:])
-        expects = None
-        if self._nE:
-            expects = b['expects'].reshape(*bshape, *b['expects'].shape[1:])
+        ex = b['expects'].reshape(*bshape, *b['expects'].shape[1:])
+        expects = ex[..., :self._n_user_E, :] if self._n_user_E else None
+        import torch
+
+        checks = {'norm': ex[..., self._n_user_E, :].to(torch.complex128).real}
         infos = b['infos'].reshape(*bshape, 3)
         info = AdaptiveStepInfos(infos[..., 0], infos[..., 1], infos[..., 2])
         extra = None
@@ -157,7 +161,7 @@ class SESolveB200Integrator:
                 extra = vals
         return SESolveResult(tsave=self.ts, method=self.method, gradient=self.gradient,
                              options=self.options, states=states, expects=expects, infos=info,
-                             extra=extra)
+                             extra=extra, checks=checks)
 
 
 def sesolve(H, psi0, tsave, *, exp_ops=None, method: Method = Tsit5(),  # noqa: B008

@@ -1,24 +1,20 @@
-"""Piecewise-constant time-dependent operators for ``mesolve``.
+"""Time-dependent operators for ``mesolve``.
 
-Mirrors the reference's ``dq.pwc`` / ``PWCTimeQArray`` (``dynamiqs/time_qarray.py:53-120,
-572-640``): ``pwc(times, values, qarray)`` is the operator
-``O(t) = c_k O_0`` for ``t`` in ``[t_k, t_{k+1})`` and ``0`` outside ``[t_0, t_N)``, and a
-constant operator plus PWC terms (``H0 + pwc(...) + ...``) is a summed time-dependent
-operator.  The reference integrates such a Hamiltonian with its discontinuity times passed
-to the step-size controller as ``jump_ts`` (``dynamiqs/integrators/core/
-diffrax_integrator.py:64-72``), so that no step crosses a discontinuity.  Here the solve is
-split at the discontinuities instead: each piece is a constant-operator solve on the GPU
-(one batched kernel launch), started from the previous piece's final state.  Every step
-therefore also stays inside one constant piece; what differs from the reference is the
-first step of each piece, which comes from the starting-step heuristic rather than from the
-controller's last proposal, so step counts differ slightly while the accuracy (rtol, atol)
-is the same.
+Mirrors the reference's ``dq.pwc`` / ``PWCTimeQArray`` and ``dq.modulated`` /
+``ModulatedTimeQArray`` (``dynamiqs/time_qarray.py:53-170,572-754``):
+``pwc(times, values, qarray)`` is ``O(t) = c_k O_0`` for ``t`` in ``[t_k, t_{k+1})`` and
+``0`` outside ``[t_0, t_N)``; ``modulated(f, qarray)`` is ``O(t) = f(t) O_0``; a constant
+operator plus such terms (``H0 + pwc(...) + modulated(...)``) is a summed time-dependent
+operator whose discontinuity times (the PWC times and the ``discontinuity_ts`` of modulated
+terms) reach the step-size controller as ``jump_ts`` (``dynamiqs/integrators/core/
+diffrax_integrator.py:59-72``).
 
-Scope: ``H0``'s constant part and the jump operators are unbatched; ``rho0`` may be
-batched; PWC values may carry batch dimensions ``(..., N)`` (broadcast together across the
-terms), solved one value-batch item at a time with cartesian batching (H's batch dimensions
-first, as the reference orders them).  Modulated (callable)
-prefactors are not supported: a Python callable cannot be evaluated inside the kernels.
+On the GPU the prefactors are evaluated by the kernels at every stage time, so ``f`` must
+be one they can evaluate: a :class:`Wave` (amplitude, angular frequency, phase, optional
+Gaussian envelope and support) -- a Python callable cannot run inside a kernel.  Problems
+with n <= 64 and at most four time-dependent terms run in one persistent launch with the
+reference's discontinuity handling; larger PWC problems are split at the discontinuities
+(one constant-operator solve per piece, each started with a fresh starting step).
 """
 
 from __future__ import annotations
@@ -27,7 +23,8 @@ import numpy as np
 
 from .qarrays import SparseDIA
 
-__all__ = ['PWCTimeQArray', 'SummedTimeQArray', 'pwc']
+__all__ = ['PWCTimeQArray', 'ModulatedTimeQArray', 'SummedTimeQArray', 'Wave', 'pwc',
+           'modulated']
 
 
 def _dense_op(x) -> np.ndarray:
@@ -94,8 +91,90 @@ class PWCTimeQArray:
     __radd__ = __add__
 
 
+class Wave:
+    """A prefactor the kernels evaluate: ``f(t) = amplitude * cos(omega t + phase) * env(t)``
+    for ``t_start <= t < t_end`` and ``0`` elsewhere, with ``env(t) = exp(-(t - t_center)^2
+    / (2 sigma^2))`` when ``sigma > 0`` and ``1`` otherwise.  ``amplitude`` may be complex;
+    ``omega = 0`` gives a constant, ``phase = -pi/2`` a sine."""
+
+    def __init__(self, omega: float = 0.0, phase: float = 0.0, amplitude: complex = 1.0, *,
+                 t_center: float = 0.0, sigma: float = 0.0, t_start: float = -np.inf,
+                 t_end: float = np.inf):
+        self.omega = float(omega)
+        self.phase = float(phase)
+        self.amplitude = complex(amplitude)
+        self.t_center = float(t_center)
+        self.sigma = float(sigma)
+        self.t_start = float(t_start)
+        self.t_end = float(t_end)
+        if self.sigma < 0:
+            raise ValueError('Argument `sigma` must be >= 0.')
+
+    def __call__(self, t: float) -> complex:
+        if not (self.t_start <= t < self.t_end):
+            return 0.0
+        f = np.cos(self.omega * t + self.phase)
+        if self.sigma > 0:
+            f *= np.exp(-0.5 * ((t - self.t_center) / self.sigma) ** 2)
+        return self.amplitude * f
+
+    @property
+    def discontinuity_ts(self) -> np.ndarray:
+        return np.asarray([t for t in (self.t_start, self.t_end) if np.isfinite(t)])
+
+
+class ModulatedTimeQArray:
+    """``O(t) = f(t) * qarray`` with ``f`` a :class:`Wave` (``ModulatedTimeQArray``,
+    ``dynamiqs/time_qarray.py:669-754``)."""
+
+    __array_ufunc__ = None
+
+    def __init__(self, f, qarray, discontinuity_ts=None):
+        if not isinstance(f, Wave):
+            raise NotImplementedError(
+                'dynamiqs_b200.modulated needs a prefactor the GPU kernels can evaluate: a '
+                '`Wave` (amplitude, omega, phase, optional Gaussian envelope and support); an '
+                'arbitrary Python callable cannot run inside a kernel.')
+        self.f = f
+        self.qarray = _dense_op(qarray)
+        if self.qarray.ndim != 2 or self.qarray.shape[0] != self.qarray.shape[1]:
+            raise ValueError('Argument `qarray` must be a square (n, n) operator.')
+        extra = np.asarray([] if discontinuity_ts is None else discontinuity_ts, dtype=np.float64)
+        self._disc = np.unique(np.concatenate([extra, f.discontinuity_ts]))
+
+    @property
+    def shape(self) -> tuple[int, ...]:
+        return self.qarray.shape
+
+    @property
+    def batch_shape(self) -> tuple[int, ...]:
+        return ()
+
+    def item(self, idx: tuple) -> ModulatedTimeQArray:
+        return self
+
+    @property
+    def discontinuity_ts(self) -> np.ndarray:
+        return self._disc
+
+    def prefactor(self, t: float) -> complex:
+        return complex(self.f(t))
+
+    def __call__(self, t: float) -> np.ndarray:
+        return (self.prefactor(t) * self.qarray).astype(np.complex64)
+
+    def __add__(self, other) -> SummedTimeQArray:
+        return SummedTimeQArray([self, other])
+
+    __radd__ = __add__
+
+
+_TD_TYPES = (PWCTimeQArray, ModulatedTimeQArray)
+
+
 class SummedTimeQArray:
-    """A sum of constant operators and :class:`PWCTimeQArray` terms."""
+    """A sum of constant operators and :class:`PWCTimeQArray` / :class:`ModulatedTimeQArray`
+    terms."""
 
     __array_ufunc__ = None
 
@@ -103,8 +182,8 @@ class SummedTimeQArray:
         flat = []
         for t in terms:
             flat.extend(t.terms if isinstance(t, SummedTimeQArray) else [t])
-        self.pwc_terms = [t for t in flat if isinstance(t, PWCTimeQArray)]
-        const = [_dense_op(t) for t in flat if not isinstance(t, PWCTimeQArray)]
+        self.pwc_terms = [t for t in flat if isinstance(t, _TD_TYPES)]
+        const = [_dense_op(t) for t in flat if not isinstance(t, _TD_TYPES)]
         n = (self.pwc_terms[0].shape if self.pwc_terms else const[0].shape)[-1]
         for c in const:
             if c.ndim != 2:
@@ -133,8 +212,16 @@ class SummedTimeQArray:
         return SummedTimeQArray([self.constant] + [t.item(idx) for t in self.pwc_terms])
 
     @property
+    def td_terms(self) -> list:
+        return self.pwc_terms
+
+    @property
+    def only_pwc(self) -> bool:
+        return all(isinstance(t, PWCTimeQArray) for t in self.pwc_terms)
+
+    @property
     def discontinuity_ts(self) -> np.ndarray:
-        ts = [t.times for t in self.pwc_terms]
+        ts = [t.discontinuity_ts for t in self.pwc_terms]
         return np.unique(np.concatenate(ts)) if ts else np.zeros(0)
 
     def __call__(self, t: float) -> np.ndarray:
@@ -153,6 +240,12 @@ def pwc(times, values, qarray) -> PWCTimeQArray:
     """Piecewise-constant operator ``O(t) = sum_k c_k 1_[t_k, t_{k+1})(t) O_0``
     (``dq.pwc``, ``dynamiqs/time_qarray.py:53-120``)."""
     return PWCTimeQArray(times, values, qarray)
+
+
+def modulated(f, qarray, *, discontinuity_ts=None) -> ModulatedTimeQArray:
+    """Modulated operator ``O(t) = f(t) O_0`` (``dq.modulated``,
+    ``dynamiqs/time_qarray.py:123-170``); ``f`` must be a :class:`Wave`."""
+    return ModulatedTimeQArray(f, qarray, discontinuity_ts)
 
 
 def as_summed(H) -> SummedTimeQArray:

@@ -178,6 +178,63 @@ DQB_API int dqb_lindblad_rhs_dense_prec(const dqb_dense_problem* problem, int32_
 DQB_API int dqb_mesolve_dense_noalloc(const dqb_dense_problem* problem, const dqb_ode_options* options,
                                       const dqb_outputs* outputs, void* stream);
 
+/* ---- gradients (n <= 64 kernel, constant operators) ----------------------------------- */
+/* Reverse-mode derivatives of a dqb_mesolve_dense solve with respect to H, the jump
+ * operators and rho0, through the discrete Runge-Kutta steps the solve took (the step sizes
+ * are constants, as in the reference's Direct / BackwardCheckpointed gradients,
+ * dynamiqs/gradient.py:10-110, diffrax_integrator.py:88-99).  A first taped solve records
+ * every accepted step (its start time, size and starting state); the adjoint pass then runs
+ * the steps backwards.  Complex gradients use the convention dLoss = Re tr(G^+ dA) (torch's
+ * and JAX's for a real loss).  The stage states are taken hermitian, as every stage of a
+ * hermitian rho0 is. */
+typedef struct dqb_tape {
+  double* t;      /* device float64 [batch, capacity]: start time of each accepted step  */
+  double* h;      /* device float64 [batch, capacity]: its size                          */
+  void* y;        /* device complex64, dqb_mesolve_dense_tape_bytes(n, capacity, batch):
+                     its starting state, padded to 16, 32 or 64                          */
+  int32_t capacity; /* accepted steps recorded per instance (steps beyond it are not)  */
+} dqb_tape;
+
+typedef struct dqb_cotangents {
+  const void* states;   /* complex64 [batch, nsave, n, n] dLoss/dstates, or NULL           */
+  const void* expects;  /* complex64 [batch, n_exp, n_tsave] dLoss/dexpects, or NULL      */
+} dqb_cotangents;
+
+typedef struct dqb_gradients {
+  void* rho0;  /* complex64 [batch, n, n], or [batch, n] when rho0_is_ket (dLoss/dpsi0)    */
+  void* H;     /* complex64 [batch, n, n]: each instance's gradient of its own H            */
+  void* L;     /* complex64 [batch, n_jumps, n, n]                                         */
+} dqb_gradients;
+
+DQB_API size_t dqb_mesolve_dense_tape_bytes(int32_t n, int32_t capacity, int64_t batch);
+
+/* dqb_mesolve_dense (FP32 CUDA cores), recording `tape`; results are bitwise those of
+ * dqb_mesolve_dense. */
+DQB_API int dqb_mesolve_dense_taped(const dqb_dense_problem* problem, const dqb_ode_options* options,
+                                    const dqb_outputs* outputs, const dqb_tape* tape, void* workspace,
+                                    size_t workspace_bytes, void* stream);
+
+DQB_API size_t dqb_mesolve_dense_adjoint_workspace_size(int32_t n, int32_t n_jumps, int64_t batch);
+
+/* The adjoint pass: `naccepted` is the device int32 [batch] of accepted steps the taped
+ * solve reported (infos[:, 1]); every one of them must be on the tape. */
+DQB_API int dqb_mesolve_dense_adjoint(const dqb_dense_problem* problem, const dqb_ode_options* options,
+                                      const dqb_tape* tape, const int32_t* naccepted,
+                                      const dqb_cotangents* cotangents, const dqb_gradients* gradients,
+                                      void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- bounded waits (diagnostics) ----------------------------------------------------- */
+/* Every mbarrier wait of the tensor-core kernels gives up after a time limit (2 s by
+ * default) instead of spinning for ever: the instance then ends with DQB_INST_NONFINITE,
+ * the kernel waits (2 s at most) for the MMAs it had issued, frees its tensor memory and
+ * returns.  dqb_set_tc_wait_limit_ns changes the limit for the n <= 64 tensor-core kernel
+ * (F16X3) of later launches in this process (0 restores 2 s; 1 makes every wait give up at
+ * once, so that a test drives the failure path deterministically); dqb_probe_bounded_wait runs one wait that nothing ever completes with
+ * `limit_ns` (<= 1 s) and writes result[0] = 1 if it gave up, result[1] = microseconds
+ * waited (device int32 [2]).  No counterpart in the reference. */
+DQB_API void dqb_set_tc_wait_limit_ns(uint64_t ns);
+DQB_API int dqb_probe_bounded_wait(uint64_t limit_ns, int32_t* result, void* stream);
+
 /* ---- time-dependent Hamiltonians (n <= 64 kernel) ------------------------------------ */
 /* H(t) = H + sum_m c_m(t) ops[m] (the reference's ConstantTimeQArray + PWCTimeQArray /
  * ModulatedTimeQArray sums, dynamiqs/time_qarray.py:497-754), with prefactors the device

@@ -41,17 +41,34 @@ def _as_dense(op, n):
 def mesolve(H, Ls, rho0, tsave, exp_ops=None, *, method='Tsit5', rtol=1e-6, atol=1e-6,
             safety=0.9, factormin=0.2, factormax=5.0, max_steps=100_000, t0=None,
             save_states=True, form='hermitian', dtype=np.complex128,
-            time_dtype=np.float64) -> OracleResult:
+            time_dtype=np.float64, jump_ts=None) -> OracleResult:
     """Solve one Lindblad problem.  ``H`` and each ``L`` are dense arrays or DIA
-    ``(offsets, diags)`` tuples; ``rho0`` is a ket ``(n, 1)`` or a density matrix."""
+    ``(offsets, diags)`` tuples; ``rho0`` is a ket ``(n, 1)`` or a density matrix.  A
+    callable ``H`` is a time-dependent Hamiltonian ``t -> (n, n)`` (``TimeQArray.__call__``,
+    dynamiqs/time_qarray.py:430-451), solved in the hermitian form with ``jump_ts`` handed
+    to the step-size controller (``diffrax_integrator.py:59-72``)."""
     rho0 = np.asarray(rho0, dtype=dtype)
     n = rho0.shape[-2]
     if rho0.shape[-1] == 1:  # todm (dynamiqs/utils/general.py:821)
         rho0 = rho0 @ lb.dag(rho0)
     dia = isinstance(H, tuple) or any(isinstance(L, tuple) for L in Ls)
-    Hd = _as_dense(H, n).astype(dtype)
+    time_dependent = callable(H) and not isinstance(H, (np.ndarray, tuple))
+    Hd = None if time_dependent else _as_dense(H, n).astype(dtype)
     Lsd = [_as_dense(L, n).astype(dtype) for L in Ls]
-    if form == 'hermitian':
+    if time_dependent:
+        if form != 'hermitian':
+            raise ValueError('time-dependent H: hermitian form only')
+        LsH = [lb.dag(L) for L in Lsd]
+
+        def f(t, y):
+            Hnh = lb.hnh_dense(np.asarray(H(t), dtype=dtype), Lsd)
+            tmp = Hnh @ y
+            for L, Lh in zip(Lsd, LsH):
+                tmp = tmp + 0.5 * (L @ y @ Lh)
+            return tmp + lb.dag(tmp)
+        y0 = rho0
+        unvec = lambda y: y  # noqa: E731
+    elif form == 'hermitian':
         if dia:
             Hdia = H if isinstance(H, tuple) else lb.dense_to_dia(Hd)
             Ldia = [L if isinstance(L, tuple) else lb.dense_to_dia(Ld)
@@ -96,7 +113,7 @@ def mesolve(H, Ls, rho0, tsave, exp_ops=None, *, method='Tsit5', rtol=1e-6, atol
 
     out = solve(f, y0, tsave, method=method, rtol=rtol, atol=atol, safety=safety,
                 factormin=factormin, factormax=factormax, max_steps=max_steps, t0=t0,
-                time_dtype=time_dtype, save_fn=save_fn)
+                time_dtype=time_dtype, save_fn=save_fn, jump_ts=jump_ts)
     final = unvec(out.ylast)
     if out.ysave:
         states = np.stack([s[0] for s in out.ysave])

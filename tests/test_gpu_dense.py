@@ -207,3 +207,20 @@ def test_start_order_changes_no_result(cuda_device):
     b = prep.launch().result()
     assert np.array_equal(sa, b.states.cpu().numpy())
     assert np.array_equal(ia, b.infos.nsteps.cpu().numpy())
+
+
+def test_fp64_checks_of_saved_states(cuda_device):
+    """result.checks: tr(rho) at every save point (FP64 sums in the kernel) and the FP64
+    hermiticity defect of every saved state, on the three solve paths."""
+    w = workloads.batched_kerr(batch=3, n=20, seed=1)
+    res = dq.mesolve(w['H'], w['jump_ops'], w['rho0'], w['tsave'], exp_ops=w['exp_ops'],
+                     method=w['method'])
+    tr = res.checks['trace'].cpu().numpy()
+    assert tr.shape == (3, 51) and np.abs(tr - 1).max() < 1e-5
+    assert res.checks['hermiticity'].shape == (3, 51)
+    assert float(res.checks['hermiticity'].max()) < 1e-6
+    assert res.expects.shape == (3, 1, 51)  # the trace row is not among the user's expects
+    std = dq.mesolve(w['H'], w['jump_ops'], w['rho0'], w['tsave'],
+                     options=dq.Options(assume_hermitian=False))
+    assert std.expects is None and np.abs(std.checks['trace'].cpu().numpy() - 1).max() < 1e-5
+    assert float(std.checks['hermiticity'].max()) < 1e-5

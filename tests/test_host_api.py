@@ -46,7 +46,7 @@ def test_options_and_method_checks():
 
     with pytest.raises(TypeError, match='Method of type `Euler` is not supported'):
         dq.mesolve(H, Ls, r, ts, method=Euler())
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(ValueError, match='does not support gradient `object`'):
         dq.mesolve(H, Ls, r, ts, gradient=object())
 
 

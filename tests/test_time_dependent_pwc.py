@@ -118,10 +118,11 @@ def test_pwc_mesolve_on_gpu_matches_exact(cuda_device):
     assert err.max() < 1e-5
     n_ref = np.real(np.einsum('ij,tji->t', np.asarray(E[0]), ref))
     assert np.abs(res.expects.cpu().numpy()[0] - n_ref).max() < 1e-5
-    # same piecewise algorithm on the CPU oracle: the same steps within one per piece
-    o = _mesolve_piecewise(H, L, rho0, TSAVE, exp_ops=E, method=m, gradient=None,
-                           options=dq.Options(), solve=_oracle_solve)
-    assert abs(int(res.infos.nsteps) - int(o.infos.nsteps)) <= 5
+    # the controller clips its steps at the discontinuities as the reference's jump_ts
+    # does: the oracle with the same handling takes the same steps
+    o = oracle_mesolve(as_summed(H), L, rho0, TSAVE, rtol=m.rtol, atol=m.atol,
+                       jump_ts=as_summed(H).discontinuity_ts)
+    assert (int(res.infos.nsteps), int(res.infos.nrejected)) == (o.nsteps, o.nrejected)
 
 
 VALUES2 = [[1.0, -0.5, 2.0], [0.2, 0.7, -1.0]]
@@ -179,3 +180,32 @@ def test_piece_plan_edge_cases():
     assert np.allclose(plan[2][2], 2 * np.eye(2))
     only = dq.pwc([1.0, 2.0], [4.0], np.eye(2))
     assert np.allclose(as_summed(only)(0.5), 0) and np.allclose(as_summed(only)(1.5), 4 * np.eye(2))
+
+
+def test_oracle_jump_ts_matches_exact():
+    """The oracle's discontinuity handling (steps clipped just before each PWC time, the
+    next one restarted on it with a fresh first stage) against the exact solution; with
+    ``jump_ts`` no step straddles a jump, so the error is that of the tolerances."""
+    H, H0, drive, L, rho0, E = _system()
+    Hs = as_summed(H)
+    r = oracle_mesolve(Hs, L, rho0, TSAVE, exp_ops=E, rtol=1e-9, atol=1e-11,
+                       jump_ts=Hs.discontinuity_ts)
+    ref = _exact(H0, drive, L, rho0, TSAVE)
+    err = np.linalg.norm(r.states - ref, axis=(-2, -1)) / np.linalg.norm(ref, axis=(-2, -1))
+    assert err.max() < 1e-7
+    starts = [t for (t, _h, _e) in r.errors]
+    for J in TIMES:
+        assert any(t == J for t in starts)  # a step starts exactly on each discontinuity
+
+
+def test_wave_prefactor_semantics():
+    w = dq.Wave(2.0, 0.3, 1.5 - 0.5j, t_center=1.0, sigma=0.4, t_start=0.2, t_end=2.0)
+    t = 1.3
+    ref = (1.5 - 0.5j) * np.cos(2.0 * t + 0.3) * np.exp(-0.5 * ((t - 1.0) / 0.4) ** 2)
+    assert abs(w(t) - ref) < 1e-15
+    assert w(0.1) == 0.0 and w(2.0) == 0.0 and w(0.2) != 0.0
+    M = dq.modulated(w, np.eye(2), discontinuity_ts=[0.7])
+    assert list(M.discontinuity_ts) == [0.2, 0.7, 2.0]
+    with pytest.raises(NotImplementedError, match='Wave'):
+        dq.modulated(lambda t: np.cos(t), np.eye(2))
+

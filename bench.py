@@ -338,13 +338,17 @@ def _workload(name, args, rank):
     return w
 
 
-def _kernels_per_launch(path: str, K: int, iterations: int) -> int:
+def _kernels_per_launch(path: str, K: int, iterations: int, stepper: str = 'auto') -> int:
     """Kernels of this library executed by one solve call."""
     if path == 'dqb_mesolve_dense':
         return 1  # the persistent kernel (plus a 256-byte memset of its work counter)
     if path == 'dqb_mesolve_dia':
-        body = 6 * 2 + 4          # 6 x (combine + stencil) + error, control, save, commit
-        init = 10                 # set-up, Hnh, rho0, 2 RHS, norms, controls, probe
+        if stepper == 'stages':
+            body = 6 * 2 + 4      # 6 x (combine + stencil) + error, control, save, commit
+            init = 10             # set-up, Hnh, rho0, 2 RHS, norms, controls, probe
+        else:
+            body = 6 + 4          # 6 basis stencils + combination, control, save, commit
+            init = 9              # set-up, Hnh, rho0, 2 RHS, 2 norms, 2 controls
         return init + body * iterations + 3
     rhs = (2 if K else 1) + 1 + ((K + 1) // 4 if K > 3 else 0)  # L X, sums, symmetrize
     body = 6 * (1 + rhs) + 4
@@ -352,23 +356,45 @@ def _kernels_per_launch(path: str, K: int, iterations: int) -> int:
     return init + body * iterations + 3
 
 
-def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which, nsave=0):
+def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which, nsave=0, nacc=None,
+              stepper='auto'):
     """Roofline record of the dominant kernel of a solve launch: `nsteps` (tensor) is the
-    attempted RK steps of every instance, `mean_ms` the launch's mean duration."""
+    attempted RK steps of every instance, `nacc` the accepted ones, `mean_ms` the launch's
+    mean duration."""
     import torch
 
     if config == 'dia':
-        # algorithmic HBM bytes per attempted step and instance (a fully fused Tsit5 step
-        # touches 34 n x n complex64 matrices: stages 2-6 read y and k_1..k_{i-1} and write
-        # k_i, 25 passes; y1, k7 and the error estimate 9 more)
-        nbytes = float((34 * 8.0 * n * n * nsteps).sum())
+        mat = 8.0 * n * n
+        # the stage-by-stage step touches at least 34 n x n complex64 matrices per attempt
+        # (stages 2-6 read y and k_1..k_{i-1} and write k_i: 25 passes; y1, k7 and the error
+        # 9 more) -- the figure of a fully fused stage-form step
+        stage_bytes = float((34 * mat * nsteps).sum())
+        if stepper == 'stages':
+            nbytes = stage_bytes
+            note = ('bytes = 34 n^2 complex64 matrix passes per attempted RK step per '
+                    'instance (the fused stage-form minimum); the kernels make 54')
+        else:
+            # the Krylov form: per accepted step six right-hand sides build the basis (read
+            # one matrix, write one: 12 passes); per attempt one pass reads u_0..u_7 and
+            # writes y1 and the next first stage (10 passes); per save point the dense
+            # output reads the basis and writes the state (9 passes)
+            nbytes = float((mat * (12 * nacc + 10 * nsteps)).sum()) + 9 * mat * nsave * B
+            note = ('bytes = the Krylov-form step: 12 n^2 complex64 passes per accepted step '
+                    '(basis), 10 per attempt (combination), 9 per save point; the same step '
+                    'in the stage form needs at least 34 per attempt')
         achieved = nbytes / (mean_ms / 1e3) / 1e9
-        return {'bound': 'hbm', 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
+        roof = {'bound': 'hbm', 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
                 'frac': achieved / peaks['hbm_gbs'], 'peak_source': f'hbm_gbs ({which})',
-                'traffic': _traffic(config, precision, B, nsteps, nsave),
-                'algorithmic_bytes_per_launch': nbytes,
-                'note': 'bytes = 34 n^2 complex64 matrix passes per attempted RK step per '
-                        'instance (the fused-step minimum); the kernels today make 54'}
+                'traffic': _traffic(config, precision, B, nsteps, nsave, stepper),
+                'algorithmic_bytes_per_launch': nbytes, 'note': note}
+        if stepper != 'stages':
+            eff = stage_bytes / (mean_ms / 1e3) / 1e9
+            roof['stage_form_equivalent'] = {
+                'achieved': eff, 'frac': eff / peaks['hbm_gbs'],
+                'note': 'the 34-pass stage-form bytes of the same attempted steps over the '
+                        'measured time: the HBM bandwidth a stage-form step would need to '
+                        'match this speed'}
+        return roof
     rhs_evals = float((6 * nsteps + 2).sum())
     flops = rhs_evals * _flops_per_rhs(n, K)
     achieved = flops / (mean_ms / 1e3) / 1e12
@@ -407,13 +433,13 @@ def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which, nsave=0
 #     loop: 7.19 GB = 54 passes over the 134 MB matrix) plus 1.22 GB per save point;
 #     profiles/dia_stepper_n4096_coupled_kerr_traffic.md.
 TRAFFIC_PER_UNIT = {
-    ('kerr', 'fp32'): ('instance', 2.837e6, 0.0),
-    ('dia', 'fp32'): ('instance_step', 7.19e9, 1.22e9),
+    ('kerr', 'fp32', 'auto'): ('instance', 2.837e6, 0.0),
+    ('dia', 'fp32', 'stages'): ('instance_step', 7.19e9, 1.22e9),
 }
 
 
-def _traffic(config, precision, B, nsteps, nsave=0):
-    key = (config, precision)
+def _traffic(config, precision, B, nsteps, nsave=0, stepper='auto'):
+    key = (config, precision, stepper if config == 'dia' else 'auto')
     if key not in TRAFFIC_PER_UNIT:
         return None
     unit, per, per_save = TRAFFIC_PER_UNIT[key]
@@ -448,7 +474,7 @@ def run_b200(args):
 
     w = _workload(args.config, args, rank)
     Es = w.get('exp_ops')
-    opts = dq.Options(precision=args.precision)
+    opts = dq.Options(precision=args.precision, stepper=args.stepper)
     plan = make_batch_plan(w['H'], w['jump_ops'], w['rho0'], True)
     integ = MESolveB200Integrator(ts=w['tsave'], y0=w['rho0'], method=w['method'], gradient=None,
                                   options=opts, H=w['H'], Ls=w['jump_ops'], Es=Es, plan=plan)
@@ -485,6 +511,7 @@ def run_b200(args):
     kernel_ms = [a.elapsed_time(b) for a, b in ev]
     infos = prep.bufs['infos']
     nsteps = infos[:, 0].to(torch.float64)
+    nacc = infos[:, 1].to(torch.float64)
     kern = float(np.sum(kernel_ms))
     if dist is not None:
         tt = torch.tensor([kern], device=dev, dtype=torch.float64)
@@ -494,7 +521,7 @@ def run_b200(args):
     mean_ms = kern / args.steps
     peaks, which = _peaks()
     roof = _roofline(args.config, args.precision, n, K, nsteps, mean_ms, B, peaks, which,
-                     len(w['tsave']))
+                     len(w['tsave']), nacc, args.stepper)
 
     # ---- e2e: public API from host inputs --------------------------------------------
     e2e = None
@@ -579,11 +606,13 @@ def run_b200(args):
                    'n_tsave': len(w['tsave']), 'method': type(w['method']).__name__,
                    'rtol': w['method'].rtol, 'atol': w['method'].atol, 'path': prep.name,
                    'precision': args.precision,
+                   **({'stepper': args.stepper} if args.config == 'dia' else {}),
                    'l2': 'flushed between iterations (256 MiB write)',
                    'parallelism': f'instances sharded over {world} GPU(s), no collective',
                    'avg_rk_steps': float(nsteps.mean()), 'max_rk_steps': float(nsteps.max())},
         'e2e': e2e,
-        'gpu_launches': args.steps * _kernels_per_launch(prep.name, K, int(nsteps.max())),
+        'gpu_launches': args.steps * _kernels_per_launch(prep.name, K, int(nsteps.max()),
+                                                         args.stepper),
         'roofline': roof,
         **extra,
         'clocks': clocks,
@@ -630,6 +659,7 @@ def _extra_configs(args, dev, stream, flush, peaks, which):
             torch.cuda.synchronize()
             ms.append(e0.elapsed_time(e1))
         nsteps = prep.bufs['infos'][:, 0].to(torch.float64)
+        nacc = prep.bufs['infos'][:, 1].to(torch.float64)
         B = plan.batch
         n = int(w['H'].shape[-1])
         mean_ms = float(np.mean(ms))
@@ -638,7 +668,9 @@ def _extra_configs(args, dev, stream, flush, peaks, which):
                     'steps': 2, 'warmup': 3, 'batch': B, 'avg_rk_steps': float(nsteps.mean()),
                     'max_rk_steps': float(nsteps.max()),
                     'roofline': _roofline(cfg, prec, n, len(w['jump_ops']), nsteps, mean_ms, B,
-                                          peaks, which, len(w['tsave']))}
+                                          peaks, which, len(w['tsave']), nacc)}
+        if cfg == 'dia':
+            out[key]['stepper'] = 'auto (krylov)'
         del prep
         torch.cuda.empty_cache()
     return out
@@ -665,6 +697,8 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-extra', action='store_true',
                     help='skip the GEMM-path and DIA lines the kerr run adds (extra_configs)')
+    ap.add_argument('--stepper', default='auto', choices=['auto', 'stages', 'krylov'],
+                    help='dia: form of the RK step (auto = krylov)')
     ap.add_argument('--precision', default='fp32',
                     choices=['fp32', 'tf32x3', 'bf16x3', 'tf32', 'f16x3', 'auto'],
                     help='arithmetic of the complex products (tf32x3 / bf16x3 / tf32: GEMM '

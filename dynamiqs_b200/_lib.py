@@ -44,6 +44,10 @@ PREC_TF32X3 = 1
 PREC_BF16X3 = 2
 PREC_TF32 = 3
 PREC_F16X3 = 4
+STEPPER_AUTO = 0
+STEPPER_STAGES = 1
+STEPPER_KRYLOV = 2
+STEPPERS = {'auto': STEPPER_AUTO, 'stages': STEPPER_STAGES, 'krylov': STEPPER_KRYLOV}
 PRECISIONS = {'fp32': PREC_FP32, 'tf32x3': PREC_TF32X3, 'bf16x3': PREC_BF16X3, 'tf32': PREC_TF32,
               'f16x3': PREC_F16X3}
 
@@ -63,6 +67,7 @@ class OdeOptions(ctypes.Structure):
         ('check_hermitian', ctypes.c_int32),
         ('precision', ctypes.c_int32),
         ('tile', ctypes.c_int32),
+        ('stepper', ctypes.c_int32),
     ]
 
 

@@ -34,6 +34,11 @@ struct Inst {
   int status, run, keep, save_idx, save_lo, save_hi, herm_bad, retired;
   long long nsteps, nacc, nrej;
   int sy, sy1, sk[7];
+  // Krylov form (kry_* kernels): sk[q - 1] holds u_q = (tau L)^q y for q = 1..7, except
+  // that the true u_1 is sig1 times the stored one; kvalid = how many of u_0..u_7 are
+  // current; sf = the slot that receives tau L y1 (the next step's u_1)
+  double tau, sig1;
+  int kvalid, sf;
   // the instance's own problem data and outputs (shared arrays or a ragged descriptor)
   int nts, nE, save_states, is_ket;
   const double* ts;
@@ -142,6 +147,9 @@ static __global__ void setup_kernel(Common c) {
   I.sy = 0;
   I.sy1 = 1;
   for (int j = 0; j < 7; ++j) I.sk[j] = 2 + j;
+  I.tau = I.sig1 = 1.0;
+  I.kvalid = 0;
+  I.sf = kX;
 }
 
 // grid (tiles, B): rho0 (or psi psi^+) into y, hermiticity check, expects sums zeroed.
@@ -296,7 +304,9 @@ static __global__ void error_kernel(Common c) {
 }
 
 // Starting-step norms.  phase 0: acc[0] += |y/sc|^2, acc[1] += |k1/sc|^2;
-// phase 1: acc[2] += |(k2 - k1)/sc|^2 (k2 = f(y + h0 k1)).
+// phase 1: acc[2] += |(k2 - k1)/sc|^2 (k2 = f(y + h0 k1));
+// phase 2 (Krylov form, k2 holding L k1): acc[2] += |h0 L k1 / sc|^2, the same quantity
+// for a linear right-hand side.
 static __global__ void init_norm_kernel(Common c, int phase) {
   __shared__ double red[40];
   const int b = blockIdx.y;
@@ -314,9 +324,13 @@ static __global__ void init_norm_kernel(Common c, int phase) {
     if (phase == 0) {
       s0 += (double)cabs2f(yv) / (sc * sc);
       s1 += (double)cabs2f(f0) / (sc * sc);
-    } else {
+    } else if (phase == 1) {
       const float2 f1 = k2[e];
       const double dx = (double)f1.x - f0.x, dy = (double)f1.y - f0.y;
+      s0 += (dx * dx + dy * dy) / (sc * sc);
+    } else {
+      const float2 f1 = k2[e];
+      const double dx = I.h0 * f1.x, dy = I.h0 * f1.y;
       s0 += (dx * dx + dy * dy) / (sc * sc);
     }
   }
@@ -359,6 +373,11 @@ static __global__ void init_ctrl_kernel(Common c, int phase) {
     I.h = I.tnext - I.t;
     I.run = I.t < I.t1;
     I.acc[0] = I.acc[1] = I.acc[2] = 0.0;
+    // Krylov form: the basis of the first step is scaled by its trial step, and the stored
+    // u_1 is L y (sk[0], from the starting-step probe)
+    I.tau = I.h;
+    I.sig1 = I.h;
+    I.kvalid = 2;
   }
 }
 
@@ -484,6 +503,262 @@ static __global__ void commit_kernel(Common c, cudaGraphConditionalHandle handle
       }
       I.tnext = next_tend(I.t, I.dtnew, I.t1, I.keep);
       I.h = I.tnext - I.t;
+      I.run = I.t < I.t1;
+    }
+    I.save_lo = I.save_hi = I.save_idx;
+    any |= I.run;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    const long long it = ++(*c.iter);
+    const bool more = any && it < c.o.max_steps + 2;
+    if (flag)
+      *flag = more ? 1 : 0;
+    else
+      cudaGraphSetConditional(handle, more ? 1u : 0u);
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Krylov form of the step, for a linear right-hand side with constant operators
+// ------------------------------------------------------------------------------------
+//
+// For dy/dt = L y with L linear and constant, every quantity of an explicit RK step is a
+// polynomial in hL applied to y.  With the basis u_q = (tau L)^q y (q = 0..7; tau = the
+// step the basis was built for, r = h / tau):
+//   h k_j   = sum_{q=1}^{j} alpha_{j,q-1} r^q u_q,
+//             alpha_{j,0} = 1,  alpha_{j,m} = sum_{l<j} a_{jl} alpha_{l,m-1}
+//   y1      = sum_q beta_q r^q u_q,          beta_0 = 1,  beta_q = sum_j b_j alpha_{j,q-1}
+//   error   = sum_q eps_q r^q u_q,           eps_q = sum_j btilde_j alpha_{j,q-1}
+//   y(theta)= sum_q delta_q(theta) r^q u_q,  delta_q = sum_j w_j(theta) alpha_{j,q-1}
+//   tau L y1 = sum_{q<7} beta_q r^q u_{q+1}  (the next step's first stage, FSAL)
+// -- the same numbers as the stage-by-stage form in exact arithmetic (a_7j = b_j for both
+// tableaux, so stage 7 is L y1).  The basis costs six pure right-hand sides u_{q+1} =
+// tau L u_q per accepted step, and y1, the error and the next first stage are one
+// streaming pass over u_0..u_7: 22 passes over the state per attempted step instead of 54.
+// A rejected step keeps its basis (only r changes), so a retry is that one pass alone.
+// The error needs no cancellation either: eps_q = 0 for q up to the embedded order, so
+// the estimate is a sum of the O(h^5) terms themselves.
+
+// alpha_{j,m} of the method (j = stage 0..6, m = power 0..6).
+__device__ inline void kry_alpha(int method, double al[7][7]) {
+  const Tableau& T = c_tab[method];
+  for (int j = 0; j < 7; ++j) {
+    al[j][0] = 1.0;
+    for (int m = 1; m < 7; ++m) {
+      double v = 0.0;
+      for (int l = 0; l < j; ++l) v += T.a[j][l] * al[l][m - 1];
+      al[j][m] = v;
+    }
+  }
+}
+
+// Coefficients of u_0..u_7 in y1 (cy), the error (ce) and tau L y1 (cs) for r = h / tau;
+// the stored u_1 is scaled by sig1.
+__device__ inline void kry_step_coefs(int method, double r, double sig1, float cy[8], float ce[8], float cs[8]) {
+  const Tableau& T = c_tab[method];
+  double al[7][7];
+  kry_alpha(method, al);
+  double beta[8], eps[8], rp[8];
+  rp[0] = 1.0;
+  for (int q = 1; q < 8; ++q) rp[q] = rp[q - 1] * r;
+  beta[0] = 1.0;
+  eps[0] = 0.0;
+  for (int q = 1; q < 8; ++q) {
+    double bq = 0.0, eq = 0.0;
+    for (int j = 0; j < 7; ++j) {
+      bq += T.b[j] * al[j][q - 1];
+      eq += T.btilde[j] * al[j][q - 1];
+    }
+    beta[q] = bq;
+    eps[q] = eq;
+  }
+  for (int q = 0; q < 8; ++q) {
+    const double s = q == 1 ? sig1 : 1.0;
+    cy[q] = (float)(beta[q] * rp[q] * s);
+    ce[q] = (float)(eps[q] * rp[q] * s);
+    cs[q] = q == 0 ? 0.f : (float)(beta[q - 1] * rp[q - 1] * s);
+  }
+}
+
+// Coefficients of u_0..u_7 in the dense output at theta (same scaling rules).
+__device__ inline void kry_dense_coefs(int method, double theta, double r, double sig1, float cw[8]) {
+  double al[7][7], w[7];
+  kry_alpha(method, al);
+  dense_weights(method, theta, w);
+  double rp = 1.0;
+  cw[0] = 1.f;
+  for (int q = 1; q < 8; ++q) {
+    rp *= r;
+    double d = 0.0;
+    for (int j = 0; j < 7; ++j) d += w[j] * al[j][q - 1];
+    cw[q] = (float)(d * rp * (q == 1 ? sig1 : 1.0));
+  }
+}
+
+__device__ __forceinline__ double kry_ratio(const Inst& I) { return I.tau > 0.0 ? I.h / I.tau : 0.0; }
+
+// grid (tiles, B): y1, tau L y1 and the error sum of the trial step from u_0..u_7, for
+// every running instance (a retried step included).
+static __global__ void kry_combine_kernel(Common c) {
+  __shared__ double red[40];
+  __shared__ float cf[3][8];
+  const int b = blockIdx.y;
+  Inst& I = c.inst[b];
+  if (!I.run) return;
+  if (threadIdx.x == 0) kry_step_coefs(c.o.method, kry_ratio(I), I.sig1, cf[0], cf[1], cf[2]);
+  __syncthreads();
+  float cy[8], ce[8], cs[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) cy[q] = cf[0][q], ce[q] = cf[1][q], cs[q] = cf[2][q];
+  const float2* u[8];
+  u[0] = slot(c, b, I.sy);
+#pragma unroll
+  for (int q = 1; q < 8; ++q) u[q] = slot(c, b, I.sk[q - 1]);
+  float2* y1 = slot(c, b, I.sy1);
+  float2* s1 = slot(c, b, I.sf);
+  const double atol = c.o.atol, rtol = c.o.rtol;
+  double s = 0.0;
+  auto one = [&](const float2 (&v)[8], float2& oy, float2& os) {
+    float2 a = make_float2(0.f, 0.f), e = make_float2(0.f, 0.f), f = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      a = caxpy(cy[q], v[q], a);
+      e = caxpy(ce[q], v[q], e);
+      f = caxpy(cs[q], v[q], f);
+    }
+    oy = a;
+    os = f;
+    const float ya = cabsf(v[0]), y1a = cabsf(a);
+    const double sc = atol + rtol * (double)(ya > y1a ? ya : y1a);
+    const double ex = e.x, ey = e.y;
+    s += (ex * ex + ey * ey) / (sc * sc);
+  };
+  if ((c.nn & 1) == 0 && (reinterpret_cast<uintptr_t>(c.mats) & 15) == 0) {
+    // two complex values per 16-byte access, as in combine_kernel
+    const long long nn2 = c.nn >> 1;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn2;
+         e += (long long)gridDim.x * blockDim.x) {
+      float4 v4[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v4[q] = reinterpret_cast<const float4*>(u[q])[e];
+      float2 lo[8], hi[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) lo[q] = make_float2(v4[q].x, v4[q].y), hi[q] = make_float2(v4[q].z, v4[q].w);
+      float2 ya, sa, yb, sb;
+      one(lo, ya, sa);
+      one(hi, yb, sb);
+      reinterpret_cast<float4*>(y1)[e] = make_float4(ya.x, ya.y, yb.x, yb.y);
+      reinterpret_cast<float4*>(s1)[e] = make_float4(sa.x, sa.y, sb.x, sb.y);
+    }
+  } else {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
+         e += (long long)gridDim.x * blockDim.x) {
+      float2 v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = u[q][e];
+      one(v, y1[e], s1[e]);
+    }
+  }
+  block_atomic_add(s, &I.acc[0], red);
+}
+
+// grid (tiles, B): states and tr(E rho) at the saves crossed by an accepted step, from the
+// basis (the Krylov counterpart of save_kernel with interp = 1).
+static __global__ void kry_save_kernel(Common c) {
+  __shared__ double red[40];
+  __shared__ float cws[8];
+  const int b = blockIdx.y;
+  const Inst& I = c.inst[b];
+  const int lo = I.save_lo, hi = I.save_hi;
+  if (hi <= lo) return;
+  const float2* u[8];
+  u[0] = slot(c, b, I.sy);
+  for (int q = 1; q < 8; ++q) u[q] = slot(c, b, I.sk[q - 1]);
+  const int n = c.n;
+  const bool herm = c.form == DQB_FORM_HERMITIAN;
+  const double r = kry_ratio(I);
+  for (int s = lo; s < hi; ++s) {
+    __syncthreads();  // cws of the previous save point is no longer read
+    if (threadIdx.x == 0) {
+      const double theta = I.h > 0.0 ? (I.ts[s] - I.t) / I.h : 1.0;
+      kry_dense_coefs(c.o.method, theta, r, I.sig1, cws);
+    }
+    __syncthreads();
+    float cw[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) cw[q] = cws[q];
+    float2* dst = I.states + (long long)s * c.nn;
+    for (int m0 = 0; m0 == 0 || m0 < I.nE; m0 += 4) {
+      const int mc = I.nE - m0 < 4 ? I.nE - m0 : 4;
+      double er[4] = {0, 0, 0, 0}, ei[4] = {0, 0, 0, 0};
+      for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
+           e += (long long)gridDim.x * blockDim.x) {
+        float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v = caxpy(cw[q], u[q][e], v);
+        if (m0 == 0 && I.save_states) dst[e] = v;
+        if (mc > 0) {
+          float2 rt;
+          if (herm) {
+            rt = cconj(v);
+          } else {
+            const int i = (int)(e / n), j = (int)(e % n);
+            const long long et = (long long)j * n + i;
+            rt = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) rt = caxpy(cw[q], u[q][et], rt);
+          }
+#pragma unroll
+          for (int m = 0; m < 4; ++m) {
+            if (m < mc) {
+              const float2 ev = I.E[(long long)(m0 + m) * c.nn + e];
+              er[m] += (double)ev.x * rt.x - (double)ev.y * rt.y;
+              ei[m] += (double)ev.x * rt.y + (double)ev.y * rt.x;
+            }
+          }
+        }
+      }
+      for (int m = 0; m < mc; ++m) {
+        double2* acc = I.eacc + (long long)(m0 + m) * I.nts + s;
+        const double sr = block_sum(er[m], red);
+        const double si = block_sum(ei[m], red);
+        if (threadIdx.x == 0) {
+          atomicAdd(&acc->x, sr);
+          atomicAdd(&acc->y, si);
+        }
+      }
+    }
+  }
+}
+
+// One block: per-instance commit of the Krylov form, then the WHILE-node condition (as
+// commit_kernel).  An accepted step makes y1 the new u_0 and tau L y1 the new (scaled)
+// u_1, and rebuilds the basis for the next trial step; a rejected one keeps the basis.
+static __global__ void kry_commit_kernel(Common c, cudaGraphConditionalHandle handle, int* flag) {
+  int any = 0;
+  for (int b = threadIdx.x; b < c.B; b += blockDim.x) {
+    Inst& I = c.inst[b];
+    if (I.run) {
+      if (I.keep) {
+        int tmp = I.sy;
+        I.sy = I.sy1;
+        I.sy1 = tmp;
+        tmp = I.sk[0];
+        I.sk[0] = I.sf;
+        I.sf = tmp;
+        I.t = I.tnext;
+        I.save_idx = I.save_hi;
+      }
+      I.tnext = next_tend(I.t, I.dtnew, I.t1, I.keep);
+      I.h = I.tnext - I.t;
+      if (I.keep) {
+        I.sig1 = I.tau > 0.0 ? I.h / I.tau : 1.0;
+        I.tau = I.h;
+        I.kvalid = 2;
+      } else {
+        I.kvalid = 8;
+      }
       I.run = I.t < I.t1;
     }
     I.save_lo = I.save_hi = I.save_idx;

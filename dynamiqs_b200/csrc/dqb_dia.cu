@@ -93,24 +93,55 @@ __global__ void hnh_dia_kernel(DiaOps d, int B) {
 constexpr int kRhsCols = 128;
 constexpr int kRhsRows = 8;
 
+// Input, output and output scale of one instance's right-hand side inside a solve.
+// kry = 0: k[out_k] = f(input) with input 0 = y, 1 = y1, 2 = X, 3 = k1, for the running
+// instances (need_run = 1) or those with status OK (need_run = 0).  kry = q in 1..6 (the
+// Krylov form): u_{q+1} = tau L u_q for the running instances whose basis lacks it, with
+// the stored u_1 scaled by sig1.  Returns false when the instance has nothing to do.
+struct RhsIo {
+  const float2* X;
+  float2* out;
+  float scale;
+};
+__device__ __forceinline__ bool rhs_io(const big::Common& c, int b, int in_sel, int out_k, int need_run, int kry,
+                                       RhsIo& io) {
+  const big::Inst& I = c.inst[b];
+  io.scale = 1.f;
+  if (kry > 0) {
+    if (!I.run || I.kvalid >= kry + 2) return false;
+    io.X = big::slot(c, b, I.sk[kry - 1]);
+    io.out = big::slot(c, b, I.sk[kry]);
+    io.scale = (float)(kry == 1 ? I.tau * I.sig1 : I.tau);
+    return true;
+  }
+  if (need_run ? !I.run : I.status != DQB_INST_OK) return false;
+  io.X = big::slot(c, b, in_sel == 0 ? I.sy : (in_sel == 1 ? I.sy1 : (in_sel == 3 ? I.sk[0] : big::kX)));
+  io.out = big::slot(c, b, I.sk[out_k]);
+  return true;
+}
+
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
 // Generic f(X) for DIA operators (any number of diagonals).  grid (n / 128, n / 8, B),
 // block 128: each thread owns one column and 8 consecutive rows.
 // in_sel: 0 = y, 1 = y1, 2 = X.  need_run: 1 = running instances, 0 = status OK.
 __global__ void __launch_bounds__(kRhsCols) rhs_dia_generic_kernel(big::Common c, DiaOps d, int in_sel, int out_k,
-                                                                   int need_run, const float2* ext_in,
+                                                                   int need_run, int kry, const float2* ext_in,
                                                                    float2* ext_out) {
   const int b = blockIdx.z;
   const float2* X;
   float2* out;
+  float scale = 1.f;
   const float2* L;
   if (ext_in) {  // stand-alone evaluation (dqb_lindblad_rhs_dia)
     X = ext_in + (long long)b * d.n * d.n;
     out = ext_out + (long long)b * d.n * d.n;
   } else {
-    const big::Inst& I = c.inst[b];
-    if (need_run ? !I.run : I.status != DQB_INST_OK) return;
-    X = big::slot(c, b, in_sel == 0 ? I.sy : (in_sel == 1 ? I.sy1 : big::kX));
-    out = big::slot(c, b, I.sk[out_k]);
+    RhsIo io;
+    if (!rhs_io(c, b, in_sel, out_k, need_run, kry, io)) return;
+    X = io.X;
+    out = io.out;
+    scale = io.scale;
   }
   const long long li = d.Lidx ? d.Lidx[b] : b;
   L = d.L + li * d.nl * d.n;
@@ -147,7 +178,7 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_generic_kernel(big::Common c
         }
       }
     }
-    out[(long long)i * n + j] = acc;
+    out[(long long)i * n + j] = cscale(acc, scale);
   }
 }
 
@@ -172,20 +203,22 @@ constexpr int kTiledMaxTerms = 20;
 
 template <int R>
 __global__ void __launch_bounds__(kRhsCols) rhs_dia_tiled_kernel(big::Common c, DiaOps d, int in_sel, int out_k,
-                                                                int need_run, const float2* ext_in,
+                                                                int need_run, int kry, const float2* ext_in,
                                                                 float2* ext_out) {
   extern __shared__ DiaCoef dia_tab[];
   const int b = blockIdx.z;
   const float2* X;
   float2* out;
+  float scale = 1.f;
   if (ext_in) {  // stand-alone evaluation (dqb_lindblad_rhs_dia)
     X = ext_in + (long long)b * d.n * d.n;
     out = ext_out + (long long)b * d.n * d.n;
   } else {
-    const big::Inst& I = c.inst[b];
-    if (need_run ? !I.run : I.status != DQB_INST_OK) return;
-    X = big::slot(c, b, in_sel == 0 ? I.sy : (in_sel == 1 ? I.sy1 : big::kX));
-    out = big::slot(c, b, I.sk[out_k]);
+    RhsIo io;
+    if (!rhs_io(c, b, in_sel, out_k, need_run, kry, io)) return;
+    X = io.X;
+    out = io.out;
+    scale = io.scale;
   }
   const int n = d.n, nh = d.nh, np = d.npair, nt = nh + np;
   const long long li = d.Lidx ? d.Lidx[b] : b;
@@ -260,7 +293,7 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_tiled_kernel(big::Common c, 
       const DiaCoef cc = colt[t * kRhsCols + threadIdx.x];
       acc = cfma(cmul(rc.f, cc.f), __ldg(&X[rc.idx + cc.idx]), acc);
     }
-    out[(long long)i * n + j] = acc;
+    out[(long long)i * n + j] = cscale(acc, scale);
   }
 }
 
@@ -293,20 +326,22 @@ struct DiaStage {
 
 template <int R>
 __global__ void __launch_bounds__(kRhsCols) rhs_dia_staged_kernel(big::Common c, DiaOps d, DiaStage st, int in_sel,
-                                                                 int out_k, int need_run, const float2* ext_in,
-                                                                 float2* ext_out) {
+                                                                 int out_k, int need_run, int kry,
+                                                                 const float2* ext_in, float2* ext_out) {
   extern __shared__ float4 dia_stage_raw[];
   const int b = blockIdx.z;
   const float2* X;
   float2* out;
+  float scale = 1.f;
   if (ext_in) {  // stand-alone evaluation (dqb_lindblad_rhs_dia)
     X = ext_in + (long long)b * d.n * d.n;
     out = ext_out + (long long)b * d.n * d.n;
   } else {
-    const big::Inst& I = c.inst[b];
-    if (need_run ? !I.run : I.status != DQB_INST_OK) return;
-    X = big::slot(c, b, in_sel == 0 ? I.sy : (in_sel == 1 ? I.sy1 : big::kX));
-    out = big::slot(c, b, I.sk[out_k]);
+    RhsIo io;
+    if (!rhs_io(c, b, in_sel, out_k, need_run, kry, io)) return;
+    X = io.X;
+    out = io.out;
+    scale = io.scale;
   }
   const int n = d.n, nt = st.n0 + st.n1 + st.n2, tid = threadIdx.x;
   const long long li = d.Lidx ? d.Lidx[b] : b;
@@ -389,7 +424,188 @@ __global__ void __launch_bounds__(kRhsCols) rhs_dia_staged_kernel(big::Common c,
     for (int t = e1; t < nt; ++t)
       acc = cfma(cmul(rowc[t * R + r], colc[t * kRhsCols + tid]), S[st.t_base[t] + r * st.t_stride[t] + tid],
                  acc);
-    out[(long long)(i0 + r) * n + j] = acc;
+    out[(long long)(i0 + r) * n + j] = cscale(acc, scale);
+  }
+}
+
+// Wide f(X): C = 2 or 4 consecutive columns per thread, walked down R rows per CTA.  Every
+// read of the stencil is C adjacent values X[i + ro][j + co .. j + co + C - 1]: 16-byte
+// loads when j + co is even (j is a multiple of C, so that is when co is even), 8-byte
+// loads at the odd ends otherwise.  The column factors of the thread's columns stay in
+// registers for the whole walk (they do not depend on the row); the row factors of the
+// CTA's R rows are a shared-memory table, as in the tiled kernel.  Terms (the host's
+// DiaWide):
+//   center   X[i][j]             hnh_0[i] + conj(hnh_0[j])       (row and column term of
+//                                                                  Hnh's diagonal 0 at once)
+//   row      X[i + k][j]         hnh_k[i + k]                     for Hnh's offsets k != 0
+//   column   X[i][j + k]         conj(hnh_k[j + k])
+//   pair     X[i + q_p][j + q_s] l_p[i + q_p] conj(l_s[j + q_s])
+// -- the generic kernel's terms with fewer instructions per element: one load per two
+// elements for most terms, and the column factors loaded once per thread instead of once
+// per element.  Needs n to be a multiple of C (16-byte aligned rows); NR and NP are the
+// numbers of row (= column) terms and pairs, padded by zero terms.
+constexpr int kWideMaxNR = 8;
+constexpr int kWideMaxNP = 4;
+
+struct DiaWide {
+  int has0, q0;                 // Hnh has diagonal 0, at index q0
+  int nr;                       // real row / column terms (<= NR)
+  int rq[kWideMaxNR];           // Hnh diagonal of each
+  int rk[kWideMaxNR];           // its offset
+  int np;                       // real pairs (<= NP)
+  int pp[kWideMaxNP], ps[kWideMaxNP];    // jump diagonals p, s
+  int pro[kWideMaxNP], pco[kWideMaxNP];  // their offsets
+};
+
+struct __align__(16) WideRow {
+  float2 f;   // row factor
+  int off;    // clamped source row times n
+  int pad;
+};
+
+// C values X[row][col .. col + C - 1] (row pointer given); `inb`: all C columns inside the
+// matrix (else every column is clamped: its factor is zero, the read only has to be a
+// valid entry).
+template <int C>
+__device__ __forceinline__ void wide_load(const float2* __restrict__ rp, int col, bool inb, int n, float2 (&v)[C]) {
+  if (inb) {
+    if ((col & 1) == 0) {
+#pragma unroll
+      for (int h = 0; h < C / 2; ++h) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(rp + col + 2 * h));
+        v[2 * h] = make_float2(a.x, a.y), v[2 * h + 1] = make_float2(a.z, a.w);
+      }
+    } else {
+      v[0] = __ldg(rp + col);
+#pragma unroll
+      for (int h = 0; h < C / 2 - 1; ++h) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(rp + col + 1 + 2 * h));
+        v[1 + 2 * h] = make_float2(a.x, a.y), v[2 + 2 * h] = make_float2(a.z, a.w);
+      }
+      v[C - 1] = __ldg(rp + col + C - 1);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < C; ++q) {
+      const int cc = col + q;
+      v[q] = __ldg(rp + (cc < 0 ? 0 : (cc >= n ? n - 1 : cc)));
+    }
+  }
+}
+
+template <int R, int NR, int NP, int C>
+__global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c, DiaOps d, DiaWide w, int in_sel,
+                                                                  int out_k, int need_run, int kry,
+                                                                  const float2* ext_in, float2* ext_out) {
+  constexpr int NT = 1 + NR + NP;  // row-table terms: center, rows, pairs
+  __shared__ WideRow rowt[NT][R];
+  const int b = blockIdx.z;
+  const float2* X;
+  float2* out;
+  float scale = 1.f;
+  if (ext_in) {  // stand-alone evaluation (dqb_lindblad_rhs_dia)
+    X = ext_in + (long long)b * d.n * d.n;
+    out = ext_out + (long long)b * d.n * d.n;
+  } else {
+    RhsIo io;
+    if (!rhs_io(c, b, in_sel, out_k, need_run, kry, io)) return;
+    X = io.X;
+    out = io.out;
+    scale = io.scale;
+  }
+  const int n = d.n;
+  const long long li = d.Lidx ? d.Lidx[b] : b;
+  const float2* L = d.L + li * d.nl * n;
+  const float2* hnh = d.hnh + (long long)b * d.nh * n;
+  const int i0 = blockIdx.y * R;
+  const int j = (blockIdx.x * kRhsCols + threadIdx.x) * C;
+
+  // row factors of the CTA's R rows
+  for (int e = threadIdx.x; e < NT * R; e += blockDim.x) {
+    const int t = e / R, r = e % R, i = i0 + r;
+    int off = 0;
+    const float2* diag = nullptr;
+    if (t == 0) {
+      if (w.has0) diag = hnh + w.q0 * n;
+    } else if (t <= NR) {
+      if (t - 1 < w.nr) off = w.rk[t - 1], diag = hnh + w.rq[t - 1] * n;
+    } else {
+      if (t - 1 - NR < w.np) off = w.pro[t - 1 - NR], diag = L + w.pp[t - 1 - NR] * n;
+    }
+    const int src = i + off;
+    const bool in = diag != nullptr && i < n && src >= 0 && src < n;
+    WideRow v;
+    v.f = in ? __ldg(&diag[src]) : make_float2(0.f, 0.f);
+    v.off = (src < 0 ? 0 : (src >= n ? n - 1 : src)) * n;
+    v.pad = 0;
+    rowt[t][r] = v;
+  }
+  __syncthreads();
+  if (j >= n) return;
+
+  // column factors of the thread's C columns
+  float2 cc0[C], ccol[NR][C], cpair[NP][C];
+  unsigned inb_col = 0, inb_pair = 0;
+#pragma unroll
+  for (int q = 0; q < C; ++q) cc0[q] = w.has0 ? cconj(__ldg(&hnh[w.q0 * n + j + q])) : make_float2(0.f, 0.f);
+#pragma unroll
+  for (int t = 0; t < NR; ++t) {
+    const int k = t < w.nr ? w.rk[t] : 0;
+    if (j + k >= 0 && j + k + C - 1 < n) inb_col |= 1u << t;
+#pragma unroll
+    for (int q = 0; q < C; ++q) {
+      const int src = j + q + k;
+      ccol[t][q] = (t < w.nr && src >= 0 && src < n) ? cconj(__ldg(&hnh[w.rq[t] * n + src])) : make_float2(0.f, 0.f);
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < NP; ++t) {
+    const int k = t < w.np ? w.pco[t] : 0;
+    if (j + k >= 0 && j + k + C - 1 < n) inb_pair |= 1u << t;
+#pragma unroll
+    for (int q = 0; q < C; ++q) {
+      const int src = j + q + k;
+      cpair[t][q] = (t < w.np && src >= 0 && src < n) ? cconj(__ldg(&L[w.ps[t] * n + src])) : make_float2(0.f, 0.f);
+    }
+  }
+
+  const int rows = min(R, n - i0);
+#pragma unroll 1
+  for (int r = 0; r < rows; ++r) {
+    const int i = i0 + r;
+    const float2* Xi = X + (long long)i * n;
+    float2 acc[C];
+    float2 v[C];
+    {
+      const WideRow rc = rowt[0][r];
+      wide_load<C>(Xi, j, true, n, v);
+#pragma unroll
+      for (int q = 0; q < C; ++q) acc[q] = cmul(cadd(rc.f, cc0[q]), v[q]);
+    }
+#pragma unroll
+    for (int t = 0; t < NR; ++t) {
+      const WideRow rc = rowt[1 + t][r];
+      wide_load<C>(X + rc.off, j, true, n, v);
+#pragma unroll
+      for (int q = 0; q < C; ++q) acc[q] = cfma(rc.f, v[q], acc[q]);
+      const int k = t < w.nr ? w.rk[t] : 0;
+      wide_load<C>(Xi, j + k, (inb_col >> t) & 1u, n, v);
+#pragma unroll
+      for (int q = 0; q < C; ++q) acc[q] = cfma(ccol[t][q], v[q], acc[q]);
+    }
+#pragma unroll
+    for (int t = 0; t < NP; ++t) {
+      const WideRow rc = rowt[1 + NR + t][r];
+      const int k = t < w.np ? w.pco[t] : 0;
+      wide_load<C>(X + rc.off, j + k, (inb_pair >> t) & 1u, n, v);
+#pragma unroll
+      for (int q = 0; q < C; ++q) acc[q] = cfma(cmul(rc.f, cpair[t][q]), v[q], acc[q]);
+    }
+    float4* o = reinterpret_cast<float4*>(out + (long long)i * n + j);
+#pragma unroll
+    for (int h = 0; h < C / 2; ++h)
+      o[h] = make_float4(acc[2 * h].x * scale, acc[2 * h].y * scale, acc[2 * h + 1].x * scale,
+                         acc[2 * h + 1].y * scale);
   }
 }
 
@@ -554,12 +770,56 @@ bool plan_stage(const DiaOps& d, int R, DiaStage* st, size_t* smem) {
   return *smem <= kStageMaxSmem;
 }
 
+// Terms of the wide kernel (see rhs_dia_wide_kernel); false when the operators have more
+// row / column or pair terms than it holds, or rows it cannot address.
+bool plan_wide(const DiaOps& d, int C, DiaWide* w) {
+  std::memset(w, 0, sizeof(*w));
+  if (d.n % C != 0 || d.n > 46340 || d.npair > kWideMaxNP) return false;
+  w->q0 = 0;
+  for (int q = 0; q < d.nh; ++q) {
+    if (d.hoff[q] == 0) {
+      w->has0 = 1;
+      w->q0 = q;
+    } else {
+      if (w->nr == kWideMaxNR) return false;
+      w->rq[w->nr] = q;
+      w->rk[w->nr] = d.hoff[q];
+      w->nr++;
+    }
+  }
+  w->np = d.npair;
+  for (int t = 0; t < d.npair; ++t) {
+    w->pp[t] = d.pair_p[t];
+    w->ps[t] = d.pair_s[t];
+    w->pro[t] = d.loff[d.pair_p[t]];
+    w->pco[t] = d.loff[d.pair_s[t]];
+  }
+  return true;
+}
+
+// Compile-time term counts of the wide kernel's instances: NR in {4, 8}, NP in {2, 4},
+// padded by zero terms.
+int wide_nr(int nr) { return nr <= 4 ? 4 : 8; }
+int wide_np(int np) { return np <= 2 ? 2 : 4; }
+
+// Shape codes of the wide kernel: 200 + R (C = 4 columns per thread) or 300 + R (C = 2),
+// R = 8 or 16 rows per CTA.
+bool is_wide(int rows) { return rows == 208 || rows == 216 || rows == 308 || rows == 316; }
+int wide_c(int rows) { return rows >= 300 ? 2 : 4; }
+int wide_r(int rows) { return rows % 100; }
+
 // Launch shape of the stencil from `tile`: 4, 8 or 16 = the tiled kernel with that many rows
 // per thread (when the operators have at most kTiledMaxTerms diagonal terms); 108 or 116 =
-// the staged kernel with 8 or 16 rows per CTA (when its plan fits); anything else (0 =
+// the staged kernel with 8 or 16 rows per CTA (when its plan fits); 208 or 216 (4 columns
+// per thread), 308 or 316 (2 columns) = the wide kernel with 8 or 16 rows per CTA (when
+// its plan fits); anything else (0 =
 // default, 1) = the generic kernel.  The autotuner picks among them per problem shape.
 // Returns the shape code (1 = generic).
 int rows_for(const DiaOps& d, int tile) {
+  if (is_wide(tile)) {
+    DiaWide w;
+    if (plan_wide(d, wide_c(tile), &w)) return tile;
+  }
   if (tile == 108 || tile == 116) {
     DiaStage st;
     size_t sm;
@@ -570,34 +830,63 @@ int rows_for(const DiaOps& d, int tile) {
 }
 
 dim3 rhs_grid(const DiaOps& d, int rows, int B) {
+  if (is_wide(rows)) {
+    const int r = wide_r(rows), cols = kRhsCols * wide_c(rows);
+    return dim3((d.n + cols - 1) / cols, (d.n + r - 1) / r, B);
+  }
   const int r = rows == 1 ? kRhsRows : (rows > 100 ? rows - 100 : rows);
   return dim3((d.n + kRhsCols - 1) / kRhsCols, (d.n + r - 1) / r, B);
+}
+
+template <int R, int C>
+void launch_wide(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, const DiaWide& w, int in_sel,
+                 int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out) {
+  const int nr = wide_nr(w.nr), np = wide_np(w.np);
+  if (nr == 4 && np == 2)
+    rhs_dia_wide_kernel<R, 4, 2, C><<<g, kRhsCols, 0, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
+  else if (nr == 4)
+    rhs_dia_wide_kernel<R, 4, 4, C><<<g, kRhsCols, 0, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
+  else if (np == 2)
+    rhs_dia_wide_kernel<R, 8, 2, C><<<g, kRhsCols, 0, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
+  else
+    rhs_dia_wide_kernel<R, 8, 4, C><<<g, kRhsCols, 0, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
 }
 
 // One right-hand side of every instance: k[out_k] = f(input), through the kernel the shape
 // code `rows` selects (rows_for).
 void launch_rhs_dia(cudaStream_t s, const big::Common& c, const DiaOps& d, int B, int rows, int in_sel,
-                    int out_k, int need_run, const float2* ext_in, float2* ext_out) {
+                    int out_k, int need_run, const float2* ext_in, float2* ext_out, int kry = 0) {
   const dim3 g = rhs_grid(d, rows, B);
+  if (is_wide(rows)) {
+    DiaWide w;
+    plan_wide(d, wide_c(rows), &w);  // rows_for checked that it fits
+    switch (rows) {
+      case 208: launch_wide<8, 4>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out); break;
+      case 216: launch_wide<16, 4>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out); break;
+      case 308: launch_wide<8, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out); break;
+      default: launch_wide<16, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
+    }
+    return;
+  }
   if (rows > 100) {
     DiaStage st;
     size_t sm = 0;
     plan_stage(d, rows - 100, &st, &sm);  // rows_for checked that it fits
     if (rows == 116)
-      rhs_dia_staged_kernel<16><<<g, kRhsCols, sm, s>>>(c, d, st, in_sel, out_k, need_run, ext_in, ext_out);
+      rhs_dia_staged_kernel<16><<<g, kRhsCols, sm, s>>>(c, d, st, in_sel, out_k, need_run, kry, ext_in, ext_out);
     else
-      rhs_dia_staged_kernel<8><<<g, kRhsCols, sm, s>>>(c, d, st, in_sel, out_k, need_run, ext_in, ext_out);
+      rhs_dia_staged_kernel<8><<<g, kRhsCols, sm, s>>>(c, d, st, in_sel, out_k, need_run, kry, ext_in, ext_out);
     return;
   }
   const size_t sm = tiled_smem(d, rows);
   if (rows == 4) {
-    rhs_dia_tiled_kernel<4><<<g, kRhsCols, sm, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
+    rhs_dia_tiled_kernel<4><<<g, kRhsCols, sm, s>>>(c, d, in_sel, out_k, need_run, kry, ext_in, ext_out);
   } else if (rows == 8) {
-    rhs_dia_tiled_kernel<8><<<g, kRhsCols, sm, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
+    rhs_dia_tiled_kernel<8><<<g, kRhsCols, sm, s>>>(c, d, in_sel, out_k, need_run, kry, ext_in, ext_out);
   } else if (rows == 16) {
-    rhs_dia_tiled_kernel<16><<<g, kRhsCols, sm, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
+    rhs_dia_tiled_kernel<16><<<g, kRhsCols, sm, s>>>(c, d, in_sel, out_k, need_run, kry, ext_in, ext_out);
   } else {
-    rhs_dia_generic_kernel<<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, ext_in, ext_out);
+    rhs_dia_generic_kernel<<<g, kRhsCols, 0, s>>>(c, d, in_sel, out_k, need_run, kry, ext_in, ext_out);
   }
 }
 
@@ -606,7 +895,7 @@ GraphCache g_cache;
 struct LaunchKey {
   big::Common c;
   DiaOps d;
-  int grid_e, grid_r_x, grid_r_y;
+  int grid_e, grid_r_x, grid_r_y, krylov;
 };
 
 }  // namespace
@@ -627,6 +916,9 @@ static void init_carveouts() {
     prefer_max_shared(big::control_kernel);
     prefer_max_shared(big::save_kernel);
     prefer_max_shared(big::commit_kernel);
+    prefer_max_shared(big::kry_combine_kernel);
+    prefer_max_shared(big::kry_save_kernel);
+    prefer_max_shared(big::kry_commit_kernel);
     prefer_max_shared(big::pre_finalize_kernel);
     prefer_max_shared(big::finalize_kernel);
     prefer_max_shared(zero_words_kernel);
@@ -672,7 +964,9 @@ extern "C" int dqb_lindblad_rhs_dia_tiled(const dqb_dia_problem* p, int32_t form
   hnh_dia_kernel<<<dim3((p->n + 255) / 256, (unsigned)p->batch), 256, 0, s>>>(d, (int)p->batch);
   big::Common c;
   std::memset(&c, 0, sizeof(c));
-  launch_rhs_dia(s, c, d, (int)p->batch, rows_for(d, tile), 2, 0, 0, (const float2*)rho, (float2*)outp);
+  int rows = rows_for(d, tile);
+  if (is_wide(rows) && ((reinterpret_cast<uintptr_t>(rho) | reinterpret_cast<uintptr_t>(outp)) & 15)) rows = 1;
+  launch_rhs_dia(s, c, d, (int)p->batch, rows, 2, 0, 0, (const float2*)rho, (float2*)outp);
   return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
 }
 
@@ -685,6 +979,7 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   if (o->method != DQB_METHOD_TSIT5 && o->method != DQB_METHOD_DOPRI5) return DQB_ERR_INVALID_ARGUMENT;
   if (o->form != DQB_FORM_HERMITIAN && o->form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
   if (!(o->rtol >= 0) || !(o->atol >= 0) || o->max_steps < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if (o->stepper < DQB_STEPPER_AUTO || o->stepper > DQB_STEPPER_KRYLOV) return DQB_ERR_INVALID_ARGUMENT;
   if (p->batch == 0) return DQB_OK;
   DiaOps d;
   rc = build_ops(p, &d);
@@ -724,7 +1019,9 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   int grid_e = (int)std::min<long long>((nn + big::kElemThreads - 1) / big::kElemThreads, 1184);
   if (grid_e < 1) grid_e = 1;
   const dim3 ge(grid_e, B);
-  const int rows = rows_for(d, o->tile);
+  int rows = rows_for(d, o->tile);
+  if (is_wide(rows) && (reinterpret_cast<uintptr_t>(c.mats) & 15)) rows = 1;
+  const bool krylov = o->stepper != DQB_STEPPER_STAGES;
   const dim3 gi((B + 127) / 128);
   const int T = big::kElemThreads;
 
@@ -736,14 +1033,28 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   launch_rhs_dia(s, c, d, B, rows, 0, 0, 0, nullptr, nullptr);
   big::init_norm_kernel<<<ge, T, 0, s>>>(c, 0);
   big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 0);
-  big::combine_kernel<<<ge, T, 0, s>>>(c, 6);
-  launch_rhs_dia(s, c, d, B, rows, 2, 1, 0, nullptr, nullptr);
-  big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
+  if (krylov) {
+    // the probe f(y + h0 k1) - f(y) of the starting step is h0 L k1 for a linear f
+    launch_rhs_dia(s, c, d, B, rows, 3, 1, 0, nullptr, nullptr);
+    big::init_norm_kernel<<<ge, T, 0, s>>>(c, 2);
+  } else {
+    big::combine_kernel<<<ge, T, 0, s>>>(c, 6);
+    launch_rhs_dia(s, c, d, B, rows, 2, 1, 0, nullptr, nullptr);
+    big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
+  }
   big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 1);
   if (cudaGetLastError() != cudaSuccess) return DQB_ERR_CUDA;
 
   // ---- the RK loop: graph with a WHILE node ------------------------------------------
   auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h, int* flag) {
+    if (krylov) {
+      for (int q = 1; q <= 6; ++q) launch_rhs_dia(cs, c, d, B, rows, 0, 0, 1, nullptr, nullptr, q);
+      big::kry_combine_kernel<<<ge, T, 0, cs>>>(c);
+      big::control_kernel<<<gi, 128, 0, cs>>>(c);
+      big::kry_save_kernel<<<ge, T, 0, cs>>>(c);
+      big::kry_commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
+      return;
+    }
     for (int st = 0; st < 5; ++st) {
       big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
       launch_rhs_dia(cs, c, d, B, rows, 2, st + 1, 1, nullptr, nullptr);
@@ -765,6 +1076,7 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
     key.grid_e = grid_e;
     key.grid_r_x = rows;
     key.grid_r_y = fast_ok(d);
+    key.krylov = krylov;
     cudaGraphExec_t exec = g_cache.find(&key, sizeof(key));
     if (!exec) {
       if (build_while_graph(body, &exec) != cudaSuccess) return DQB_ERR_CUDA;

@@ -270,6 +270,21 @@ class PreparedSolve:
                                        b['infos'], b['status'])
 
 
+# Shape codes of the sparse-DIA stencil (dqb_ode_options.tile) the autotuner times: the
+# generic kernel, the tiled one with 4, 8, 16 rows per thread, the staged one with 8 or 16
+# rows per CTA, the wide one with 4 or 2 columns per thread and 8 or 16 rows per CTA.
+DIA_STENCIL_SHAPES = (1, 4, 8, 16, 108, 116, 208, 216, 308, 316)
+
+
+def _stepper_code(o) -> int:
+    """DQB_STEPPER_* for ``Options.stepper``."""
+    try:
+        return _lib.STEPPERS[o.stepper]
+    except KeyError:
+        raise ValueError(f'Option `stepper` must be one of {sorted(_lib.STEPPERS)}, '
+                         f'got {o.stepper!r}.') from None
+
+
 def _precision_code(o, form: int, path: str = 'large') -> int:
     """DQB_PREC_* for ``Options.precision`` on `path` ('small': the n <= 64 kernel,
     'large': the GEMM path, 'dia'); the tensor-core modes need the hermitian form.
@@ -329,7 +344,7 @@ class MESolveB200Integrator:
             max_steps=int(m.max_steps), t0=self.t0, save_states=int(bool(o.save_states)),
             check_hermitian=int(bool(o.assume_hermitian)),
             precision=self._tuned.get('precision', _precision_code(o, form, self._path)),
-            tile=self._tuned.get('tile', 0))
+            tile=self._tuned.get('tile', 0), stepper=_stepper_code(o))
 
     def _form(self) -> int:
         o = self.options
@@ -569,9 +584,8 @@ class MESolveB200Integrator:
                              ws_bytes, dev, nE)
 
     def _tune_dia_tile(self, lib, prob, ws, ws_bytes, dev, pattern) -> None:
-        """Launch shape of the DIA stencil for this (n, sparsity pattern): the generic
-        kernel (1), the tiled one with 4, 8 or 16 rows per thread, or the staged one with 8
-        or 16 rows per CTA (108, 116), timed on one right-hand side of one instance."""
+        """Launch shape of the DIA stencil for this (n, sparsity pattern), among
+        ``DIA_STENCIL_SHAPES``, timed on one right-hand side of one instance."""
         import ctypes
 
         import torch
@@ -593,9 +607,9 @@ class MESolveB200Integrator:
                     ws.data_ptr(), ws_bytes, stream), 'dqb_lindblad_rhs_dia_tiled')
             return run
 
-        key = ('dia_tile', torch.cuda.get_device_name(dev), n, prob.n_jumps, pattern,
+        key = ('dia_stencil', torch.cuda.get_device_name(dev), n, prob.n_jumps, pattern,
                autotune.batch_bucket(prob.batch))
-        self._tuned['tile'] = autotune.choose(key, [1, 4, 8, 16, 108, 116], make_run, 1)
+        self._tuned['tile'] = autotune.choose(key, list(DIA_STENCIL_SHAPES), make_run, 1)
 
     # kept for callers that select a path explicitly (tests)
     def _run_dense_small(self, lib) -> MESolveResult:

@@ -31,6 +31,13 @@ class Options:
     # the autotuner pick the faster of 'fp32' and 'tf32x3' on the GEMM path and means
     # 'fp32' elsewhere.  The sparse-DIA kernels always run FP32.
     precision: str = 'fp32'
+    # How the sparse-DIA path forms an RK step (an addition of this library): 'stages'
+    # (stage by stage, as diffrax does), 'krylov' (every stage, y1, the error estimate and
+    # the dense output as polynomials in hL applied to y, from the basis (hL)^q y, q <= 7:
+    # the same method in exact arithmetic, 22 instead of 54 passes over the state per
+    # step, and a rejected step reuses its basis), or 'auto' (= 'krylov').  Other paths
+    # always run 'stages'.
+    stepper: str = 'auto'
 
     def initialise(self) -> Options:
         return self
@@ -39,7 +46,7 @@ class Options:
 _SUPPORTED = {
     'sesolve': ('save_states', 'cartesian_batching', 'progress_meter', 't0', 'save_extra'),
     'mesolve': ('save_states', 'cartesian_batching', 'progress_meter', 't0', 'save_extra',
-                'vectorized', 'assume_hermitian', 'precision'),
+                'vectorized', 'assume_hermitian', 'precision', 'stepper'),
 }
 
 

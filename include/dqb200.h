@@ -87,10 +87,28 @@ typedef struct dqb_ode_options {
   int32_t precision;       /* DQB_PREC_* (0 = FP32; see above for the paths of each)   */
   int32_t tile;            /* launch-shape choice of the sparse-DIA stencil: 4, 8 or 16 =
                               tiled kernel with that many rows per thread; 108 or 116 =
-                              staged kernel with 8 or 16 rows per CTA; 0 (default) or 1 =
-                              generic kernel; shapes that do not fit the operators fall
-                              back to the generic kernel; ignored by other paths          */
+                              staged kernel with 8 or 16 rows per CTA; 208 or 216 (4
+                              columns per thread), 308 or 316 (2 columns) = wide kernel
+                              with 8 or 16 rows per CTA; 0 (default) or 1 = generic
+                              kernel; shapes that do not fit the operators fall back to
+                              the generic kernel; ignored by other paths                  */
+  int32_t stepper;         /* DQB_STEPPER_* (0 = AUTO): how the sparse-DIA path forms an RK
+                              step; ignored by other paths (they run STAGES)             */
 } dqb_ode_options;
+
+/* Forms of an RK step (dqb_ode_options.stepper), for the sparse-DIA path:
+ *   STAGES: stage by stage, as diffrax does (six right-hand sides per attempted step);
+ *   KRYLOV: for the linear constant-operator right-hand side every stage, y1, the error
+ *           estimate and the dense output are polynomials in hL applied to y: six
+ *           right-hand sides build u_q = (tau L)^q y, q <= 7, once per accepted step,
+ *           and one streaming pass over u_0..u_7 forms y1, the error and the next first
+ *           stage; a rejected step keeps the basis.  Equal to STAGES in exact arithmetic
+ *           (the same steps, states and counts up to rounding), 22 instead of 54 passes
+ *           over the state per attempted step.
+ *   AUTO:   KRYLOV. */
+#define DQB_STEPPER_AUTO 0
+#define DQB_STEPPER_STAGES 1
+#define DQB_STEPPER_KRYLOV 2
 
 /* Outputs of a batched solve.  nsave = n_tsave if save_states else 1. */
 typedef struct dqb_outputs {

@@ -45,7 +45,7 @@ def test_dia_tiles_equal_and_cached(cuda_device, tmp_path, monkeypatch):
     import torch
 
     from dynamiqs_b200 import _lib, workloads
-    from dynamiqs_b200.mesolve import MESolveB200Integrator, make_batch_plan
+    from dynamiqs_b200.mesolve import DIA_STENCIL_SHAPES, MESolveB200Integrator, make_batch_plan
 
     monkeypatch.setenv('DQB_AUTOTUNE_CACHE', str(tmp_path / 'tune.json'))
     autotune.clear_memory_cache()
@@ -55,7 +55,7 @@ def test_dia_tiles_equal_and_cached(cuda_device, tmp_path, monkeypatch):
                                   options=__import__('dynamiqs_b200').Options(), H=w['H'],
                                   Ls=w['jump_ops'], Es=None, plan=plan)
     prep = integ.prepare()
-    assert integ._tuned['tile'] in (1, 4, 8, 16, 108, 116)
+    assert integ._tuned['tile'] in DIA_STENCIL_SHAPES
     assert (tmp_path / 'tune.json').exists()
     lib = _lib.load()
     n = w['H'].diags.shape[-1]
@@ -63,7 +63,7 @@ def test_dia_tiles_equal_and_cached(cuda_device, tmp_path, monkeypatch):
     Y = rng.normal(size=(2, n, n)) + 1j * rng.normal(size=(2, n, n))
     rho = torch.from_numpy((Y @ np.conj(np.swapaxes(Y, -1, -2)) / n).astype(np.complex64)).cuda()
     outs = []
-    for tile in (1, 4, 8, 16, 108, 116):
+    for tile in DIA_STENCIL_SHAPES:
         out = torch.empty_like(rho)
         _lib.check(lib.dqb_lindblad_rhs_dia_tiled(
             ctypes.byref(prep.prob), _lib.FORM_HERMITIAN, tile, rho.data_ptr(), out.data_ptr(),

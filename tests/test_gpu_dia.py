@@ -51,7 +51,7 @@ def _problem_struct(H, Ls, n, batch):
     return p, [h_off, l_nd, l_off, H_d, L_d]
 
 
-@pytest.mark.parametrize('tile', [0, 8, 108, 116])
+@pytest.mark.parametrize('tile', [0, 8, 108, 116, 208, 316])
 @pytest.mark.parametrize('form', [_lib.FORM_HERMITIAN, _lib.FORM_STANDARD])
 @pytest.mark.parametrize('n', [10, 77, 300])
 def test_rhs_dia_matches_oracle(cuda_device, form, n, tile):
@@ -156,7 +156,7 @@ def coupled_kerr_4096_rhs():
     return w, X, ref
 
 
-@pytest.mark.parametrize('tile', [0, 4, 8, 16, 108, 116])
+@pytest.mark.parametrize('tile', [0, 4, 8, 16, 108, 116, 208, 216, 308, 316])
 def test_rhs_dia_full_size_every_stencil(cuda_device, coupled_kerr_4096_rhs, tile):
     """One right-hand side at n = 4096 with the workload's own offsets (+-63/+-64 select
     other row groups in the staged kernel and other halos in the tiled one than the small
@@ -213,3 +213,30 @@ def test_dia_path_dopri5_vs_oracle(cuda_device):
     assert int((res.infos.nsteps > 0).sum()) == 2
     for b in range(2):
         _oracle_compare(res, w, b, method='Dopri5')
+
+
+@pytest.mark.parametrize('method', ['Tsit5', 'Dopri5'])
+@pytest.mark.parametrize('hermitian', [True, False])
+def test_krylov_stepper_vs_stages_and_oracle(cuda_device, method, hermitian):
+    """The Krylov form of the step (the DIA path's default) against the stage-by-stage
+    form and the oracle, on strongly driven coupled Kerr modes (n = 100) whose solves
+    reject steps (a rejected step reuses its basis), with expectation values."""
+    w = workloads.coupled_kerr_dia(batch=2, m=10, seed=5, kerr=1.0, eps=3.0)
+    m = (dq.Tsit5 if method == 'Tsit5' else dq.Dopri5)(rtol=1e-4, atol=1e-6)
+    E = [np.diag(np.arange(100)).astype(np.complex64)]
+    runs = {}
+    for stepper in ('krylov', 'stages'):
+        o = dq.Options(stepper=stepper, assume_hermitian=hermitian)
+        runs[stepper] = dq.mesolve(w['H'], w['jump_ops'], w['rho0'], w['tsave'], exp_ops=E,
+                                   method=m, options=o)
+    kr, st = runs['krylov'], runs['stages']
+    assert int(kr.infos.nrejected.sum()) > 0
+    assert rel_frob(kr.states.cpu().numpy(), st.states.cpu().numpy()).max() < 2e-5
+    dn = np.abs(kr.infos.nsteps.cpu().numpy() - st.infos.nsteps.cpu().numpy())
+    assert dn.max() <= 2
+    for b in range(2):
+        H = (w['H'].offsets, w['H'].diags[b])
+        Ls = [(L.offsets, L.diags) for L in w['jump_ops']]
+        assert_solve_parity(kr.states[b].cpu().numpy(), kr.expects[b].cpu().numpy(),
+                            int(kr.infos.nsteps[b]), H, Ls, w['rho0'], w['tsave'], E, method,
+                            m.rtol, m.atol)

@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 import dynamiqs_b200 as dq
+from dynamiqs_b200 import _lib
 from dynamiqs_b200 import operators as ops
 from dynamiqs_b200.mesolve import make_batch_plan
 
@@ -48,6 +49,14 @@ def test_options_and_method_checks():
         dq.mesolve(H, Ls, r, ts, method=Euler())
     with pytest.raises(ValueError, match='does not support gradient `object`'):
         dq.mesolve(H, Ls, r, ts, gradient=object())
+    from dynamiqs_b200.mesolve import _stepper_code
+
+    assert _stepper_code(dq.Options()) == _lib.STEPPER_AUTO
+    assert _stepper_code(dq.Options(stepper='stages')) == _lib.STEPPER_STAGES
+    with pytest.raises(ValueError, match='Option `stepper` must be one of'):
+        _stepper_code(dq.Options(stepper='rk4'))
+    with pytest.raises(ValueError, match='Option `stepper` was set'):
+        dq.sesolve(H, r, ts, options=dq.Options(stepper='stages'))
 
 
 def test_cartesian_batch_plan():

@@ -351,8 +351,12 @@ def _kernels_per_launch(path: str, K: int, iterations: int, stepper: str = 'auto
             init = 9              # set-up, Hnh, rho0, 2 RHS, 2 norms, 2 controls
         return init + body * iterations + 3
     rhs = (2 if K else 1) + 1 + ((K + 1) // 4 if K > 3 else 0)  # L X, sums, symmetrize
-    body = 6 * (1 + rhs) + 4
-    init = 3 + 2 * rhs + 5 + (K + 3) // 4
+    if stepper == 'stages':
+        body = 6 * (1 + rhs) + 4  # 6 x (combine + RHS) + error, control, save, commit
+        init = 3 + 2 * rhs + 5 + (K + 3) // 4
+    else:
+        body = 6 * rhs + 4        # 6 basis RHS + combination, control, save, commit
+        init = 3 + 2 * rhs + 4 + (K + 3) // 4
     return init + body * iterations + 3
 
 
@@ -606,7 +610,7 @@ def run_b200(args):
                    'n_tsave': len(w['tsave']), 'method': type(w['method']).__name__,
                    'rtol': w['method'].rtol, 'atol': w['method'].atol, 'path': prep.name,
                    'precision': args.precision,
-                   **({'stepper': args.stepper} if args.config == 'dia' else {}),
+                   **({'stepper': args.stepper} if args.config in ('dia', 'transmon') else {}),
                    'l2': 'flushed between iterations (256 MiB write)',
                    'parallelism': f'instances sharded over {world} GPU(s), no collective',
                    'avg_rk_steps': float(nsteps.mean()), 'max_rk_steps': float(nsteps.max())},
@@ -669,8 +673,7 @@ def _extra_configs(args, dev, stream, flush, peaks, which):
                     'max_rk_steps': float(nsteps.max()),
                     'roofline': _roofline(cfg, prec, n, len(w['jump_ops']), nsteps, mean_ms, B,
                                           peaks, which, len(w['tsave']), nacc)}
-        if cfg == 'dia':
-            out[key]['stepper'] = 'auto (krylov)'
+        out[key]['stepper'] = 'auto (krylov)'
         del prep
         torch.cuda.empty_cache()
     return out
@@ -698,7 +701,7 @@ def main():
     ap.add_argument('--no-extra', action='store_true',
                     help='skip the GEMM-path and DIA lines the kerr run adds (extra_configs)')
     ap.add_argument('--stepper', default='auto', choices=['auto', 'stages', 'krylov'],
-                    help='dia: form of the RK step (auto = krylov)')
+                    help='dia, transmon: form of the RK step (auto = krylov)')
     ap.add_argument('--precision', default='fp32',
                     choices=['fp32', 'tf32x3', 'bf16x3', 'tf32', 'f16x3', 'auto'],
                     help='arithmetic of the complex products (tf32x3 / bf16x3 / tf32: GEMM '

@@ -414,111 +414,6 @@ static __global__ void control_kernel(Common c) {
   }
 }
 
-// grid (tiles, B): states and tr(E rho) at the saves crossed by an accepted step.
-// interp = 0 saves y itself (saves at or before t0 when t1 <= t0).
-static __global__ void save_kernel(Common c, int interp) {
-  __shared__ double red[40];
-  const int b = blockIdx.y;
-  const Inst& I = c.inst[b];
-  const int lo = I.save_lo, hi = I.save_hi;
-  if (hi <= lo) return;
-  const float2* y = slot(c, b, I.sy);
-  const float2* k[7];
-  for (int j = 0; j < 7; ++j) k[j] = slot(c, b, I.sk[j]);
-  const int n = c.n;
-  const bool herm = c.form == DQB_FORM_HERMITIAN;
-  for (int s = lo; s < hi; ++s) {
-    float cw[7];
-    if (interp) {
-      double w[7];
-      const double theta = I.h > 0.0 ? (I.ts[s] - I.t) / I.h : 1.0;
-      dense_weights(c.o.method, theta, w);
-      for (int j = 0; j < 7; ++j) cw[j] = (float)(I.h * w[j]);
-    }
-    float2* dst = I.states + (long long)s * c.nn;
-    for (int m0 = 0; m0 == 0 || m0 < I.nE; m0 += 4) {
-      const int mc = I.nE - m0 < 4 ? I.nE - m0 : 4;
-      double er[4] = {0, 0, 0, 0}, ei[4] = {0, 0, 0, 0};
-      for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
-           e += (long long)gridDim.x * blockDim.x) {
-        float2 v = y[e];
-        if (interp) {
-#pragma unroll
-          for (int j = 0; j < 7; ++j) v = caxpy(cw[j], k[j][e], v);
-        }
-        if (m0 == 0 && I.save_states) dst[e] = v;
-        if (mc > 0) {
-          // tr(E rho) = sum_ij E_ij rho_ji; rho_ji = conj(rho_ij) when rho is hermitian
-          float2 rt;
-          if (herm) {
-            rt = cconj(v);
-          } else {
-            const int i = (int)(e / n), j = (int)(e % n);
-            const long long et = (long long)j * n + i;
-            rt = y[et];
-            if (interp) {
-#pragma unroll
-              for (int q = 0; q < 7; ++q) rt = caxpy(cw[q], k[q][et], rt);
-            }
-          }
-#pragma unroll
-          for (int m = 0; m < 4; ++m) {
-            if (m < mc) {
-              const float2 ev = I.E[(long long)(m0 + m) * c.nn + e];
-              er[m] += (double)ev.x * rt.x - (double)ev.y * rt.y;
-              ei[m] += (double)ev.x * rt.y + (double)ev.y * rt.x;
-            }
-          }
-        }
-      }
-      for (int m = 0; m < mc; ++m) {
-        double2* acc = I.eacc + (long long)(m0 + m) * I.nts + s;
-        const double sr = block_sum(er[m], red);
-        const double si = block_sum(ei[m], red);
-        if (threadIdx.x == 0) {
-          atomicAdd(&acc->x, sr);
-          atomicAdd(&acc->y, si);
-        }
-      }
-    }
-  }
-}
-
-// One block: per-instance commit, then the WHILE-node condition (or, when the loop is
-// driven from the host, the same condition written to `flag`).
-static __global__ void commit_kernel(Common c, cudaGraphConditionalHandle handle, int* flag) {
-  int any = 0;
-  for (int b = threadIdx.x; b < c.B; b += blockDim.x) {
-    Inst& I = c.inst[b];
-    if (I.run) {
-      if (I.keep) {
-        int tmp = I.sy;
-        I.sy = I.sy1;
-        I.sy1 = tmp;
-        tmp = I.sk[0];
-        I.sk[0] = I.sk[6];
-        I.sk[6] = tmp;
-        I.t = I.tnext;
-        I.save_idx = I.save_hi;
-      }
-      I.tnext = next_tend(I.t, I.dtnew, I.t1, I.keep);
-      I.h = I.tnext - I.t;
-      I.run = I.t < I.t1;
-    }
-    I.save_lo = I.save_hi = I.save_idx;
-    any |= I.run;
-  }
-  any = __syncthreads_or(any);
-  if (threadIdx.x == 0) {
-    const long long it = ++(*c.iter);
-    const bool more = any && it < c.o.max_steps + 2;
-    if (flag)
-      *flag = more ? 1 : 0;
-    else
-      cudaGraphSetConditional(handle, more ? 1u : 0u);
-  }
-}
-
 // ------------------------------------------------------------------------------------
 // Krylov form of the step, for a linear right-hand side with constant operators
 // ------------------------------------------------------------------------------------
@@ -598,6 +493,144 @@ __device__ inline void kry_dense_coefs(int method, double theta, double r, doubl
 
 __device__ __forceinline__ double kry_ratio(const Inst& I) { return I.tau > 0.0 ? I.h / I.tau : 0.0; }
 
+// grid (tiles, B): states and tr(E rho) at the saves an accepted step crossed, up to
+// kSaveChunk save points per pass over the inputs (one pass for the usual one or few).
+// mode 0: y itself (the saves left over after the loop: t1 <= t0, or a stopped instance);
+// mode 1: the dense output y + h sum_j w_j(theta) k_j of the stage form;
+// mode 2: the dense output sum_q delta_q(theta) r^q u_q of the Krylov form.
+constexpr int kSaveChunk = 4;
+
+static __global__ void save_kernel(Common c, int mode) {
+  __shared__ double red[40];
+  __shared__ float cws[kSaveChunk][8];
+  const int b = blockIdx.y;
+  const Inst& I = c.inst[b];
+  const int lo = I.save_lo, hi = I.save_hi;
+  if (hi <= lo) return;
+  const float2* p[8];
+  p[0] = slot(c, b, I.sy);
+  for (int q = 1; q < 8; ++q) p[q] = slot(c, b, I.sk[q - 1]);
+  const int nq = mode == 0 ? 1 : 8;
+  const int n = c.n;
+  const bool herm = c.form == DQB_FORM_HERMITIAN;
+  for (int s0 = lo; s0 < hi; s0 += kSaveChunk) {
+    const int ns = hi - s0 < kSaveChunk ? hi - s0 : kSaveChunk;
+    __syncthreads();  // the previous chunk's weights are no longer read
+    if (threadIdx.x < ns) {
+      float* cw = cws[threadIdx.x];
+      const double theta = I.h > 0.0 ? (I.ts[s0 + threadIdx.x] - I.t) / I.h : 1.0;
+      if (mode == 2) {
+        kry_dense_coefs(c.o.method, theta, kry_ratio(I), I.sig1, cw);
+      } else {
+        double w[7];
+        dense_weights(c.o.method, theta, w);
+        cw[0] = 1.f;
+        for (int j = 0; j < 7; ++j) cw[j + 1] = mode == 0 ? 0.f : (float)(I.h * w[j]);
+      }
+    }
+    __syncthreads();
+    for (int m0 = 0; m0 == 0 || m0 < I.nE; m0 += 2) {
+      const int mc = I.nE - m0 < 2 ? I.nE - m0 : 2;
+      double er[kSaveChunk][2], ei[kSaveChunk][2];
+#pragma unroll
+      for (int si = 0; si < kSaveChunk; ++si) er[si][0] = er[si][1] = ei[si][0] = ei[si][1] = 0.0;
+      for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
+           e += (long long)gridDim.x * blockDim.x) {
+        float2 x[8], xt[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) x[q] = q < nq ? p[q][e] : make_float2(0.f, 0.f);
+        long long et = e;
+        if (mc > 0 && !herm) {
+          const int i = (int)(e / n), j = (int)(e % n);
+          et = (long long)j * n + i;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) xt[q] = q < nq ? p[q][et] : make_float2(0.f, 0.f);
+        }
+        float2 ev[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll
+        for (int m = 0; m < 2; ++m)
+          if (m < mc) ev[m] = I.E[(long long)(m0 + m) * c.nn + e];
+#pragma unroll
+        for (int si = 0; si < kSaveChunk; ++si) {
+          if (si < ns) {
+            float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v = caxpy(cws[si][q], x[q], v);
+            if (m0 == 0 && I.save_states) I.states[(long long)(s0 + si) * c.nn + e] = v;
+            if (mc > 0) {
+              // tr(E rho) = sum_ij E_ij rho_ji; rho_ji = conj(rho_ij) when rho is hermitian
+              float2 rt;
+              if (herm) {
+                rt = cconj(v);
+              } else {
+                rt = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) rt = caxpy(cws[si][q], xt[q], rt);
+              }
+#pragma unroll
+              for (int m = 0; m < 2; ++m) {
+                if (m < mc) {
+                  er[si][m] += (double)ev[m].x * rt.x - (double)ev[m].y * rt.y;
+                  ei[si][m] += (double)ev[m].x * rt.y + (double)ev[m].y * rt.x;
+                }
+              }
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int si = 0; si < kSaveChunk; ++si)
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+          if (si < ns && m < mc) {  // uniform over the block
+            double2* acc = I.eacc + (long long)(m0 + m) * I.nts + s0 + si;
+            const double sr = block_sum(er[si][m], red);
+            const double sim = block_sum(ei[si][m], red);
+            if (threadIdx.x == 0) {
+              atomicAdd(&acc->x, sr);
+              atomicAdd(&acc->y, sim);
+            }
+          }
+        }
+    }
+  }
+}
+
+// One block: per-instance commit, then the WHILE-node condition (or, when the loop is
+// driven from the host, the same condition written to `flag`).
+static __global__ void commit_kernel(Common c, cudaGraphConditionalHandle handle, int* flag) {
+  int any = 0;
+  for (int b = threadIdx.x; b < c.B; b += blockDim.x) {
+    Inst& I = c.inst[b];
+    if (I.run) {
+      if (I.keep) {
+        int tmp = I.sy;
+        I.sy = I.sy1;
+        I.sy1 = tmp;
+        tmp = I.sk[0];
+        I.sk[0] = I.sk[6];
+        I.sk[6] = tmp;
+        I.t = I.tnext;
+        I.save_idx = I.save_hi;
+      }
+      I.tnext = next_tend(I.t, I.dtnew, I.t1, I.keep);
+      I.h = I.tnext - I.t;
+      I.run = I.t < I.t1;
+    }
+    I.save_lo = I.save_hi = I.save_idx;
+    any |= I.run;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    const long long it = ++(*c.iter);
+    const bool more = any && it < c.o.max_steps + 2;
+    if (flag)
+      *flag = more ? 1 : 0;
+    else
+      cudaGraphSetConditional(handle, more ? 1u : 0u);
+  }
+}
+
 // grid (tiles, B): y1, tau L y1 and the error sum of the trial step from u_0..u_7, for
 // every running instance (a retried step included).
 static __global__ void kry_combine_kernel(Common c) {
@@ -661,75 +694,6 @@ static __global__ void kry_combine_kernel(Common c) {
     }
   }
   block_atomic_add(s, &I.acc[0], red);
-}
-
-// grid (tiles, B): states and tr(E rho) at the saves crossed by an accepted step, from the
-// basis (the Krylov counterpart of save_kernel with interp = 1).
-static __global__ void kry_save_kernel(Common c) {
-  __shared__ double red[40];
-  __shared__ float cws[8];
-  const int b = blockIdx.y;
-  const Inst& I = c.inst[b];
-  const int lo = I.save_lo, hi = I.save_hi;
-  if (hi <= lo) return;
-  const float2* u[8];
-  u[0] = slot(c, b, I.sy);
-  for (int q = 1; q < 8; ++q) u[q] = slot(c, b, I.sk[q - 1]);
-  const int n = c.n;
-  const bool herm = c.form == DQB_FORM_HERMITIAN;
-  const double r = kry_ratio(I);
-  for (int s = lo; s < hi; ++s) {
-    __syncthreads();  // cws of the previous save point is no longer read
-    if (threadIdx.x == 0) {
-      const double theta = I.h > 0.0 ? (I.ts[s] - I.t) / I.h : 1.0;
-      kry_dense_coefs(c.o.method, theta, r, I.sig1, cws);
-    }
-    __syncthreads();
-    float cw[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) cw[q] = cws[q];
-    float2* dst = I.states + (long long)s * c.nn;
-    for (int m0 = 0; m0 == 0 || m0 < I.nE; m0 += 4) {
-      const int mc = I.nE - m0 < 4 ? I.nE - m0 : 4;
-      double er[4] = {0, 0, 0, 0}, ei[4] = {0, 0, 0, 0};
-      for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.nn;
-           e += (long long)gridDim.x * blockDim.x) {
-        float2 v = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int q = 0; q < 8; ++q) v = caxpy(cw[q], u[q][e], v);
-        if (m0 == 0 && I.save_states) dst[e] = v;
-        if (mc > 0) {
-          float2 rt;
-          if (herm) {
-            rt = cconj(v);
-          } else {
-            const int i = (int)(e / n), j = (int)(e % n);
-            const long long et = (long long)j * n + i;
-            rt = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int q = 0; q < 8; ++q) rt = caxpy(cw[q], u[q][et], rt);
-          }
-#pragma unroll
-          for (int m = 0; m < 4; ++m) {
-            if (m < mc) {
-              const float2 ev = I.E[(long long)(m0 + m) * c.nn + e];
-              er[m] += (double)ev.x * rt.x - (double)ev.y * rt.y;
-              ei[m] += (double)ev.x * rt.y + (double)ev.y * rt.x;
-            }
-          }
-        }
-      }
-      for (int m = 0; m < mc; ++m) {
-        double2* acc = I.eacc + (long long)(m0 + m) * I.nts + s;
-        const double sr = block_sum(er[m], red);
-        const double si = block_sum(ei[m], red);
-        if (threadIdx.x == 0) {
-          atomicAdd(&acc->x, sr);
-          atomicAdd(&acc->y, si);
-        }
-      }
-    }
-  }
 }
 
 // One block: per-instance commit of the Krylov form, then the WHILE-node condition (as

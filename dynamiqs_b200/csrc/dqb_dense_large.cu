@@ -57,9 +57,19 @@ struct GemmJob {
   int kdst;      // jump index for SRC_T; for GEMMs over all jumps, kdst = -1 (blockIdx.z % K)
   int add_miH;   // epilogue: C += -i H (Hnh set-up)
   int accumulate;  // epilogue: C += result (further terms of a long sum)
-  int in_sel;    // 0 = y, 1 = y1, 2 = X
+  int in_sel;    // 0 = y, 1 = y1, 2 = X, 2 + q = k_q (the Krylov form's u_q)
   int need_run;  // 1: running instances, 0: status OK, 2: all (stand-alone)
+  int kry;       // q > 0: Krylov basis right-hand side u_{q+1} = tau L u_q (skipped where the
+                 // instance's basis already has it)
 };
+
+// Whether instance b takes no part in a job (need_run and the Krylov basis state).
+__device__ __forceinline__ bool job_skips(const big::Common& c, int b, int need_run, int kry) {
+  if (need_run == 2) return false;
+  const big::Inst& I = c.inst[b];
+  if (need_run == 1 ? !I.run : I.status != DQB_INST_OK) return true;
+  return kry > 0 && I.kvalid >= kry + 2;
+}
 
 constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
 
@@ -71,7 +81,7 @@ __device__ __forceinline__ const float2* src_ptr(const big::Common& c, const Lar
       if (ext_in) return ext_in + b * nn;
       {
         const big::Inst& I = c.inst[b];
-        return big::slot(c, b, in_sel == 0 ? I.sy : (in_sel == 1 ? I.sy1 : big::kX));
+        return big::slot(c, b, in_sel == 0 ? I.sy : (in_sel == 1 ? I.sy1 : (in_sel == 2 ? big::kX : I.sk[in_sel - 3])));
       }
     case SRC_HNH: return d.hnh + b * nn;
     case SRC_L: {
@@ -140,10 +150,7 @@ __global__ void __launch_bounds__(NT) cgemm_kernel(big::Common c, LargeOps d, Ge
   const int Kz = job.kdst < 0 ? d.K : 1;
   const int b = blockIdx.z / Kz;
   const int kz = job.kdst < 0 ? (int)(blockIdx.z % Kz) : job.kdst;
-  if (job.need_run != 2) {
-    const big::Inst& I = c.inst[b];
-    if (job.need_run == 1 ? !I.run : I.status != DQB_INST_OK) return;
-  }
+  if (job_skips(c, b, job.need_run, job.kry)) return;
   const int Kb = jumps_of(d, b);
   if (job.kdst < 0 && kz >= Kb) return;  // this instance has fewer jumps
   const int tiles = (n + BM - 1) / BM;
@@ -255,19 +262,22 @@ __global__ void __launch_bounds__(NT) cgemm_kernel(big::Common c, LargeOps d, Ge
   }
 }
 
-// k_out = tmp + tmp^+ (hermitian form) via 32 x 32 shared-memory tile pairs, or a copy.
+// k_out = tmp + tmp^+ (hermitian form) via 32 x 32 shared-memory tile pairs, or a copy;
+// for a Krylov basis right-hand side (kry = q > 0) times tau (and sig1 for q = 1).
 // grid (tiles32 * tiles32, B).
 __global__ void __launch_bounds__(256) symmetrize_kernel(big::Common c, LargeOps d, int out_k, int need_run,
-                                                         int herm, float2* ext_out) {
+                                                         int herm, int kry, float2* ext_out) {
   __shared__ float2 tT[32][33];
   const int b = blockIdx.y;
   float2* out;
+  float scale = 1.f;
   if (ext_out) {
     out = ext_out + (long long)b * d.n * d.n;
   } else {
+    if (job_skips(c, b, need_run, kry)) return;
     const big::Inst& I = c.inst[b];
-    if (need_run ? !I.run : I.status != DQB_INST_OK) return;
     out = big::slot(c, b, I.sk[out_k]);
+    if (kry > 0) scale = (float)(kry == 1 ? I.tau * I.sig1 : I.tau);
   }
   const int n = d.n;
   const float2* tmp = d.tmp + (long long)b * n * n;
@@ -287,7 +297,7 @@ __global__ void __launch_bounds__(256) symmetrize_kernel(big::Common c, LargeOps
     if (gr >= n || gc >= n) continue;
     float2 v = tmp[(long long)gr * n + gc];
     if (herm) v = cadd(v, cconj(tT[r][lx]));
-    out[(long long)gr * n + gc] = v;
+    out[(long long)gr * n + gc] = make_float2(v.x * scale, v.y * scale);
   }
 }
 
@@ -320,12 +330,27 @@ namespace tcg {
 constexpr int kProdWarps = 8;
 constexpr int kProd = kProdWarps * 32;
 constexpr int kThreads = kProd + 32;
-constexpr uint32_t kA = 128 * 128;             // one 128-row operand tile (bytes)
-constexpr uint32_t kB = 256 * 128;             // one 256-row operand tile
-constexpr uint32_t kStage = 2 * kA + 2 * kB;   // A hi, A lo, B hi, B lo
-constexpr int kStages = 2;
-constexpr int kSmem = kStages * kStage + 1024;  // + alignment slack
 constexpr uint32_t kAccCols = 256;             // one FP32 accumulator: 128 lanes x 256 columns
+// Stage geometry for a K-slice of RB bytes of every operand row (RB = 128: 128-byte
+// swizzle, two 96 KB stages; RB = 64: 64-byte swizzle, four 48 KB stages).
+template <int RB>
+struct Cfg {
+  static constexpr uint32_t kA = 128 * RB;                // one 128-row operand tile (bytes)
+  static constexpr uint32_t kB = 256 * RB;                // one 256-row operand tile
+  static constexpr uint32_t kStage = 2 * kA + 2 * kB;     // A hi, A lo, B hi, B lo
+  static constexpr int kStages = RB == 128 ? 2 : 4;
+  static constexpr int kSmem = kStages * kStage + 1024;   // + alignment slack
+  static constexpr int kChunks = RB / 16;                 // 16-byte chunks per tile row
+  static constexpr int kJobs = 128 * kChunks / kProd;     // chunks of A (and of M) per producer
+  static constexpr int kMma = RB / 32;                    // MMAs (32 bytes of K each) per stage
+  // byte offset of chunk c of row r in a swizzled K-major tile
+  static __device__ __forceinline__ uint32_t off(uint32_t r, uint32_t c) {
+    return RB == 128 ? r * 128 + ((c ^ (r & 7)) << 4) : r * 64 + ((c ^ ((r >> 1) & 3)) << 4);
+  }
+  static __device__ __forceinline__ uint64_t desc(uint32_t saddr) {
+    return RB == 128 ? tc::smem_desc_k128(saddr) : tc::smem_desc_k64(saddr);
+  }
+};
 }  // namespace tcg
 
 __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
@@ -361,47 +386,50 @@ __device__ __forceinline__ void st_split_bf16(uint32_t hi_addr, uint32_t lo_addr
   st_shared_v4(lo_addr, l0, l1, l2, l3);
 }
 
-// The 128-byte slice [k0, k0 + KC) of this thread's four A rows and four M rows.  Job
-// e = ptid + 256 q covers row e / 8, 16-byte shared-memory chunk e % 8; a chunk is one
-// float4 (two complex values) for TF32 and two float4 (four complex values) for BF16.
-template <bool BF16>
-__device__ __forceinline__ void tc_load_stage(float4 (&v)[BF16 ? 16 : 8], const float2* __restrict__ A,
-                                              const float2* __restrict__ M, int n, int row0, int col0, int k0,
-                                              int ptid) {
+// The RB-byte slice [k0, k0 + KC) of this thread's A and M chunks.  Job e = ptid + 256 q
+// covers row e / kChunks, 16-byte shared-memory chunk e % kChunks; a chunk is one float4
+// (two complex values) for TF32 and two float4 (four complex values) for BF16.
+template <int RB, bool BF16>
+__device__ __forceinline__ void tc_load_stage(float4 (&v)[(BF16 ? 4 : 2) * tcg::Cfg<RB>::kJobs],
+                                              const float2* __restrict__ A, const float2* __restrict__ M, int n,
+                                              int row0, int col0, int k0, int ptid) {
+  using C = tcg::Cfg<RB>;
   constexpr int PER = BF16 ? 2 : 1;
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
+  for (int q = 0; q < C::kJobs; ++q) {
     const int e = ptid + tcg::kProd * q;
-    const int r = e >> 3, cc = e & 7;
+    const int r = e / C::kChunks, cc = e % C::kChunks;
     const int gr = row0 + r, gj = col0 + r;
 #pragma unroll
     for (int p = 0; p < PER; ++p) {
       const int k = k0 + (cc * PER + p) * 2;  // n is even, so a float4 is all in or all out
       v[q * PER + p] = (gr < n && k < n) ? __ldg(reinterpret_cast<const float4*>(A + (long long)gr * n + k))
                                          : make_float4(0.f, 0.f, 0.f, 0.f);
-      v[4 * PER + q * PER + p] = (gj < n && k < n)
-                                     ? __ldg(reinterpret_cast<const float4*>(M + (long long)gj * n + k))
-                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+      v[C::kJobs * PER + q * PER + p] = (gj < n && k < n)
+                                            ? __ldg(reinterpret_cast<const float4*>(M + (long long)gj * n + k))
+                                            : make_float4(0.f, 0.f, 0.f, 0.f);
     }
   }
 }
 
-template <bool BF16, bool SPLIT>
-__device__ __forceinline__ void tc_store_stage(const float4 (&v)[BF16 ? 16 : 8], uint32_t st, int ptid) {
-  const uint32_t Ahi = st, Alo = st + tcg::kA, Bhi = st + 2 * tcg::kA, Blo = st + 2 * tcg::kA + tcg::kB;
+template <int RB, bool BF16, bool SPLIT>
+__device__ __forceinline__ void tc_store_stage(const float4 (&v)[(BF16 ? 4 : 2) * tcg::Cfg<RB>::kJobs], uint32_t st,
+                                               int ptid) {
+  using C = tcg::Cfg<RB>;
+  const uint32_t Ahi = st, Alo = st + C::kA, Bhi = st + 2 * C::kA, Blo = st + 2 * C::kA + C::kB;
+  constexpr int MJ = (BF16 ? 2 : 1) * C::kJobs;  // first M value in v
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
+  for (int q = 0; q < C::kJobs; ++q) {
     const int e = ptid + tcg::kProd * q;
-    const uint32_t r = e >> 3, cc = e & 7;
-    const uint32_t oa = r * 128 + ((cc ^ (r & 7)) << 4);
-    const uint32_t r0 = 2 * r, r1 = 2 * r + 1;
-    const uint32_t ob0 = r0 * 128 + ((cc ^ (r0 & 7)) << 4);
-    const uint32_t ob1 = r1 * 128 + ((cc ^ (r1 & 7)) << 4);
+    const uint32_t r = e / C::kChunks, cc = e % C::kChunks;
+    const uint32_t oa = C::off(r, cc);
+    const uint32_t ob0 = C::off(2 * r, cc);
+    const uint32_t ob1 = C::off(2 * r + 1, cc);
     // The (-Im, Re) row of M is the (Re, Im) row's split with its pairs swapped and the
     // first element negated: the hi/lo split commutes with negation, so each value of M is
     // split once.
     if (!BF16) {
-      const float4 a = v[q], m = v[4 + q];
+      const float4 a = v[q], m = v[MJ + q];
       st_split_tf32(Ahi + oa, Alo + oa, a, SPLIT);
       float h0, h1, h2, h3, l0, l1, l2, l3;
       tc::split_tf32(m.x, h0, l0);
@@ -415,7 +443,7 @@ __device__ __forceinline__ void tc_store_stage(const float4 (&v)[BF16 ? 16 : 8],
         st_shared_v4(Blo + ob1, __float_as_uint(-l1), __float_as_uint(l0), __float_as_uint(-l3), __float_as_uint(l2));
       }
     } else {
-      const float4 a0 = v[2 * q], a1 = v[2 * q + 1], m0 = v[8 + 2 * q], m1 = v[8 + 2 * q + 1];
+      const float4 a0 = v[2 * q], a1 = v[2 * q + 1], m0 = v[MJ + 2 * q], m1 = v[MJ + 2 * q + 1];
       st_split_bf16(Ahi + oa, Alo + oa, a0, a1);
       uint32_t l0, l1, l2, l3;
       const uint32_t h0 = pack_bf16(m0.x, m0.y, l0);
@@ -436,16 +464,17 @@ __device__ __forceinline__ void tc_store_stage(const float4 (&v)[BF16 ? 16 : 8],
 // semantics as cgemm_kernel, restricted to terms A M^+ (opA = 0; opB = 1, or B = the
 // hermitian stage input) with one alpha; on a wait that runs out the tile is written as
 // NaN, which the error norm turns into DQB_INST_NONFINITE.
-template <int PREC>
+template <int PREC, int RB>
 __global__ void __launch_bounds__(tcg::kThreads, 1)
     tc_cgemm_kernel(big::Common c, LargeOps d, GemmJob job, const float2* ext_in, float2* ext_out) {
+  using Cf = tcg::Cfg<RB>;
   constexpr bool kBf16 = PREC == DQB_PREC_BF16X3;
   constexpr bool kSplit = PREC != DQB_PREC_TF32;
-  constexpr int KC = kBf16 ? 32 : 16;  // complex contraction values per stage
-  constexpr int NV = kBf16 ? 16 : 8;
+  constexpr int KC = kBf16 ? RB / 4 : RB / 8;  // complex contraction values per stage
+  constexpr int NV = (kBf16 ? 4 : 2) * Cf::kJobs;
   constexpr uint32_t kCols = kSplit ? 2 * tcg::kAccCols : tcg::kAccCols;
   extern __shared__ uint8_t tc_dsm[];
-  __shared__ uint64_t bars[2 * tcg::kStages + 1];
+  __shared__ uint64_t bars[2 * Cf::kStages + 1];
   __shared__ uint32_t tmem_sh;
   __shared__ int fail_sh;
 
@@ -453,10 +482,7 @@ __global__ void __launch_bounds__(tcg::kThreads, 1)
   const int Kz = job.kdst < 0 ? d.K : 1;
   const int b = blockIdx.z / Kz;
   const int kz = job.kdst < 0 ? (int)(blockIdx.z % Kz) : job.kdst;
-  if (job.need_run != 2) {
-    const big::Inst& I = c.inst[b];
-    if (job.need_run == 1 ? !I.run : I.status != DQB_INST_OK) return;
-  }
+  if (job_skips(c, b, job.need_run, job.kry)) return;
   const int Kb = jumps_of(d, b);
   if (job.kdst < 0 && kz >= Kb) return;
   const int tiles = (n + 127) >> 7;
@@ -481,13 +507,13 @@ __global__ void __launch_bounds__(tcg::kThreads, 1)
   const uint32_t sbase = (raw + 1023u) & ~1023u;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t bar_full = tc::smem_u32(&bars[0]);
-  const uint32_t bar_empty = tc::smem_u32(&bars[tcg::kStages]);
-  const uint32_t bar_done = tc::smem_u32(&bars[2 * tcg::kStages]);
+  const uint32_t bar_empty = tc::smem_u32(&bars[Cf::kStages]);
+  const uint32_t bar_done = tc::smem_u32(&bars[2 * Cf::kStages]);
   if (warp == tcg::kProdWarps) {
     tc::tmem_alloc(tc::smem_u32(&tmem_sh), kCols);
     tc::tmem_relinquish();
     if (lane == 0) {
-      for (int s = 0; s < tcg::kStages; ++s) {
+      for (int s = 0; s < Cf::kStages; ++s) {
         tc::mbar_init(bar_full + 8 * s, tcg::kProd);
         tc::mbar_init(bar_empty + 8 * s, 1);
       }
@@ -503,26 +529,27 @@ __global__ void __launch_bounds__(tcg::kThreads, 1)
 
   if (warp < tcg::kProdWarps) {
     // ---- producers ----
-    // Global loads run PRE stages ahead of the shared-memory stores (two for TF32, whose
-    // stage fits twice more in registers; one for BF16).
-    constexpr int PRE = kBf16 ? 1 : 2;
+    // Global loads run PRE stages ahead of the shared-memory stores (as many as the
+    // registers hold: two 128-byte TF32 stages or one BF16 stage; twice that for 64 bytes).
+    constexpr int PRE = (kBf16 ? 1 : 2) * (128 / RB);
     const int ptid = threadIdx.x;
     float4 buf[PRE + 1][NV];
 #pragma unroll
     for (int p = 0; p < PRE; ++p)
       if (p < total)
-        tc_load_stage<kBf16>(buf[p], Ap[p / kchunks], Mp[p / kchunks], n, row0, col0, (p % kchunks) * KC, ptid);
+        tc_load_stage<RB, kBf16>(buf[p], Ap[p / kchunks], Mp[p / kchunks], n, row0, col0, (p % kchunks) * KC,
+                                 ptid);
     for (int it = 0; it < total; ++it) {
-      const int s = it % tcg::kStages;
+      const int s = it % Cf::kStages;
       if (it + PRE < total) {
         const int term = (it + PRE) / kchunks;
-        tc_load_stage<kBf16>(buf[PRE], Ap[term], Mp[term], n, row0, col0, ((it + PRE) % kchunks) * KC, ptid);
+        tc_load_stage<RB, kBf16>(buf[PRE], Ap[term], Mp[term], n, row0, col0, ((it + PRE) % kchunks) * KC, ptid);
       }
-      if (it >= tcg::kStages && !tc::mbar_wait(bar_empty + 8 * s, ((it / tcg::kStages) - 1) & 1)) {
+      if (it >= Cf::kStages && !tc::mbar_wait(bar_empty + 8 * s, ((it / Cf::kStages) - 1) & 1)) {
         fail_sh = 1;
         break;
       }
-      tc_store_stage<kBf16, kSplit>(buf[0], sbase + s * tcg::kStage, ptid);
+      tc_store_stage<RB, kBf16, kSplit>(buf[0], sbase + s * Cf::kStage, ptid);
       tc::fence_proxy_async_smem();
       tc::mbar_arrive(bar_full + 8 * s);
 #pragma unroll
@@ -534,19 +561,19 @@ __global__ void __launch_bounds__(tcg::kThreads, 1)
     // ---- MMA issuer ----
     constexpr uint32_t idesc = tc::instr_desc(kBf16 ? 1u : 2u, 128, 256);
     for (int it = 0; it < total; ++it) {
-      const int s = it % tcg::kStages;
-      if (!tc::mbar_wait(bar_full + 8 * s, (it / tcg::kStages) & 1)) {
+      const int s = it % Cf::kStages;
+      if (!tc::mbar_wait(bar_full + 8 * s, (it / Cf::kStages) & 1)) {
         fail_sh = 1;
         break;
       }
       tc::tc_fence_after();
-      const uint32_t st = sbase + s * tcg::kStage;
+      const uint32_t st = sbase + s * Cf::kStage;
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        const uint64_t ah = tc::smem_desc_k128(st + kk * 32);
-        const uint64_t al = tc::smem_desc_k128(st + tcg::kA + kk * 32);
-        const uint64_t bh = tc::smem_desc_k128(st + 2 * tcg::kA + kk * 32);
-        const uint64_t bl = tc::smem_desc_k128(st + 2 * tcg::kA + tcg::kB + kk * 32);
+      for (int kk = 0; kk < Cf::kMma; ++kk) {
+        const uint64_t ah = Cf::desc(st + kk * 32);
+        const uint64_t al = Cf::desc(st + Cf::kA + kk * 32);
+        const uint64_t bh = Cf::desc(st + 2 * Cf::kA + kk * 32);
+        const uint64_t bl = Cf::desc(st + 2 * Cf::kA + Cf::kB + kk * 32);
         const uint32_t acc = (it | kk) ? 1u : 0u;
         const uint32_t small = tmem + tcg::kAccCols;
         if (kBf16) {
@@ -645,22 +672,42 @@ bool use_tc(const LargeOps& d, int form) {
   return d.prec != DQB_PREC_FP32 && form == DQB_FORM_HERMITIAN && (d.n % 2) == 0;
 }
 
+// K-slice of the tensor-core GEMM's stages: 64 bytes (four stages) unless DQB_TC_SLICE=128
+// in the environment (two stages of 128 bytes), read once.
+inline int tc_slice() {
+  static const int rb = [] {
+    const char* v = std::getenv("DQB_TC_SLICE");
+    return (v != nullptr && std::atoi(v) == 128) ? 128 : 64;
+  }();
+  return rb;
+}
+
+template <int RB>
+void launch_tc(cudaStream_t s, dim3 g, const big::Common& c, const LargeOps& d, const GemmJob& j,
+               const float2* ext_in, float2* ext_out) {
+  constexpr int sm = tcg::Cfg<RB>::kSmem;
+  switch (d.prec) {
+    case DQB_PREC_TF32X3:
+      tc_cgemm_kernel<DQB_PREC_TF32X3, RB><<<g, tcg::kThreads, sm, s>>>(c, d, j, ext_in, ext_out);
+      break;
+    case DQB_PREC_BF16X3:
+      tc_cgemm_kernel<DQB_PREC_BF16X3, RB><<<g, tcg::kThreads, sm, s>>>(c, d, j, ext_in, ext_out);
+      break;
+    default:
+      tc_cgemm_kernel<DQB_PREC_TF32, RB><<<g, tcg::kThreads, sm, s>>>(c, d, j, ext_in, ext_out);
+      break;
+  }
+}
+
 void launch_gemm(cudaStream_t s, const big::Common& c, const LargeOps& d, const GemmJob& j, int zdim,
                  const float2* ext_in, float2* ext_out, bool tcp) {
   if (tcp) {
     const int t = (d.n + 127) / 128;
     const dim3 g(t * t, 1, zdim);
-    switch (d.prec) {
-      case DQB_PREC_TF32X3:
-        tc_cgemm_kernel<DQB_PREC_TF32X3><<<g, tcg::kThreads, tcg::kSmem, s>>>(c, d, j, ext_in, ext_out);
-        break;
-      case DQB_PREC_BF16X3:
-        tc_cgemm_kernel<DQB_PREC_BF16X3><<<g, tcg::kThreads, tcg::kSmem, s>>>(c, d, j, ext_in, ext_out);
-        break;
-      default:
-        tc_cgemm_kernel<DQB_PREC_TF32><<<g, tcg::kThreads, tcg::kSmem, s>>>(c, d, j, ext_in, ext_out);
-        break;
-    }
+    if (tc_slice() == 128)
+      launch_tc<128>(s, g, c, d, j, ext_in, ext_out);
+    else
+      launch_tc<64>(s, g, c, d, j, ext_in, ext_out);
   } else {
     const int t = (d.n + BM - 1) / BM;
     cgemm_kernel<<<dim3(t * t, 1, zdim), NT, 0, s>>>(c, d, j, ext_in, ext_out);
@@ -689,7 +736,7 @@ LargeLayout large_layout(int n, int K, int nE, int ntsave, long long B) {
 
 // The three launches of one right-hand side (T_k, tmp, symmetrize).
 void launch_rhs(cudaStream_t s, const big::Common& c, const LargeOps& d, int B, int in_sel, int out_k,
-                int need_run, int form, const float2* ext_in, float2* ext_out) {
+                int need_run, int form, const float2* ext_in, float2* ext_out, int kry = 0) {
   const int n = d.n;
   const bool tcp = use_tc(d, form);
   const float sc = form == DQB_FORM_HERMITIAN ? 0.5f : 1.0f;
@@ -702,6 +749,7 @@ void launch_rhs(cudaStream_t s, const big::Common& c, const LargeOps& d, int B, 
     j1.kdst = -1;
     j1.in_sel = in_sel;
     j1.need_run = need_run;
+    j1.kry = kry;
     launch_gemm(s, c, d, j1, B * d.K, ext_in, nullptr, tcp);
   }
   // tmp = Hnh X + sum_k T_k L_k^+ [+ X Hnh^+]: at most 4 summed terms per launch, the
@@ -712,6 +760,7 @@ void launch_rhs(cudaStream_t s, const big::Common& c, const LargeOps& d, int B, 
   j2.kdst = 0;
   j2.in_sel = in_sel;
   j2.need_run = need_run;
+  j2.kry = kry;
   int nt = 0;
   j2.t[nt++] = Term{SRC_HNH, 0, 0, SRC_IN, 0, 0, 1.0f};
   if (form == DQB_FORM_STANDARD) j2.t[nt++] = Term{SRC_IN, 0, 0, SRC_HNH, 0, 1, 1.0f};
@@ -725,7 +774,7 @@ void launch_rhs(cudaStream_t s, const big::Common& c, const LargeOps& d, int B, 
     nt = 0;
   }
   const int t32 = (n + 31) / 32;
-  symmetrize_kernel<<<dim3(t32 * t32, B), 256, 0, s>>>(c, d, out_k, need_run, form == DQB_FORM_HERMITIAN,
+  symmetrize_kernel<<<dim3(t32 * t32, B), 256, 0, s>>>(c, d, out_k, need_run, form == DQB_FORM_HERMITIAN, kry,
                                                        ext_out);
 }
 
@@ -738,6 +787,9 @@ int check_dense_large(const dqb_dense_problem* p) {
   return DQB_OK;
 }
 
+// Form of the RK step on the GEMM path: the Krylov form unless the stage form is asked for.
+bool large_krylov(const dqb_ode_options& o) { return o.stepper != DQB_STEPPER_STAGES; }
+
 int check_precision(int prec, int form, int n) {
   if (prec < DQB_PREC_FP32 || prec > DQB_PREC_TF32) return DQB_ERR_INVALID_ARGUMENT;
   if (prec != DQB_PREC_FP32 && (form != DQB_FORM_HERMITIAN || n % 2 != 0)) return DQB_ERR_UNSUPPORTED;
@@ -749,7 +801,7 @@ GraphCache g_cache;
 struct LaunchKey {
   big::Common c;
   LargeOps d;
-  int form;
+  int form, krylov;
 };
 
 LargeOps make_ops(const dqb_dense_problem* p, char* ws, const LargeLayout& lay) {
@@ -804,22 +856,28 @@ static void init_carveouts() {
     prefer_max_shared(big::control_kernel);
     prefer_max_shared(big::save_kernel);
     prefer_max_shared(big::commit_kernel);
+    prefer_max_shared(big::kry_combine_kernel);
+    prefer_max_shared(big::kry_commit_kernel);
     prefer_max_shared(big::retire_kernel);
     prefer_max_shared(big::pre_finalize_kernel);
     prefer_max_shared(big::finalize_kernel);
     prefer_max_shared(zero_words_kernel);
     prefer_max_shared(cgemm_kernel);
     prefer_max_shared(symmetrize_kernel);
-    prefer_max_shared(tc_cgemm_kernel<DQB_PREC_TF32X3>);
-    prefer_max_shared(tc_cgemm_kernel<DQB_PREC_BF16X3>);
-    prefer_max_shared(tc_cgemm_kernel<DQB_PREC_TF32>);
-    cudaFuncSetAttribute(tc_cgemm_kernel<DQB_PREC_TF32X3>, cudaFuncAttributeMaxDynamicSharedMemorySize, tcg::kSmem);
-    cudaFuncSetAttribute(tc_cgemm_kernel<DQB_PREC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize, tcg::kSmem);
-    cudaFuncSetAttribute(tc_cgemm_kernel<DQB_PREC_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, tcg::kSmem);
+    auto tc_attrs = [](auto kern, int smem) {
+      prefer_max_shared(kern);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    };
+    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32X3, 128>, tcg::Cfg<128>::kSmem);
+    tc_attrs(tc_cgemm_kernel<DQB_PREC_BF16X3, 128>, tcg::Cfg<128>::kSmem);
+    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32, 128>, tcg::Cfg<128>::kSmem);
+    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32X3, 64>, tcg::Cfg<64>::kSmem);
+    tc_attrs(tc_cgemm_kernel<DQB_PREC_BF16X3, 64>, tcg::Cfg<64>::kSmem);
+    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32, 64>, tcg::Cfg<64>::kSmem);
   });
 }
 
-static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s) {
+static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bool krylov) {
   init_carveouts();
   const int B = c.B;
   int grid_e = (int)std::min<long long>((c.nn + big::kElemThreads - 1) / big::kElemThreads, 1184);
@@ -835,13 +893,28 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s) {
   launch_rhs(s, c, d, B, 0, 0, 0, form, nullptr, nullptr);
   big::init_norm_kernel<<<ge, T, 0, s>>>(c, 0);
   big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 0);
-  big::combine_kernel<<<ge, T, 0, s>>>(c, 6);
-  launch_rhs(s, c, d, B, 2, 1, 0, form, nullptr, nullptr);
-  big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
+  if (krylov) {
+    // the probe f(y + h0 k1) - f(y) of the starting step is h0 L k1 for a linear f
+    launch_rhs(s, c, d, B, 3, 1, 0, form, nullptr, nullptr);
+    big::init_norm_kernel<<<ge, T, 0, s>>>(c, 2);
+  } else {
+    big::combine_kernel<<<ge, T, 0, s>>>(c, 6);
+    launch_rhs(s, c, d, B, 2, 1, 0, form, nullptr, nullptr);
+    big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
+  }
   big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 1);
   if (cudaGetLastError() != cudaSuccess) return DQB_ERR_CUDA;
 
   auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h, int* flag) {
+    if (krylov) {
+      for (int q = 1; q <= 6; ++q) launch_rhs(cs, c, d, B, q + 2, q, 1, form, nullptr, nullptr, q);
+      big::kry_combine_kernel<<<ge, T, 0, cs>>>(c);
+      big::control_kernel<<<gi, 128, 0, cs>>>(c);
+      big::save_kernel<<<ge, T, 0, cs>>>(c, 2);
+      big::kry_commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
+      if (c.rag) big::retire_kernel<<<B, 256, 0, cs>>>(c);
+      return;
+    }
     for (int st = 0; st < 5; ++st) {
       big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
       launch_rhs(cs, c, d, B, 2, st + 1, 1, form, nullptr, nullptr);
@@ -862,6 +935,7 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s) {
     key.c = c;
     key.d = d;
     key.form = form;
+    key.krylov = krylov;
     cudaGraphExec_t exec = g_cache.find(&key, sizeof(key));
     if (!exec) {
       if (build_while_graph(body, &exec) != cudaSuccess) return DQB_ERR_CUDA;
@@ -928,6 +1002,7 @@ extern "C" int dqb_mesolve_dense_large_ragged(const dqb_ragged_instance* instanc
   if (o->method != DQB_METHOD_TSIT5 && o->method != DQB_METHOD_DOPRI5) return DQB_ERR_INVALID_ARGUMENT;
   if (o->form != DQB_FORM_HERMITIAN && o->form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
   if (!(o->rtol >= 0) || !(o->atol >= 0) || o->max_steps < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if (o->stepper < DQB_STEPPER_AUTO || o->stepper > DQB_STEPPER_KRYLOV) return DQB_ERR_INVALID_ARGUMENT;
   if (int prc = check_precision(o->precision, o->form, n)) return prc;
   if (count == 0) return DQB_OK;
   if (!instances) return DQB_ERR_INVALID_ARGUMENT;
@@ -956,7 +1031,7 @@ extern "C" int dqb_mesolve_dense_large_ragged(const dqb_ragged_instance* instanc
   c.iter = (long long*)(ws + lay.off_iter);
   c.rag = instances;
   c.count_dev = count_device;
-  return run_large(c, d, (cudaStream_t)stream);
+  return run_large(c, d, (cudaStream_t)stream, large_krylov(*o));
 }
 
 extern "C" int dqb_mesolve_dense_large(const dqb_dense_problem* p, const dqb_ode_options* o, const dqb_outputs* out,
@@ -970,6 +1045,7 @@ extern "C" int dqb_mesolve_dense_large(const dqb_dense_problem* p, const dqb_ode
   if (o->method != DQB_METHOD_TSIT5 && o->method != DQB_METHOD_DOPRI5) return DQB_ERR_INVALID_ARGUMENT;
   if (o->form != DQB_FORM_HERMITIAN && o->form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
   if (!(o->rtol >= 0) || !(o->atol >= 0) || o->max_steps < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if (o->stepper < DQB_STEPPER_AUTO || o->stepper > DQB_STEPPER_KRYLOV) return DQB_ERR_INVALID_ARGUMENT;
   if (int prc = check_precision(o->precision, o->form, p->n)) return prc;
   if (p->batch == 0) return DQB_OK;
   const LargeLayout lay = large_layout(p->n, p->n_jumps, p->n_exp, p->n_tsave, p->batch);
@@ -1002,5 +1078,5 @@ extern "C" int dqb_mesolve_dense_large(const dqb_dense_problem* p, const dqb_ode
   c.ridx = p->rho0_index;
   c.iter = (long long*)(ws + lay.off_iter);
 
-  return run_large(c, d, (cudaStream_t)stream);
+  return run_large(c, d, (cudaStream_t)stream, large_krylov(*o));
 }

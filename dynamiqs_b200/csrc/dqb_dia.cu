@@ -917,7 +917,6 @@ static void init_carveouts() {
     prefer_max_shared(big::save_kernel);
     prefer_max_shared(big::commit_kernel);
     prefer_max_shared(big::kry_combine_kernel);
-    prefer_max_shared(big::kry_save_kernel);
     prefer_max_shared(big::kry_commit_kernel);
     prefer_max_shared(big::pre_finalize_kernel);
     prefer_max_shared(big::finalize_kernel);
@@ -1051,7 +1050,7 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
       for (int q = 1; q <= 6; ++q) launch_rhs_dia(cs, c, d, B, rows, 0, 0, 1, nullptr, nullptr, q);
       big::kry_combine_kernel<<<ge, T, 0, cs>>>(c);
       big::control_kernel<<<gi, 128, 0, cs>>>(c);
-      big::kry_save_kernel<<<ge, T, 0, cs>>>(c);
+      big::save_kernel<<<ge, T, 0, cs>>>(c, 2);
       big::kry_commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
       return;
     }

@@ -130,6 +130,18 @@ __device__ __forceinline__ uint64_t smem_desc_k128(uint32_t saddr) {
   return d;
 }
 
+// The same for tiles with the 64-byte swizzle: 64-byte rows, 8-row atoms 512 bytes apart,
+// 16-byte chunk c of row r stored at chunk position c ^ ((r / 2) % 4).
+__device__ __forceinline__ uint64_t smem_desc_k64(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(512u >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)4 << 61;
+  return d;
+}
+
 // Instruction descriptor of kind::tf32 / kind::f16 with FP32 accumulation, both operands
 // K-major.  fmt: 1 = BF16, 2 = TF32.
 __host__ __device__ constexpr uint32_t instr_desc(uint32_t fmt, int M, int N) {

@@ -31,12 +31,12 @@ class Options:
     # the autotuner pick the faster of 'fp32' and 'tf32x3' on the GEMM path and means
     # 'fp32' elsewhere.  The sparse-DIA kernels always run FP32.
     precision: str = 'fp32'
-    # How the sparse-DIA path forms an RK step (an addition of this library): 'stages'
-    # (stage by stage, as diffrax does), 'krylov' (every stage, y1, the error estimate and
-    # the dense output as polynomials in hL applied to y, from the basis (hL)^q y, q <= 7:
-    # the same method in exact arithmetic, 22 instead of 54 passes over the state per
-    # step, and a rejected step reuses its basis), or 'auto' (= 'krylov').  Other paths
-    # always run 'stages'.
+    # How the sparse-DIA and dense GEMM (n > 64) paths form an RK step (an addition of
+    # this library): 'stages' (stage by stage, as diffrax does), 'krylov' (every stage, y1,
+    # the error estimate and the dense output as polynomials in hL applied to y, from the
+    # basis (hL)^q y, q <= 7: the same method in exact arithmetic, 22 instead of 54 passes
+    # over the state per step, and a rejected step reuses its basis), or 'auto'
+    # (= 'krylov').  The n <= 64 kernel, sesolve and the vectorized form run 'stages'.
     stepper: str = 'auto'
 
     def initialise(self) -> Options:

@@ -92,11 +92,12 @@ typedef struct dqb_ode_options {
                               with 8 or 16 rows per CTA; 0 (default) or 1 = generic
                               kernel; shapes that do not fit the operators fall back to
                               the generic kernel; ignored by other paths                  */
-  int32_t stepper;         /* DQB_STEPPER_* (0 = AUTO): how the sparse-DIA path forms an RK
-                              step; ignored by other paths (they run STAGES)             */
+  int32_t stepper;         /* DQB_STEPPER_* (0 = AUTO): how the sparse-DIA and dense GEMM
+                              (n > 64) paths form an RK step; the n <= 64 kernel, sesolve
+                              and the vectorized form always run STAGES                  */
 } dqb_ode_options;
 
-/* Forms of an RK step (dqb_ode_options.stepper), for the sparse-DIA path:
+/* Forms of an RK step (dqb_ode_options.stepper), for the sparse-DIA and GEMM paths:
  *   STAGES: stage by stage, as diffrax does (six right-hand sides per attempted step);
  *   KRYLOV: for the linear constant-operator right-hand side every stage, y1, the error
  *           estimate and the dense output are polynomials in hL applied to y: six

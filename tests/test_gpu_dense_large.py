@@ -131,3 +131,23 @@ def test_transmon_full_size_full_horizon(cuda_device):
     tr = torch.diagonal(st, dim1=-2, dim2=-1).sum(-1)
     assert float((tr - 1).abs().max()) < 1e-5
     assert float((st - st.conj().transpose(-1, -2)).abs().max()) < 1e-6
+
+
+@pytest.mark.parametrize('precision', ['fp32', 'tf32x3'])
+@pytest.mark.parametrize('method', ['Tsit5', 'Dopri5'])
+def test_large_path_krylov_stepper_vs_oracle(cuda_device, precision, method):
+    """The Krylov form of the step on the GEMM path (Options(stepper='krylov')):
+    transmon(2) x cavity(40), n = 80, 3 instances, against the oracle under the parity bar,
+    and against the stage form (step counts within two)."""
+    w = workloads.transmon_cavity(batch=3, nq=2, nc=40, seed=1)
+    ts = np.linspace(0.0, 5.0, 11)
+    m = (dq.Tsit5 if method == 'Tsit5' else dq.Dopri5)(rtol=1e-6, atol=1e-8)
+    res = {}
+    for stepper in ('krylov', 'stages'):
+        res[stepper] = dq.mesolve(w['H'], w['jump_ops'], w['rho0'], ts, exp_ops=w['exp_ops'],
+                                  method=m, options=dq.Options(stepper=stepper, precision=precision))
+    kr = res['krylov']
+    for b in range(3):
+        _check_vs_oracle(kr, w['H'][b], w['jump_ops'], w['rho0'], ts, w['exp_ops'], m, b)
+    dn = np.abs(kr.infos.nsteps.cpu().numpy() - res['stages'].infos.nsteps.cpu().numpy())
+    assert dn.max() <= 2

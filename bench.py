@@ -343,7 +343,7 @@ def _kernels_per_launch(path: str, K: int, iterations: int, stepper: str = 'auto
     if path == 'dqb_mesolve_dense':
         return 1  # the persistent kernel (plus a 256-byte memset of its work counter)
     if path == 'dqb_mesolve_dia':
-        if stepper == 'stages':
+        if stepper != 'krylov':
             body = 6 * 2 + 4      # 6 x (combine + stencil) + error, control, save, commit
             init = 10             # set-up, Hnh, rho0, 2 RHS, norms, controls, probe
         else:
@@ -351,7 +351,7 @@ def _kernels_per_launch(path: str, K: int, iterations: int, stepper: str = 'auto
             init = 9              # set-up, Hnh, rho0, 2 RHS, 2 norms, 2 controls
         return init + body * iterations + 3
     rhs = (2 if K else 1) + 1 + ((K + 1) // 4 if K > 3 else 0)  # L X, sums, symmetrize
-    if stepper == 'stages':
+    if stepper != 'krylov':
         body = 6 * (1 + rhs) + 4  # 6 x (combine + RHS) + error, control, save, commit
         init = 3 + 2 * rhs + 5 + (K + 3) // 4
     else:
@@ -373,7 +373,7 @@ def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which, nsave=0
         # (stages 2-6 read y and k_1..k_{i-1} and write k_i: 25 passes; y1, k7 and the error
         # 9 more) -- the figure of a fully fused stage-form step
         stage_bytes = float((34 * mat * nsteps).sum())
-        if stepper == 'stages':
+        if stepper != 'krylov':
             nbytes = stage_bytes
             note = ('bytes = 34 n^2 complex64 matrix passes per attempted RK step per '
                     'instance (the fused stage-form minimum); the kernels make 54')
@@ -389,9 +389,9 @@ def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which, nsave=0
         achieved = nbytes / (mean_ms / 1e3) / 1e9
         roof = {'bound': 'hbm', 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
                 'frac': achieved / peaks['hbm_gbs'], 'peak_source': f'hbm_gbs ({which})',
-                'traffic': _traffic(config, precision, B, nsteps, nsave, stepper),
+                'traffic': _traffic(config, precision, B, nsteps, nsave, stepper, nacc),
                 'algorithmic_bytes_per_launch': nbytes, 'note': note}
-        if stepper != 'stages':
+        if stepper == 'krylov':
             eff = stage_bytes / (mean_ms / 1e3) / 1e9
             roof['stage_form_equivalent'] = {
                 'achieved': eff, 'frac': eff / peaks['hbm_gbs'],
@@ -433,22 +433,27 @@ def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which, nsave=0
 #   kerr / fp32: per instance (148 instances, the full t in [0, 10] and 51 saves: 419.9 MB
 #     for 148 = 2.837 MB; inputs, states and expectation values, the RK slots stay in L2);
 #     profiles/mesolve_small_kernel_n64_kerr.md.
-#   dia / fp32: per attempted RK step of one instance (every kernel of the stepper, host
-#     loop: 7.19 GB = 54 passes over the 134 MB matrix) plus 1.22 GB per save point;
-#     profiles/dia_stepper_n4096_coupled_kerr_traffic.md.
+#   dia / fp32, stage form: per attempted RK step of one instance (every kernel of the
+#     stepper, host loop: 7.19 GB = 54 passes over the 134 MB matrix) plus 1.22 GB per save
+#     point; profiles/dia_stepper_n4096_coupled_kerr_traffic.md.
+#   dia / fp32, Krylov form: 1.387 GB per accepted step (six basis stencils, 134.6 MB read
+#     + 96.5 MB written each), 1.324 GB per attempt (the combination pass: 1073.8 MB read,
+#     249.7 MB written) and 1.34 GB per save point; profiles/dia_krylov_n4096_coupled_kerr.md.
 TRAFFIC_PER_UNIT = {
-    ('kerr', 'fp32', 'auto'): ('instance', 2.837e6, 0.0),
-    ('dia', 'fp32', 'stages'): ('instance_step', 7.19e9, 1.22e9),
+    ('kerr', 'fp32', 'auto'): ('instance', 2.837e6, 0.0, 0.0),
+    ('dia', 'fp32', 'stages'): ('instance_step', 7.19e9, 0.0, 1.22e9),
+    ('dia', 'fp32', 'krylov'): ('instance_step', 1.324e9, 1.387e9, 1.34e9),
 }
 
 
-def _traffic(config, precision, B, nsteps, nsave=0, stepper='auto'):
-    key = (config, precision, stepper if config == 'dia' else 'auto')
+def _traffic(config, precision, B, nsteps, nsave=0, stepper='auto', nacc=None):
+    key = (config, precision, ('krylov' if stepper == 'krylov' else 'stages') if config == 'dia' else 'auto')
     if key not in TRAFFIC_PER_UNIT:
         return None
-    unit, per, per_save = TRAFFIC_PER_UNIT[key]
+    unit, per, per_acc, per_save = TRAFFIC_PER_UNIT[key]
     units = B if unit == 'instance' else float(nsteps.sum())
-    return float(per * units + per_save * nsave * B)
+    acc = 0.0 if nacc is None else float(nacc.sum())
+    return float(per * units + per_acc * acc + per_save * nsave * B)
 
 
 def run_b200(args):
@@ -634,20 +639,25 @@ def _extra_configs(args, dev, stream, flush, peaks, which):
     """The tensor-core GEMM path (transmon x cavity, n = 256, 3xTF32) and the sparse-DIA
     path (coupled Kerr modes, n = 4096) measured in the same run as the headline, on
     device-resident inputs with the headline's timing rules (CUDA events on the launching
-    stream, L2 flushed between launches), 3 warm-up and 2 timed launches each."""
+    stream, L2 flushed between launches), 3 warm-up and 2 timed launches each; each with the
+    default stage form of the step and with the opt-in Krylov form."""
     import torch
 
     import dynamiqs_b200 as dq
     from dynamiqs_b200.mesolve import MESolveB200Integrator, make_batch_plan
 
     out = {}
-    for key, cfg, prec in (('transmon_tf32x3', 'transmon', 'tf32x3'), ('coupled_kerr_dia', 'dia', 'fp32')):
+    for key, cfg, prec, stepper in (('transmon_tf32x3', 'transmon', 'tf32x3', 'auto'),
+                                    ('transmon_tf32x3_krylov', 'transmon', 'tf32x3', 'krylov'),
+                                    ('coupled_kerr_dia', 'dia', 'fp32', 'auto'),
+                                    ('coupled_kerr_dia_krylov', 'dia', 'fp32', 'krylov')):
         sub = argparse.Namespace(**vars(args))
         sub.batch, sub.n, sub.tend = 0, 0, 10.0
         w = _workload(cfg, sub, 0)
         plan = make_batch_plan(w['H'], w['jump_ops'], w['rho0'], True)
         prep = MESolveB200Integrator(ts=w['tsave'], y0=w['rho0'], method=w['method'], gradient=None,
-                                     options=dq.Options(precision=prec), H=w['H'], Ls=w['jump_ops'],
+                                     options=dq.Options(precision=prec, stepper=stepper), H=w['H'],
+                                     Ls=w['jump_ops'],
                                      Es=w.get('exp_ops'), plan=plan).prepare()
         for _ in range(3):
             prep.launch(stream.cuda_stream)
@@ -671,9 +681,9 @@ def _extra_configs(args, dev, stream, flush, peaks, which):
                     'value': B / (mean_ms / 1e3), 'unit': 'solves/s', 'ms_per_step': mean_ms,
                     'steps': 2, 'warmup': 3, 'batch': B, 'avg_rk_steps': float(nsteps.mean()),
                     'max_rk_steps': float(nsteps.max()),
+                    'stepper': stepper,
                     'roofline': _roofline(cfg, prec, n, len(w['jump_ops']), nsteps, mean_ms, B,
-                                          peaks, which, len(w['tsave']), nacc)}
-        out[key]['stepper'] = 'auto (krylov)'
+                                          peaks, which, len(w['tsave']), nacc, stepper)}
         del prep
         torch.cuda.empty_cache()
     return out
@@ -701,7 +711,7 @@ def main():
     ap.add_argument('--no-extra', action='store_true',
                     help='skip the GEMM-path and DIA lines the kerr run adds (extra_configs)')
     ap.add_argument('--stepper', default='auto', choices=['auto', 'stages', 'krylov'],
-                    help='dia, transmon: form of the RK step (auto = krylov)')
+                    help='dia, transmon: form of the RK step (auto = stages)')
     ap.add_argument('--precision', default='fp32',
                     choices=['fp32', 'tf32x3', 'bf16x3', 'tf32', 'f16x3', 'auto'],
                     help='arithmetic of the complex products (tf32x3 / bf16x3 / tf32: GEMM '

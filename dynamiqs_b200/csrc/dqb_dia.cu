@@ -493,12 +493,24 @@ __device__ __forceinline__ void wide_load(const float2* __restrict__ rp, int col
   }
 }
 
-template <int R, int NR, int NP, int C>
+// HERM (the hermitian form, X hermitian): f(X) is hermitian, so only the elements on and
+// above the diagonal are computed -- a CTA whose tile lies below the diagonal exits at
+// once -- and each strictly-upper element is also written, conjugated, at its mirror
+// position, through a shared-memory strip of the CTA's R x (128 C) outputs so that the
+// mirrored rows leave as contiguous R-value segments.  About half the stencil work, and
+// the output is hermitian to the last bit.
+template <int R, int NR, int NP, int C, bool HERM>
 __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c, DiaOps d, DiaWide w, int in_sel,
                                                                   int out_k, int need_run, int kry,
                                                                   const float2* ext_in, float2* ext_out) {
   constexpr int NT = 1 + NR + NP;  // row-table terms: center, rows, pairs
+  constexpr int W = kRhsCols * C;  // columns of the CTA's tile
+  constexpr int SW = W + 1;        // row stride of the strip (the mirror reads down columns)
   __shared__ WideRow rowt[NT][R];
+  extern __shared__ float2 strip[];  // [R][SW] when HERM
+  const int i0 = blockIdx.y * R;
+  const int j0 = blockIdx.x * W;
+  if (HERM && j0 + W - 1 < i0) return;  // the whole tile is below the diagonal
   const int b = blockIdx.z;
   const float2* X;
   float2* out;
@@ -517,8 +529,7 @@ __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c
   const long long li = d.Lidx ? d.Lidx[b] : b;
   const float2* L = d.L + li * d.nl * n;
   const float2* hnh = d.hnh + (long long)b * d.nh * n;
-  const int i0 = blockIdx.y * R;
-  const int j = (blockIdx.x * kRhsCols + threadIdx.x) * C;
+  const int j = j0 + threadIdx.x * C;
 
   // row factors of the CTA's R rows
   for (int e = threadIdx.x; e < NT * R; e += blockDim.x) {
@@ -541,8 +552,10 @@ __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c
     rowt[t][r] = v;
   }
   __syncthreads();
-  if (j >= n) return;
-
+  const bool active = j < n;  // n is a multiple of C: all C columns or none
+  const int rows = min(R, n - i0);
+  if (!HERM && !active) return;
+  if (active) {
   // column factors of the thread's C columns
   float2 cc0[C], ccol[NR][C], cpair[NP][C];
   unsigned inb_col = 0, inb_pair = 0;
@@ -569,10 +582,10 @@ __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c
     }
   }
 
-  const int rows = min(R, n - i0);
 #pragma unroll 1
   for (int r = 0; r < rows; ++r) {
     const int i = i0 + r;
+    if (HERM && j + C - 1 < i) break;  // this and the later rows lie below the diagonal
     const float2* Xi = X + (long long)i * n;
     float2 acc[C];
     float2 v[C];
@@ -601,11 +614,33 @@ __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c
 #pragma unroll
       for (int q = 0; q < C; ++q) acc[q] = cfma(cmul(rc.f, cpair[t][q]), v[q], acc[q]);
     }
-    float4* o = reinterpret_cast<float4*>(out + (long long)i * n + j);
 #pragma unroll
-    for (int h = 0; h < C / 2; ++h)
-      o[h] = make_float4(acc[2 * h].x * scale, acc[2 * h].y * scale, acc[2 * h + 1].x * scale,
-                         acc[2 * h + 1].y * scale);
+    for (int q = 0; q < C; ++q) acc[q] = make_float2(acc[q].x * scale, acc[q].y * scale);
+    float2* orow = out + (long long)i * n + j;
+    if (!HERM || j >= i) {  // every column on or above the diagonal
+#pragma unroll
+      for (int h = 0; h < C / 2; ++h)
+        reinterpret_cast<float4*>(orow)[h] = make_float4(acc[2 * h].x, acc[2 * h].y, acc[2 * h + 1].x, acc[2 * h + 1].y);
+    } else {
+#pragma unroll
+      for (int q = 0; q < C; ++q)
+        if (j + q >= i) orow[q] = acc[q];
+    }
+    if (HERM) {
+#pragma unroll
+      for (int q = 0; q < C; ++q) strip[r * SW + threadIdx.x * C + q] = acc[q];
+    }
+  }
+  }  // active
+  if (HERM) {
+    // mirror: out[jj][i0 + r] = conj(f[i0 + r][jj]) for jj > i0 + r, R contiguous values per
+    // target row (R threads per row, one value each)
+    __syncthreads();
+    for (int e = threadIdx.x; e < W * R; e += kRhsCols) {
+      const int r = e % R, cj = e / R;
+      const int i = i0 + r, jj = j0 + cj;
+      if (r < rows && jj < n && jj > i) out[(long long)jj * n + i] = cconj(strip[r * SW + cj]);
+    }
   }
 }
 
@@ -838,33 +873,48 @@ dim3 rhs_grid(const DiaOps& d, int rows, int B) {
   return dim3((d.n + kRhsCols - 1) / kRhsCols, (d.n + r - 1) / r, B);
 }
 
+template <int R, int C, bool HERM>
+void launch_wide_form(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, const DiaWide& w,
+                      int in_sel, int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out) {
+  const int nr = wide_nr(w.nr), np = wide_np(w.np);
+  const size_t sm = HERM ? (size_t)R * (kRhsCols * C + 1) * sizeof(float2) : 0;
+  if (nr == 4 && np == 2)
+    rhs_dia_wide_kernel<R, 4, 2, C, HERM><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in,
+                                                                 ext_out);
+  else if (nr == 4)
+    rhs_dia_wide_kernel<R, 4, 4, C, HERM><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in,
+                                                                 ext_out);
+  else if (np == 2)
+    rhs_dia_wide_kernel<R, 8, 2, C, HERM><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in,
+                                                                 ext_out);
+  else
+    rhs_dia_wide_kernel<R, 8, 4, C, HERM><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in,
+                                                                 ext_out);
+}
+
 template <int R, int C>
 void launch_wide(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, const DiaWide& w, int in_sel,
-                 int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out) {
-  const int nr = wide_nr(w.nr), np = wide_np(w.np);
-  if (nr == 4 && np == 2)
-    rhs_dia_wide_kernel<R, 4, 2, C><<<g, kRhsCols, 0, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
-  else if (nr == 4)
-    rhs_dia_wide_kernel<R, 4, 4, C><<<g, kRhsCols, 0, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
-  else if (np == 2)
-    rhs_dia_wide_kernel<R, 8, 2, C><<<g, kRhsCols, 0, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
+                 int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out, bool herm) {
+  if (herm)
+    launch_wide_form<R, C, true>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
   else
-    rhs_dia_wide_kernel<R, 8, 4, C><<<g, kRhsCols, 0, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
+    launch_wide_form<R, C, false>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
 }
 
 // One right-hand side of every instance: k[out_k] = f(input), through the kernel the shape
 // code `rows` selects (rows_for).
 void launch_rhs_dia(cudaStream_t s, const big::Common& c, const DiaOps& d, int B, int rows, int in_sel,
-                    int out_k, int need_run, const float2* ext_in, float2* ext_out, int kry = 0) {
+                    int out_k, int need_run, const float2* ext_in, float2* ext_out, int kry = 0,
+                    bool herm = false) {
   const dim3 g = rhs_grid(d, rows, B);
   if (is_wide(rows)) {
     DiaWide w;
     plan_wide(d, wide_c(rows), &w);  // rows_for checked that it fits
     switch (rows) {
-      case 208: launch_wide<8, 4>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out); break;
-      case 216: launch_wide<16, 4>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out); break;
-      case 308: launch_wide<8, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out); break;
-      default: launch_wide<16, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
+      case 208: launch_wide<8, 4>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm); break;
+      case 216: launch_wide<16, 4>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm); break;
+      case 308: launch_wide<8, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm); break;
+      default: launch_wide<16, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm);
     }
     return;
   }
@@ -928,6 +978,15 @@ static void init_carveouts() {
     prefer_max_shared(rhs_dia_tiled_kernel<16>);
     prefer_max_shared(rhs_dia_staged_kernel<8>);
     prefer_max_shared(rhs_dia_staged_kernel<16>);
+    auto herm_attr = [](auto kern) {
+      prefer_max_shared(kern);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           16 * (kRhsCols * 4 + 1) * (int)sizeof(float2));
+    };
+    herm_attr(rhs_dia_wide_kernel<16, 4, 2, 4, true>);
+    herm_attr(rhs_dia_wide_kernel<16, 4, 4, 4, true>);
+    herm_attr(rhs_dia_wide_kernel<16, 8, 2, 4, true>);
+    herm_attr(rhs_dia_wide_kernel<16, 8, 4, 4, true>);
     cudaFuncSetAttribute(rhs_dia_staged_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageMaxSmem);
     cudaFuncSetAttribute(rhs_dia_staged_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageMaxSmem);
   });
@@ -965,7 +1024,8 @@ extern "C" int dqb_lindblad_rhs_dia_tiled(const dqb_dia_problem* p, int32_t form
   std::memset(&c, 0, sizeof(c));
   int rows = rows_for(d, tile);
   if (is_wide(rows) && ((reinterpret_cast<uintptr_t>(rho) | reinterpret_cast<uintptr_t>(outp)) & 15)) rows = 1;
-  launch_rhs_dia(s, c, d, (int)p->batch, rows, 2, 0, 0, (const float2*)rho, (float2*)outp);
+  launch_rhs_dia(s, c, d, (int)p->batch, rows, 2, 0, 0, (const float2*)rho, (float2*)outp, 0,
+                 form == DQB_FORM_HERMITIAN);
   return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
 }
 
@@ -1020,7 +1080,8 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   const dim3 ge(grid_e, B);
   int rows = rows_for(d, o->tile);
   if (is_wide(rows) && (reinterpret_cast<uintptr_t>(c.mats) & 15)) rows = 1;
-  const bool krylov = o->stepper != DQB_STEPPER_STAGES;
+  const bool krylov = o->stepper == DQB_STEPPER_KRYLOV;
+  const bool herm = o->form == DQB_FORM_HERMITIAN;
   const dim3 gi((B + 127) / 128);
   const int T = big::kElemThreads;
 
@@ -1029,16 +1090,16 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   big::setup_kernel<<<gi, 128, 0, s>>>(c);
   hnh_dia_kernel<<<dim3((p->n + 255) / 256, B), 256, 0, s>>>(d, B);
   big::load_rho0_kernel<<<ge, T, 0, s>>>(c);
-  launch_rhs_dia(s, c, d, B, rows, 0, 0, 0, nullptr, nullptr);
+  launch_rhs_dia(s, c, d, B, rows, 0, 0, 0, nullptr, nullptr, 0, herm);
   big::init_norm_kernel<<<ge, T, 0, s>>>(c, 0);
   big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 0);
   if (krylov) {
     // the probe f(y + h0 k1) - f(y) of the starting step is h0 L k1 for a linear f
-    launch_rhs_dia(s, c, d, B, rows, 3, 1, 0, nullptr, nullptr);
+    launch_rhs_dia(s, c, d, B, rows, 3, 1, 0, nullptr, nullptr, 0, herm);
     big::init_norm_kernel<<<ge, T, 0, s>>>(c, 2);
   } else {
     big::combine_kernel<<<ge, T, 0, s>>>(c, 6);
-    launch_rhs_dia(s, c, d, B, rows, 2, 1, 0, nullptr, nullptr);
+    launch_rhs_dia(s, c, d, B, rows, 2, 1, 0, nullptr, nullptr, 0, herm);
     big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
   }
   big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 1);
@@ -1047,7 +1108,7 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   // ---- the RK loop: graph with a WHILE node ------------------------------------------
   auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h, int* flag) {
     if (krylov) {
-      for (int q = 1; q <= 6; ++q) launch_rhs_dia(cs, c, d, B, rows, 0, 0, 1, nullptr, nullptr, q);
+      for (int q = 1; q <= 6; ++q) launch_rhs_dia(cs, c, d, B, rows, 0, 0, 1, nullptr, nullptr, q, herm);
       big::kry_combine_kernel<<<ge, T, 0, cs>>>(c);
       big::control_kernel<<<gi, 128, 0, cs>>>(c);
       big::save_kernel<<<ge, T, 0, cs>>>(c, 2);
@@ -1056,10 +1117,10 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
     }
     for (int st = 0; st < 5; ++st) {
       big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
-      launch_rhs_dia(cs, c, d, B, rows, 2, st + 1, 1, nullptr, nullptr);
+      launch_rhs_dia(cs, c, d, B, rows, 2, st + 1, 1, nullptr, nullptr, 0, herm);
     }
     big::combine_kernel<<<ge, T, 0, cs>>>(c, 5);
-    launch_rhs_dia(cs, c, d, B, rows, 1, 6, 1, nullptr, nullptr);
+    launch_rhs_dia(cs, c, d, B, rows, 1, 6, 1, nullptr, nullptr, 0, herm);
     big::error_kernel<<<ge, T, 0, cs>>>(c);
     big::control_kernel<<<gi, 128, 0, cs>>>(c);
     big::save_kernel<<<ge, T, 0, cs>>>(c, 1);

@@ -103,10 +103,12 @@ typedef struct dqb_ode_options {
  *           estimate and the dense output are polynomials in hL applied to y: six
  *           right-hand sides build u_q = (tau L)^q y, q <= 7, once per accepted step,
  *           and one streaming pass over u_0..u_7 forms y1, the error and the next first
- *           stage; a rejected step keeps the basis.  Equal to STAGES in exact arithmetic
- *           (the same steps, states and counts up to rounding), 22 instead of 54 passes
- *           over the state per attempted step.
- *   AUTO:   KRYLOV. */
+ *           stage; a rejected step keeps the basis.  Equal to STAGES in exact arithmetic,
+ *           22 instead of 54 passes over the state per attempted step; in FP32 the
+ *           expanded polynomial rounds worse than the stages' nested evaluation on stiff
+ *           problems (up to ~5x the stage form's rounding error, still inside the solve's
+ *           tolerance), so it is an opt-in;
+ *   AUTO:   STAGES. */
 #define DQB_STEPPER_AUTO 0
 #define DQB_STEPPER_STAGES 1
 #define DQB_STEPPER_KRYLOV 2

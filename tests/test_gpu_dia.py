@@ -172,7 +172,11 @@ def test_rhs_dia_full_size_every_stencil(cuda_device, coupled_kerr_4096_rhs, til
     _lib.check(lib.dqb_lindblad_rhs_dia_tiled(p, _lib.FORM_HERMITIAN, tile, r_d.data_ptr(),
                                               out.data_ptr(), ws.data_ptr(), ws.numel(),
                                               torch.cuda.current_stream().cuda_stream), 'rhs_dia')
-    assert rel_frob(out[0].cpu().numpy(), ref) < 2e-6
+    got = out[0].cpu().numpy()
+    assert rel_frob(got, ref) < 2e-6
+    if tile >= 200:
+        # the wide kernel computes the upper triangle and mirrors it: hermitian to the bit
+        assert np.array_equal(got, np.conj(got.T))
 
 
 def test_dia_full_size_short_solve_vs_oracle(cuda_device):
@@ -218,15 +222,17 @@ def test_dia_path_dopri5_vs_oracle(cuda_device):
 @pytest.mark.parametrize('method', ['Tsit5', 'Dopri5'])
 @pytest.mark.parametrize('hermitian', [True, False])
 def test_krylov_stepper_vs_stages_and_oracle(cuda_device, method, hermitian):
-    """The Krylov form of the step (the DIA path's default) against the stage-by-stage
+    """The Krylov form of the step (an opt-in) against the stage-by-stage
     form (the reference's arithmetic, in the same FP32), on strongly driven coupled Kerr
     modes (n = 100) whose solves reject steps (a rejected step reuses its basis), with
     expectation values: step counts within two, states within the solve's tolerance of
     each other, and each form's error against a tight FP64 oracle solution (rtol and atol
-    1000 times smaller) no larger for the Krylov form than twice the stage form's.  (At
-    rtol 1e-4 over ~200 steps the FP32 rounding of either form, ~2e-5, exceeds the FP64
-    oracle's own error at the same tolerances, so the oracle-relative bar of the other
-    tests does not apply; the stage-form solves meet the parity bar in the tests above.)"""
+    1000 times smaller) inside the tolerance: the stage form within twice the FP64
+    oracle's own error, the Krylov form within max(2x the stage form's, rtol / 2).  On this
+    stiff problem the Krylov form's expanded polynomial rounds ~4x worse in FP32 than the
+    stages' nested evaluation (2.6e-5 against 6.0e-6 on the expectation values; a numpy
+    emulation in complex64 gives the same, in complex128 the two are equal), which is why
+    it is an opt-in."""
     w = workloads.coupled_kerr_dia(batch=2, m=10, seed=5, kerr=1.0, eps=3.0)
     m = (dq.Tsit5 if method == 'Tsit5' else dq.Dopri5)(rtol=1e-4, atol=1e-6)
     E = [np.diag(np.arange(100)).astype(np.complex64)]
@@ -251,5 +257,8 @@ def test_krylov_stepper_vs_stages_and_oracle(cuda_device, method, hermitian):
             ee = (np.abs(res.expects[b].cpu().numpy() - tight.expects)
                   / np.maximum(np.abs(tight.expects), 1.0)).max()
             err[name] = (es, ee)
-        assert err['krylov'][0] <= 2 * err['stages'][0] + 1e-6, err
-        assert err['krylov'][1] <= 2 * err['stages'][1] + 1e-6, err
+        ref_s = rel_frob(oracle_mesolve(H, Ls, w['rho0'], w['tsave'], method=method, rtol=m.rtol,
+                                        atol=m.atol).states, tight.states).max()
+        assert err['stages'][0] <= 2 * ref_s + 1e-6, (err, ref_s)
+        for i in (0, 1):
+            assert err['krylov'][i] <= max(2 * err['stages'][i], 0.5 * m.rtol), err

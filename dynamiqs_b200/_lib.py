@@ -34,6 +34,7 @@ INST_OK = 0
 INST_MAX_STEPS = 1
 INST_NONFINITE = 2
 INST_NOT_HERMITIAN = 3
+INST_CANCELLED = 4
 
 METHOD_TSIT5 = 0
 METHOD_DOPRI5 = 1
@@ -141,6 +142,7 @@ class RaggedInstance(ctypes.Structure):
         ('expects', ctypes.c_void_p),
         ('infos', ctypes.c_void_p),
         ('status', ctypes.c_void_p),
+        ('cancel', ctypes.c_void_p),
     ]
 
 

@@ -49,6 +49,7 @@ struct Inst {
   double2* eacc;
   int* infos;
   int* status_out;
+  const volatile int* cancel;  // ragged launches: the caller's stop word, or null
 };
 
 struct Common {
@@ -116,8 +117,10 @@ static __global__ void setup_kernel(Common c) {
     I.eacc = c.eacc + (long long)b * c.eacc_stride;
     I.infos = r.infos;
     I.status_out = r.status;
+    I.cancel = r.cancel;
     I.t = r.t0;
   } else {
+    I.cancel = nullptr;
     const long long ri = c.ridx ? c.ridx[b] : b;
     I.nts = c.ntsave;
     I.nE = c.nE;
@@ -391,6 +394,11 @@ static __global__ void control_kernel(Common c) {
   if (!I.run) return;
   if (I.nsteps >= c.o.max_steps) {
     I.status = DQB_INST_MAX_STEPS;
+    I.run = 0;
+    return;
+  }
+  if (I.cancel != nullptr && *I.cancel != 0) {  // a caller's stop request
+    I.status = DQB_INST_CANCELLED;
     I.run = 0;
     return;
   }
@@ -762,7 +770,8 @@ static __global__ void pre_finalize_kernel(Common c) {
 static __global__ void retire_kernel(Common c) {
   const int b = blockIdx.x;
   Inst& I = c.inst[b];
-  if (I.retired || I.run || I.status != DQB_INST_OK || I.save_idx < I.nts) return;
+  if (I.retired || I.run) return;
+  if (!(I.status == DQB_INST_OK && I.save_idx >= I.nts) && I.status != DQB_INST_CANCELLED) return;
   if (!I.save_states) {
     const float2* y = slot(c, b, I.sy);
     for (long long e = threadIdx.x; e < c.nn; e += blockDim.x) I.states[e] = y[e];

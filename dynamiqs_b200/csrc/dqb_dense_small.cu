@@ -1072,6 +1072,7 @@ __global__ void __launch_bounds__(kSmallThreads, NP == 64 ? 1 : (NP == 32 ? 3 : 
     v.expects = (float2*)r.expects;
     v.infos = r.infos;
     v.status = r.status;
+    v.cancel = r.cancel;
     v.inst = inst;
     v.n_jump = 0;
     v.jump_ts = nullptr;

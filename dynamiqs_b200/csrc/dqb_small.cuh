@@ -149,6 +149,7 @@ struct InstView {
   float2* expects;     // nE x ntsave
   int* infos;          // 3
   int* status;         // 1
+  const volatile int* cancel;  // nonzero: stop (ragged launches), or null
   long long inst;      // index of the instance in its batch
   int n_jump;          // discontinuity times (the controller's jump_ts)
   const double* jump_ts;
@@ -161,6 +162,7 @@ struct InstView {
 __device__ __forceinline__ InstView view_of(const DenseSmallArgs& a, long long inst) {
   InstView v;
   v.inst = inst;
+  v.cancel = nullptr;
   v.n_jump = a.td.n_jump;
   v.jump_ts = a.td.jump_ts;
   v.tape_cap = a.tape_cap;
@@ -340,6 +342,12 @@ __device__ void solve_one(Engine& eng, const InstView& a, const CtrlOpts& o, flo
     if (ctl.nsteps >= o.max_steps) {
       if (tid == 0) ctl.status = DQB_INST_MAX_STEPS;
       break;
+    }
+    if (a.cancel != nullptr && (ctl.nsteps & 15) == 0) {  // a caller's stop request
+      __syncthreads();  // every thread has read ctl before thread 0 may change it
+      if (tid == 0 && *a.cancel != 0) ctl.status = DQB_INST_CANCELLED;
+      __syncthreads();
+      if (ctl.status == DQB_INST_CANCELLED) break;
     }
     const double h = ctl.tnext - ctl.t;
     float2* yv = slot + ctl.sy * NN;

@@ -25,6 +25,12 @@ the rest of its wave (a quick request does not wait for a slow one launched with
 Tickets record submit, launch and completion times, from which :meth:`stats` reports
 solves/s and p50 / p99 latency.
 
+:meth:`Ticket.cancel` stops a request: a waiting one leaves the queue, a running one gets
+its cancel word (page-locked host memory, one per request, named in its kernel
+descriptor) set; the kernels read the word between RK steps and end the request with the
+cancelled status, which the dispatcher hands out like any other end.  The other requests
+of its wave are not affected (each instance is independent).
+
 CUDA maps streams onto ``CUDA_DEVICE_MAX_CONNECTIONS`` hardware queues (8 by default);
 streams that share a queue run one after the other.  Set it to at least the number of
 server streams (32 at most) before CUDA is initialised in the process, or a wave can
@@ -38,7 +44,7 @@ import dataclasses
 import threading
 import time
 from collections import deque
-from concurrent.futures import ThreadPoolExecutor
+from concurrent.futures import CancelledError, ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -56,6 +62,10 @@ __all__ = ['MESolveServer', 'Ticket']
 
 def _align(x: int) -> int:
     return (x + 255) & ~255
+
+
+# Per request, page-locked: step counts (3 int32), status word, cancel word, padding.
+_INFO = 32
 
 
 class _Arena:
@@ -118,9 +128,19 @@ class Ticket:
     _result: MESolveResult | None = None
     _error: BaseException | None = None
     _out: tuple | None = None  # (arena, offset, nbytes) of the result buffers
+    _server: object = None
+    _cancel_word: int | None = None  # index of the cancel word in the pinned int32 view
+    _cancel_requested: bool = False
 
     def done(self) -> bool:
         return self._event.is_set()
+
+    def cancel(self) -> bool:
+        """Stop the request.  A waiting request leaves the queue at once; a running one
+        stops at its next check (between RK steps) and its ticket then ends.  Either way
+        :meth:`result` raises ``concurrent.futures.CancelledError``.  Returns False when
+        the request had already finished."""
+        return self._server._cancel(self) if self._server is not None else False
 
     def result(self, timeout: float | None = None) -> MESolveResult:
         if not self._event.wait(timeout):
@@ -200,6 +220,7 @@ class MESolveServer:
         self._pending: dict[tuple, deque] = {}
         self._inflight: list[_Wave] = []
         self._lock = threading.Lock()
+        self._cancel_lock = threading.Lock()
         self._wake = threading.Condition(self._lock)
         self._closing = False
         self._next_id = 0
@@ -241,6 +262,7 @@ class MESolveServer:
                    Es=[to_dense(E).astype(np.complex64) for E in Es] if Es else None,
                    method=method, options=options)
         key = self._class_of(t)
+        t._server = self
         with self._lock:
             if self._closing:
                 raise RuntimeError('server is closed')
@@ -250,6 +272,21 @@ class MESolveServer:
             self._pending.setdefault(key, deque()).append(t)
             self._wake.notify()
         return t
+
+    def _cancel(self, t: Ticket) -> bool:
+        with self._lock:
+            if t._event.is_set():
+                return False
+            for q in self._pending.values():
+                if t in q:  # still waiting: leave the queue
+                    q.remove(t)
+                    self._fail([t], CancelledError(f'request {t.id} cancelled'))
+                    return True
+        with self._cancel_lock:  # launched, or being launched: the kernel stops it
+            t._cancel_requested = True
+            if t._cancel_word is not None:
+                self._host_i32[t._cancel_word] = 1
+        return True
 
     def close(self, wait: bool = True) -> None:
         with self._lock:
@@ -461,7 +498,7 @@ class MESolveServer:
                                    'E': put(max(sum(E.nbytes for E in t.Es), 8) if t.Es else 8),
                                    'tsave': put(t.tsave.nbytes)})
                 desc_off = put(ctypes.sizeof(_lib.RaggedInstance) * len(group))
-                info_off = put(16 * len(group))
+                info_off = put(_INFO * len(group))
                 in_bytes = off
                 maxK = max(len(t.Ls) for t in group)
                 count = len(group)
@@ -547,12 +584,20 @@ class MESolveServer:
                     # step counts and status go straight to page-locked host memory, which
                     # the device reaches through unified addressing: the dispatcher polls
                     # the status word and hands a result out as soon as it is written
-                    d.infos = host_in + info_off + 16 * i
-                    d.status = host_in + info_off + 16 * i + 12
+                    d.infos = host_in + info_off + _INFO * i
+                    d.status = host_in + info_off + _INFO * i + 12
+                    d.cancel = host_in + info_off + _INFO * i + 16
                     t.t_launch = now
                 raw = np.frombuffer(bytes(descs), dtype=np.uint8)
                 sv[desc_off:desc_off + raw.size] = raw
-                sv[info_off:info_off + 16 * len(group)].view(np.int32).reshape(-1, 4)[:, 3] = -1
+                words = sv[info_off:info_off + _INFO * len(group)].view(np.int32).reshape(-1, _INFO // 4)
+                words[:, 3] = -1  # status: not yet written
+                words[:, 4] = 0   # cancel word
+                with self._cancel_lock:  # a cancel() that came during the launch
+                    for i, t in enumerate(group):
+                        t._cancel_word = (h_in + info_off + _INFO * i + 16) // 4
+                        if t._cancel_requested:
+                            words[i, 4] = 1
                 count = len(group)
                 if key[0] == 'large':  # descriptors and live count go to the stream's slot
                     sv[info_off:info_off + 4] = np.array([count], np.int32).view(np.uint8)
@@ -587,7 +632,7 @@ class MESolveServer:
                     ex = self._dev_buf[o + sb:o + sb + nE * len(t.tsave) * 8]
                     outputs[t.id] = (st.view(torch.complex64).view(nsave, t.n, t.n),
                                      ex.view(torch.complex64).view(nE, len(t.tsave)) if nE else None)
-                    infos_host[t.id] = (h_in + info_off + 16 * i)
+                    infos_host[t.id] = (h_in + info_off + _INFO * i)
                     t._out = (self._dev, o, nb)
             t1 = time.perf_counter()
             ev = torch.cuda.Event()
@@ -677,6 +722,8 @@ class MESolveServer:
                                     'the integration.')
         elif status == _lib.INST_NOT_HERMITIAN:
             t._error = RuntimeError('Argument y0 is not hermitian.')
+        elif status == _lib.INST_CANCELLED:
+            t._error = CancelledError(f'request {t.id} cancelled')
         elif status != _lib.INST_OK:
             t._error = RuntimeError(f'request ended with status {status}')
         if t._error is not None:

@@ -48,6 +48,7 @@ extern "C" {
 #define DQB_INST_MAX_STEPS 1     /* diffrax "maximum number of method steps" error   */
 #define DQB_INST_NONFINITE 2     /* NaN/inf in the state or the error estimate       */
 #define DQB_INST_NOT_HERMITIAN 3 /* check_hermitian(rho0) failed (rtol = atol = 1e-5) */
+#define DQB_INST_CANCELLED 4     /* stopped by its ragged descriptor's cancel word      */
 
 /* ---- options ----------------------------------------------------------------- */
 #define DQB_METHOD_TSIT5 0
@@ -354,6 +355,12 @@ typedef struct dqb_ragged_instance {
   void* expects;
   int32_t* infos;
   int32_t* status;
+  /* NULL, or a word the caller may set nonzero at any time (page-locked host memory the
+   * device reaches through unified addressing, or device memory): the kernels read it
+   * between RK steps (every 16th step on the n <= 64 kernel, every step on the GEMM
+   * path) and end the instance with DQB_INST_CANCELLED, writing its counts and status as
+   * for any other end.  Its outputs are then incomplete. */
+  const volatile int32_t* cancel;
 } dqb_ragged_instance;
 
 /* Scratch bytes for dqb_mesolve_ragged. */

@@ -105,3 +105,50 @@ def test_quick_request_leaves_before_slow_one_of_its_wave(cuda_device):
         alone = dq.mesolve(r['H'], r['jump_ops'], r['rho0'], r['tsave'], method=r['method'])
         assert _rel(got.states.cpu().numpy(), alone.states.cpu().numpy()) < 1e-5
         assert int(got.infos.nsteps) == int(alone.infos.nsteps)
+
+
+def test_cancel_running_and_waiting_requests(cuda_device):
+    """Ticket.cancel(): a waiting request leaves the queue without launching; a running
+    request stops at its next check between RK steps (n <= 64 kernel and GEMM path), ends
+    with CancelledError soon after, and the other request of its wave is unaffected."""
+    import time
+    from concurrent.futures import CancelledError
+
+    from dynamiqs_b200 import operators as ops
+
+    def kerr(n, kerr_, t_end):
+        H = workloads.kerr_hamiltonians(n, [0.3], [kerr_], [1.0])[0]
+        a = ops.destroy(n, layout='dense')
+        return dict(H=H, jump_ops=[np.float32(np.sqrt(0.1)) * a], rho0=ops.fock(n, 0),
+                    tsave=np.linspace(0.0, t_end, 5), method=dq.Tsit5(rtol=1e-6, atol=1e-6))
+
+    srv = MESolveServer(n_streams=2)  # one stream per class
+    for n in (64, 80):
+        blocker, slow, quick = kerr(n, 0.1, 0.5), kerr(n, 0.5, 400.0), kerr(n, 0.1, 0.05)
+        # the blocker holds the class's only stream, so slow and quick form the next wave
+        ts = [srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'], method=r['method'])
+              for r in (blocker, slow, quick)]
+        t0 = time.perf_counter()
+        while ts[1].t_launch == 0.0 and time.perf_counter() - t0 < 120:
+            time.sleep(0.01)
+        assert ts[1].t_launch > 0.0 and ts[2].t_launch == ts[1].t_launch
+        # a request that arrives now waits: the class's stream runs the slow wave
+        waiting = srv.submit(quick['H'], quick['jump_ops'], quick['rho0'], quick['tsave'],
+                             method=quick['method'])
+        assert waiting.cancel()
+        with pytest.raises(CancelledError):
+            waiting.result(timeout=1)
+        assert waiting.t_launch == 0.0
+        got_quick = ts[2].result(timeout=600)
+        t_cancel = time.perf_counter()
+        assert ts[1].cancel()
+        with pytest.raises(CancelledError):
+            ts[1].result(timeout=60)
+        assert ts[1].t_done - t_cancel < 5.0
+        assert not ts[1].cancel()  # already finished
+        alone = dq.mesolve(quick['H'], quick['jump_ops'], quick['rho0'], quick['tsave'],
+                           method=quick['method'])
+        assert _rel(got_quick.states.cpu().numpy(), alone.states.cpu().numpy()) < 1e-5
+        for t in (ts[0], ts[2]):
+            t.release()
+    srv.close()

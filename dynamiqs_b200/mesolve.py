@@ -873,6 +873,10 @@ def _mesolve_piecewise(H, jump_ops, rho0, tsave, *, exp_ops, method, gradient, o
     tsave = check_times(np.asarray(tsave.detach().cpu().numpy() if hasattr(tsave, 'detach')
                                    else tsave, dtype=np.float64), 'tsave')
     t0 = float(tsave[0] if options.t0 is None else options.t0)
+    if t0 > tsave[0]:
+        # the pieces start at t0: save points before it would be dropped silently
+        raise ValueError(f'Option `t0` ({t0}) must not be after the first save time '
+                         f'tsave[0] ({tsave[0]}) with a piecewise-constant Hamiltonian.')
     piece_opts = dataclasses.replace(options, t0=None)
     states, expects, infos = [], [], None
     state = rho0

@@ -52,6 +52,7 @@ class PWCTimeQArray:
                              f'{values.shape}.')
         self.times = times
         self.values = values.astype(np.complex128)
+        self.source = qarray  # as given (a SparseDIA stays sparse in the piecewise path)
         self.qarray = _dense_op(qarray)
         if self.qarray.ndim != 2 or self.qarray.shape[0] != self.qarray.shape[1]:
             raise ValueError('Argument `qarray` must be a square (n, n) operator.')
@@ -72,7 +73,7 @@ class PWCTimeQArray:
             return self
         tail = idx[len(idx) - len(bs):]
         sub = self.values[tuple(0 if size == 1 else i for i, size in zip(tail, bs))]
-        return PWCTimeQArray(self.times, sub, self.qarray)
+        return PWCTimeQArray(self.times, sub, self.source)
 
     @property
     def discontinuity_ts(self) -> np.ndarray:
@@ -136,6 +137,7 @@ class ModulatedTimeQArray:
                 '`Wave` (amplitude, omega, phase, optional Gaussian envelope and support); an '
                 'arbitrary Python callable cannot run inside a kernel.')
         self.f = f
+        self.source = qarray
         self.qarray = _dense_op(qarray)
         if self.qarray.ndim != 2 or self.qarray.shape[0] != self.qarray.shape[1]:
             raise ValueError('Argument `qarray` must be a square (n, n) operator.')
@@ -183,7 +185,8 @@ class SummedTimeQArray:
         for t in terms:
             flat.extend(t.terms if isinstance(t, SummedTimeQArray) else [t])
         self.pwc_terms = [t for t in flat if isinstance(t, _TD_TYPES)]
-        const = [_dense_op(t) for t in flat if not isinstance(t, _TD_TYPES)]
+        self._const_src = [t for t in flat if not isinstance(t, _TD_TYPES)]
+        const = [_dense_op(t) for t in self._const_src]
         n = (self.pwc_terms[0].shape if self.pwc_terms else const[0].shape)[-1]
         for c in const:
             if c.ndim != 2:
@@ -209,7 +212,28 @@ class SummedTimeQArray:
 
     def item(self, idx: tuple) -> SummedTimeQArray:
         """The unbatched operator at index ``idx`` of :attr:`batch_shape`."""
-        return SummedTimeQArray([self.constant] + [t.item(idx) for t in self.pwc_terms])
+        const = self._const_src if self.is_dia else [self.constant]
+        return SummedTimeQArray(list(const) + [t.item(idx) for t in self.pwc_terms])
+
+    @property
+    def is_dia(self) -> bool:
+        """Every term (constant or time-dependent) is a SparseDIA operator."""
+        return (all(isinstance(c, SparseDIA) for c in self._const_src)
+                and all(isinstance(t.source, SparseDIA) for t in self.pwc_terms))
+
+    def piece(self, t: float):
+        """The constant operator at time ``t``: a SparseDIA (diagonals summed over the
+        terms) when every term is one, so that a piece's solve stays on the DIA path, else
+        a dense array."""
+        if not self.is_dia:
+            return self(t)
+        out = None
+        for c in self._const_src:
+            out = c if out is None else out + c
+        for term in self.pwc_terms:
+            x = term.source * np.complex64(term.prefactor(t))
+            out = x if out is None else out + x
+        return out.astype(np.complex64)
 
     @property
     def td_terms(self) -> list:
@@ -267,5 +291,5 @@ def piecewise_plan(H: SummedTimeQArray, tsave: np.ndarray, t0: float):
         inside = [float(t) for t in tsave if (a < t <= b) or (i == 0 and t == a)]
         ts = sorted(set([a, b] + inside))
         keep = [ts.index(t) for t in inside]
-        plan.append((a, b, H(0.5 * (a + b)), np.asarray(ts), keep))
+        plan.append((a, b, H.piece(0.5 * (a + b)), np.asarray(ts), keep))
     return plan

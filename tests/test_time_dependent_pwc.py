@@ -107,6 +107,15 @@ def test_piecewise_driver_with_oracle_matches_exact():
     assert int(r.infos.nsteps) > 0
 
 
+def test_piecewise_rejects_t0_after_first_save():
+    """Pieces start at t0: a t0 after tsave[0] would drop save points silently, so it is
+    an error."""
+    H, H0, drive, L, rho0, E = _system()
+    with pytest.raises(ValueError, match='must not be after the first save time'):
+        _mesolve_piecewise(H, L, rho0, TSAVE, exp_ops=E, method=dq.Tsit5(), gradient=None,
+                           options=dq.Options(t0=float(TSAVE[1])), solve=_oracle_solve)
+
+
 @pytest.mark.gpu
 def test_pwc_mesolve_on_gpu_matches_exact(cuda_device):
     H, H0, drive, L, rho0, E = _system()
@@ -209,3 +218,22 @@ def test_wave_prefactor_semantics():
     with pytest.raises(NotImplementedError, match='Wave'):
         dq.modulated(lambda t: np.cos(t), np.eye(2))
 
+
+
+def test_dia_terms_stay_sparse_in_pieces():
+    """A piecewise-constant H whose every term is a SparseDIA operator gives SparseDIA
+    pieces (the sum of the terms' diagonals), so each piece's solve runs on the DIA path;
+    their dense form equals the dense evaluation of H at the piece's midpoint."""
+    from dynamiqs_b200.qarrays import SparseDIA
+
+    a = ops.destroy(6, layout='dia')
+    H = (a.dag() @ a) * np.float32(0.5) + dq.pwc([0.0, 1.0, 2.0], [0.3, -0.7], a + a.dag())
+    Hs = as_summed(H)
+    assert Hs.is_dia
+    plan = piecewise_plan(Hs, np.linspace(0.0, 2.0, 5), 0.0)
+    assert len(plan) == 2
+    for (a_, b_, Hp, _, _) in plan:
+        assert isinstance(Hp, SparseDIA)
+        np.testing.assert_allclose(Hp.to_dense(), Hs(0.5 * (a_ + b_)), rtol=1e-6, atol=1e-6)
+    dense = as_summed(np.asarray((a.dag() @ a).to_dense()) + dq.pwc([0.0, 1.0], [1.0], a))
+    assert not dense.is_dia

@@ -616,6 +616,7 @@ __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c
     }
 #pragma unroll
     for (int q = 0; q < C; ++q) acc[q] = make_float2(acc[q].x * scale, acc[q].y * scale);
+    if (HERM && j <= i && i < j + C) acc[i - j].y = 0.f;  // a hermitian matrix's diagonal is real
     float2* orow = out + (long long)i * n + j;
     if (!HERM || j >= i) {  // every column on or above the diagonal
 #pragma unroll

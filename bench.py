@@ -434,14 +434,16 @@ def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which, nsave=0
 #     for 148 = 2.837 MB; inputs, states and expectation values, the RK slots stay in L2);
 #     profiles/mesolve_small_kernel_n64_kerr.md.
 #   dia / fp32, stage form: per attempted RK step of one instance (every kernel of the
-#     stepper, host loop: 7.19 GB = 54 passes over the 134 MB matrix) plus 1.22 GB per save
-#     point; profiles/dia_stepper_n4096_coupled_kerr_traffic.md.
+#     stepper, host loop: six stage combinations 4.20 GB, six hermitian-half stencils
+#     0.92 GB, the error pass 1.21 GB: 6.33 GB) plus 1.34 GB per save point (the save pass
+#     reads y and the seven stages once, writes the state);
+#     profiles/rhs_dia_wide_kernel_n4096_coupled_kerr.md.
 #   dia / fp32, Krylov form: 1.387 GB per accepted step (six basis stencils, 134.6 MB read
 #     + 96.5 MB written each), 1.324 GB per attempt (the combination pass: 1073.8 MB read,
 #     249.7 MB written) and 1.34 GB per save point; profiles/dia_krylov_n4096_coupled_kerr.md.
 TRAFFIC_PER_UNIT = {
     ('kerr', 'fp32', 'auto'): ('instance', 2.837e6, 0.0, 0.0),
-    ('dia', 'fp32', 'stages'): ('instance_step', 7.19e9, 0.0, 1.22e9),
+    ('dia', 'fp32', 'stages'): ('instance_step', 6.33e9, 0.0, 1.34e9),
     ('dia', 'fp32', 'krylov'): ('instance_step', 1.324e9, 1.387e9, 1.34e9),
 }
 

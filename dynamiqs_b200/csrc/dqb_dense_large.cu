@@ -332,13 +332,13 @@ constexpr int kProd = kProdWarps * 32;
 constexpr int kThreads = kProd + 32;
 constexpr uint32_t kAccCols = 256;             // one FP32 accumulator: 128 lanes x 256 columns
 // Stage geometry for a K-slice of RB bytes of every operand row (RB = 128: 128-byte
-// swizzle, 96 KB stages; RB = 64: 64-byte swizzle, 48 KB stages) and ST stages.
-template <int RB, int ST = (RB == 128 ? 2 : 4)>
+// swizzle, two 96 KB stages; RB = 64: 64-byte swizzle, four 48 KB stages).
+template <int RB>
 struct Cfg {
   static constexpr uint32_t kA = 128 * RB;                // one 128-row operand tile (bytes)
   static constexpr uint32_t kB = 256 * RB;                // one 256-row operand tile
   static constexpr uint32_t kStage = 2 * kA + 2 * kB;     // A hi, A lo, B hi, B lo
-  static constexpr int kStages = ST;
+  static constexpr int kStages = RB == 128 ? 2 : 4;
   static constexpr int kSmem = kStages * kStage + 1024;   // + alignment slack
   static constexpr int kChunks = RB / 16;                 // 16-byte chunks per tile row
   static constexpr int kJobs = 128 * kChunks / kProd;     // chunks of A (and of M) per producer
@@ -464,18 +464,15 @@ __device__ __forceinline__ void tc_store_stage(const float4 (&v)[(BF16 ? 4 : 2) 
 // semantics as cgemm_kernel, restricted to terms A M^+ (opA = 0; opB = 1, or B = the
 // hermitian stage input) with one alpha; on a wait that runs out the tile is written as
 // NaN, which the error norm turns into DQB_INST_NONFINITE.
-// DUAL: two CTAs per SM, so that one CTA's prologue and epilogue overlap the other's
-// main loop -- 64-byte slices in two 48 KB stages, and the small cross products
-// accumulated into the same TMEM accumulator as hi*hi (256 columns per CTA).
-template <int PREC, int RB, bool DUAL>
-__global__ void __launch_bounds__(tcg::kThreads, DUAL ? 2 : 1)
+template <int PREC, int RB>
+__global__ void __launch_bounds__(tcg::kThreads, 1)
     tc_cgemm_kernel(big::Common c, LargeOps d, GemmJob job, const float2* ext_in, float2* ext_out) {
-  using Cf = tcg::Cfg<RB, DUAL ? 2 : (RB == 128 ? 2 : 4)>;
+  using Cf = tcg::Cfg<RB>;
   constexpr bool kBf16 = PREC == DQB_PREC_BF16X3;
   constexpr bool kSplit = PREC != DQB_PREC_TF32;
   constexpr int KC = kBf16 ? RB / 4 : RB / 8;  // complex contraction values per stage
   constexpr int NV = (kBf16 ? 4 : 2) * Cf::kJobs;
-  constexpr uint32_t kCols = (kSplit && !DUAL) ? 2 * tcg::kAccCols : tcg::kAccCols;
+  constexpr uint32_t kCols = kSplit ? 2 * tcg::kAccCols : tcg::kAccCols;
   extern __shared__ uint8_t tc_dsm[];
   __shared__ uint64_t bars[2 * Cf::kStages + 1];
   __shared__ uint32_t tmem_sh;
@@ -534,7 +531,7 @@ __global__ void __launch_bounds__(tcg::kThreads, DUAL ? 2 : 1)
     // ---- producers ----
     // Global loads run PRE stages ahead of the shared-memory stores (as many as the
     // registers hold: two 128-byte TF32 stages or one BF16 stage; twice that for 64 bytes).
-    constexpr int PRE = DUAL ? (kBf16 ? 1 : 2) : (kBf16 ? 1 : 2) * (128 / RB);
+    constexpr int PRE = (kBf16 ? 1 : 2) * (128 / RB);
     const int ptid = threadIdx.x;
     float4 buf[PRE + 1][NV];
 #pragma unroll
@@ -578,15 +575,15 @@ __global__ void __launch_bounds__(tcg::kThreads, DUAL ? 2 : 1)
         const uint64_t bh = Cf::desc(st + 2 * Cf::kA + kk * 32);
         const uint64_t bl = Cf::desc(st + 2 * Cf::kA + Cf::kB + kk * 32);
         const uint32_t acc = (it | kk) ? 1u : 0u;
-        const uint32_t small = DUAL ? tmem : tmem + tcg::kAccCols;
+        const uint32_t small = tmem + tcg::kAccCols;
         if (kBf16) {
           tc::mma_bf16(small, al, bh, idesc, acc);
           tc::mma_bf16(small, ah, bl, idesc, 1u);
-          tc::mma_bf16(tmem, ah, bh, idesc, DUAL ? 1u : acc);
+          tc::mma_bf16(tmem, ah, bh, idesc, acc);
         } else if (kSplit) {
           tc::mma_tf32(small, al, bh, idesc, acc);
           tc::mma_tf32(small, ah, bl, idesc, 1u);
-          tc::mma_tf32(tmem, ah, bh, idesc, DUAL ? 1u : acc);
+          tc::mma_tf32(tmem, ah, bh, idesc, acc);
         } else {
           tc::mma_tf32(tmem, ah, bh, idesc, acc);
         }
@@ -622,7 +619,7 @@ __global__ void __launch_bounds__(tcg::kThreads, DUAL ? 2 : 1)
       if (!bad && total > 0) {
         const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)fcol;
         tc::tmem_ld16(ta, v);
-        if (kSplit && !DUAL) {
+        if (kSplit) {
           float w[16];
           tc::tmem_ld16(ta + tcg::kAccCols, w);
           tc::tmem_ld_wait();
@@ -675,36 +672,31 @@ bool use_tc(const LargeOps& d, int form) {
   return d.prec != DQB_PREC_FP32 && form == DQB_FORM_HERMITIAN && (d.n % 2) == 0;
 }
 
-// Pipeline of the tensor-core GEMM, read once from DQB_TC_SLICE: "128" (default: 128-byte
-// K-slices, two 96 KB stages, one CTA per SM), "64" (64-byte slices, four 48 KB stages) or
-// "64x2" (64-byte slices, two stages, two CTAs per SM with one accumulator each).  The
-// 128-byte slice measured faster than "64": 67.3 against 50.4 solves/s on the transmon x
-// cavity workload (n = 256, 3xTF32), the shorter slice doubling the barrier round trips
-// and MMA issues per byte.
-inline int tc_mode() {
-  static const int m = [] {
+// K-slice of the tensor-core GEMM's stages: 128 bytes (two 96 KB stages) unless
+// DQB_TC_SLICE=64 in the environment (four 48 KB stages), read once.  The 128-byte slice is
+// the faster one: 67.3 against 50.4 solves/s on the transmon x cavity workload (n = 256,
+// 3xTF32), as the shorter slice doubles the barrier round trips and MMA issues per byte.
+inline int tc_slice() {
+  static const int rb = [] {
     const char* v = std::getenv("DQB_TC_SLICE");
-    if (v == nullptr) return 0;
-    if (std::strcmp(v, "64") == 0) return 1;
-    if (std::strcmp(v, "64x2") == 0) return 2;
-    return 0;
+    return (v != nullptr && std::atoi(v) == 64) ? 64 : 128;
   }();
-  return m;
+  return rb;
 }
 
-template <int RB, bool DUAL>
+template <int RB>
 void launch_tc(cudaStream_t s, dim3 g, const big::Common& c, const LargeOps& d, const GemmJob& j,
                const float2* ext_in, float2* ext_out) {
-  constexpr int sm = tcg::Cfg<RB, DUAL ? 2 : (RB == 128 ? 2 : 4)>::kSmem;
+  constexpr int sm = tcg::Cfg<RB>::kSmem;
   switch (d.prec) {
     case DQB_PREC_TF32X3:
-      tc_cgemm_kernel<DQB_PREC_TF32X3, RB, DUAL><<<g, tcg::kThreads, sm, s>>>(c, d, j, ext_in, ext_out);
+      tc_cgemm_kernel<DQB_PREC_TF32X3, RB><<<g, tcg::kThreads, sm, s>>>(c, d, j, ext_in, ext_out);
       break;
     case DQB_PREC_BF16X3:
-      tc_cgemm_kernel<DQB_PREC_BF16X3, RB, DUAL><<<g, tcg::kThreads, sm, s>>>(c, d, j, ext_in, ext_out);
+      tc_cgemm_kernel<DQB_PREC_BF16X3, RB><<<g, tcg::kThreads, sm, s>>>(c, d, j, ext_in, ext_out);
       break;
     default:
-      tc_cgemm_kernel<DQB_PREC_TF32, RB, DUAL><<<g, tcg::kThreads, sm, s>>>(c, d, j, ext_in, ext_out);
+      tc_cgemm_kernel<DQB_PREC_TF32, RB><<<g, tcg::kThreads, sm, s>>>(c, d, j, ext_in, ext_out);
       break;
   }
 }
@@ -714,11 +706,10 @@ void launch_gemm(cudaStream_t s, const big::Common& c, const LargeOps& d, const 
   if (tcp) {
     const int t = (d.n + 127) / 128;
     const dim3 g(t * t, 1, zdim);
-    switch (tc_mode()) {
-      case 1: launch_tc<64, false>(s, g, c, d, j, ext_in, ext_out); break;
-      case 2: launch_tc<64, true>(s, g, c, d, j, ext_in, ext_out); break;
-      default: launch_tc<128, false>(s, g, c, d, j, ext_in, ext_out);
-    }
+    if (tc_slice() == 128)
+      launch_tc<128>(s, g, c, d, j, ext_in, ext_out);
+    else
+      launch_tc<64>(s, g, c, d, j, ext_in, ext_out);
   } else {
     const int t = (d.n + BM - 1) / BM;
     cgemm_kernel<<<dim3(t * t, 1, zdim), NT, 0, s>>>(c, d, j, ext_in, ext_out);
@@ -879,15 +870,12 @@ static void init_carveouts() {
       prefer_max_shared(kern);
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     };
-    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32X3, 128, false>, tcg::Cfg<128>::kSmem);
-    tc_attrs(tc_cgemm_kernel<DQB_PREC_BF16X3, 128, false>, tcg::Cfg<128>::kSmem);
-    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32, 128, false>, tcg::Cfg<128>::kSmem);
-    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32X3, 64, false>, tcg::Cfg<64>::kSmem);
-    tc_attrs(tc_cgemm_kernel<DQB_PREC_BF16X3, 64, false>, tcg::Cfg<64>::kSmem);
-    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32, 64, false>, tcg::Cfg<64>::kSmem);
-    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32X3, 64, true>, tcg::Cfg<64, 2>::kSmem);
-    tc_attrs(tc_cgemm_kernel<DQB_PREC_BF16X3, 64, true>, tcg::Cfg<64, 2>::kSmem);
-    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32, 64, true>, tcg::Cfg<64, 2>::kSmem);
+    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32X3, 128>, tcg::Cfg<128>::kSmem);
+    tc_attrs(tc_cgemm_kernel<DQB_PREC_BF16X3, 128>, tcg::Cfg<128>::kSmem);
+    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32, 128>, tcg::Cfg<128>::kSmem);
+    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32X3, 64>, tcg::Cfg<64>::kSmem);
+    tc_attrs(tc_cgemm_kernel<DQB_PREC_BF16X3, 64>, tcg::Cfg<64>::kSmem);
+    tc_attrs(tc_cgemm_kernel<DQB_PREC_TF32, 64>, tcg::Cfg<64>::kSmem);
   });
 }
 

@@ -51,7 +51,7 @@ import numpy as np
 
 from . import _lib
 from .mesolve import (_as_op, _check_mesolve_args, _MAX_STEPS_MSG, _precision_code,
-                      assert_method_supported, check_times)
+                      _stepper_code, assert_method_supported, check_times)
 from .method import Tsit5
 from .options import Options, check_options
 from .qarrays import to_dense
@@ -456,7 +456,7 @@ class MESolveServer:
             factormin=float(m.min_factor), factormax=float(m.max_factor),
             max_steps=int(m.max_steps), t0=0.0, save_states=1,
             check_hermitian=int(bool(o.assume_hermitian)),
-            precision=self._precision_of(t, form, count))
+            precision=self._precision_of(t, form, count), stepper=_stepper_code(o))
 
     def _launch_wave(self, tickets, key, stream) -> _Wave | None:
         """Pack the wave's inputs into pinned staging (one host-to-device copy), give every
@@ -469,7 +469,8 @@ class MESolveServer:
             groups.setdefault((type(t.method), t.method.rtol, t.method.atol,
                                t.method.safety_factor, t.method.min_factor, t.method.max_factor,
                                t.method.max_steps, t.options.assume_hermitian,
-                               t.options.vectorized, t.options.precision), []).append(t)
+                               t.options.vectorized, t.options.precision,
+                               t.options.stepper), []).append(t)
         held = []  # (arena, offset, nbytes) released when the wave retires
         outs_held = {}  # per ticket output region
         plans = []

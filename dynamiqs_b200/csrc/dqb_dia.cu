@@ -499,7 +499,7 @@ __device__ __forceinline__ void wide_load(const float2* __restrict__ rp, int col
 // position, through a shared-memory strip of the CTA's R x (128 C) outputs so that the
 // mirrored rows leave as contiguous R-value segments.  About half the stencil work, and
 // the output is hermitian to the last bit.
-template <int R, int NR, int NP, int C, bool HERM>
+template <int R, int NR, int NP, int C, bool HERM, int U = 1>
 __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c, DiaOps d, DiaWide w, int in_sel,
                                                                   int out_k, int need_run, int kry,
                                                                   const float2* ext_in, float2* ext_out) {
@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c
     }
   }
 
-#pragma unroll 1
+#pragma unroll U  // U = 2: two rows' loads in flight per thread
   for (int r = 0; r < rows; ++r) {
     const int i = i0 + r;
     if (HERM && j + C - 1 < i) break;  // this and the later rows lie below the diagonal
@@ -840,15 +840,17 @@ int wide_np(int np) { return np <= 2 ? 2 : 4; }
 
 // Shape codes of the wide kernel: 200 + R (C = 4 columns per thread) or 300 + R (C = 2),
 // R = 8 or 16 rows per CTA.
-bool is_wide(int rows) { return rows == 208 || rows == 216 || rows == 308 || rows == 316; }
-int wide_c(int rows) { return rows >= 300 ? 2 : 4; }
+bool is_wide(int rows) {
+  return rows == 208 || rows == 216 || rows == 308 || rows == 316 || rows == 408 || rows == 508;
+}
+int wide_c(int rows) { return (rows / 100) % 2 == 1 ? 2 : 4; }  // 2xx, 4xx: 4; 3xx, 5xx: 2
 int wide_r(int rows) { return rows % 100; }
 
 // Launch shape of the stencil from `tile`: 4, 8 or 16 = the tiled kernel with that many rows
 // per thread (when the operators have at most kTiledMaxTerms diagonal terms); 108 or 116 =
 // the staged kernel with 8 or 16 rows per CTA (when its plan fits); 208 or 216 (4 columns
-// per thread), 308 or 316 (2 columns) = the wide kernel with 8 or 16 rows per CTA (when
-// its plan fits); anything else (0 =
+// per thread), 308 or 316 (2 columns) = the wide kernel with 8 or 16 rows per CTA, 408 /
+// 508 = 8 rows with two rows in flight per thread (when its plan fits); anything else (0 =
 // default, 1) = the generic kernel.  The autotuner picks among them per problem shape.
 // Returns the shape code (1 = generic).
 int rows_for(const DiaOps& d, int tile) {
@@ -874,32 +876,32 @@ dim3 rhs_grid(const DiaOps& d, int rows, int B) {
   return dim3((d.n + kRhsCols - 1) / kRhsCols, (d.n + r - 1) / r, B);
 }
 
-template <int R, int C, bool HERM>
+template <int R, int C, bool HERM, int U>
 void launch_wide_form(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, const DiaWide& w,
                       int in_sel, int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out) {
   const int nr = wide_nr(w.nr), np = wide_np(w.np);
   const size_t sm = HERM ? (size_t)R * (kRhsCols * C + 1) * sizeof(float2) : 0;
   if (nr == 4 && np == 2)
-    rhs_dia_wide_kernel<R, 4, 2, C, HERM><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in,
-                                                                 ext_out);
+    rhs_dia_wide_kernel<R, 4, 2, C, HERM, U><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
+                                                                    ext_in, ext_out);
   else if (nr == 4)
-    rhs_dia_wide_kernel<R, 4, 4, C, HERM><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in,
-                                                                 ext_out);
+    rhs_dia_wide_kernel<R, 4, 4, C, HERM, U><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
+                                                                    ext_in, ext_out);
   else if (np == 2)
-    rhs_dia_wide_kernel<R, 8, 2, C, HERM><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in,
-                                                                 ext_out);
+    rhs_dia_wide_kernel<R, 8, 2, C, HERM, U><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
+                                                                    ext_in, ext_out);
   else
-    rhs_dia_wide_kernel<R, 8, 4, C, HERM><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry, ext_in,
-                                                                 ext_out);
+    rhs_dia_wide_kernel<R, 8, 4, C, HERM, U><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
+                                                                    ext_in, ext_out);
 }
 
-template <int R, int C>
+template <int R, int C, int U = 1>
 void launch_wide(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, const DiaWide& w, int in_sel,
                  int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out, bool herm) {
   if (herm)
-    launch_wide_form<R, C, true>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
+    launch_wide_form<R, C, true, U>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
   else
-    launch_wide_form<R, C, false>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
+    launch_wide_form<R, C, false, U>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
 }
 
 // One right-hand side of every instance: k[out_k] = f(input), through the kernel the shape
@@ -915,6 +917,8 @@ void launch_rhs_dia(cudaStream_t s, const big::Common& c, const DiaOps& d, int B
       case 208: launch_wide<8, 4>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm); break;
       case 216: launch_wide<16, 4>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm); break;
       case 308: launch_wide<8, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm); break;
+      case 408: launch_wide<8, 4, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm); break;
+      case 508: launch_wide<8, 2, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm); break;
       default: launch_wide<16, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm);
     }
     return;

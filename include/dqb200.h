@@ -90,7 +90,8 @@ typedef struct dqb_ode_options {
                               tiled kernel with that many rows per thread; 108 or 116 =
                               staged kernel with 8 or 16 rows per CTA; 208 or 216 (4
                               columns per thread), 308 or 316 (2 columns) = wide kernel
-                              with 8 or 16 rows per CTA; 0 (default) or 1 = generic
+                              with 8 or 16 rows per CTA, 408 / 508 = 8 rows with two
+                              rows in flight per thread; 0 (default) or 1 = generic
                               kernel; shapes that do not fit the operators fall back to
                               the generic kernel; ignored by other paths                  */
   int32_t stepper;         /* DQB_STEPPER_* (0 = AUTO): how the sparse-DIA and dense GEMM

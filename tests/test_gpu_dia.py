@@ -51,7 +51,7 @@ def _problem_struct(H, Ls, n, batch):
     return p, [h_off, l_nd, l_off, H_d, L_d]
 
 
-@pytest.mark.parametrize('tile', [0, 8, 108, 116, 208, 316])
+@pytest.mark.parametrize('tile', [0, 8, 108, 116, 208, 316, 408, 508])
 @pytest.mark.parametrize('form', [_lib.FORM_HERMITIAN, _lib.FORM_STANDARD])
 @pytest.mark.parametrize('n', [10, 77, 300])
 def test_rhs_dia_matches_oracle(cuda_device, form, n, tile):
@@ -156,7 +156,7 @@ def coupled_kerr_4096_rhs():
     return w, X, ref
 
 
-@pytest.mark.parametrize('tile', [0, 4, 8, 16, 108, 116, 208, 216, 308, 316])
+@pytest.mark.parametrize('tile', [0, 4, 8, 16, 108, 116, 208, 216, 308, 316, 408, 508])
 def test_rhs_dia_full_size_every_stencil(cuda_device, coupled_kerr_4096_rhs, tile):
     """One right-hand side at n = 4096 with the workload's own offsets (+-63/+-64 select
     other row groups in the staged kernel and other halos in the tiled one than the small

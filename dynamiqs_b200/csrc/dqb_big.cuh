@@ -306,6 +306,149 @@ static __global__ void error_kernel(Common c) {
   block_atomic_add(s, &I.acc[0], red);
 }
 
+// ------------------------------------------------------------------------------------
+// hermitian-form elementwise kernels: upper-triangle tiles, mirrored writes
+// ------------------------------------------------------------------------------------
+//
+// In the hermitian form every matrix the stepper combines -- y, the stages k_j (the
+// right-hand sides write exactly hermitian outputs), the stage inputs, y1 and the Krylov
+// basis -- is hermitian, so an elementwise pass needs to read only the tiles on and above
+// the diagonal: each CTA takes one 32 x 32 tile (ti <= tj), computes it, writes it, and for
+// ti < tj writes its conjugate transpose to tile (tj, ti) through shared memory (rows of 32
+// contiguous values both ways).  Reads fall to a little over half; writes are unchanged.
+// Diagonal tiles are computed whole and not mirrored.  Sums over all elements (the error
+// norm) weight an off-diagonal tile twice: its mirror has the same magnitudes.
+// grid (T (T + 1) / 2, B) with T = ceil(n / 32), 256 threads (32 x 8, 4 rows each).
+
+constexpr int kHT = 32;
+
+__device__ __forceinline__ int herm_row_start(int r, int T) { return r * T - r * (r - 1) / 2; }
+
+__device__ __forceinline__ void herm_tile(int t, int T, int& ti, int& tj) {
+  // t-th upper tile in row-major order of the upper triangle: row r holds T - r tiles and
+  // starts at r T - r (r - 1) / 2; the root of that quadratic, then exact integer fix-ups
+  const float b = 2.f * T + 1.f;
+  int r = (int)((b - sqrtf(fmaxf(b * b - 8.f * t, 0.f))) * 0.5f);
+  r = r < 0 ? 0 : (r > T - 1 ? T - 1 : r);
+  while (r > 0 && herm_row_start(r, T) > t) --r;
+  while (r < T - 1 && herm_row_start(r + 1, T) <= t) ++r;
+  ti = r;
+  tj = r + (t - herm_row_start(r, T));
+}
+
+// Writes v (this thread's tile values, rows ly + 8q) at tile (ti, tj) and, for ti < tj, its
+// conjugate transpose at (tj, ti).  `sh` is a 32 x 33 shared tile.
+__device__ __forceinline__ void herm_store(float2* __restrict__ out, int n, int ti, int tj, const float2 (&v)[4],
+                                           float2 (*sh)[kHT + 1]) {
+  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+  const int c = tj * kHT + lx;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int r = ti * kHT + ly + 8 * q;
+    if (r < n && c < n) out[(long long)r * n + c] = v[q];
+  }
+  if (ti == tj) return;  // uniform over the block
+  __syncthreads();       // the tile is free (a previous use has been read)
+#pragma unroll
+  for (int q = 0; q < 4; ++q) sh[ly + 8 * q][lx] = v[q];
+  __syncthreads();
+  // row tj*32 + ly + 8q of the output takes column (ly + 8q) of the tile, conjugated
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int r = tj * kHT + ly + 8 * q, cc = ti * kHT + lx;
+    if (r < n && cc < n) out[(long long)r * n + cc] = cconj(sh[lx][ly + 8 * q]);
+  }
+}
+
+// combine_kernel for the hermitian form (same modes).
+static __global__ void combine_h_kernel(Common c, int mode) {
+  __shared__ float2 sh[kHT][kHT + 1];
+  const int b = blockIdx.y;
+  const Inst& I = c.inst[b];
+  if (mode == 6) {
+    if (I.status != DQB_INST_OK) return;
+  } else if (!I.run) {
+    return;
+  }
+  const Tableau& Tb = c_tab[c.o.method];
+  float cf[6];
+  int nterm;
+  if (mode == 6) {
+    cf[0] = (float)I.h0;
+    nterm = 1;
+  } else if (mode == 5) {
+    for (int j = 0; j < 6; ++j) cf[j] = (float)(I.h * Tb.b[j]);
+    nterm = 6;
+  } else {
+    for (int j = 0; j < 6; ++j) cf[j] = (float)(I.h * Tb.a[mode + 1][j]);
+    nterm = mode + 1;
+  }
+  const int n = c.n, T = (n + kHT - 1) / kHT;
+  int ti, tj;
+  herm_tile(blockIdx.x, T, ti, tj);
+  const float2* y = slot(c, b, I.sy);
+  const float2* k[6];
+  for (int j = 0; j < 6; ++j) k[j] = slot(c, b, I.sk[j]);
+  float2* out = slot(c, b, mode == 5 ? I.sy1 : kX);
+  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+  const int col = tj * kHT + lx;
+  float2 v[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int r = ti * kHT + ly + 8 * q;
+    float2 x = make_float2(0.f, 0.f);
+    if (r < n && col < n) {
+      const long long e = (long long)r * n + col;
+      x = y[e];
+#pragma unroll
+      for (int j = 0; j < 6; ++j)
+        if (j < nterm) x = caxpy(cf[j], k[j][e], x);
+    }
+    v[q] = x;
+  }
+  herm_store(out, n, ti, tj, v, sh);
+}
+
+// error_kernel for the hermitian form: the same FP64 sum, off-diagonal tiles counted twice.
+static __global__ void error_h_kernel(Common c) {
+  __shared__ double red[40];
+  const int b = blockIdx.y;
+  Inst& I = c.inst[b];
+  if (!I.run) return;
+  const Tableau& Tb = c_tab[c.o.method];
+  double cb[7];
+  for (int j = 0; j < 7; ++j) cb[j] = I.h * Tb.btilde[j];
+  const int n = c.n, T = (n + kHT - 1) / kHT;
+  int ti, tj;
+  herm_tile(blockIdx.x, T, ti, tj);
+  const float2* y = slot(c, b, I.sy);
+  const float2* y1 = slot(c, b, I.sy1);
+  const float2* k[7];
+  for (int j = 0; j < 7; ++j) k[j] = slot(c, b, I.sk[j]);
+  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+  const int col = tj * kHT + lx;
+  double s = 0.0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int r = ti * kHT + ly + 8 * q;
+    if (r < n && col < n) {
+      const long long e = (long long)r * n + col;
+      double ex = 0.0, ey = 0.0;
+#pragma unroll
+      for (int j = 0; j < 7; ++j) {
+        const float2 kv = k[j][e];
+        ex = fma(cb[j], (double)kv.x, ex);
+        ey = fma(cb[j], (double)kv.y, ey);
+      }
+      const float ya = cabsf(y[e]), y1a = cabsf(y1[e]);
+      const double sc = c.o.atol + c.o.rtol * (double)(ya > y1a ? ya : y1a);
+      s += (ex * ex + ey * ey) / (sc * sc);
+    }
+  }
+  if (ti != tj) s *= 2.0;
+  block_atomic_add(s, &I.acc[0], red);
+}
+
 // Starting-step norms.  phase 0: acc[0] += |y/sc|^2, acc[1] += |k1/sc|^2;
 // phase 1: acc[2] += |(k2 - k1)/sc|^2 (k2 = f(y + h0 k1));
 // phase 2 (Krylov form, k2 holding L k1): acc[2] += |h0 L k1 / sc|^2, the same quantity
@@ -704,6 +847,59 @@ static __global__ void kry_combine_kernel(Common c) {
   block_atomic_add(s, &I.acc[0], red);
 }
 
+// kry_combine_kernel for the hermitian form (upper-triangle tiles, mirrored writes).
+static __global__ void kry_combine_h_kernel(Common c) {
+  __shared__ double red[40];
+  __shared__ float cf[3][8];
+  __shared__ float2 sh[kHT][kHT + 1];
+  const int b = blockIdx.y;
+  Inst& I = c.inst[b];
+  if (!I.run) return;
+  if (threadIdx.x == 0) kry_step_coefs(c.o.method, kry_ratio(I), I.sig1, cf[0], cf[1], cf[2]);
+  __syncthreads();
+  float cy[8], ce[8], cs[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) cy[q] = cf[0][q], ce[q] = cf[1][q], cs[q] = cf[2][q];
+  const int n = c.n, T = (n + kHT - 1) / kHT;
+  int ti, tj;
+  herm_tile(blockIdx.x, T, ti, tj);
+  const float2* u[8];
+  u[0] = slot(c, b, I.sy);
+#pragma unroll
+  for (int q = 1; q < 8; ++q) u[q] = slot(c, b, I.sk[q - 1]);
+  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+  const int col = tj * kHT + lx;
+  float2 vy[4], vs[4];
+  double s = 0.0;
+#pragma unroll
+  for (int q4 = 0; q4 < 4; ++q4) {
+    const int r = ti * kHT + ly + 8 * q4;
+    float2 a = make_float2(0.f, 0.f), e = make_float2(0.f, 0.f), f = make_float2(0.f, 0.f);
+    if (r < n && col < n) {
+      const long long el = (long long)r * n + col;
+      float2 v0 = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const float2 v = u[q][el];
+        if (q == 0) v0 = v;
+        a = caxpy(cy[q], v, a);
+        e = caxpy(ce[q], v, e);
+        f = caxpy(cs[q], v, f);
+      }
+      const float ya = cabsf(v0), y1a = cabsf(a);
+      const double sc = c.o.atol + c.o.rtol * (double)(ya > y1a ? ya : y1a);
+      const double ex = e.x, ey = e.y;
+      s += (ex * ex + ey * ey) / (sc * sc);
+    }
+    vy[q4] = a;
+    vs[q4] = f;
+  }
+  if (ti != tj) s *= 2.0;
+  herm_store(slot(c, b, I.sy1), n, ti, tj, vy, sh);
+  herm_store(slot(c, b, I.sf), n, ti, tj, vs, sh);
+  block_atomic_add(s, &I.acc[0], red);
+}
+
 // One block: per-instance commit of the Krylov form, then the WHILE-node condition (as
 // commit_kernel).  An accepted step makes y1 the new u_0 and tau L y1 the new (scaled)
 // u_1, and rebuilds the basis for the next trial step; a rejected one keeps the basis.
@@ -745,6 +941,32 @@ static __global__ void kry_commit_kernel(Common c, cudaGraphConditionalHandle ha
     else
       cudaGraphSetConditional(handle, more ? 1u : 0u);
   }
+}
+
+// ------------------------------------------------------------------------------------
+// launch helpers: the hermitian-half elementwise kernels in the hermitian form
+// ------------------------------------------------------------------------------------
+inline dim3 herm_grid(int n, int B) {
+  const int T = (n + kHT - 1) / kHT;
+  return dim3((unsigned)(T * (T + 1) / 2), (unsigned)B);
+}
+inline void launch_combine(cudaStream_t s, const Common& c, dim3 ge, int mode) {
+  if (c.form == DQB_FORM_HERMITIAN)
+    combine_h_kernel<<<herm_grid(c.n, c.B), 256, 0, s>>>(c, mode);
+  else
+    combine_kernel<<<ge, kElemThreads, 0, s>>>(c, mode);
+}
+inline void launch_error(cudaStream_t s, const Common& c, dim3 ge) {
+  if (c.form == DQB_FORM_HERMITIAN)
+    error_h_kernel<<<herm_grid(c.n, c.B), 256, 0, s>>>(c);
+  else
+    error_kernel<<<ge, kElemThreads, 0, s>>>(c);
+}
+inline void launch_kry_combine(cudaStream_t s, const Common& c, dim3 ge) {
+  if (c.form == DQB_FORM_HERMITIAN)
+    kry_combine_h_kernel<<<herm_grid(c.n, c.B), 256, 0, s>>>(c);
+  else
+    kry_combine_kernel<<<ge, kElemThreads, 0, s>>>(c);
 }
 
 // One block per instance after the loop: the saves left over (t1 <= t0, or a

@@ -859,6 +859,9 @@ static void init_carveouts() {
     prefer_max_shared(big::save_kernel);
     prefer_max_shared(big::commit_kernel);
     prefer_max_shared(big::kry_combine_kernel);
+    prefer_max_shared(big::combine_h_kernel);
+    prefer_max_shared(big::error_h_kernel);
+    prefer_max_shared(big::kry_combine_h_kernel);
     prefer_max_shared(big::kry_commit_kernel);
     prefer_max_shared(big::retire_kernel);
     prefer_max_shared(big::pre_finalize_kernel);
@@ -900,7 +903,7 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bo
     launch_rhs(s, c, d, B, 3, 1, 0, form, nullptr, nullptr);
     big::init_norm_kernel<<<ge, T, 0, s>>>(c, 2);
   } else {
-    big::combine_kernel<<<ge, T, 0, s>>>(c, 6);
+    big::launch_combine(s, c, ge, 6);
     launch_rhs(s, c, d, B, 2, 1, 0, form, nullptr, nullptr);
     big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
   }
@@ -910,7 +913,7 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bo
   auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h, int* flag) {
     if (krylov) {
       for (int q = 1; q <= 6; ++q) launch_rhs(cs, c, d, B, q + 2, q, 1, form, nullptr, nullptr, q);
-      big::kry_combine_kernel<<<ge, T, 0, cs>>>(c);
+      big::launch_kry_combine(cs, c, ge);
       big::control_kernel<<<gi, 128, 0, cs>>>(c);
       big::save_kernel<<<ge, T, 0, cs>>>(c, 2);
       big::kry_commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
@@ -918,12 +921,12 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bo
       return;
     }
     for (int st = 0; st < 5; ++st) {
-      big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
+      big::launch_combine(cs, c, ge, st);
       launch_rhs(cs, c, d, B, 2, st + 1, 1, form, nullptr, nullptr);
     }
-    big::combine_kernel<<<ge, T, 0, cs>>>(c, 5);
+    big::launch_combine(cs, c, ge, 5);
     launch_rhs(cs, c, d, B, 1, 6, 1, form, nullptr, nullptr);
-    big::error_kernel<<<ge, T, 0, cs>>>(c);
+    big::launch_error(cs, c, ge);
     big::control_kernel<<<gi, 128, 0, cs>>>(c);
     big::save_kernel<<<ge, T, 0, cs>>>(c, 1);
     big::commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);

@@ -972,6 +972,9 @@ static void init_carveouts() {
     prefer_max_shared(big::save_kernel);
     prefer_max_shared(big::commit_kernel);
     prefer_max_shared(big::kry_combine_kernel);
+    prefer_max_shared(big::combine_h_kernel);
+    prefer_max_shared(big::error_h_kernel);
+    prefer_max_shared(big::kry_combine_h_kernel);
     prefer_max_shared(big::kry_commit_kernel);
     prefer_max_shared(big::pre_finalize_kernel);
     prefer_max_shared(big::finalize_kernel);
@@ -1103,7 +1106,7 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
     launch_rhs_dia(s, c, d, B, rows, 3, 1, 0, nullptr, nullptr, 0, herm);
     big::init_norm_kernel<<<ge, T, 0, s>>>(c, 2);
   } else {
-    big::combine_kernel<<<ge, T, 0, s>>>(c, 6);
+    big::launch_combine(s, c, ge, 6);
     launch_rhs_dia(s, c, d, B, rows, 2, 1, 0, nullptr, nullptr, 0, herm);
     big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
   }
@@ -1114,19 +1117,19 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h, int* flag) {
     if (krylov) {
       for (int q = 1; q <= 6; ++q) launch_rhs_dia(cs, c, d, B, rows, 0, 0, 1, nullptr, nullptr, q, herm);
-      big::kry_combine_kernel<<<ge, T, 0, cs>>>(c);
+      big::launch_kry_combine(cs, c, ge);
       big::control_kernel<<<gi, 128, 0, cs>>>(c);
       big::save_kernel<<<ge, T, 0, cs>>>(c, 2);
       big::kry_commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
       return;
     }
     for (int st = 0; st < 5; ++st) {
-      big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
+      big::launch_combine(cs, c, ge, st);
       launch_rhs_dia(cs, c, d, B, rows, 2, st + 1, 1, nullptr, nullptr, 0, herm);
     }
-    big::combine_kernel<<<ge, T, 0, cs>>>(c, 5);
+    big::launch_combine(cs, c, ge, 5);
     launch_rhs_dia(cs, c, d, B, rows, 1, 6, 1, nullptr, nullptr, 0, herm);
-    big::error_kernel<<<ge, T, 0, cs>>>(c);
+    big::launch_error(cs, c, ge);
     big::control_kernel<<<gi, 128, 0, cs>>>(c);
     big::save_kernel<<<ge, T, 0, cs>>>(c, 1);
     big::commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);

@@ -151,3 +151,14 @@ def test_large_path_krylov_stepper_vs_oracle(cuda_device, precision, method):
         _check_vs_oracle(kr, w['H'][b], w['jump_ops'], w['rho0'], ts, w['exp_ops'], m, b)
     dn = np.abs(kr.infos.nsteps.cpu().numpy() - res['stages'].infos.nsteps.cpu().numpy())
     assert dn.max() <= 2
+
+
+def test_large_path_krylov_standard_form(cuda_device):
+    """The Krylov form on the GEMM path in the standard form (a non-hermitian rho0, FP32
+    products): n = 90, three jumps, against the oracle's standard form."""
+    H, Ls, rho = random_problem(90, 3, seed=21, hermitian_rho=False)
+    ts = np.linspace(0, 1.0, 5)
+    res = dq.mesolve(H, Ls, rho, ts, options=dq.Options(assume_hermitian=False, stepper='krylov'))
+    m = dq.Tsit5()
+    assert_solve_parity(res.states.cpu().numpy(), None, int(res.infos.nsteps), H, Ls, rho, ts,
+                        None, 'Tsit5', m.rtol, m.atol, form='standard')

@@ -381,7 +381,9 @@ def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which, nsave=0
             # the Krylov form: per accepted step six right-hand sides build the basis (read
             # one matrix, write one: 12 passes); per attempt one pass reads u_0..u_7 and
             # writes y1 and the next first stage (10 passes); per save point the dense
-            # output reads the basis and writes the state (9 passes)
+            # output reads the basis and writes the state (9 passes).  (The hermitian-half
+            # kernels read about half of each hermitian matrix: the counts are of whole
+            # matrices, as the stage form's 34.)
             nbytes = float((mat * (12 * nacc + 10 * nsteps)).sum()) + 9 * mat * nsave * B
             note = ('bytes = the Krylov-form step: 12 n^2 complex64 passes per accepted step '
                     '(basis), 10 per attempt (combination), 9 per save point; the same step '
@@ -434,17 +436,17 @@ def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which, nsave=0
 #     for 148 = 2.837 MB; inputs, states and expectation values, the RK slots stay in L2);
 #     profiles/mesolve_small_kernel_n64_kerr.md.
 #   dia / fp32, stage form: per attempted RK step of one instance (every kernel of the
-#     stepper, host loop: six stage combinations 4.20 GB, six hermitian-half stencils
-#     0.92 GB, the error pass 1.21 GB: 6.33 GB) plus 1.34 GB per save point (the save pass
-#     reads y and the seven stages once, writes the state);
-#     profiles/rhs_dia_wide_kernel_n4096_coupled_kerr.md.
-#   dia / fp32, Krylov form: 1.387 GB per accepted step (six basis stencils, 134.6 MB read
-#     + 96.5 MB written each), 1.324 GB per attempt (the combination pass: 1073.8 MB read,
-#     249.7 MB written) and 1.34 GB per save point; profiles/dia_krylov_n4096_coupled_kerr.md.
+#     stepper, host loop: six hermitian-half stage combinations 2.37 GB, six hermitian-half
+#     stencils 0.92 GB, the hermitian-half error pass 0.61 GB: 3.90 GB) plus 1.34 GB per
+#     save point (the save pass reads y and the seven stages once, writes the state);
+#     profiles/dia_stepper_n4096_coupled_kerr_traffic.md.
+#   dia / fp32, Krylov form: 0.918 GB per accepted step (six basis stencils, 69.9 MB read
+#     + 83.0 MB written each), 0.777 GB per attempt (the hermitian-half combination pass:
+#     541.2 MB read, 236.0 MB written) and 1.34 GB per save point; same profile.
 TRAFFIC_PER_UNIT = {
     ('kerr', 'fp32', 'auto'): ('instance', 2.837e6, 0.0, 0.0),
-    ('dia', 'fp32', 'stages'): ('instance_step', 6.33e9, 0.0, 1.34e9),
-    ('dia', 'fp32', 'krylov'): ('instance_step', 1.324e9, 1.387e9, 1.34e9),
+    ('dia', 'fp32', 'stages'): ('instance_step', 3.90e9, 0.0, 1.34e9),
+    ('dia', 'fp32', 'krylov'): ('instance_step', 0.777e9, 0.918e9, 1.34e9),
 }
 
 

@@ -282,21 +282,34 @@ __global__ void __launch_bounds__(256) symmetrize_kernel(big::Common c, LargeOps
   const int n = d.n;
   const float2* tmp = d.tmp + (long long)b * n * n;
   const int tiles = (n + 31) / 32;
-  const int ti = blockIdx.x / tiles, tj = blockIdx.x % tiles;
   const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;  // 32 x 8
   if (herm) {
-    // stage tile (tj, ti) transposed
+    // one tile pair per block (grid over the upper tiles): k(ti, tj) = tmp(ti, tj) +
+    // tmp(tj, ti)^+ written directly, k(tj, ti) its conjugate transpose (mirrored), so
+    // every element of tmp is read once
+    int ti, tj;
+    big::herm_tile(blockIdx.x, tiles, ti, tj);
     for (int r = ly; r < 32; r += 8) {
       const int gr = tj * 32 + r, gc = ti * 32 + lx;
       tT[lx][r] = (gr < n && gc < n) ? tmp[(long long)gr * n + gc] : make_float2(0.f, 0.f);
     }
     __syncthreads();
+    float2 v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = ly + 8 * q, gr = ti * 32 + r, gc = tj * 32 + lx;
+      float2 x = make_float2(0.f, 0.f);
+      if (gr < n && gc < n) x = cadd(tmp[(long long)gr * n + gc], cconj(tT[r][lx]));
+      v[q] = make_float2(x.x * scale, x.y * scale);
+    }
+    big::herm_store(out, n, ti, tj, v, tT);
+    return;
   }
+  const int ti = blockIdx.x / tiles, tj = blockIdx.x % tiles;
   for (int r = ly; r < 32; r += 8) {
     const int gr = ti * 32 + r, gc = tj * 32 + lx;
     if (gr >= n || gc >= n) continue;
     float2 v = tmp[(long long)gr * n + gc];
-    if (herm) v = cadd(v, cconj(tT[r][lx]));
     out[(long long)gr * n + gc] = make_float2(v.x * scale, v.y * scale);
   }
 }
@@ -776,7 +789,8 @@ void launch_rhs(cudaStream_t s, const big::Common& c, const LargeOps& d, int B, 
     nt = 0;
   }
   const int t32 = (n + 31) / 32;
-  symmetrize_kernel<<<dim3(t32 * t32, B), 256, 0, s>>>(c, d, out_k, need_run, form == DQB_FORM_HERMITIAN, kry,
+  const bool herm = form == DQB_FORM_HERMITIAN;
+  symmetrize_kernel<<<herm ? big::herm_grid(n, B) : dim3(t32 * t32, B), 256, 0, s>>>(c, d, out_k, need_run, herm, kry,
                                                        ext_out);
 }
 

@@ -336,31 +336,96 @@ __device__ __forceinline__ void herm_tile(int t, int T, int& ti, int& tj) {
   tj = r + (t - herm_row_start(r, T));
 }
 
-// Writes v (this thread's tile values, rows ly + 8q) at tile (ti, tj) and, for ti < tj, its
-// conjugate transpose at (tj, ti).  `sh` is a 32 x 33 shared tile.
+// A thread's four elements of a 32 x 32 tile.  VEC = false: rows ly + 8q (ly = tid / 32),
+// column tid % 32.  VEC = true (n even): rows ly + 16q (ly = tid / 16, q < 2), columns
+// 2 (tid % 16) and the next, read and written as one 16-byte access per row; element
+// 2q + p is row q, column p.
+template <bool VEC>
+struct HTile {
+  int lx, ly;
+  __device__ __forceinline__ HTile() : lx(VEC ? threadIdx.x & 15 : threadIdx.x & 31),
+                                       ly(VEC ? threadIdx.x >> 4 : threadIdx.x >> 5) {}
+  __device__ __forceinline__ int row(int q) const { return VEC ? ly + 16 * (q >> 1) : ly + 8 * q; }
+  __device__ __forceinline__ int col(int q) const { return VEC ? 2 * lx + (q & 1) : lx; }
+};
+
+// Loads the thread's four elements of tile (ti, tj) of M (zeros outside the matrix).
+template <bool VEC>
+__device__ __forceinline__ void htile_load(const float2* __restrict__ M, int n, int ti, int tj, float2 (&v)[4]) {
+  const HTile<VEC> t;
+  if (VEC) {
+#pragma unroll
+    for (int q = 0; q < 4; q += 2) {
+      const int r = ti * kHT + t.row(q), c0 = tj * kHT + t.col(q);
+      float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (r < n && c0 < n) x = *reinterpret_cast<const float4*>(M + (long long)r * n + c0);
+      v[q] = make_float2(x.x, x.y);
+      v[q + 1] = make_float2(x.z, x.w);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = ti * kHT + t.row(q), c = tj * kHT + t.col(q);
+      v[q] = (r < n && c < n) ? M[(long long)r * n + c] : make_float2(0.f, 0.f);
+    }
+  }
+}
+
+// Whether the thread's element q lies inside the matrix.
+template <bool VEC>
+__device__ __forceinline__ bool htile_in(int n, int ti, int tj, int q) {
+  const HTile<VEC> t;
+  return ti * kHT + t.row(q) < n && tj * kHT + t.col(q) < n;
+}
+
+// Writes v at tile (ti, tj) and, for ti < tj, its conjugate transpose at (tj, ti) through
+// the 32 x 33 shared tile `sh`.
+template <bool VEC>
 __device__ __forceinline__ void herm_store(float2* __restrict__ out, int n, int ti, int tj, const float2 (&v)[4],
                                            float2 (*sh)[kHT + 1]) {
-  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
-  const int c = tj * kHT + lx;
+  const HTile<VEC> t;
+  if (VEC) {
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int r = ti * kHT + ly + 8 * q;
-    if (r < n && c < n) out[(long long)r * n + c] = v[q];
+    for (int q = 0; q < 4; q += 2) {
+      const int r = ti * kHT + t.row(q), c0 = tj * kHT + t.col(q);
+      if (r < n && c0 < n)
+        *reinterpret_cast<float4*>(out + (long long)r * n + c0) = make_float4(v[q].x, v[q].y, v[q + 1].x, v[q + 1].y);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = ti * kHT + t.row(q), c = tj * kHT + t.col(q);
+      if (r < n && c < n) out[(long long)r * n + c] = v[q];
+    }
   }
   if (ti == tj) return;  // uniform over the block
   __syncthreads();       // the tile is free (a previous use has been read)
 #pragma unroll
-  for (int q = 0; q < 4; ++q) sh[ly + 8 * q][lx] = v[q];
+  for (int q = 0; q < 4; ++q) sh[t.row(q)][t.col(q)] = v[q];
   __syncthreads();
-  // row tj*32 + ly + 8q of the output takes column (ly + 8q) of the tile, conjugated
+  // output row tj*32 + a, column ti*32 + b takes the conjugate of the tile's (b, a)
+  if (VEC) {
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int r = tj * kHT + ly + 8 * q, cc = ti * kHT + lx;
-    if (r < n && cc < n) out[(long long)r * n + cc] = cconj(sh[lx][ly + 8 * q]);
+    for (int q = 0; q < 4; q += 2) {
+      const int a = t.row(q), b0 = t.col(q);
+      const int r = tj * kHT + a, c0 = ti * kHT + b0;
+      if (r < n && c0 < n) {
+        const float2 w0 = cconj(sh[b0][a]), w1 = cconj(sh[b0 + 1][a]);
+        *reinterpret_cast<float4*>(out + (long long)r * n + c0) = make_float4(w0.x, w0.y, w1.x, w1.y);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int a = t.row(q), b = t.col(q);
+      const int r = tj * kHT + a, c = ti * kHT + b;
+      if (r < n && c < n) out[(long long)r * n + c] = cconj(sh[b][a]);
+    }
   }
 }
 
 // combine_kernel for the hermitian form (same modes).
+template <bool VEC>
 static __global__ void combine_h_kernel(Common c, int mode) {
   __shared__ float2 sh[kHT][kHT + 1];
   const int b = blockIdx.y;
@@ -386,63 +451,51 @@ static __global__ void combine_h_kernel(Common c, int mode) {
   const int n = c.n, T = (n + kHT - 1) / kHT;
   int ti, tj;
   herm_tile(blockIdx.x, T, ti, tj);
-  const float2* y = slot(c, b, I.sy);
-  const float2* k[6];
-  for (int j = 0; j < 6; ++j) k[j] = slot(c, b, I.sk[j]);
-  float2* out = slot(c, b, mode == 5 ? I.sy1 : kX);
-  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
-  const int col = tj * kHT + lx;
-  float2 v[4];
+  float2 v[4], w[4];
+  htile_load<VEC>(slot(c, b, I.sy), n, ti, tj, v);
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int r = ti * kHT + ly + 8 * q;
-    float2 x = make_float2(0.f, 0.f);
-    if (r < n && col < n) {
-      const long long e = (long long)r * n + col;
-      x = y[e];
+  for (int j = 0; j < 6; ++j)
+    if (j < nterm) {
+      htile_load<VEC>(slot(c, b, I.sk[j]), n, ti, tj, w);
 #pragma unroll
-      for (int j = 0; j < 6; ++j)
-        if (j < nterm) x = caxpy(cf[j], k[j][e], x);
+      for (int q = 0; q < 4; ++q) v[q] = caxpy(cf[j], w[q], v[q]);
     }
-    v[q] = x;
-  }
-  herm_store(out, n, ti, tj, v, sh);
+  herm_store<VEC>(slot(c, b, mode == 5 ? I.sy1 : kX), n, ti, tj, v, sh);
 }
 
 // error_kernel for the hermitian form: the same FP64 sum, off-diagonal tiles counted twice.
+template <bool VEC>
 static __global__ void error_h_kernel(Common c) {
   __shared__ double red[40];
   const int b = blockIdx.y;
   Inst& I = c.inst[b];
   if (!I.run) return;
   const Tableau& Tb = c_tab[c.o.method];
-  double cb[7];
-  for (int j = 0; j < 7; ++j) cb[j] = I.h * Tb.btilde[j];
   const int n = c.n, T = (n + kHT - 1) / kHT;
   int ti, tj;
   herm_tile(blockIdx.x, T, ti, tj);
-  const float2* y = slot(c, b, I.sy);
-  const float2* y1 = slot(c, b, I.sy1);
-  const float2* k[7];
-  for (int j = 0; j < 7; ++j) k[j] = slot(c, b, I.sk[j]);
-  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
-  const int col = tj * kHT + lx;
+  double ex[4] = {0, 0, 0, 0}, ey[4] = {0, 0, 0, 0};
+  float2 w[4];
+#pragma unroll
+  for (int j = 0; j < 7; ++j) {
+    const double cb = I.h * Tb.btilde[j];
+    htile_load<VEC>(slot(c, b, I.sk[j]), n, ti, tj, w);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      ex[q] = fma(cb, (double)w[q].x, ex[q]);
+      ey[q] = fma(cb, (double)w[q].y, ey[q]);
+    }
+  }
+  float2 yv[4], y1v[4];
+  htile_load<VEC>(slot(c, b, I.sy), n, ti, tj, yv);
+  htile_load<VEC>(slot(c, b, I.sy1), n, ti, tj, y1v);
   double s = 0.0;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const int r = ti * kHT + ly + 8 * q;
-    if (r < n && col < n) {
-      const long long e = (long long)r * n + col;
-      double ex = 0.0, ey = 0.0;
-#pragma unroll
-      for (int j = 0; j < 7; ++j) {
-        const float2 kv = k[j][e];
-        ex = fma(cb[j], (double)kv.x, ex);
-        ey = fma(cb[j], (double)kv.y, ey);
-      }
-      const float ya = cabsf(y[e]), y1a = cabsf(y1[e]);
+    if (htile_in<VEC>(n, ti, tj, q)) {
+      const float ya = cabsf(yv[q]), y1a = cabsf(y1v[q]);
       const double sc = c.o.atol + c.o.rtol * (double)(ya > y1a ? ya : y1a);
-      s += (ex * ex + ey * ey) / (sc * sc);
+      s += (ex[q] * ex[q] + ey[q] * ey[q]) / (sc * sc);
     }
   }
   if (ti != tj) s *= 2.0;
@@ -848,6 +901,7 @@ static __global__ void kry_combine_kernel(Common c) {
 }
 
 // kry_combine_kernel for the hermitian form (upper-triangle tiles, mirrored writes).
+template <bool VEC>
 static __global__ void kry_combine_h_kernel(Common c) {
   __shared__ double red[40];
   __shared__ float cf[3][8];
@@ -857,46 +911,41 @@ static __global__ void kry_combine_h_kernel(Common c) {
   if (!I.run) return;
   if (threadIdx.x == 0) kry_step_coefs(c.o.method, kry_ratio(I), I.sig1, cf[0], cf[1], cf[2]);
   __syncthreads();
-  float cy[8], ce[8], cs[8];
-#pragma unroll
-  for (int q = 0; q < 8; ++q) cy[q] = cf[0][q], ce[q] = cf[1][q], cs[q] = cf[2][q];
   const int n = c.n, T = (n + kHT - 1) / kHT;
   int ti, tj;
   herm_tile(blockIdx.x, T, ti, tj);
-  const float2* u[8];
-  u[0] = slot(c, b, I.sy);
+  float2 u0[4], vy[4], ve[4], vs[4], w[4];
+  htile_load<VEC>(slot(c, b, I.sy), n, ti, tj, u0);
 #pragma unroll
-  for (int q = 1; q < 8; ++q) u[q] = slot(c, b, I.sk[q - 1]);
-  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
-  const int col = tj * kHT + lx;
-  float2 vy[4], vs[4];
+  for (int q = 0; q < 4; ++q) {
+    vy[q] = make_float2(cf[0][0] * u0[q].x, cf[0][0] * u0[q].y);
+    ve[q] = make_float2(0.f, 0.f);
+    vs[q] = make_float2(0.f, 0.f);
+  }
+#pragma unroll
+  for (int k = 1; k < 8; ++k) {
+    htile_load<VEC>(slot(c, b, I.sk[k - 1]), n, ti, tj, w);
+    const float a = cf[0][k], e = cf[1][k], f = cf[2][k];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      vy[q] = caxpy(a, w[q], vy[q]);
+      ve[q] = caxpy(e, w[q], ve[q]);
+      vs[q] = caxpy(f, w[q], vs[q]);
+    }
+  }
   double s = 0.0;
 #pragma unroll
-  for (int q4 = 0; q4 < 4; ++q4) {
-    const int r = ti * kHT + ly + 8 * q4;
-    float2 a = make_float2(0.f, 0.f), e = make_float2(0.f, 0.f), f = make_float2(0.f, 0.f);
-    if (r < n && col < n) {
-      const long long el = (long long)r * n + col;
-      float2 v0 = make_float2(0.f, 0.f);
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const float2 v = u[q][el];
-        if (q == 0) v0 = v;
-        a = caxpy(cy[q], v, a);
-        e = caxpy(ce[q], v, e);
-        f = caxpy(cs[q], v, f);
-      }
-      const float ya = cabsf(v0), y1a = cabsf(a);
+  for (int q = 0; q < 4; ++q) {
+    if (htile_in<VEC>(n, ti, tj, q)) {
+      const float ya = cabsf(u0[q]), y1a = cabsf(vy[q]);
       const double sc = c.o.atol + c.o.rtol * (double)(ya > y1a ? ya : y1a);
-      const double ex = e.x, ey = e.y;
+      const double ex = ve[q].x, ey = ve[q].y;
       s += (ex * ex + ey * ey) / (sc * sc);
     }
-    vy[q4] = a;
-    vs[q4] = f;
   }
   if (ti != tj) s *= 2.0;
-  herm_store(slot(c, b, I.sy1), n, ti, tj, vy, sh);
-  herm_store(slot(c, b, I.sf), n, ti, tj, vs, sh);
+  herm_store<VEC>(slot(c, b, I.sy1), n, ti, tj, vy, sh);
+  herm_store<VEC>(slot(c, b, I.sf), n, ti, tj, vs, sh);
   block_atomic_add(s, &I.acc[0], red);
 }
 
@@ -950,23 +999,31 @@ inline dim3 herm_grid(int n, int B) {
   const int T = (n + kHT - 1) / kHT;
   return dim3((unsigned)(T * (T + 1) / 2), (unsigned)B);
 }
+// 16-byte accesses when every row starts on a 16-byte boundary (n even, slots aligned).
+inline bool herm_vec(const Common& c) { return (c.n % 2) == 0 && (reinterpret_cast<uintptr_t>(c.mats) & 15) == 0; }
 inline void launch_combine(cudaStream_t s, const Common& c, dim3 ge, int mode) {
-  if (c.form == DQB_FORM_HERMITIAN)
-    combine_h_kernel<<<herm_grid(c.n, c.B), 256, 0, s>>>(c, mode);
-  else
+  if (c.form != DQB_FORM_HERMITIAN)
     combine_kernel<<<ge, kElemThreads, 0, s>>>(c, mode);
+  else if (herm_vec(c))
+    combine_h_kernel<true><<<herm_grid(c.n, c.B), 256, 0, s>>>(c, mode);
+  else
+    combine_h_kernel<false><<<herm_grid(c.n, c.B), 256, 0, s>>>(c, mode);
 }
 inline void launch_error(cudaStream_t s, const Common& c, dim3 ge) {
-  if (c.form == DQB_FORM_HERMITIAN)
-    error_h_kernel<<<herm_grid(c.n, c.B), 256, 0, s>>>(c);
-  else
+  if (c.form != DQB_FORM_HERMITIAN)
     error_kernel<<<ge, kElemThreads, 0, s>>>(c);
+  else if (herm_vec(c))
+    error_h_kernel<true><<<herm_grid(c.n, c.B), 256, 0, s>>>(c);
+  else
+    error_h_kernel<false><<<herm_grid(c.n, c.B), 256, 0, s>>>(c);
 }
 inline void launch_kry_combine(cudaStream_t s, const Common& c, dim3 ge) {
-  if (c.form == DQB_FORM_HERMITIAN)
-    kry_combine_h_kernel<<<herm_grid(c.n, c.B), 256, 0, s>>>(c);
-  else
+  if (c.form != DQB_FORM_HERMITIAN)
     kry_combine_kernel<<<ge, kElemThreads, 0, s>>>(c);
+  else if (herm_vec(c))
+    kry_combine_h_kernel<true><<<herm_grid(c.n, c.B), 256, 0, s>>>(c);
+  else
+    kry_combine_h_kernel<false><<<herm_grid(c.n, c.B), 256, 0, s>>>(c);
 }
 
 // One block per instance after the loop: the saves left over (t1 <= t0, or a

@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(256) symmetrize_kernel(big::Common c, LargeOps
       }
       v[q] = make_float2(x.x * scale, x.y * scale);
     }
-    big::herm_store(out, n, ti, tj, v, tT);
+    big::herm_store<false>(out, n, ti, tj, v, tT);
     return;
   }
   const int ti = blockIdx.x / tiles, tj = blockIdx.x % tiles;
@@ -916,9 +916,12 @@ static void init_carveouts() {
     prefer_max_shared(big::save_kernel);
     prefer_max_shared(big::commit_kernel);
     prefer_max_shared(big::kry_combine_kernel);
-    prefer_max_shared(big::combine_h_kernel);
-    prefer_max_shared(big::error_h_kernel);
-    prefer_max_shared(big::kry_combine_h_kernel);
+    prefer_max_shared(big::combine_h_kernel<true>);
+    prefer_max_shared(big::combine_h_kernel<false>);
+    prefer_max_shared(big::error_h_kernel<true>);
+    prefer_max_shared(big::error_h_kernel<false>);
+    prefer_max_shared(big::kry_combine_h_kernel<true>);
+    prefer_max_shared(big::kry_combine_h_kernel<false>);
     prefer_max_shared(big::kry_commit_kernel);
     prefer_max_shared(big::retire_kernel);
     prefer_max_shared(big::pre_finalize_kernel);

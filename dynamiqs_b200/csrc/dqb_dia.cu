@@ -972,9 +972,12 @@ static void init_carveouts() {
     prefer_max_shared(big::save_kernel);
     prefer_max_shared(big::commit_kernel);
     prefer_max_shared(big::kry_combine_kernel);
-    prefer_max_shared(big::combine_h_kernel);
-    prefer_max_shared(big::error_h_kernel);
-    prefer_max_shared(big::kry_combine_h_kernel);
+    prefer_max_shared(big::combine_h_kernel<true>);
+    prefer_max_shared(big::combine_h_kernel<false>);
+    prefer_max_shared(big::error_h_kernel<true>);
+    prefer_max_shared(big::error_h_kernel<false>);
+    prefer_max_shared(big::kry_combine_h_kernel<true>);
+    prefer_max_shared(big::kry_combine_h_kernel<false>);
     prefer_max_shared(big::kry_commit_kernel);
     prefer_max_shared(big::pre_finalize_kernel);
     prefer_max_shared(big::finalize_kernel);

@@ -27,7 +27,7 @@
 namespace dqb {
 namespace {
 
-enum Src : int { SRC_IN = 0, SRC_HNH = 1, SRC_L = 2, SRC_T = 3, SRC_TMP = 4, SRC_H = 5, SRC_S = 6 };
+enum Src : int { SRC_IN = 0, SRC_HNH = 1, SRC_L = 2, SRC_T = 3, SRC_TMP = 4, SRC_H = 5 };
 
 struct Term {
   int srcA, kA, opA;  // opA: 0 = A, 1 = A^+
@@ -44,7 +44,6 @@ struct LargeOps {
   float2* hnh;  // [B, n, n]
   float2* T;    // [B, K, n, n]
   float2* tmp;  // [B, n, n]
-  float2* S;    // [B, n, n]: sum_k L_k X L_k^+ (hermitian form; upper tiles)
   const dqb_ragged_instance* rag;  // per-instance operators (ragged batches), or null
   int prec;                        // DQB_PREC_*: FP32 CUDA cores or a tensor-core mode
 };
@@ -54,7 +53,7 @@ __device__ __forceinline__ int jumps_of(const LargeOps& d, int b) { return d.rag
 struct GemmJob {
   int nterms;
   Term t[4];
-  int dst;       // SRC_T (with kdst), SRC_TMP, SRC_S, SRC_HNH
+  int dst;       // SRC_T (with kdst), SRC_TMP, SRC_HNH
   int kdst;      // jump index for SRC_T; for GEMMs over all jumps, kdst = -1 (blockIdx.z % K)
   int add_miH;   // epilogue: C += -i H (Hnh set-up)
   int accumulate;  // epilogue: C += result (further terms of a long sum)
@@ -62,7 +61,6 @@ struct GemmJob {
   int need_run;  // 1: running instances, 0: status OK, 2: all (stand-alone)
   int kry;       // q > 0: Krylov basis right-hand side u_{q+1} = tau L u_q (skipped where the
                  // instance's basis already has it)
-  int upper;     // 1: only the output tiles on and above the diagonal (a hermitian result)
 };
 
 // Whether instance b takes no part in a job (need_run and the Krylov basis state).
@@ -156,11 +154,7 @@ __global__ void __launch_bounds__(NT) cgemm_kernel(big::Common c, LargeOps d, Ge
   const int Kb = jumps_of(d, b);
   if (job.kdst < 0 && kz >= Kb) return;  // this instance has fewer jumps
   const int tiles = (n + BM - 1) / BM;
-  int tr, tc;
-  if (job.upper)
-    big::herm_tile(blockIdx.x, tiles, tr, tc);
-  else
-    tr = blockIdx.x / tiles, tc = blockIdx.x % tiles;
+  const int tr = blockIdx.x / tiles, tc = blockIdx.x % tiles;
   const int r0 = tr * BM, c0 = tc * BN;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   float2 acc[4][4];
@@ -244,8 +238,6 @@ __global__ void __launch_bounds__(NT) cgemm_kernel(big::Common c, LargeOps d, Ge
     C = d.T + ((long long)b * d.K + kz) * (long long)n * n;
   } else if (job.dst == SRC_TMP) {
     C = d.tmp + (long long)b * n * n;
-  } else if (job.dst == SRC_S) {
-    C = d.S + (long long)b * n * n;
   } else {
     C = d.hnh + (long long)b * n * n;
   }
@@ -270,11 +262,11 @@ __global__ void __launch_bounds__(NT) cgemm_kernel(big::Common c, LargeOps d, Ge
   }
 }
 
-// k_out = tmp + tmp^+ (+ S, hermitian form) via 32 x 32 shared-memory tile pairs, or a copy;
+// k_out = tmp + tmp^+ (hermitian form) via 32 x 32 shared-memory tile pairs, or a copy;
 // for a Krylov basis right-hand side (kry = q > 0) times tau (and sig1 for q = 1).
 // grid (tiles32 * tiles32, B).
 __global__ void __launch_bounds__(256) symmetrize_kernel(big::Common c, LargeOps d, int out_k, int need_run,
-                                                         int herm, int kry, int add_s, float2* ext_out) {
+                                                         int herm, int kry, float2* ext_out) {
   __shared__ float2 tT[32][33];
   const int b = blockIdx.y;
   float2* out;
@@ -289,7 +281,6 @@ __global__ void __launch_bounds__(256) symmetrize_kernel(big::Common c, LargeOps
   }
   const int n = d.n;
   const float2* tmp = d.tmp + (long long)b * n * n;
-  const float2* Sb = d.S + (long long)b * n * n;
   const int tiles = (n + 31) / 32;
   const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;  // 32 x 8
   if (herm) {
@@ -308,11 +299,7 @@ __global__ void __launch_bounds__(256) symmetrize_kernel(big::Common c, LargeOps
     for (int q = 0; q < 4; ++q) {
       const int r = ly + 8 * q, gr = ti * 32 + r, gc = tj * 32 + lx;
       float2 x = make_float2(0.f, 0.f);
-      if (gr < n && gc < n) {
-        const long long e = (long long)gr * n + gc;
-        x = cadd(tmp[e], cconj(tT[r][lx]));
-        if (add_s) x = cadd(x, Sb[e]);  // S's upper-or-diagonal GEMM tiles cover this tile
-      }
+      if (gr < n && gc < n) x = cadd(tmp[(long long)gr * n + gc], cconj(tT[r][lx]));
       v[q] = make_float2(x.x * scale, x.y * scale);
     }
     big::herm_store<false>(out, n, ti, tj, v, tT);
@@ -512,12 +499,7 @@ __global__ void __launch_bounds__(tcg::kThreads, 1)
   const int Kb = jumps_of(d, b);
   if (job.kdst < 0 && kz >= Kb) return;
   const int tiles = (n + 127) >> 7;
-  int trow, tcol;
-  if (job.upper)
-    big::herm_tile(blockIdx.x, tiles, trow, tcol);
-  else
-    trow = blockIdx.x / tiles, tcol = blockIdx.x % tiles;
-  const int row0 = trow * 128, col0 = tcol * 128;
+  const int row0 = (blockIdx.x / tiles) * 128, col0 = (blockIdx.x % tiles) * 128;
 
   const float2* Ap[4];
   const float2* Mp[4];
@@ -638,8 +620,6 @@ __global__ void __launch_bounds__(tcg::kThreads, 1)
       C = ext_out + (long long)b * n * n;
     } else if (job.dst == SRC_T) {
       C = d.T + ((long long)b * d.K + kz) * (long long)n * n;
-    } else if (job.dst == SRC_S) {
-      C = d.S + (long long)b * n * n;
     } else {
       C = d.tmp + (long long)b * n * n;
     }
@@ -738,21 +718,21 @@ void launch_gemm(cudaStream_t s, const big::Common& c, const LargeOps& d, const 
                  const float2* ext_in, float2* ext_out, bool tcp) {
   if (tcp) {
     const int t = (d.n + 127) / 128;
-    const dim3 g(j.upper ? t * (t + 1) / 2 : t * t, 1, zdim);
+    const dim3 g(t * t, 1, zdim);
     if (tc_slice() == 128)
       launch_tc<128>(s, g, c, d, j, ext_in, ext_out);
     else
       launch_tc<64>(s, g, c, d, j, ext_in, ext_out);
   } else {
     const int t = (d.n + BM - 1) / BM;
-    cgemm_kernel<<<dim3(j.upper ? t * (t + 1) / 2 : t * t, 1, zdim), NT, 0, s>>>(c, d, j, ext_in, ext_out);
+    cgemm_kernel<<<dim3(t * t, 1, zdim), NT, 0, s>>>(c, d, j, ext_in, ext_out);
   }
 }
 
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct LargeLayout {
-  size_t off_iter, off_inst, off_eacc, off_hnh, off_T, off_tmp, off_S, off_mats, total;
+  size_t off_iter, off_inst, off_eacc, off_hnh, off_T, off_tmp, off_mats, total;
 };
 
 LargeLayout large_layout(int n, int K, int nE, int ntsave, long long B) {
@@ -764,8 +744,7 @@ LargeLayout large_layout(int n, int K, int nE, int ntsave, long long B) {
   l.off_hnh = align_up(l.off_eacc + B * (size_t)nE * ntsave * sizeof(double2));
   l.off_T = align_up(l.off_hnh + B * nn * sizeof(float2));
   l.off_tmp = align_up(l.off_T + B * (size_t)K * nn * sizeof(float2));
-  l.off_S = align_up(l.off_tmp + B * nn * sizeof(float2));
-  l.off_mats = align_up(l.off_S + B * nn * sizeof(float2));
+  l.off_mats = align_up(l.off_tmp + B * nn * sizeof(float2));
   l.total = l.off_mats + B * (size_t)big::kSlots * nn * sizeof(float2);
   return l;
 }
@@ -775,12 +754,12 @@ void launch_rhs(cudaStream_t s, const big::Common& c, const LargeOps& d, int B, 
                 int need_run, int form, const float2* ext_in, float2* ext_out, int kry = 0) {
   const int n = d.n;
   const bool tcp = use_tc(d, form);
-  const bool herm = form == DQB_FORM_HERMITIAN;
-  if (d.K > 0) {  // T_k = L_k X
+  const float sc = form == DQB_FORM_HERMITIAN ? 0.5f : 1.0f;
+  if (d.K > 0) {
     GemmJob j1;
     std::memset(&j1, 0, sizeof(j1));
     j1.nterms = 1;
-    j1.t[0] = Term{SRC_L, -1, 0, SRC_IN, 0, 0, 1.0f};
+    j1.t[0] = Term{SRC_L, -1, 0, SRC_IN, 0, 0, sc};
     j1.dst = SRC_T;
     j1.kdst = -1;
     j1.in_sel = in_sel;
@@ -788,10 +767,8 @@ void launch_rhs(cudaStream_t s, const big::Common& c, const LargeOps& d, int B, 
     j1.kry = kry;
     launch_gemm(s, c, d, j1, B * d.K, ext_in, nullptr, tcp);
   }
-  // Hermitian form: tmp = Hnh X, and the hermitian S = sum_k T_k L_k^+ on the tiles on and
-  // above the diagonal only; the output is tmp + tmp^+ + S (symmetrize mirrors S).
-  // Standard form: tmp = Hnh X + X Hnh^+ + sum_k T_k L_k^+, copied out.  At most four
-  // summed terms per launch, the rest accumulated by further launches.
+  // tmp = Hnh X + sum_k T_k L_k^+ [+ X Hnh^+]: at most 4 summed terms per launch, the
+  // rest accumulated by further launches into tmp
   GemmJob j2;
   std::memset(&j2, 0, sizeof(j2));
   j2.dst = SRC_TMP;
@@ -801,39 +778,20 @@ void launch_rhs(cudaStream_t s, const big::Common& c, const LargeOps& d, int B, 
   j2.kry = kry;
   int nt = 0;
   j2.t[nt++] = Term{SRC_HNH, 0, 0, SRC_IN, 0, 0, 1.0f};
-  if (!herm) j2.t[nt++] = Term{SRC_IN, 0, 0, SRC_HNH, 0, 1, 1.0f};
-  if (herm) {
+  if (form == DQB_FORM_STANDARD) j2.t[nt++] = Term{SRC_IN, 0, 0, SRC_HNH, 0, 1, 1.0f};
+  int k = 0;
+  for (;;) {
+    while (k < d.K && nt < 4) j2.t[nt++] = Term{SRC_T, k, 0, SRC_L, k, 1, 1.0f}, ++k;
     j2.nterms = nt;
     launch_gemm(s, c, d, j2, B, ext_in, nullptr, tcp);
-    if (d.K > 0) {
-      GemmJob j3 = j2;
-      j3.dst = SRC_S;
-      j3.upper = 1;
-      j3.accumulate = 0;
-      int k = 0;
-      for (;;) {
-        nt = 0;
-        while (k < d.K && nt < 4) j3.t[nt++] = Term{SRC_T, k, 0, SRC_L, k, 1, 1.0f}, ++k;
-        j3.nterms = nt;
-        launch_gemm(s, c, d, j3, B, ext_in, nullptr, tcp);
-        if (k >= d.K) break;
-        j3.accumulate = 1;
-      }
-    }
-  } else {
-    int k = 0;
-    for (;;) {
-      while (k < d.K && nt < 4) j2.t[nt++] = Term{SRC_T, k, 0, SRC_L, k, 1, 1.0f}, ++k;
-      j2.nterms = nt;
-      launch_gemm(s, c, d, j2, B, ext_in, nullptr, tcp);
-      if (k >= d.K) break;
-      j2.accumulate = 1;
-      nt = 0;
-    }
+    if (k >= d.K) break;
+    j2.accumulate = 1;
+    nt = 0;
   }
   const int t32 = (n + 31) / 32;
-  symmetrize_kernel<<<herm ? big::herm_grid(n, B) : dim3(t32 * t32, B), 256, 0, s>>>(
-      c, d, out_k, need_run, herm, kry, herm && d.K > 0, ext_out);
+  const bool herm = form == DQB_FORM_HERMITIAN;
+  symmetrize_kernel<<<herm ? big::herm_grid(n, B) : dim3(t32 * t32, B), 256, 0, s>>>(c, d, out_k, need_run, herm, kry,
+                                                       ext_out);
 }
 
 int check_dense_large(const dqb_dense_problem* p) {
@@ -874,7 +832,6 @@ LargeOps make_ops(const dqb_dense_problem* p, char* ws, const LargeLayout& lay) 
   d.hnh = (float2*)(ws + lay.off_hnh);
   d.T = (float2*)(ws + lay.off_T);
   d.tmp = (float2*)(ws + lay.off_tmp);
-  d.S = (float2*)(ws + lay.off_S);
   return d;
 }
 

@@ -377,18 +377,15 @@ DQB_API int dqb_mesolve_ragged(const dqb_ragged_instance* instances, int64_t cou
 
 /* ---- dense operators, large n ---------------------------------------------------- */
 /* Scratch bytes for dqb_mesolve_dense_large (10 n x n slots per instance, Hnh, K product
- * buffers, one sum buffer, one hermitian dissipator buffer, controller state, FP64
- * expectation accumulators). */
+ * buffers, one sum buffer, controller state, FP64 expectation accumulators). */
 DQB_API size_t dqb_mesolve_dense_large_workspace_size(int32_t n, int32_t n_jumps, int32_t n_exp,
                                                      int32_t n_tsave, int64_t batch);
 
 /* Batched adaptive solve with dense operators of any n (meant for n > 64, where one
  * instance no longer fits a CTA).  Same problem, options and outputs as
  * dqb_mesolve_dense (DiffraxIntegrator.run, diffrax_integrator.py:135-147, 283-378):
- * each right-hand side is T_k = L_k X, then in the hermitian form tmp = Hnh X and the
- * hermitian S = sum T_k L_k^+ on the tiles on and above the diagonal, out = tmp + tmp^+ + S
- * (S mirrored), in the standard form tmp = Hnh X + X Hnh^+ + sum T_k L_k^+, as batched
- * complex GEMMs; the RK loop runs as a CUDA-graph WHILE node. */
+ * each right-hand side is T_k = s L_k X, tmp = Hnh X + sum T_k L_k^+ (+ X Hnh^+), then
+ * tmp + tmp^+, as batched complex GEMMs; the RK loop runs as a CUDA-graph WHILE node. */
 DQB_API int dqb_mesolve_dense_large(const dqb_dense_problem* problem, const dqb_ode_options* options,
                                     const dqb_outputs* outputs, void* workspace,
                                     size_t workspace_bytes, void* stream);

@@ -29,11 +29,10 @@ def test_large_workspace_size_arithmetic():
     n, K, nE, nt, B = 130, 2, 1, 5, 3
     got = lib.dqb_mesolve_dense_large_workspace_size(n, K, nE, nt, B)
     nn = n * n * 8
-    # 10 RK slots, Hnh, K product buffers, one sum buffer and the hermitian dissipator
-    # buffer per instance, plus the controller records and FP64 expectation accumulators
-    # (256-byte aligned blocks)
-    assert got >= B * (10 + 1 + K + 2) * nn
-    assert got < B * (10 + 1 + K + 2) * nn + 64 * 1024
+    # 10 RK slots, Hnh, K product buffers and one sum buffer per instance, plus the
+    # controller records and FP64 expectation accumulators (256-byte aligned blocks)
+    assert got >= B * (10 + 1 + K + 1) * nn
+    assert got < B * (10 + 1 + K + 1) * nn + 64 * 1024
     assert lib.dqb_mesolve_dense_large_workspace_size(1, K, nE, nt, B) == 0  # n < 2
     assert lib.dqb_mesolve_dense_large_workspace_size(n, K, nE, 0, B) == 0   # no tsave
     assert lib.dqb_mesolve_dense_large_ragged_workspace_size(n, K, nE, nt, B) == got

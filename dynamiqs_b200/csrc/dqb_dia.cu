@@ -28,6 +28,7 @@
 
 #include "dqb_big.cuh"
 #include "dqb_graph.cuh"
+#include "dqb_tc.cuh"
 
 namespace dqb {
 
@@ -645,6 +646,210 @@ __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c
   }
 }
 
+// Bulk-staged f(X), hermitian form: the rows of X a CTA's stencil reads are copied into
+// shared memory by the bulk-copy (TMA) engine, one copy per staged row, two stages in
+// flight, and every term then reads shared memory at its shifted position.  A CTA owns
+// 256 columns (one per thread) and a band of kBulkBand rows, walked in stages of R rows;
+// per stage it stages each group of row offsets that lie close together (DiaBulk: R +
+// span rows of the group, its column halo included), so every row of X leaves L2 about
+// three times instead of once per term, and no load of the stencil waits on L2.  Tiles
+// below the diagonal are skipped and the strictly-upper elements mirrored, as in the wide
+// kernel's hermitian half.  Rows and columns outside the matrix are zero in shared
+// memory (zero-filled by the threads; the copies are clipped to the matrix).  Every wait
+// is bounded; a wait that runs out makes the CTA drain its copies and write nothing.
+constexpr int kBulkW = 256;      // columns per CTA (threads)
+constexpr unsigned long long kBulkWaitNs = 200000000ull;  // 0.2 s: a stage's copies take microseconds
+constexpr int kBulkBand = 256;   // rows per CTA
+constexpr int kBulkMaxGroups = 4;
+constexpr int kBulkMaxTerms = 1 + 2 * kWideMaxNR + kWideMaxNP;
+
+struct DiaBulk {
+  int ngroup;
+  int g_rlo[kBulkMaxGroups];   // row offset of the group's first staged row
+  int g_rows[kBulkMaxGroups];  // staged rows per stage: R + span of the group's row offsets
+  int g_clo[kBulkMaxGroups];   // column offset of the first staged column (even)
+  int g_cols[kBulkMaxGroups];  // staged columns (even)
+  int g_off[kBulkMaxGroups];   // offset of the group in a stage buffer (complex values, even)
+  int r_lo, r_hi, c_lo, c_hi;  // extreme row and column offsets staged (interior test)
+  int stage;                   // complex values per stage buffer (even)
+  // terms: 0 = center, 1..NR = row terms, NR+1..2NR = column terms, then the pairs
+  int t_base[kBulkMaxTerms];   // stage offset of (row 0 of the stage, thread 0)
+  int t_stride[kBulkMaxTerms]; // row stride of the term's group
+};
+
+template <int R, int NR, int NP>
+__global__ void __launch_bounds__(kBulkW, 1) rhs_dia_bulk_kernel(big::Common c, DiaOps d, DiaWide w, DiaBulk pl,
+                                                                int in_sel, int out_k, int need_run, int kry,
+                                                                const float2* ext_in, float2* ext_out) {
+  constexpr int NT = 1 + NR + NP;  // row-table terms: center, rows, pairs
+  extern __shared__ float4 bulk_raw[];
+  __shared__ uint64_t bars[2];
+  __shared__ WideRow rowt[NT][R];
+  __shared__ int fail_sh;
+  const int j0 = blockIdx.x * kBulkW, I0 = blockIdx.y * kBulkBand;
+  if (j0 + kBulkW - 1 < I0) return;  // the whole band is below the diagonal
+  const int b = blockIdx.z;
+  const float2* X;
+  float2* out;
+  float scale = 1.f;
+  if (ext_in) {
+    X = ext_in + (long long)b * d.n * d.n;
+    out = ext_out + (long long)b * d.n * d.n;
+  } else {
+    RhsIo io;
+    if (!rhs_io(c, b, in_sel, out_k, need_run, kry, io)) return;
+    X = io.X;
+    out = io.out;
+    scale = io.scale;
+  }
+  const int n = d.n, tid = threadIdx.x;
+  const long long li = d.Lidx ? d.Lidx[b] : b;
+  const float2* L = d.L + li * d.nl * n;
+  const float2* hnh = d.hnh + (long long)b * d.nh * n;
+  float2* buf[2];
+  buf[0] = reinterpret_cast<float2*>(bulk_raw);
+  buf[1] = buf[0] + pl.stage;
+  float2* strip = buf[1] + pl.stage;  // [R][kBulkW + 1]
+  const uint32_t bar[2] = {tc::smem_u32(&bars[0]), tc::smem_u32(&bars[1])};
+  // stages of this CTA: rows I0 .. I0 + kBulkBand - 1 inside the matrix, up to the last
+  // stage that reaches the diagonal of the CTA's columns
+  const int band_rows = min(kBulkBand, n - I0);
+  int nst = (band_rows + R - 1) / R;
+  nst = min(nst, (j0 + kBulkW - 1 - I0) / R + 1);
+  if (tid == 0) {
+    tc::mbar_init(bar[0], 1);
+    tc::mbar_init(bar[1], 1);
+    tc::fence_mbar_init();
+    fail_sh = 0;
+  }
+  __syncthreads();
+
+  // column factors of this thread's column
+  const int j = j0 + tid;
+  const bool jin = j < n;
+  float2 ccen = make_float2(0.f, 0.f), ccol[NR], cpair[NP];
+  if (jin && w.has0) ccen = cconj(__ldg(&hnh[w.q0 * n + j]));
+#pragma unroll
+  for (int t = 0; t < NR; ++t) {
+    const int src = j + (t < w.nr ? w.rk[t] : 0);
+    ccol[t] = (jin && t < w.nr && src >= 0 && src < n) ? cconj(__ldg(&hnh[w.rq[t] * n + src])) : make_float2(0.f, 0.f);
+  }
+#pragma unroll
+  for (int t = 0; t < NP; ++t) {
+    const int src = j + (t < w.np ? w.pco[t] : 0);
+    cpair[t] = (jin && t < w.np && src >= 0 && src < n) ? cconj(__ldg(&L[w.ps[t] * n + src])) : make_float2(0.f, 0.f);
+  }
+
+  // stage st into buffer st & 1: the threads zero what the copies do not cover, then one
+  // thread issues the copies (their bytes announced on the stage's barrier first)
+  auto prep = [&](int st) {
+    float2* B = buf[st & 1];
+    const int is = I0 + st * R;
+    const bool rows_in = is + pl.r_lo >= 0 && is + R - 1 + pl.r_hi < n;
+    const bool cols_in = j0 + pl.c_lo >= 0 && j0 + kBulkW - 1 + pl.c_hi < n;
+    if (!(rows_in && cols_in)) {
+      for (int g = 0; g < pl.ngroup; ++g) {
+        const int gr0 = is + pl.g_rlo[g], gc0 = j0 + pl.g_clo[g], cols = pl.g_cols[g];
+        for (int e = tid; e < pl.g_rows[g] * cols; e += kBulkW) {
+          const int rr = e / cols, cc = e % cols;
+          const int gr = gr0 + rr, gc = gc0 + cc;
+          if (gr < 0 || gr >= n || gc < 0 || gc >= n) B[pl.g_off[g] + e] = make_float2(0.f, 0.f);
+        }
+      }
+    }
+    if (tid == 0) {
+      uint32_t bytes = 0;
+      for (int g = 0; g < pl.ngroup; ++g) {
+        const int gc0 = j0 + pl.g_clo[g];
+        const int c_a = max(gc0, 0), c_b = min(gc0 + pl.g_cols[g], n);
+        if (c_b <= c_a) continue;
+        for (int rr = 0; rr < pl.g_rows[g]; ++rr) {
+          const int gr = is + pl.g_rlo[g] + rr;
+          if (gr >= 0 && gr < n) bytes += (uint32_t)(c_b - c_a) * 8u;
+        }
+      }
+      tc::mbar_arrive_expect_tx(bar[st & 1], bytes);
+      for (int g = 0; g < pl.ngroup; ++g) {
+        const int gc0 = j0 + pl.g_clo[g];
+        const int c_a = max(gc0, 0), c_b = min(gc0 + pl.g_cols[g], n);
+        if (c_b <= c_a) continue;
+        for (int rr = 0; rr < pl.g_rows[g]; ++rr) {
+          const int gr = is + pl.g_rlo[g] + rr;
+          if (gr < 0 || gr >= n) continue;
+          float2* dst = B + pl.g_off[g] + rr * pl.g_cols[g] + (c_a - gc0);
+          tc::bulk_copy_g2s(tc::smem_u32(dst), X + (long long)gr * n + c_a, (uint32_t)(c_b - c_a) * 8u,
+                            bar[st & 1]);
+        }
+      }
+    }
+  };
+
+  if (nst > 0) prep(0);
+  int st = 0;
+  for (; st < nst; ++st) {
+    if (st + 1 < nst) prep(st + 1);
+    const int is = I0 + st * R;
+    // row factors of the stage's rows
+    for (int e = tid; e < NT * R; e += kBulkW) {
+      const int t = e / R, r = e % R, i = is + r;
+      int off = 0;
+      const float2* diag = nullptr;
+      if (t == 0) {
+        if (w.has0) diag = hnh + w.q0 * n;
+      } else if (t <= NR) {
+        if (t - 1 < w.nr) off = w.rk[t - 1], diag = hnh + w.rq[t - 1] * n;
+      } else {
+        if (t - 1 - NR < w.np) off = w.pro[t - 1 - NR], diag = L + w.pp[t - 1 - NR] * n;
+      }
+      const int src = i + off;
+      WideRow v;
+      v.f = (diag != nullptr && i < n && src >= 0 && src < n) ? __ldg(&diag[src]) : make_float2(0.f, 0.f);
+      v.off = 0;
+      v.pad = 0;
+      rowt[t][r] = v;
+    }
+    __syncthreads();  // row table and this stage's zero-fill visible
+    const bool ok = tc::mbar_wait_for(bar[st & 1], (uint32_t)((st >> 1) & 1), kBulkWaitNs);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) fail_sh = 1;
+      break;
+    }
+    const float2* B = buf[st & 1];
+    const int rows = min(R, n - is);
+#pragma unroll 1
+    for (int r = 0; r < rows; ++r) {
+      const int i = is + r;
+      if (!jin || j < i) continue;  // outside the matrix or below the diagonal
+      float2 acc = cmul(cadd(rowt[0][r].f, ccen), B[pl.t_base[0] + r * pl.t_stride[0] + tid]);
+#pragma unroll
+      for (int t = 0; t < NR; ++t) {
+        acc = cfma(rowt[1 + t][r].f, B[pl.t_base[1 + t] + r * pl.t_stride[1 + t] + tid], acc);
+        acc = cfma(ccol[t], B[pl.t_base[1 + NR + t] + r * pl.t_stride[1 + NR + t] + tid], acc);
+      }
+#pragma unroll
+      for (int t = 0; t < NP; ++t)
+        acc = cfma(cmul(rowt[1 + NR + t][r].f, cpair[t]),
+                   B[pl.t_base[1 + 2 * NR + t] + r * pl.t_stride[1 + 2 * NR + t] + tid], acc);
+      acc = make_float2(acc.x * scale, i == j ? 0.f : acc.y * scale);  // a hermitian diagonal is real
+      out[(long long)i * n + j] = acc;
+      strip[r * (kBulkW + 1) + tid] = acc;
+    }
+    __syncthreads();
+    // mirror: out[jj][i] = conj(f[i][jj]) for jj > i, R contiguous values per target row
+    for (int e = tid; e < kBulkW * R; e += kBulkW) {
+      const int r = e % R, cj = e / R;
+      const int i = is + r, jj = j0 + cj;
+      if (r < rows && jj < n && jj > i) out[(long long)jj * n + i] = cconj(strip[r * (kBulkW + 1) + cj]);
+    }
+    __syncthreads();  // strip, row table and buffer st & 1 are free again
+  }
+  if (fail_sh) {
+    // drain (bounded): the failed stage's copies and the next stage's may still be in flight
+    tc::mbar_wait_for(bar[st & 1], (uint32_t)((st >> 1) & 1), kBulkWaitNs);
+    if (st + 1 < nst) tc::mbar_wait_for(bar[(st + 1) & 1], (uint32_t)(((st + 1) >> 1) & 1), kBulkWaitNs);
+  }
+}
+
 // ------------------------------------------------------------------------------------
 // host side
 // ------------------------------------------------------------------------------------
@@ -833,6 +1038,69 @@ bool plan_wide(const DiaOps& d, int C, DiaWide* w) {
   return true;
 }
 
+// Staging plan of rhs_dia_bulk_kernel<R> (see DiaBulk) from the wide kernel's terms; false
+// when the groups or the shared memory do not fit.
+bool plan_bulk(const DiaOps& d, const DiaWide& w, int R, int NR, int NP, DiaBulk* pl, size_t* smem) {
+  std::memset(pl, 0, sizeof(*pl));
+  if (d.n % 2 != 0 || d.n > 46340) return false;
+  const int nt = 1 + 2 * NR + NP;
+  int ro[kBulkMaxTerms], co[kBulkMaxTerms];
+  ro[0] = co[0] = 0;
+  for (int t = 0; t < NR; ++t) {
+    const int k = t < w.nr ? w.rk[t] : 0;
+    ro[1 + t] = k, co[1 + t] = 0;
+    ro[1 + NR + t] = 0, co[1 + NR + t] = k;
+  }
+  for (int t = 0; t < NP; ++t) {
+    ro[1 + 2 * NR + t] = t < w.np ? w.pro[t] : 0;
+    co[1 + 2 * NR + t] = t < w.np ? w.pco[t] : 0;
+  }
+  std::vector<int> rs(ro, ro + nt);
+  std::sort(rs.begin(), rs.end());
+  rs.erase(std::unique(rs.begin(), rs.end()), rs.end());
+  int glo[kBulkMaxGroups], ghi[kBulkMaxGroups], ng = 0;
+  for (int v : rs) {
+    if (ng > 0 && v - ghi[ng - 1] <= R) {
+      ghi[ng - 1] = v;
+    } else {
+      if (ng == kBulkMaxGroups) return false;
+      glo[ng] = ghi[ng] = v;
+      ++ng;
+    }
+  }
+  pl->ngroup = ng;
+  int total = 0;
+  pl->r_lo = pl->c_lo = 1 << 30;
+  pl->r_hi = pl->c_hi = -(1 << 30);
+  for (int g = 0; g < ng; ++g) {
+    int clo = 1 << 30, chi = -(1 << 30);
+    for (int t = 0; t < nt; ++t)
+      if (ro[t] >= glo[g] && ro[t] <= ghi[g]) clo = std::min(clo, co[t]), chi = std::max(chi, co[t]);
+    const int clo_e = clo - (((clo % 2) + 2) % 2);  // even (16-byte aligned copies)
+    int cols = kBulkW + chi - clo_e;
+    cols += cols % 2;
+    pl->g_rlo[g] = glo[g];
+    pl->g_rows[g] = R + ghi[g] - glo[g];
+    pl->g_clo[g] = clo_e;
+    pl->g_cols[g] = cols;
+    pl->g_off[g] = total;
+    total += pl->g_rows[g] * cols;
+    pl->r_lo = std::min(pl->r_lo, glo[g]);
+    pl->r_hi = std::max(pl->r_hi, ghi[g]);
+    pl->c_lo = std::min(pl->c_lo, clo_e);
+    pl->c_hi = std::max(pl->c_hi, clo_e + cols - kBulkW);
+  }
+  pl->stage = total;
+  for (int t = 0; t < nt; ++t) {
+    int g = 0;
+    while (!(ro[t] >= glo[g] && ro[t] <= ghi[g])) ++g;
+    pl->t_stride[t] = pl->g_cols[g];
+    pl->t_base[t] = pl->g_off[g] + (ro[t] - glo[g]) * pl->g_cols[g] + (co[t] - pl->g_clo[g]);
+  }
+  *smem = (2 * (size_t)total + (size_t)R * (kBulkW + 1)) * sizeof(float2);
+  return *smem <= kStageMaxSmem;
+}
+
 // Compile-time term counts of the wide kernel's instances: NR in {4, 8}, NP in {2, 4},
 // padded by zero terms.
 int wide_nr(int nr) { return nr <= 4 ? 4 : 8; }
@@ -843,6 +1111,7 @@ int wide_np(int np) { return np <= 2 ? 2 : 4; }
 bool is_wide(int rows) {
   return rows == 208 || rows == 216 || rows == 308 || rows == 316 || rows == 408 || rows == 508;
 }
+bool is_bulk(int rows) { return rows == 604 || rows == 608; }
 int wide_c(int rows) { return (rows / 100) % 2 == 1 ? 2 : 4; }  // 2xx, 4xx: 4; 3xx, 5xx: 2
 int wide_r(int rows) { return rows % 100; }
 
@@ -854,6 +1123,12 @@ int wide_r(int rows) { return rows % 100; }
 // default, 1) = the generic kernel.  The autotuner picks among them per problem shape.
 // Returns the shape code (1 = generic).
 int rows_for(const DiaOps& d, int tile) {
+  if (is_bulk(tile)) {
+    DiaWide w;
+    DiaBulk pl;
+    size_t sm;
+    if (plan_wide(d, 2, &w) && plan_bulk(d, w, tile - 600, wide_nr(w.nr), wide_np(w.np), &pl, &sm)) return tile;
+  }
   if (is_wide(tile)) {
     DiaWide w;
     if (plan_wide(d, wide_c(tile), &w)) return tile;
@@ -868,6 +1143,7 @@ int rows_for(const DiaOps& d, int tile) {
 }
 
 dim3 rhs_grid(const DiaOps& d, int rows, int B) {
+  if (is_bulk(rows)) return dim3((d.n + kBulkW - 1) / kBulkW, (d.n + kBulkBand - 1) / kBulkBand, B);
   if (is_wide(rows)) {
     const int r = wide_r(rows), cols = kRhsCols * wide_c(rows);
     return dim3((d.n + cols - 1) / cols, (d.n + r - 1) / r, B);
@@ -895,6 +1171,23 @@ void launch_wide_form(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps
                                                                     ext_in, ext_out);
 }
 
+template <int R>
+void launch_bulk(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, const DiaWide& w, int in_sel,
+                 int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out) {
+  const int nr = wide_nr(w.nr), np = wide_np(w.np);
+  DiaBulk pl;
+  size_t sm = 0;
+  plan_bulk(d, w, R, nr, np, &pl, &sm);  // rows_for checked that it fits
+  if (nr == 4 && np == 2)
+    rhs_dia_bulk_kernel<R, 4, 2><<<g, kBulkW, sm, s>>>(c, d, w, pl, in_sel, out_k, need_run, kry, ext_in, ext_out);
+  else if (nr == 4)
+    rhs_dia_bulk_kernel<R, 4, 4><<<g, kBulkW, sm, s>>>(c, d, w, pl, in_sel, out_k, need_run, kry, ext_in, ext_out);
+  else if (np == 2)
+    rhs_dia_bulk_kernel<R, 8, 2><<<g, kBulkW, sm, s>>>(c, d, w, pl, in_sel, out_k, need_run, kry, ext_in, ext_out);
+  else
+    rhs_dia_bulk_kernel<R, 8, 4><<<g, kBulkW, sm, s>>>(c, d, w, pl, in_sel, out_k, need_run, kry, ext_in, ext_out);
+}
+
 template <int R, int C, int U = 1>
 void launch_wide(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, const DiaWide& w, int in_sel,
                  int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out, bool herm) {
@@ -909,7 +1202,17 @@ void launch_wide(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, 
 void launch_rhs_dia(cudaStream_t s, const big::Common& c, const DiaOps& d, int B, int rows, int in_sel,
                     int out_k, int need_run, const float2* ext_in, float2* ext_out, int kry = 0,
                     bool herm = false) {
+  if (is_bulk(rows) && !herm) rows = 308;  // the bulk kernel is hermitian-only
   const dim3 g = rhs_grid(d, rows, B);
+  if (is_bulk(rows)) {
+    DiaWide w;
+    plan_wide(d, 2, &w);
+    if (rows == 604)
+      launch_bulk<4>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
+    else
+      launch_bulk<8>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
+    return;
+  }
   if (is_wide(rows)) {
     DiaWide w;
     plan_wide(d, wide_c(rows), &w);  // rows_for checked that it fits
@@ -994,6 +1297,18 @@ static void init_carveouts() {
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            16 * (kRhsCols * 4 + 1) * (int)sizeof(float2));
     };
+    auto bulk_attr = [](auto kern) {
+      prefer_max_shared(kern);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageMaxSmem);
+    };
+    bulk_attr(rhs_dia_bulk_kernel<4, 4, 2>);
+    bulk_attr(rhs_dia_bulk_kernel<4, 4, 4>);
+    bulk_attr(rhs_dia_bulk_kernel<4, 8, 2>);
+    bulk_attr(rhs_dia_bulk_kernel<4, 8, 4>);
+    bulk_attr(rhs_dia_bulk_kernel<8, 4, 2>);
+    bulk_attr(rhs_dia_bulk_kernel<8, 4, 4>);
+    bulk_attr(rhs_dia_bulk_kernel<8, 8, 2>);
+    bulk_attr(rhs_dia_bulk_kernel<8, 8, 4>);
     herm_attr(rhs_dia_wide_kernel<16, 4, 2, 4, true>);
     herm_attr(rhs_dia_wide_kernel<16, 4, 4, 4, true>);
     herm_attr(rhs_dia_wide_kernel<16, 8, 2, 4, true>);
@@ -1034,7 +1349,9 @@ extern "C" int dqb_lindblad_rhs_dia_tiled(const dqb_dia_problem* p, int32_t form
   big::Common c;
   std::memset(&c, 0, sizeof(c));
   int rows = rows_for(d, tile);
-  if (is_wide(rows) && ((reinterpret_cast<uintptr_t>(rho) | reinterpret_cast<uintptr_t>(outp)) & 15)) rows = 1;
+  if ((is_wide(rows) || is_bulk(rows)) &&
+      ((reinterpret_cast<uintptr_t>(rho) | reinterpret_cast<uintptr_t>(outp)) & 15))
+    rows = 1;
   launch_rhs_dia(s, c, d, (int)p->batch, rows, 2, 0, 0, (const float2*)rho, (float2*)outp, 0,
                  form == DQB_FORM_HERMITIAN);
   return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
@@ -1090,7 +1407,7 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   if (grid_e < 1) grid_e = 1;
   const dim3 ge(grid_e, B);
   int rows = rows_for(d, o->tile);
-  if (is_wide(rows) && (reinterpret_cast<uintptr_t>(c.mats) & 15)) rows = 1;
+  if ((is_wide(rows) || is_bulk(rows)) && (reinterpret_cast<uintptr_t>(c.mats) & 15)) rows = 1;
   const bool krylov = o->stepper == DQB_STEPPER_KRYLOV;
   const bool herm = o->form == DQB_FORM_HERMITIAN;
   const dim3 gi((B + 127) / 128);

@@ -91,7 +91,10 @@ typedef struct dqb_ode_options {
                               staged kernel with 8 or 16 rows per CTA; 208 or 216 (4
                               columns per thread), 308 or 316 (2 columns) = wide kernel
                               with 8 or 16 rows per CTA, 408 / 508 = 8 rows with two
-                              rows in flight per thread; 0 (default) or 1 = generic
+                              rows in flight per thread; 604 / 608 = bulk-staged kernel
+                              (rows of X copied into shared memory by the bulk-copy
+                              engine, stages of 4 / 8 rows; hermitian form, else 308);
+                              0 (default) or 1 = generic
                               kernel; shapes that do not fit the operators fall back to
                               the generic kernel; ignored by other paths                  */
   int32_t stepper;         /* DQB_STEPPER_* (0 = AUTO): how the sparse-DIA and dense GEMM

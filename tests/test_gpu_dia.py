@@ -51,7 +51,7 @@ def _problem_struct(H, Ls, n, batch):
     return p, [h_off, l_nd, l_off, H_d, L_d]
 
 
-@pytest.mark.parametrize('tile', [0, 8, 108, 116, 208, 316, 408, 508])
+@pytest.mark.parametrize('tile', [0, 8, 108, 116, 208, 316, 408, 508, 604, 608])
 @pytest.mark.parametrize('form', [_lib.FORM_HERMITIAN, _lib.FORM_STANDARD])
 @pytest.mark.parametrize('n', [10, 77, 300])
 def test_rhs_dia_matches_oracle(cuda_device, form, n, tile):
@@ -156,7 +156,7 @@ def coupled_kerr_4096_rhs():
     return w, X, ref
 
 
-@pytest.mark.parametrize('tile', [0, 4, 8, 16, 108, 116, 208, 216, 308, 316, 408, 508])
+@pytest.mark.parametrize('tile', [0, 4, 8, 16, 108, 116, 208, 216, 308, 316, 408, 508, 604, 608])
 def test_rhs_dia_full_size_every_stencil(cuda_device, coupled_kerr_4096_rhs, tile):
     """One right-hand side at n = 4096 with the workload's own offsets (+-63/+-64 select
     other row groups in the staged kernel and other halos in the tiled one than the small
@@ -262,3 +262,32 @@ def test_krylov_stepper_vs_stages_and_oracle(cuda_device, method, hermitian):
         assert err['stages'][0] <= 2 * ref_s + 1e-6, (err, ref_s)
         for i in (0, 1):
             assert err['krylov'][i] <= max(2 * err['stages'][i], 0.5 * m.rtol), err
+
+
+@pytest.mark.parametrize('tile', [604, 608, 208, 0])
+@pytest.mark.parametrize('m', [20, 30])
+def test_rhs_dia_bulk_ragged_edges(cuda_device, m, tile):
+    """The bulk-staged stencil (and the wide one) on coupled-Kerr operators whose size is not
+    a multiple of the 256-column CTA band (n = 400, 900): clipped copies, zero-filled halos
+    and partial row bands, against the oracle at 2e-6, with the output hermitian to the bit."""
+    w = workloads.coupled_kerr_dia(batch=1, m=m, seed=3)
+    n = m * m
+    rng = np.random.default_rng(n)
+    Y = (rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))) / (2 * n)
+    X = (Y + np.conj(Y.T)).astype(np.complex64)
+    Hb = (w['H'].offsets, w['H'].diags[0].astype(complex))
+    Lb = [(L.offsets, L.diags.astype(complex)) for L in w['jump_ops']]
+    ref = lb.vf_hermitian_dia(Hb, Lb, X.astype(complex))
+    Ls = [SparseDIA(L.offsets, L.diags[None]) for L in w['jump_ops']]
+    p, keep = _problem_struct(w['H'], Ls, n, 1)
+    r_d = torch.from_numpy(np.ascontiguousarray(X[None])).to('cuda')
+    out = torch.empty_like(r_d)
+    ws = torch.empty(1 << 22, dtype=torch.uint8, device='cuda')
+    lib = _lib.load()
+    _lib.check(lib.dqb_lindblad_rhs_dia_tiled(p, _lib.FORM_HERMITIAN, tile, r_d.data_ptr(),
+                                              out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                              torch.cuda.current_stream().cuda_stream), 'rhs_dia')
+    got = out[0].cpu().numpy()
+    assert rel_frob(got, ref) < 2e-6
+    if tile >= 200:
+        assert np.array_equal(got, np.conj(got.T))

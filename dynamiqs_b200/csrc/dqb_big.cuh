@@ -654,7 +654,7 @@ __device__ inline void kry_alpha(int method, double al[7][7]) {
 
 // Coefficients of u_0..u_7 in y1 (cy), the error (ce) and tau L y1 (cs) for r = h / tau;
 // the stored u_1 is scaled by sig1.
-__device__ inline void kry_step_coefs(int method, double r, double sig1, double cy[8], double ce[8], double cs[8]) {
+__device__ inline void kry_step_coefs(int method, double r, double sig1, float cy[8], float ce[8], float cs[8]) {
   const Tableau& T = c_tab[method];
   double al[7][7];
   kry_alpha(method, al);
@@ -674,24 +674,24 @@ __device__ inline void kry_step_coefs(int method, double r, double sig1, double 
   }
   for (int q = 0; q < 8; ++q) {
     const double s = q == 1 ? sig1 : 1.0;
-    cy[q] = beta[q] * rp[q] * s;
-    ce[q] = eps[q] * rp[q] * s;
-    cs[q] = q == 0 ? 0.0 : beta[q - 1] * rp[q - 1] * s;
+    cy[q] = (float)(beta[q] * rp[q] * s);
+    ce[q] = (float)(eps[q] * rp[q] * s);
+    cs[q] = q == 0 ? 0.f : (float)(beta[q - 1] * rp[q - 1] * s);
   }
 }
 
 // Coefficients of u_0..u_7 in the dense output at theta (same scaling rules).
-__device__ inline void kry_dense_coefs(int method, double theta, double r, double sig1, double cw[8]) {
+__device__ inline void kry_dense_coefs(int method, double theta, double r, double sig1, float cw[8]) {
   double al[7][7], w[7];
   kry_alpha(method, al);
   dense_weights(method, theta, w);
   double rp = 1.0;
-  cw[0] = 1.0;
+  cw[0] = 1.f;
   for (int q = 1; q < 8; ++q) {
     rp *= r;
     double d = 0.0;
     for (int j = 0; j < 7; ++j) d += w[j] * al[j][q - 1];
-    cw[q] = d * rp * (q == 1 ? sig1 : 1.0);
+    cw[q] = (float)(d * rp * (q == 1 ? sig1 : 1.0));
   }
 }
 
@@ -707,7 +707,6 @@ constexpr int kSaveChunk = 4;
 static __global__ void save_kernel(Common c, int mode) {
   __shared__ double red[40];
   __shared__ float cws[kSaveChunk][8];
-  __shared__ double cwd[kSaveChunk][8];  // mode 2: FP64 weights and sums (see kry_combine_kernel)
   const int b = blockIdx.y;
   const Inst& I = c.inst[b];
   const int lo = I.save_lo, hi = I.save_hi;
@@ -725,7 +724,7 @@ static __global__ void save_kernel(Common c, int mode) {
       float* cw = cws[threadIdx.x];
       const double theta = I.h > 0.0 ? (I.ts[s0 + threadIdx.x] - I.t) / I.h : 1.0;
       if (mode == 2) {
-        kry_dense_coefs(c.o.method, theta, kry_ratio(I), I.sig1, cwd[threadIdx.x]);
+        kry_dense_coefs(c.o.method, theta, kry_ratio(I), I.sig1, cw);
       } else {
         double w[7];
         dense_weights(c.o.method, theta, w);
@@ -759,15 +758,8 @@ static __global__ void save_kernel(Common c, int mode) {
         for (int si = 0; si < kSaveChunk; ++si) {
           if (si < ns) {
             float2 v = make_float2(0.f, 0.f);
-            if (mode == 2) {
-              double2 vd = make_double2(0.0, 0.0);
 #pragma unroll
-              for (int q = 0; q < 8; ++q) vd = zaxpy(cwd[si][q], x[q], vd);
-              v = make_float2((float)vd.x, (float)vd.y);
-            } else {
-#pragma unroll
-              for (int q = 0; q < 8; ++q) v = caxpy(cws[si][q], x[q], v);
-            }
+            for (int q = 0; q < 8; ++q) v = caxpy(cws[si][q], x[q], v);
             if (m0 == 0 && I.save_states) I.states[(long long)(s0 + si) * c.nn + e] = v;
             if (mc > 0) {
               // tr(E rho) = sum_ij E_ij rho_ji; rho_ji = conj(rho_ij) when rho is hermitian
@@ -775,16 +767,9 @@ static __global__ void save_kernel(Common c, int mode) {
               if (herm) {
                 rt = cconj(v);
               } else {
-                if (mode == 2) {
-                  double2 rd = make_double2(0.0, 0.0);
+                rt = make_float2(0.f, 0.f);
 #pragma unroll
-                  for (int q = 0; q < 8; ++q) rd = zaxpy(cwd[si][q], xt[q], rd);
-                  rt = make_float2((float)rd.x, (float)rd.y);
-                } else {
-                  rt = make_float2(0.f, 0.f);
-#pragma unroll
-                  for (int q = 0; q < 8; ++q) rt = caxpy(cws[si][q], xt[q], rt);
-                }
+                for (int q = 0; q < 8; ++q) rt = caxpy(cws[si][q], xt[q], rt);
               }
 #pragma unroll
               for (int m = 0; m < 2; ++m) {
@@ -854,13 +839,13 @@ static __global__ void commit_kernel(Common c, cudaGraphConditionalHandle handle
 // every running instance (a retried step included).
 static __global__ void kry_combine_kernel(Common c) {
   __shared__ double red[40];
-  __shared__ double cf[3][8];
+  __shared__ float cf[3][8];
   const int b = blockIdx.y;
   Inst& I = c.inst[b];
   if (!I.run) return;
   if (threadIdx.x == 0) kry_step_coefs(c.o.method, kry_ratio(I), I.sig1, cf[0], cf[1], cf[2]);
   __syncthreads();
-  double cy[8], ce[8], cs[8];
+  float cy[8], ce[8], cs[8];
 #pragma unroll
   for (int q = 0; q < 8; ++q) cy[q] = cf[0][q], ce[q] = cf[1][q], cs[q] = cf[2][q];
   const float2* u[8];
@@ -872,20 +857,19 @@ static __global__ void kry_combine_kernel(Common c) {
   const double atol = c.o.atol, rtol = c.o.rtol;
   double s = 0.0;
   auto one = [&](const float2 (&v)[8], float2& oy, float2& os) {
-    // FP64 sums: the expanded polynomial cancels, FP32 sums would round it worse than the
-    // stage form's nested evaluation
-    double2 a = make_double2(0.0, 0.0), e = make_double2(0.0, 0.0), f = make_double2(0.0, 0.0);
+    float2 a = make_float2(0.f, 0.f), e = make_float2(0.f, 0.f), f = make_float2(0.f, 0.f);
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      a = zaxpy(cy[q], v[q], a);
-      e = zaxpy(ce[q], v[q], e);
-      f = zaxpy(cs[q], v[q], f);
+      a = caxpy(cy[q], v[q], a);
+      e = caxpy(ce[q], v[q], e);
+      f = caxpy(cs[q], v[q], f);
     }
-    oy = make_float2((float)a.x, (float)a.y);
-    os = make_float2((float)f.x, (float)f.y);
-    const float ya = cabsf(v[0]), y1a = cabsf(oy);
+    oy = a;
+    os = f;
+    const float ya = cabsf(v[0]), y1a = cabsf(a);
     const double sc = atol + rtol * (double)(ya > y1a ? ya : y1a);
-    s += (e.x * e.x + e.y * e.y) / (sc * sc);
+    const double ex = e.x, ey = e.y;
+    s += (ex * ex + ey * ey) / (sc * sc);
   };
   if ((c.nn & 1) == 0 && (reinterpret_cast<uintptr_t>(c.mats) & 15) == 0) {
     // two complex values per 16-byte access, as in combine_kernel
@@ -920,7 +904,7 @@ static __global__ void kry_combine_kernel(Common c) {
 template <bool VEC>
 static __global__ void kry_combine_h_kernel(Common c) {
   __shared__ double red[40];
-  __shared__ double cf[3][8];
+  __shared__ float cf[3][8];
   __shared__ float2 sh[kHT][kHT + 1];
   const int b = blockIdx.y;
   Inst& I = c.inst[b];
@@ -930,42 +914,38 @@ static __global__ void kry_combine_h_kernel(Common c) {
   const int n = c.n, T = (n + kHT - 1) / kHT;
   int ti, tj;
   herm_tile(blockIdx.x, T, ti, tj);
-  // FP64 sums, as in kry_combine_kernel
-  float2 u0[4], w[4];
-  double2 vy[4], ve[4], vs[4];
+  float2 u0[4], vy[4], ve[4], vs[4], w[4];
   htile_load<VEC>(slot(c, b, I.sy), n, ti, tj, u0);
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    vy[q] = zaxpy(cf[0][0], u0[q], make_double2(0.0, 0.0));
-    ve[q] = make_double2(0.0, 0.0);
-    vs[q] = make_double2(0.0, 0.0);
+    vy[q] = make_float2(cf[0][0] * u0[q].x, cf[0][0] * u0[q].y);
+    ve[q] = make_float2(0.f, 0.f);
+    vs[q] = make_float2(0.f, 0.f);
   }
 #pragma unroll
   for (int k = 1; k < 8; ++k) {
     htile_load<VEC>(slot(c, b, I.sk[k - 1]), n, ti, tj, w);
-    const double a = cf[0][k], e = cf[1][k], f = cf[2][k];
+    const float a = cf[0][k], e = cf[1][k], f = cf[2][k];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      vy[q] = zaxpy(a, w[q], vy[q]);
-      ve[q] = zaxpy(e, w[q], ve[q]);
-      vs[q] = zaxpy(f, w[q], vs[q]);
+      vy[q] = caxpy(a, w[q], vy[q]);
+      ve[q] = caxpy(e, w[q], ve[q]);
+      vs[q] = caxpy(f, w[q], vs[q]);
     }
   }
-  float2 oy[4], os[4];
   double s = 0.0;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    oy[q] = make_float2((float)vy[q].x, (float)vy[q].y);
-    os[q] = make_float2((float)vs[q].x, (float)vs[q].y);
     if (htile_in<VEC>(n, ti, tj, q)) {
-      const float ya = cabsf(u0[q]), y1a = cabsf(oy[q]);
+      const float ya = cabsf(u0[q]), y1a = cabsf(vy[q]);
       const double sc = c.o.atol + c.o.rtol * (double)(ya > y1a ? ya : y1a);
-      s += (ve[q].x * ve[q].x + ve[q].y * ve[q].y) / (sc * sc);
+      const double ex = ve[q].x, ey = ve[q].y;
+      s += (ex * ex + ey * ey) / (sc * sc);
     }
   }
   if (ti != tj) s *= 2.0;
-  herm_store<VEC>(slot(c, b, I.sy1), n, ti, tj, oy, sh);
-  herm_store<VEC>(slot(c, b, I.sf), n, ti, tj, os, sh);
+  herm_store<VEC>(slot(c, b, I.sy1), n, ti, tj, vy, sh);
+  herm_store<VEC>(slot(c, b, I.sf), n, ti, tj, vs, sh);
   block_atomic_add(s, &I.acc[0], red);
 }
 

@@ -171,9 +171,6 @@ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(
 __device__ __forceinline__ float2 caxpy(float s, float2 x, float2 y) {  // y + s x
   return make_float2(fmaf(s, x.x, y.x), fmaf(s, x.y, y.y));
 }
-__device__ __forceinline__ double2 zaxpy(double s, float2 x, double2 y) {  // y + s x in FP64
-  return make_double2(fma(s, (double)x.x, y.x), fma(s, (double)x.y, y.y));
-}
 __device__ __forceinline__ float cabs2f(float2 a) { return fmaf(a.x, a.x, a.y * a.y); }
 __device__ __forceinline__ float cabsf(float2 a) { return sqrtf(cabs2f(a)); }
 

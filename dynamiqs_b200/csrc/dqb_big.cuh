@@ -800,6 +800,96 @@ static __global__ void save_kernel(Common c, int mode) {
   }
 }
 
+// save_kernel for the hermitian form: one 32 x 32 tile of the upper triangle per block
+// (grid (T (T + 1) / 2, B), 256 threads), so every input is read on its upper tiles only
+// -- half the bytes, and a stage slot that holds only those tiles is enough -- and each
+// saved state is written with its mirror (herm_store).  For hermitian rho,
+// tr(E rho) = sum_ij E_ij conj(rho_ij): a diagonal tile adds its own elements, an
+// off-diagonal one E_ij conj(rho_ij) + E_ji rho_ij for each of its elements.  The states
+// are the same FP32 sums in the same order as save_kernel's.
+template <bool VEC>
+static __global__ void save_h_kernel(Common c, int mode) {
+  __shared__ double red[40];
+  __shared__ float cws[kSaveChunk][8];
+  __shared__ float2 sh[kHT][kHT + 1];
+  const int b = blockIdx.y;
+  const Inst& I = c.inst[b];
+  const int lo = I.save_lo, hi = I.save_hi;
+  if (hi <= lo) return;
+  const int n = c.n, T = (n + kHT - 1) / kHT;
+  int ti, tj;
+  herm_tile(blockIdx.x, T, ti, tj);
+  const int nq = mode == 0 ? 1 : 8;
+  const HTile<VEC> t;
+  for (int s0 = lo; s0 < hi; s0 += kSaveChunk) {
+    const int ns = hi - s0 < kSaveChunk ? hi - s0 : kSaveChunk;
+    __syncthreads();  // the previous chunk's weights are no longer read
+    if (threadIdx.x < ns) {
+      float* cw = cws[threadIdx.x];
+      const double theta = I.h > 0.0 ? (I.ts[s0 + threadIdx.x] - I.t) / I.h : 1.0;
+      if (mode == 2) {
+        kry_dense_coefs(c.o.method, theta, kry_ratio(I), I.sig1, cw);
+      } else {
+        double w[7];
+        dense_weights(c.o.method, theta, w);
+        cw[0] = 1.f;
+        for (int j = 0; j < 7; ++j) cw[j + 1] = mode == 0 ? 0.f : (float)(I.h * w[j]);
+      }
+    }
+    __syncthreads();
+    float2 vs[kSaveChunk][4];
+#pragma unroll
+    for (int si = 0; si < kSaveChunk; ++si)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) vs[si][e] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      if (q < nq) {
+        float2 x[4];
+        htile_load<VEC>(slot(c, b, q == 0 ? I.sy : I.sk[q - 1]), n, ti, tj, x);
+#pragma unroll
+        for (int si = 0; si < kSaveChunk; ++si)
+          if (si < ns) {
+            const float w = cws[si][q];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) vs[si][e] = caxpy(w, x[e], vs[si][e]);
+          }
+      }
+    }
+#pragma unroll
+    for (int si = 0; si < kSaveChunk; ++si) {
+      if (si >= ns) break;  // uniform over the block
+      const float2(&v)[4] = vs[si];
+      if (I.save_states) herm_store<VEC>(I.states + (long long)(s0 + si) * c.nn, n, ti, tj, v, sh);
+      for (int m = 0; m < I.nE; ++m) {
+        const float2* E = I.E + (long long)m * c.nn;
+        double sr = 0.0, sim = 0.0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          if (htile_in<VEC>(n, ti, tj, e)) {
+            const long long r = ti * kHT + t.row(e), cc = tj * kHT + t.col(e);
+            const float2 a = E[r * n + cc];
+            sr += (double)a.x * v[e].x + (double)a.y * v[e].y;
+            sim += (double)a.y * v[e].x - (double)a.x * v[e].y;
+            if (ti != tj) {
+              const float2 a2 = E[cc * n + r];
+              sr += (double)a2.x * v[e].x - (double)a2.y * v[e].y;
+              sim += (double)a2.x * v[e].y + (double)a2.y * v[e].x;
+            }
+          }
+        }
+        sr = block_sum(sr, red);
+        sim = block_sum(sim, red);
+        if (threadIdx.x == 0) {
+          double2* acc = I.eacc + (long long)m * I.nts + s0 + si;
+          atomicAdd(&acc->x, sr);
+          atomicAdd(&acc->y, sim);
+        }
+      }
+    }
+  }
+}
+
 // One block: per-instance commit, then the WHILE-node condition (or, when the loop is
 // driven from the host, the same condition written to `flag`).
 static __global__ void commit_kernel(Common c, cudaGraphConditionalHandle handle, int* flag) {
@@ -1016,6 +1106,16 @@ inline void launch_error(cudaStream_t s, const Common& c, dim3 ge) {
     error_h_kernel<true><<<herm_grid(c.n, c.B), 256, 0, s>>>(c);
   else
     error_h_kernel<false><<<herm_grid(c.n, c.B), 256, 0, s>>>(c);
+}
+// Saves of an accepted step (or the leftovers, mode 0); the hermitian form reads the
+// upper tiles of its inputs only.
+inline void launch_save(cudaStream_t s, const Common& c, dim3 ge, int mode) {
+  if (c.form != DQB_FORM_HERMITIAN)
+    save_kernel<<<ge, kElemThreads, 0, s>>>(c, mode);
+  else if (herm_vec(c))
+    save_h_kernel<true><<<herm_grid(c.n, c.B), 256, 0, s>>>(c, mode);
+  else
+    save_h_kernel<false><<<herm_grid(c.n, c.B), 256, 0, s>>>(c, mode);
 }
 inline void launch_kry_combine(cudaStream_t s, const Common& c, dim3 ge) {
   if (c.form != DQB_FORM_HERMITIAN)

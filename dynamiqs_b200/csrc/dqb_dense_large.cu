@@ -871,6 +871,8 @@ static void init_carveouts() {
     prefer_max_shared(big::init_ctrl_kernel);
     prefer_max_shared(big::control_kernel);
     prefer_max_shared(big::save_kernel);
+    prefer_max_shared(big::save_h_kernel<true>);
+    prefer_max_shared(big::save_h_kernel<false>);
     prefer_max_shared(big::commit_kernel);
     prefer_max_shared(big::kry_combine_kernel);
     prefer_max_shared(big::combine_h_kernel<true>);
@@ -932,7 +934,7 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bo
       for (int q = 1; q <= 6; ++q) launch_rhs(cs, c, d, B, q + 2, q, 1, form, nullptr, nullptr, q);
       big::launch_kry_combine(cs, c, ge);
       big::control_kernel<<<gi, 128, 0, cs>>>(c);
-      big::save_kernel<<<ge, T, 0, cs>>>(c, 2);
+      big::launch_save(cs, c, ge, 2);
       big::kry_commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
       if (c.rag) big::retire_kernel<<<B, 256, 0, cs>>>(c);
       return;
@@ -945,7 +947,7 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bo
     launch_rhs(cs, c, d, B, 1, 6, 1, form, nullptr, nullptr);
     big::launch_error(cs, c, ge);
     big::control_kernel<<<gi, 128, 0, cs>>>(c);
-    big::save_kernel<<<ge, T, 0, cs>>>(c, 1);
+    big::launch_save(cs, c, ge, 1);
     big::commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
     if (c.rag) big::retire_kernel<<<B, 256, 0, cs>>>(c);
   };
@@ -968,7 +970,7 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bo
     if (cudaGraphLaunch(exec, s) != cudaSuccess) return DQB_ERR_CUDA;
   }
   big::pre_finalize_kernel<<<gi, 128, 0, s>>>(c);
-  big::save_kernel<<<ge, T, 0, s>>>(c, 0);
+  big::launch_save(s, c, ge, 0);
   big::finalize_kernel<<<ge, T, 0, s>>>(c);
   return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
 }

@@ -499,11 +499,15 @@ __device__ __forceinline__ void wide_load(const float2* __restrict__ rp, int col
 // once -- and each strictly-upper element is also written, conjugated, at its mirror
 // position, through a shared-memory strip of the CTA's R x (128 C) outputs so that the
 // mirrored rows leave as contiguous R-value segments.  About half the stencil work, and
-// the output is hermitian to the last bit.
+// the output is hermitian to the last bit.  `half` (HERM only): write the 32 x 32 tiles on
+// and above the diagonal and nothing else -- every element (i, j) with j >= 32 floor(i / 32),
+// the set the hermitian-half elementwise kernels read -- and no mirror, for a stage slot
+// that only those kernels consume.
 template <int R, int NR, int NP, int C, bool HERM, int U = 1>
 __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c, DiaOps d, DiaWide w, int in_sel,
                                                                   int out_k, int need_run, int kry,
-                                                                  const float2* ext_in, float2* ext_out) {
+                                                                  const float2* ext_in, float2* ext_out,
+                                                                  int half) {
   constexpr int NT = 1 + NR + NP;  // row-table terms: center, rows, pairs
   constexpr int W = kRhsCols * C;  // columns of the CTA's tile
   constexpr int SW = W + 1;        // row stride of the strip (the mirror reads down columns)
@@ -511,7 +515,8 @@ __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c
   extern __shared__ float2 strip[];  // [R][SW] when HERM
   const int i0 = blockIdx.y * R;
   const int j0 = blockIdx.x * W;
-  if (HERM && j0 + W - 1 < i0) return;  // the whole tile is below the diagonal
+  const int hmask = half ? ~31 : ~0;      // R divides 32: one diagonal tile row per CTA
+  if (HERM && j0 + W - 1 < (i0 & hmask)) return;  // the whole tile is below the diagonal
   const int b = blockIdx.z;
   const float2* X;
   float2* out;
@@ -586,7 +591,8 @@ __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c
 #pragma unroll U  // U = 2: two rows' loads in flight per thread
   for (int r = 0; r < rows; ++r) {
     const int i = i0 + r;
-    if (HERM && j + C - 1 < i) break;  // this and the later rows lie below the diagonal
+    const int ilim = i & hmask;              // first column written in row i
+    if (HERM && j + C - 1 < ilim) break;  // this and the later rows lie below the diagonal
     const float2* Xi = X + (long long)i * n;
     float2 acc[C];
     float2 v[C];
@@ -619,7 +625,7 @@ __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c
     for (int q = 0; q < C; ++q) acc[q] = make_float2(acc[q].x * scale, acc[q].y * scale);
     if (HERM && j <= i && i < j + C) acc[i - j].y = 0.f;  // a hermitian matrix's diagonal is real
     float2* orow = out + (long long)i * n + j;
-    if (!HERM || j >= i) {  // every column on or above the diagonal
+    if (!HERM || j >= ilim) {  // every column on or above the diagonal (its tile)
 #pragma unroll
       for (int h = 0; h < C / 2; ++h)
         reinterpret_cast<float4*>(orow)[h] = make_float4(acc[2 * h].x, acc[2 * h].y, acc[2 * h + 1].x, acc[2 * h + 1].y);
@@ -628,13 +634,13 @@ __global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c
       for (int q = 0; q < C; ++q)
         if (j + q >= i) orow[q] = acc[q];
     }
-    if (HERM) {
+    if (HERM && !half) {
 #pragma unroll
       for (int q = 0; q < C; ++q) strip[r * SW + threadIdx.x * C + q] = acc[q];
     }
   }
   }  // active
-  if (HERM) {
+  if (HERM && !half) {
     // mirror: out[jj][i0 + r] = conj(f[i0 + r][jj]) for jj > i0 + r, R contiguous values per
     // target row (R threads per row, one value each)
     __syncthreads();
@@ -1154,21 +1160,22 @@ dim3 rhs_grid(const DiaOps& d, int rows, int B) {
 
 template <int R, int C, bool HERM, int U>
 void launch_wide_form(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, const DiaWide& w,
-                      int in_sel, int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out) {
+                      int in_sel, int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out,
+                      int half) {
   const int nr = wide_nr(w.nr), np = wide_np(w.np);
-  const size_t sm = HERM ? (size_t)R * (kRhsCols * C + 1) * sizeof(float2) : 0;
+  const size_t sm = HERM && !half ? (size_t)R * (kRhsCols * C + 1) * sizeof(float2) : 0;
   if (nr == 4 && np == 2)
     rhs_dia_wide_kernel<R, 4, 2, C, HERM, U><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
-                                                                    ext_in, ext_out);
+                                                                    ext_in, ext_out, half);
   else if (nr == 4)
     rhs_dia_wide_kernel<R, 4, 4, C, HERM, U><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
-                                                                    ext_in, ext_out);
+                                                                    ext_in, ext_out, half);
   else if (np == 2)
     rhs_dia_wide_kernel<R, 8, 2, C, HERM, U><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
-                                                                    ext_in, ext_out);
+                                                                    ext_in, ext_out, half);
   else
     rhs_dia_wide_kernel<R, 8, 4, C, HERM, U><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
-                                                                    ext_in, ext_out);
+                                                                    ext_in, ext_out, half);
 }
 
 template <int R>
@@ -1190,18 +1197,21 @@ void launch_bulk(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, 
 
 template <int R, int C, int U = 1>
 void launch_wide(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, const DiaWide& w, int in_sel,
-                 int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out, bool herm) {
+                 int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out, bool herm, bool half) {
   if (herm)
-    launch_wide_form<R, C, true, U>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
+    launch_wide_form<R, C, true, U>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, half ? 1 : 0);
   else
-    launch_wide_form<R, C, false, U>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out);
+    launch_wide_form<R, C, false, U>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, 0);
 }
 
 // One right-hand side of every instance: k[out_k] = f(input), through the kernel the shape
-// code `rows` selects (rows_for).
+// code `rows` selects (rows_for).  `half` (hermitian form): the output only has to hold the
+// 32 x 32 tiles on and above the diagonal (a stage slot read by the hermitian-half
+// elementwise kernels alone); the wide kernels then write nothing else, the others write
+// the whole matrix all the same.
 void launch_rhs_dia(cudaStream_t s, const big::Common& c, const DiaOps& d, int B, int rows, int in_sel,
                     int out_k, int need_run, const float2* ext_in, float2* ext_out, int kry = 0,
-                    bool herm = false) {
+                    bool herm = false, bool half = false) {
   if (is_bulk(rows) && !herm) rows = 308;  // the bulk kernel is hermitian-only
   const dim3 g = rhs_grid(d, rows, B);
   if (is_bulk(rows)) {
@@ -1217,12 +1227,12 @@ void launch_rhs_dia(cudaStream_t s, const big::Common& c, const DiaOps& d, int B
     DiaWide w;
     plan_wide(d, wide_c(rows), &w);  // rows_for checked that it fits
     switch (rows) {
-      case 208: launch_wide<8, 4>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm); break;
-      case 216: launch_wide<16, 4>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm); break;
-      case 308: launch_wide<8, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm); break;
-      case 408: launch_wide<8, 4, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm); break;
-      case 508: launch_wide<8, 2, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm); break;
-      default: launch_wide<16, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm);
+      case 208: launch_wide<8, 4>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm, half); break;
+      case 216: launch_wide<16, 4>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm, half); break;
+      case 308: launch_wide<8, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm, half); break;
+      case 408: launch_wide<8, 4, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm, half); break;
+      case 508: launch_wide<8, 2, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm, half); break;
+      default: launch_wide<16, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm, half);
     }
     return;
   }
@@ -1273,6 +1283,8 @@ static void init_carveouts() {
     prefer_max_shared(big::init_ctrl_kernel);
     prefer_max_shared(big::control_kernel);
     prefer_max_shared(big::save_kernel);
+    prefer_max_shared(big::save_h_kernel<true>);
+    prefer_max_shared(big::save_h_kernel<false>);
     prefer_max_shared(big::commit_kernel);
     prefer_max_shared(big::kry_combine_kernel);
     prefer_max_shared(big::combine_h_kernel<true>);
@@ -1439,19 +1451,19 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
       for (int q = 1; q <= 6; ++q) launch_rhs_dia(cs, c, d, B, rows, 0, 0, 1, nullptr, nullptr, q, herm);
       big::launch_kry_combine(cs, c, ge);
       big::control_kernel<<<gi, 128, 0, cs>>>(c);
-      big::save_kernel<<<ge, T, 0, cs>>>(c, 2);
+      big::launch_save(cs, c, ge, 2);
       big::kry_commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
       return;
     }
     for (int st = 0; st < 5; ++st) {
       big::launch_combine(cs, c, ge, st);
-      launch_rhs_dia(cs, c, d, B, rows, 2, st + 1, 1, nullptr, nullptr, 0, herm);
+      launch_rhs_dia(cs, c, d, B, rows, 2, st + 1, 1, nullptr, nullptr, 0, herm, herm);
     }
     big::launch_combine(cs, c, ge, 5);
-    launch_rhs_dia(cs, c, d, B, rows, 1, 6, 1, nullptr, nullptr, 0, herm);
+    launch_rhs_dia(cs, c, d, B, rows, 1, 6, 1, nullptr, nullptr, 0, herm, herm);
     big::launch_error(cs, c, ge);
     big::control_kernel<<<gi, 128, 0, cs>>>(c);
-    big::save_kernel<<<ge, T, 0, cs>>>(c, 1);
+    big::launch_save(cs, c, ge, 1);
     big::commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
   };
   if (host_loop_requested()) {
@@ -1477,7 +1489,7 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
 
   // ---- leftovers and outputs -----------------------------------------------------------
   big::pre_finalize_kernel<<<gi, 128, 0, s>>>(c);
-  big::save_kernel<<<ge, T, 0, s>>>(c, 0);
+  big::launch_save(s, c, ge, 0);
   big::finalize_kernel<<<ge, T, 0, s>>>(c);
   return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
 }

@@ -376,7 +376,9 @@ def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which, nsave=0
         if stepper != 'krylov':
             nbytes = stage_bytes
             note = ('bytes = 34 n^2 complex64 matrix passes per attempted RK step per '
-                    'instance (the fused stage-form minimum); the kernels make 54')
+                    'instance (the fused stage-form minimum of whole-matrix kernels); the '
+                    'hermitian-half kernels move 3.60 GB = 27 passes per attempt (measured '
+                    'DRAM bytes, see traffic)')
         else:
             # the Krylov form: per accepted step six right-hand sides build the basis (read
             # one matrix, write one: 12 passes); per attempt one pass reads u_0..u_7 and
@@ -436,17 +438,18 @@ def _roofline(config, precision, n, K, nsteps, mean_ms, B, peaks, which, nsave=0
 #     for 148 = 2.837 MB; inputs, states and expectation values, the RK slots stay in L2);
 #     profiles/mesolve_small_kernel_n64_kerr.md.
 #   dia / fp32, stage form: per attempted RK step of one instance (every kernel of the
-#     stepper, host loop: six hermitian-half stage combinations 2.37 GB, six hermitian-half
-#     stencils 0.92 GB, the hermitian-half error pass 0.61 GB: 3.90 GB) plus 1.34 GB per
-#     save point (the save pass reads y and the seven stages once, writes the state);
-#     profiles/dia_stepper_n4096_coupled_kerr_traffic.md.
-#   dia / fp32, Krylov form: 0.918 GB per accepted step (six basis stencils, 69.9 MB read
-#     + 83.0 MB written each), 0.777 GB per attempt (the hermitian-half combination pass:
-#     541.2 MB read, 236.0 MB written) and 1.34 GB per save point; same profile.
+#     stepper, host loop: six hermitian-half stage combinations 2.36 GB, six stencils
+#     writing the upper tiles of their stage slot 0.64 GB, the hermitian-half error pass
+#     0.61 GB: 3.60 GB) plus 0.81 GB per save point (a step that crosses saves reads the
+#     upper tiles of y, the seven stages and the expectation operators, 0.68 GB, and each
+#     save writes its state, 0.13 GB); profiles/dia_stepper_n4096_coupled_kerr_traffic.md.
+#   dia / fp32, Krylov form: 0.917 GB per accepted step (six basis stencils, 69.9 MB read
+#     + 82.9 MB written each), 0.774 GB per attempt (the hermitian-half combination pass:
+#     541.1 MB read, 233.3 MB written) and 0.81 GB per save point; same profile.
 TRAFFIC_PER_UNIT = {
     ('kerr', 'fp32', 'auto'): ('instance', 2.837e6, 0.0, 0.0),
-    ('dia', 'fp32', 'stages'): ('instance_step', 3.90e9, 0.0, 1.34e9),
-    ('dia', 'fp32', 'krylov'): ('instance_step', 0.777e9, 0.918e9, 1.34e9),
+    ('dia', 'fp32', 'stages'): ('instance_step', 3.60e9, 0.0, 0.81e9),
+    ('dia', 'fp32', 'krylov'): ('instance_step', 0.774e9, 0.917e9, 0.81e9),
 }
 
 

@@ -806,12 +806,15 @@ static __global__ void save_kernel(Common c, int mode) {
 // saved state is written with its mirror (herm_store).  For hermitian rho,
 // tr(E rho) = sum_ij E_ij conj(rho_ij): a diagonal tile adds its own elements, an
 // off-diagonal one E_ij conj(rho_ij) + E_ji rho_ij for each of its elements.  The states
-// are the same FP32 sums in the same order as save_kernel's.
+// are the same FP32 sums in the same order as save_kernel's.  The mirror tile of E is
+// staged through shared memory (row-wise loads), and the two parts of each trace are
+// reduced together.
 template <bool VEC>
 static __global__ void save_h_kernel(Common c, int mode) {
-  __shared__ double red[40];
+  __shared__ double red[72];
   __shared__ float cws[kSaveChunk][8];
   __shared__ float2 sh[kHT][kHT + 1];
+  __shared__ float2 shE[kHT][kHT + 1];
   const int b = blockIdx.y;
   const Inst& I = c.inst[b];
   const int lo = I.save_lo, hi = I.save_hi;
@@ -863,6 +866,15 @@ static __global__ void save_h_kernel(Common c, int mode) {
       if (I.save_states) herm_store<VEC>(I.states + (long long)(s0 + si) * c.nn, n, ti, tj, v, sh);
       for (int m = 0; m < I.nE; ++m) {
         const float2* E = I.E + (long long)m * c.nn;
+        if (ti != tj) {  // uniform over the block: E's tile (tj, ti) into shE
+          __syncthreads();  // the previous operator's tile has been read
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int r = tj * kHT + t.row(e), cc = ti * kHT + t.col(e);
+            shE[t.row(e)][t.col(e)] = (r < n && cc < n) ? E[(long long)r * n + cc] : make_float2(0.f, 0.f);
+          }
+          __syncthreads();
+        }
         double sr = 0.0, sim = 0.0;
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
@@ -872,18 +884,17 @@ static __global__ void save_h_kernel(Common c, int mode) {
             sr += (double)a.x * v[e].x + (double)a.y * v[e].y;
             sim += (double)a.y * v[e].x - (double)a.x * v[e].y;
             if (ti != tj) {
-              const float2 a2 = E[cc * n + r];
+              const float2 a2 = shE[t.col(e)][t.row(e)];  // E_ji
               sr += (double)a2.x * v[e].x - (double)a2.y * v[e].y;
               sim += (double)a2.x * v[e].y + (double)a2.y * v[e].x;
             }
           }
         }
-        sr = block_sum(sr, red);
-        sim = block_sum(sim, red);
+        const double2 tot = block_sum2(sr, sim, red);
         if (threadIdx.x == 0) {
           double2* acc = I.eacc + (long long)m * I.nts + s0 + si;
-          atomicAdd(&acc->x, sr);
-          atomicAdd(&acc->y, sim);
+          atomicAdd(&acc->x, tot.x);
+          atomicAdd(&acc->y, tot.y);
         }
       }
     }

@@ -204,6 +204,25 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return red[32];
 }
 
+// Sums of `a` and `b` over the block at once; every thread gets both.  `red` holds >= 66
+// doubles.
+__device__ __forceinline__ double2 block_sum2(double a, double b, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  a = warp_sum(a);
+  b = warp_sum(b);
+  __syncthreads();
+  if (lane == 0) red[wid] = a, red[32 + wid] = b;
+  __syncthreads();
+  if (wid == 0) {
+    double x = lane < nw ? red[lane] : 0.0, y = lane < nw ? red[32 + lane] : 0.0;
+    x = warp_sum(x);
+    y = warp_sum(y);
+    if (lane == 0) red[64] = x, red[65] = y;
+  }
+  __syncthreads();
+  return make_double2(red[64], red[65]);
+}
+
 // Zero a few words on a stream with a kernel (a memset would order itself against the
 // work of every other stream).
 static __global__ void zero_words_kernel(unsigned int* p, int n) {

@@ -107,6 +107,36 @@ def test_coupled_kerr_dia_small_vs_oracle(cuda_device):
         _oracle_compare(res, w, b)
 
 
+@pytest.mark.parametrize('tile', [1, 8, 208, 216, 308, 316, 408, 508, 608])
+@pytest.mark.parametrize('m', [10, 18])
+def test_dia_solve_every_stencil_shape_vs_oracle(cuda_device, m, tile):
+    """The DIA solve with the stencil shape forced, hermitian form: the wide shapes
+    (2xx-5xx) write the stage slots on the upper 32 x 32 tiles only (no mirror), the
+    others the whole matrix.  n = 100 and 324 (not multiples of the 32-row tiles or of the
+    CTA's column band) against the oracle, and every shape's states and expectation values
+    against the generic kernel's within the tolerance."""
+    from dynamiqs_b200.mesolve import MESolveB200Integrator, make_batch_plan
+
+    w = workloads.coupled_kerr_dia(batch=2, m=m, seed=5)
+    E = [np.diag(np.arange(m * m)).astype(np.complex64)]
+    plan = make_batch_plan(w['H'], w['jump_ops'], w['rho0'], True)
+    integ = MESolveB200Integrator(ts=w['tsave'], y0=w['rho0'], method=w['method'], gradient=None,
+                                  options=dq.Options(), H=w['H'], Ls=w['jump_ops'], Es=E, plan=plan)
+    prep = integ._prepare_dia(_lib.load())
+    integ._tuned['tile'] = tile
+    res = prep.launch().result()
+    for b in range(2):
+        _oracle_compare(res, w, b)
+    st = res.states.cpu().numpy().copy()  # (the next launch reuses the output buffers)
+    ex = res.expects.cpu().numpy().copy()
+    assert np.abs(st - np.conj(np.swapaxes(st, -1, -2))).max() < 1e-6
+    if m == 10:
+        integ._tuned['tile'] = 1
+        ref = prep.launch().result()
+        assert rel_frob(st, ref.states.cpu().numpy()).max() < w['method'].rtol
+        np.testing.assert_allclose(ex, ref.expects.cpu().numpy(), rtol=w['method'].rtol, atol=1e-6)
+
+
 def test_dia_path_equals_dense_kernel_at_n64(cuda_device):
     """Same problem through dqb_mesolve_dia and dqb_mesolve_dense (n = 64)."""
     w = workloads.coupled_kerr_dia(batch=3, m=8, seed=2)

@@ -247,6 +247,12 @@ SIGNATURES = {
     'dqb_sesolve_dense': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
                                          ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
     'dqb_schrodinger_rhs_dense': (ctypes.c_int, [ctypes.POINTER(DenseProblem), _P, _P, _P]),
+    'dqb_sesolve_large_workspace_size': (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32,
+                                                           ctypes.c_int32, ctypes.c_int64]),
+    'dqb_sesolve_dense_large': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(OdeOptions),
+                                               ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
+    'dqb_sesolve_dia': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.POINTER(OdeOptions),
+                                       ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
     'dqb_mesolve_vectorized': (ctypes.c_int, [ctypes.POINTER(DenseProblem), _P, ctypes.POINTER(OdeOptions),
                                               ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
     'dqb_version': (ctypes.c_char_p, []),

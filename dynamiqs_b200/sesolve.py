@@ -7,7 +7,10 @@ Same signature, argument checks and batching semantics as the reference: ``H`` o
 ``(...H, n, n)``, ``psi0`` ``(...psi0, n, 1)``, ``tsave`` ``(ntsave,)``, ``exp_ops`` a
 list of ``(n, n)``; cartesian batching gives results of shape ``(...H, ...psi0, ...)``,
 flat batching broadcasts ``...H`` against ``...psi0``.  ``method`` is ``Tsit5`` (default)
-or ``Dopri5``.  Dense ``H`` with n <= 128 (sparse-DIA operators are densified).
+or ``Dopri5``.  Three kernels, by size: n <= 128 one warp per instance
+(``dqb_sesolve_dense``; sparse-DIA ``H`` is densified); n up to 8192 the batched
+large-problem stepper with a dense ``H`` (``dqb_sesolve_dense_large``) or with ``H`` kept in
+sparse-DIA storage (``dqb_sesolve_dia``).
 """
 
 from __future__ import annotations
@@ -21,7 +24,7 @@ from .mesolve import (_as_op, _check_shape, _device, _MAX_STEPS_MSG, _shape, _to
                       assert_method_supported, check_times, make_batch_plan)
 from .method import Method, Tsit5
 from .options import Options, check_options
-from .qarrays import to_dense
+from .qarrays import SparseDIA, to_dense
 from .result import AdaptiveStepInfos, MESolveResult
 
 __all__ = ['sesolve', 'SESolveResult', 'SESolveB200Integrator']
@@ -41,21 +44,31 @@ def _check_sesolve_args(H, psi0, exp_ops) -> None:
             _check_shape(E, f'exp_ops[{i}]', '(n, n)')
 
 
+# largest n of the warp-per-instance kernel and of the large-problem stepper
+WARP_MAX_N = 128
+LARGE_MAX_N = 8192
+
+
 @dataclass
 class _Prepared:
     integ: 'SESolveB200Integrator'
     prob: object
     outs: object
     bufs: dict
+    fn: str = 'dqb_sesolve_dense'
+    host: tuple = ()  # host arrays the problem struct points to
 
     def launch(self, stream=None):
+        import ctypes
+
         import torch
 
         s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
         lib = _lib.load()
-        rc = lib.dqb_sesolve_dense(self.prob, self.integ._ode_options(), self.outs,
-                                   self.bufs['workspace'].data_ptr(), self.bufs['workspace'].numel(), s)
-        _lib.check(rc, 'dqb_sesolve_dense')
+        rc = getattr(lib, self.fn)(ctypes.byref(self.prob), ctypes.byref(self.integ._ode_options()),
+                                   ctypes.byref(self.outs), self.bufs['workspace'].data_ptr(),
+                                   self.bufs['workspace'].numel(), s)
+        _lib.check(rc, self.fn)
         return self
 
     def result(self) -> SESolveResult:
@@ -73,10 +86,14 @@ class SESolveB200Integrator:
         self.gradient = gradient
         self.options = options
         self.H = H
-        # the identity's expectation value <psi|psi> (FP64 sums) is the norm check
-        self._n_user_E = len(Es) if Es else 0
-        self.Es = list(Es or []) + [np.eye(_shape(H)[-1], dtype=np.complex64)]
         self.plan = plan
+        # the identity's expectation value <psi|psi> (FP64 sums) is the norm check; with H
+        # in DIA storage (large n) a dense identity would cost more than the solve, so the
+        # norm is taken from the returned states instead
+        self._n_user_E = len(Es) if Es else 0
+        self._norm_from_states = self.path == 'dia'
+        self.Es = list(Es or []) + ([] if self._norm_from_states
+                                    else [np.eye(_shape(H)[-1], dtype=np.complex64)])
 
     @property
     def t0(self) -> float:
@@ -91,7 +108,17 @@ class SESolveB200Integrator:
             factormax=float(m.max_factor), max_steps=int(m.max_steps), t0=self.t0,
             save_states=int(bool(self.options.save_states)), check_hermitian=0)
 
+    @property
+    def path(self) -> str:
+        """'warp' (n <= 128), 'dia' (sparse-DIA H beyond that) or 'dense_large'."""
+        n = _shape(self.H)[-1]
+        if n <= WARP_MAX_N:
+            return 'warp'
+        return 'dia' if isinstance(self.plan.H_items, SparseDIA) else 'dense_large'
+
     def prepare(self) -> _Prepared:
+        import ctypes
+
         import torch
 
         dev = _device()
@@ -102,8 +129,17 @@ class SESolveB200Integrator:
         nsave = ntsave if self.options.save_states else 1
         B = plan.batch
         c64 = torch.complex64
+        path = self.path
+        lib = _lib.load()
+        if path == 'warp':
+            ws_bytes = lib.dqb_sesolve_dense_workspace_size()
+        else:
+            ws_bytes = lib.dqb_sesolve_large_workspace_size(n, nE, ntsave, B)
+            if ws_bytes == 0:
+                raise NotImplementedError(f'sesolve on the B200 path supports n <= {LARGE_MAX_N}.')
+        dia = path == 'dia'
         bufs = {
-            'H': _to_dev(plan.H_items_dense(), c64, dev),
+            'H': _to_dev(plan.H_items.diags if dia else plan.H_items_dense(), c64, dev),
             'psi0': _to_dev(plan.rho_items, c64, dev),
             'E': (_to_dev(np.stack([to_dense(E) for E in self.Es]), c64, dev) if nE
                   else torch.zeros(1, dtype=c64, device=dev)),
@@ -114,18 +150,32 @@ class SESolveB200Integrator:
             'expects': torch.empty((B, max(nE, 1), ntsave), dtype=c64, device=dev),
             'infos': torch.empty((B, 3), dtype=torch.int32, device=dev),
             'status': torch.empty((B,), dtype=torch.int32, device=dev),
-            'workspace': torch.empty(_lib.load().dqb_sesolve_dense_workspace_size(),
-                                     dtype=torch.uint8, device=dev),
+            'workspace': torch.empty(ws_bytes, dtype=torch.uint8, device=dev),
         }
-        prob = _lib.DenseProblem(
-            n=n, n_jumps=0, n_exp=nE, n_tsave=ntsave, batch=B, H=bufs['H'].data_ptr(), L=None,
-            rho0=bufs['psi0'].data_ptr(), rho0_is_ket=1, E=bufs['E'].data_ptr(),
-            tsave=bufs['tsave'].data_ptr(), H_index=bufs['H_index'].data_ptr(), L_index=None,
-            rho0_index=bufs['psi0_index'].data_ptr())
+        host = ()
+        if dia:
+            offs = tuple(int(k) for k in plan.H_items.offsets)
+            h_off = (ctypes.c_int32 * max(len(offs), 1))(*offs)
+            host = (h_off,)
+            prob = _lib.DiaProblem(
+                n=n, n_jumps=0, n_exp=nE, n_tsave=ntsave, batch=B, h_ndiag=len(offs),
+                h_offsets=ctypes.cast(h_off, ctypes.c_void_p), h_diags=bufs['H'].data_ptr(),
+                l_ndiag=None, l_offsets=None, l_diags=None, rho0=bufs['psi0'].data_ptr(),
+                rho0_is_ket=1, E=bufs['E'].data_ptr(), tsave=bufs['tsave'].data_ptr(),
+                H_index=bufs['H_index'].data_ptr(), L_index=None,
+                rho0_index=bufs['psi0_index'].data_ptr())
+        else:
+            prob = _lib.DenseProblem(
+                n=n, n_jumps=0, n_exp=nE, n_tsave=ntsave, batch=B, H=bufs['H'].data_ptr(), L=None,
+                rho0=bufs['psi0'].data_ptr(), rho0_is_ket=1, E=bufs['E'].data_ptr(),
+                tsave=bufs['tsave'].data_ptr(), H_index=bufs['H_index'].data_ptr(), L_index=None,
+                rho0_index=bufs['psi0_index'].data_ptr())
         outs = _lib.Outputs(states=bufs['states'].data_ptr(), expects=bufs['expects'].data_ptr(),
                             infos=bufs['infos'].data_ptr(), status=bufs['status'].data_ptr())
         self._nE = nE
-        return _Prepared(self, prob, outs, bufs)
+        fn = {'warp': 'dqb_sesolve_dense', 'dense_large': 'dqb_sesolve_dense_large',
+              'dia': 'dqb_sesolve_dia'}[path]
+        return _Prepared(self, prob, outs, bufs, fn, host)
 
     def run(self) -> SESolveResult:
         return self.prepare().launch().result()
@@ -143,7 +193,11 @@ class SESolveB200Integrator:
         expects = ex[..., :self._n_user_E, :] if self._n_user_E else None
         import torch
 
-        checks = {'norm': ex[..., self._n_user_E, :].to(torch.complex128).real}
+        if self._norm_from_states:  # (..., nsave): every saved state, or the final one
+            sd = states.to(torch.complex128)
+            checks = {'norm': (sd.abs() ** 2).sum(dim=(-2, -1))}
+        else:
+            checks = {'norm': ex[..., self._n_user_E, :].to(torch.complex128).real}
         infos = b['infos'].reshape(*bshape, 3)
         info = AdaptiveStepInfos(infos[..., 0], infos[..., 1], infos[..., 2])
         extra = None
@@ -189,9 +243,10 @@ def sesolve(H, psi0, tsave, *, exp_ops=None, method: Method = Tsit5(),  # noqa: 
     n = _shape(H)[-1]
     if _shape(psi0)[-2] != n:
         raise ValueError(f'Argument `psi0` must have shape (..., {n}, 1).')
-    if n > 128:
-        raise NotImplementedError('sesolve on the B200 path supports n <= 128.')
-    H = to_dense(H) if not isinstance(H, np.ndarray) else H
+    if n > LARGE_MAX_N:
+        raise NotImplementedError(f'sesolve on the B200 path supports n <= {LARGE_MAX_N}.')
+    if n <= WARP_MAX_N or not isinstance(H, SparseDIA):
+        H = to_dense(H) if not isinstance(H, np.ndarray) else H
     plan = make_batch_plan(H, [], psi0, options.cartesian_batching)
     integ = SESolveB200Integrator(ts=tsave, y0=psi0, method=method, gradient=gradient,
                                   options=options, H=H, Es=exp_ops, plan=plan)

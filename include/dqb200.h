@@ -319,6 +319,24 @@ DQB_API int dqb_sesolve_dense(const dqb_dense_problem* problem, const dqb_ode_op
                               const dqb_outputs* outputs, void* workspace, size_t workspace_bytes,
                               void* stream);
 
+/* Scratch bytes of dqb_sesolve_dense_large and dqb_sesolve_dia (controller state, FP64
+ * expectation sums and ten n-vectors per instance); 0 for n > 8192. */
+DQB_API size_t dqb_sesolve_large_workspace_size(int32_t n, int32_t n_exp, int32_t n_tsave, int64_t batch);
+
+/* dqb_sesolve_dense beyond n = 128 (1 <= n <= 8192): the same solve (tableaux, starting
+ * step, controller, RMS error norm over psi, dense output, expectation values) on the
+ * batched large-problem stepper of dqb_mesolve_dense_large / dqb_mesolve_dia, whose slots
+ * hold n-vectors here; the right-hand side -i H x is one batched matrix-vector product per
+ * stage (one warp per row of H, x in shared memory), and <psi|E|psi> is summed in FP64 by
+ * the save pass.  Same problem and output conventions as dqb_sesolve_dense; the whole
+ * solve is one CUDA-graph launch (sesolve.py:240-330, diffrax_integrator.py:221-228). */
+DQB_API int dqb_sesolve_dense_large(const dqb_dense_problem* problem, const dqb_ode_options* options,
+                                    const dqb_outputs* outputs, void* workspace, size_t workspace_bytes,
+                                    void* stream);
+
+/* (dqb_sesolve_dia, the same solve with H in sparse-DIA storage, is declared with the
+ * sparse-DIA operators below.) */
+
 /* Batched adaptive solve of the vectorized master equation d vec(rho)/dt = S vec(rho)
  * (MESolveDiffraxIntegrator.vector_field_vec with options.vectorized=True,
  * diffrax_integrator.py:325-327; S = slindbladian(H, jump_ops), utils/vectorization.py:
@@ -449,6 +467,14 @@ typedef struct dqb_dia_problem {
   const int32_t* L_index;
   const int32_t* rho0_index;
 } dqb_dia_problem;
+
+/* dqb_sesolve_dense_large with H in sparse-DIA storage (n_jumps = 0, psi0 as kets
+ * [*, n, 1] in rho0 whatever rho0_is_ket says, dense exp_ops, 1 <= n <= 8192; workspace
+ * from dqb_sesolve_large_workspace_size): -i H x as out_i = -i sum_d diag_d[i + k_d]
+ * x[i + k_d], one thread per row -- the product matmul_sparsedia_array
+ * (qarrays/sparsedia_primitives.py:232-246) with the column-indexed diagonals. */
+DQB_API int dqb_sesolve_dia(const dqb_dia_problem* problem, const dqb_ode_options* options,
+                            const dqb_outputs* outputs, void* workspace, size_t workspace_bytes, void* stream);
 
 /* Scratch bytes for dqb_mesolve_dia (10 n x n complex64 matrices per instance, plus
  * Hnh diagonals, controller state and FP64 expectation accumulators). */

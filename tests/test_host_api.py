@@ -126,3 +126,26 @@ def test_start_order_is_stiffest_first_permutation():
     assert order.dtype == np.int32 and sorted(order.tolist()) == list(range(300))
     h = np.abs(w['H']).sum(-1).max(-1)
     assert np.all(np.diff(h[order]) <= 1e-6)  # the jump operators are shared: H decides
+
+
+def test_sesolve_path_selection():
+    """sesolve picks its kernel by size and storage: one warp per instance up to n = 128
+    (sparse-DIA H densified), then the large-problem stepper with a dense H or with H kept
+    in DIA storage; beyond n = 8192 it refuses before touching a GPU."""
+    from dynamiqs_b200.mesolve import make_batch_plan
+    from dynamiqs_b200.qarrays import SparseDIA
+    from dynamiqs_b200.sesolve import SESolveB200Integrator
+
+    def path(H, n):
+        psi = np.zeros((n, 1), np.complex64)
+        plan = make_batch_plan(H, [], psi, True)
+        return SESolveB200Integrator(ts=np.array([0.0, 1.0]), y0=psi, method=dq.Tsit5(),
+                                     gradient=None, options=dq.Options(), H=H, Es=None,
+                                     plan=plan).path
+
+    assert path(np.eye(64, dtype=np.complex64), 64) == 'warp'
+    assert path(np.eye(200, dtype=np.complex64), 200) == 'dense_large'
+    assert path(SparseDIA.from_dense(np.eye(200, dtype=np.complex64)), 200) == 'dia'
+    big = SparseDIA((0,), np.ones((1, 8193), np.complex64))
+    with pytest.raises(NotImplementedError, match='n <= 8192'):
+        dq.sesolve(big, np.zeros((8193, 1), np.complex64), [0.0, 1.0])

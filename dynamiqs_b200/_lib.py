@@ -149,6 +149,7 @@ class RaggedInstance(ctypes.Structure):
 TD_PWC = 0
 TD_WAVE = 1
 TD_MAX_TERMS = 4
+DIA_MAX_HNH_DIAGS = 64  # DQB_DIA_MAX_HNH_DIAGS
 
 
 class TdTerm(ctypes.Structure):
@@ -225,6 +226,9 @@ SIGNATURES = {
                                                       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                       ctypes.POINTER(OdeOptions), _P, ctypes.c_size_t, _P]),
     'dqb_mesolve_dia_workspace_size': (ctypes.c_size_t, [ctypes.POINTER(DiaProblem)]),
+    'dqb_mesolve_dia_td': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.POINTER(TdHamiltonian),
+                                          ctypes.POINTER(OdeOptions), ctypes.POINTER(Outputs), _P,
+                                          ctypes.c_size_t, _P]),
     'dqb_mesolve_dia': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.POINTER(OdeOptions),
                                        ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
     'dqb_lindblad_rhs_dia': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.c_int32, _P, _P, _P,

@@ -39,6 +39,11 @@ struct Inst {
   // current; sf = the slot that receives tau L y1 (the next step's u_1)
   double tau, sig1;
   int kvalid, sf;
+  // discontinuities (time-dependent H): dt_prop = the controller's proposal that the last
+  // trial step was clipped from; made_jump = that step ends just before a discontinuity;
+  // refresh = the accepted step crossed one, so the first stage must be re-evaluated
+  double dt_prop;
+  int made_jump, refresh;
   // the instance's own problem data and outputs (shared arrays or a ragged descriptor)
   int nts, nE, save_states, is_ket;
   const double* ts;
@@ -72,6 +77,8 @@ struct Common {
   const dqb_ragged_instance* rag;  // per-instance descriptors, or null
   long long eacc_stride;           // expectation accumulators per instance (ragged)
   const int* count_dev;            // live instances (<= B) read at run time, or null
+  int n_jump;                      // discontinuity times of a time-dependent H (jump_ts)
+  const double* jump_ts;           // device float64 [n_jump], ascending
 };
 
 __device__ __forceinline__ float2* slot(const Common& c, int b, int s) {
@@ -153,6 +160,8 @@ static __global__ void setup_kernel(Common c) {
   I.tau = I.sig1 = 1.0;
   I.kvalid = 0;
   I.sf = kX;
+  I.dt_prop = 0.0;
+  I.made_jump = I.refresh = 0;
 }
 
 // grid (tiles, B): rho0 (or psi psi^+) into y, hermiticity check, expects sums zeroed.
@@ -566,9 +575,8 @@ static __global__ void init_ctrl_kernel(Common c, int phase) {
     const double md = d1 > d2 ? d1 : d2;
     const double h1 = md <= 1e-15 ? fmax(1e-6, I.h0 * 1e-3) : pow(0.01 / md, 0.25);
     const double dt = fmin(100.0 * I.h0, h1);
-    double tn = I.t + dt;
-    if (tn > I.t1 - 1e-10) tn = I.t1;
-    I.tnext = tn < I.t1 ? tn : I.t1;
+    I.dt_prop = dt;
+    I.tnext = next_trial(c.jump_ts, c.n_jump, I.t, dt, I.t1, true, I.made_jump);
     I.h = I.tnext - I.t;
     I.run = I.t < I.t1;
     I.acc[0] = I.acc[1] = I.acc[2] = 0.0;
@@ -610,7 +618,8 @@ static __global__ void control_kernel(Common c) {
   const bool keep = err < 1.0;
   I.keep = keep;
   if (keep) I.nacc += 1; else I.nrej += 1;
-  I.dtnew = I.h * step_factor(c.o, err, keep);
+  // after a step clipped at a discontinuity the controller scales its proposal
+  I.dtnew = (I.made_jump ? I.dt_prop : I.h) * step_factor(c.o, err, keep);
   if (keep) {
     int hi = I.save_idx;
     while (hi < I.nts && I.ts[hi] <= I.tnext) ++hi;
@@ -908,6 +917,7 @@ static __global__ void commit_kernel(Common c, cudaGraphConditionalHandle handle
   for (int b = threadIdx.x; b < c.B; b += blockDim.x) {
     Inst& I = c.inst[b];
     if (I.run) {
+      I.refresh = 0;
       if (I.keep) {
         int tmp = I.sy;
         I.sy = I.sy1;
@@ -915,10 +925,14 @@ static __global__ void commit_kernel(Common c, cudaGraphConditionalHandle handle
         tmp = I.sk[0];
         I.sk[0] = I.sk[6];
         I.sk[6] = tmp;
-        I.t = I.tnext;
+        // a step that ended just before a discontinuity: the next starts on it, with its
+        // first stage re-evaluated there (refresh)
+        I.t = I.made_jump ? nextafter(I.tnext, INFINITY) : I.tnext;
+        I.refresh = I.made_jump && I.t < I.t1;
         I.save_idx = I.save_hi;
       }
-      I.tnext = next_tend(I.t, I.dtnew, I.t1, I.keep);
+      I.dt_prop = I.dtnew;
+      I.tnext = next_trial(c.jump_ts, c.n_jump, I.t, I.dtnew, I.t1, I.keep, I.made_jump);
       I.h = I.tnext - I.t;
       I.run = I.t < I.t1;
     }

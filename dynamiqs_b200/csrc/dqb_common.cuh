@@ -223,6 +223,64 @@ __device__ __forceinline__ double2 block_sum2(double a, double b, double* red) {
   return make_double2(red[64], red[65]);
 }
 
+// One time-dependent term of H (dqb_td_term), by value in the kernel arguments.
+struct TdTerm {
+  int kind, n_times;
+  const double* times;
+  const double2* values;
+  const int* vidx;
+  double amp_re, amp_im, omega, phase, t_center, sigma, t_start, t_end;
+};
+
+// c_m(t) of term T for instance `inst`.
+__device__ __forceinline__ double2 td_coef(const TdTerm& T, long long inst, double t) {
+  if (T.kind == DQB_TD_PWC) {
+    const int nt = T.n_times;
+    if (!(t >= T.times[0]) || !(t < T.times[nt - 1])) return make_double2(0.0, 0.0);
+    int lo = 0, hi = nt - 1;  // times[lo] <= t < times[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (T.times[mid] <= t) lo = mid; else hi = mid;
+    }
+    const long long set = T.vidx ? T.vidx[inst] : 0;
+    return T.values[set * (nt - 1) + lo];
+  }
+  if (!(t >= T.t_start) || !(t < T.t_end)) return make_double2(0.0, 0.0);
+  double f = cos(T.omega * t + T.phase);
+  if (T.sigma > 0.0) {
+    const double d = (t - T.t_center) / T.sigma;
+    f *= exp(-0.5 * d * d);
+  }
+  return make_double2(T.amp_re * f, T.amp_im * f);
+}
+
+// First discontinuity strictly after t (or +inf).
+__device__ __forceinline__ double next_jump(const double* jts, int nj, double t) {
+  int lo = 0, hi = nj;  // first index with jts[idx] > t
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (jts[mid] <= t) lo = mid + 1; else hi = mid;
+  }
+  return lo < nj ? jts[lo] : INFINITY;
+}
+
+// Next trial end time from t for a step dt: clipped just before the next discontinuity
+// (made_jump), then clipped to t1 as next_tend does.
+__device__ __forceinline__ double next_trial(const double* jts, int nj, double t, double dt, double t1, bool keep,
+                                             int& made_jump) {
+  double tn = t + dt;
+  made_jump = 0;
+  if (nj > 0) {
+    const double J = next_jump(jts, nj, t);
+    if (tn >= J) {
+      tn = nextafter(J, -INFINITY);
+      made_jump = 1;
+    }
+  }
+  if (tn > t1 - 1e-10) tn = keep ? t1 : t + 0.5 * (t1 - t);
+  return tn < t1 ? tn : t1;
+}
+
 // Zero a few words on a stream with a kernel (a memset would order itself against the
 // work of every other stream).
 static __global__ void zero_words_kernel(unsigned int* p, int n) {

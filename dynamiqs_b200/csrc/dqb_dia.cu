@@ -52,6 +52,16 @@ struct DiaOps {
   const int* Hidx;
   const int* Lidx;
   float2* hnh;                        // [B, nh, n]
+  float2* hnh0;                       // [B, nh, n]: the constant part of Hnh when H depends
+                                      // on time (hnh then holds Hnh at the stage time)
+};
+
+// Time-dependent part of H for the DIA stepper: H(t) = H + sum_m c_m(t) ops_m, every ops_m
+// given by its diagonals on H's offsets ([M, h_nd, n], column-indexed like H's).
+struct DiaTd {
+  int M;
+  const float2* ops;
+  TdTerm term[DQB_TD_MAX_TERMS];
 };
 
 namespace {
@@ -91,12 +101,49 @@ __global__ void hnh_dia_kernel(DiaOps d, int B) {
   }
 }
 
+// Hnh at the time of a stage, for every instance that evaluates it:
+//   hnh = hnh0 - i sum_m c_m(t) ops_m    (on H's diagonals; jump terms are in hnh0)
+// which 1..5: stage input x_s at t + c_s h; 6: y1 at the step's end; 7: the first stage
+// re-evaluated after a discontinuity (instances with refresh set); 8: the first stage at
+// the start; 9: the starting-step probe at t + h0.  grid (ceil(n / 256), B).
+__global__ void hnh_td_kernel(big::Common c, DiaOps d, DiaTd td, int which) {
+  __shared__ float2 cm[DQB_TD_MAX_TERMS];
+  const int b = blockIdx.y;
+  const big::Inst& I = c.inst[b];
+  if (which >= 8 ? I.status != DQB_INST_OK : (!I.run || (which == 7 && !I.refresh))) return;
+  if (threadIdx.x < td.M) {
+    const Tableau& T = c_tab[c.o.method];
+    const double t = which <= 5 ? I.t + T.c[which] * I.h
+                                : (which == 6 ? I.tnext : (which == 9 ? I.t + I.h0 : I.t));
+    const double2 v = td_coef(td.term[threadIdx.x], b, t);
+    cm[threadIdx.x] = make_float2((float)v.x, (float)v.y);
+  }
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = d.n;
+  if (col >= n) return;
+  const float2* h0 = d.hnh0 + (long long)b * d.nh * n;
+  float2* out = d.hnh + (long long)b * d.nh * n;
+  for (int q = 0; q < d.nh; ++q) {
+    float2 v = h0[q * n + col];
+    const int k = d.hoff[q];
+    if (d.hmap[q] >= 0 && col - k >= 0 && col - k < n) {
+      float2 a = make_float2(0.f, 0.f);
+      for (int m = 0; m < td.M; ++m) a = cfma(cm[m], td.ops[((long long)m * d.h_nd + d.hmap[q]) * n + col], a);
+      v.x += a.y;  // -i a
+      v.y -= a.x;
+    }
+    out[q * n + col] = v;
+  }
+}
+
 constexpr int kRhsCols = 128;
 constexpr int kRhsRows = 8;
 
 // Input, output and output scale of one instance's right-hand side inside a solve.
 // kry = 0: k[out_k] = f(input) with input 0 = y, 1 = y1, 2 = X, 3 = k1, for the running
-// instances (need_run = 1) or those with status OK (need_run = 0).  kry = q in 1..6 (the
+// instances (need_run = 1), those with status OK (need_run = 0), or the running ones whose
+// first stage is re-evaluated after a discontinuity (need_run = 2).  kry = q in 1..6 (the
 // Krylov form): u_{q+1} = tau L u_q for the running instances whose basis lacks it, with
 // the stored u_1 scaled by sig1.  Returns false when the instance has nothing to do.
 struct RhsIo {
@@ -115,7 +162,7 @@ __device__ __forceinline__ bool rhs_io(const big::Common& c, int b, int in_sel, 
     io.scale = (float)(kry == 1 ? I.tau * I.sig1 : I.tau);
     return true;
   }
-  if (need_run ? !I.run : I.status != DQB_INST_OK) return false;
+  if (need_run == 2 ? !(I.run && I.refresh) : (need_run ? !I.run : I.status != DQB_INST_OK)) return false;
   io.X = big::slot(c, b, in_sel == 0 ? I.sy : (in_sel == 1 ? I.sy1 : (in_sel == 3 ? I.sk[0] : big::kX)));
   io.out = big::slot(c, b, I.sk[out_k]);
   return true;
@@ -863,7 +910,7 @@ __global__ void __launch_bounds__(kBulkW, 1) rhs_dia_bulk_kernel(big::Common c, 
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct DiaLayout {
-  size_t off_iter, off_inst, off_eacc, off_hnh, off_mats, total;
+  size_t off_iter, off_inst, off_eacc, off_hnh, off_hnh0, off_mats, total;
 };
 
 int build_ops(const dqb_dia_problem* p, DiaOps* d) {
@@ -933,7 +980,8 @@ DiaLayout layout_for(const dqb_dia_problem* p, int nh) {
   l.off_inst = 256;
   l.off_eacc = align_up(l.off_inst + B * sizeof(big::Inst));
   l.off_hnh = align_up(l.off_eacc + B * (size_t)p->n_exp * p->n_tsave * sizeof(double2));
-  l.off_mats = align_up(l.off_hnh + B * (size_t)nh * n * sizeof(float2));
+  l.off_hnh0 = align_up(l.off_hnh + B * (size_t)nh * n * sizeof(float2));
+  l.off_mats = align_up(l.off_hnh0 + B * (size_t)nh * n * sizeof(float2));
   l.total = l.off_mats + B * big::kSlots * n * n * sizeof(float2);
   return l;
 }
@@ -1263,6 +1311,7 @@ GraphCache g_cache;
 struct LaunchKey {
   big::Common c;
   DiaOps d;
+  DiaTd td;
   int grid_e, grid_r_x, grid_r_y, krylov;
 };
 
@@ -1298,6 +1347,7 @@ static void init_carveouts() {
     prefer_max_shared(big::finalize_kernel);
     prefer_max_shared(zero_words_kernel);
     prefer_max_shared(hnh_dia_kernel);
+    prefer_max_shared(hnh_td_kernel);
     prefer_max_shared(rhs_dia_generic_kernel);
     prefer_max_shared(rhs_dia_tiled_kernel<4>);
     prefer_max_shared(rhs_dia_tiled_kernel<8>);
@@ -1369,8 +1419,10 @@ extern "C" int dqb_lindblad_rhs_dia_tiled(const dqb_dia_problem* p, int32_t form
   return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
 }
 
-extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* o, const dqb_outputs* out,
-                               void* workspace, size_t workspace_bytes, void* stream) {
+// The solve; `tdh` (or null) adds the time-dependent terms of H and the discontinuity
+// times of the controller.
+static int solve_dia(const dqb_dia_problem* p, const dqb_td_hamiltonian* tdh, const dqb_ode_options* o,
+                     const dqb_outputs* out, void* workspace, size_t workspace_bytes, void* stream) {
   int rc = check_problem(p);
   if (rc) return rc;
   if (!o || !out || !out->states || !out->infos || !out->status || (p->n_exp > 0 && !out->expects))
@@ -1379,6 +1431,36 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   if (o->form != DQB_FORM_HERMITIAN && o->form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
   if (!(o->rtol >= 0) || !(o->atol >= 0) || o->max_steps < 0) return DQB_ERR_INVALID_ARGUMENT;
   if (o->stepper < DQB_STEPPER_AUTO || o->stepper > DQB_STEPPER_KRYLOV) return DQB_ERR_INVALID_ARGUMENT;
+  DiaTd td;
+  std::memset(&td, 0, sizeof(td));
+  if (tdh) {
+    // the Krylov form needs a constant right-hand side
+    if (o->stepper == DQB_STEPPER_KRYLOV) return DQB_ERR_UNSUPPORTED;
+    if (tdh->n_terms < 0 || tdh->n_terms > DQB_TD_MAX_TERMS || tdh->n_jump_ts < 0) return DQB_ERR_INVALID_ARGUMENT;
+    if ((tdh->n_terms > 0 && (!tdh->ops || !tdh->terms)) || (tdh->n_jump_ts > 0 && !tdh->jump_ts))
+      return DQB_ERR_INVALID_ARGUMENT;
+    td.M = tdh->n_terms;
+    td.ops = (const float2*)tdh->ops;
+    for (int m = 0; m < td.M; ++m) {
+      const dqb_td_term& u = tdh->terms[m];
+      TdTerm& T = td.term[m];
+      if (u.kind != DQB_TD_PWC && u.kind != DQB_TD_WAVE) return DQB_ERR_INVALID_ARGUMENT;
+      if (u.kind == DQB_TD_PWC && (u.n_times < 2 || !u.times || !u.values)) return DQB_ERR_INVALID_ARGUMENT;
+      T.kind = u.kind;
+      T.n_times = u.n_times;
+      T.times = u.times;
+      T.values = (const double2*)u.values;
+      T.vidx = u.value_index;
+      T.amp_re = u.amp_re;
+      T.amp_im = u.amp_im;
+      T.omega = u.omega;
+      T.phase = u.phase;
+      T.t_center = u.t_center;
+      T.sigma = u.sigma;
+      T.t_start = u.t_start;
+      T.t_end = u.t_end;
+    }
+  }
   if (p->batch == 0) return DQB_OK;
   DiaOps d;
   rc = build_ops(p, &d);
@@ -1387,6 +1469,8 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   if (!workspace || workspace_bytes < lay.total) return DQB_ERR_WORKSPACE_TOO_SMALL;
   char* ws = (char*)workspace;
   d.hnh = (float2*)(ws + lay.off_hnh);
+  d.hnh0 = (float2*)(ws + lay.off_hnh0);
+  const bool timedep = tdh != nullptr;
 
   big::Common c;
   std::memset(&c, 0, sizeof(c));
@@ -1411,6 +1495,10 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   c.rho0 = (const float2*)p->rho0;
   c.ridx = p->rho0_index;
   c.iter = (long long*)(ws + lay.off_iter);
+  if (timedep) {
+    c.n_jump = tdh->n_jump_ts;
+    c.jump_ts = tdh->jump_ts;
+  }
 
   cudaStream_t s = (cudaStream_t)stream;
   const int B = c.B;
@@ -1428,8 +1516,18 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   // ---- set-up and starting step (outside the graph) ----------------------------------
   init_carveouts();
   big::setup_kernel<<<gi, 128, 0, s>>>(c);
-  hnh_dia_kernel<<<dim3((p->n + 255) / 256, B), 256, 0, s>>>(d, B);
+  {
+    DiaOps d0 = d;  // the constant Hnh: into hnh, or into hnh0 when H depends on time
+    if (timedep) d0.hnh = d.hnh0;
+    hnh_dia_kernel<<<dim3((p->n + 255) / 256, B), 256, 0, s>>>(d0, B);
+  }
+  const dim3 gh((p->n + 255) / 256, B);
+  // Hnh at the time of the next right-hand side (time-dependent H only)
+  auto at_time = [&](cudaStream_t cs, int which) {
+    if (timedep) hnh_td_kernel<<<gh, 256, 0, cs>>>(c, d, td, which);
+  };
   big::load_rho0_kernel<<<ge, T, 0, s>>>(c);
+  at_time(s, 8);
   launch_rhs_dia(s, c, d, B, rows, 0, 0, 0, nullptr, nullptr, 0, herm);
   big::init_norm_kernel<<<ge, T, 0, s>>>(c, 0);
   big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 0);
@@ -1439,6 +1537,7 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
     big::init_norm_kernel<<<ge, T, 0, s>>>(c, 2);
   } else {
     big::launch_combine(s, c, ge, 6);
+    at_time(s, 9);
     launch_rhs_dia(s, c, d, B, rows, 2, 1, 0, nullptr, nullptr, 0, herm);
     big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
   }
@@ -1457,14 +1556,20 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
     }
     for (int st = 0; st < 5; ++st) {
       big::launch_combine(cs, c, ge, st);
+      at_time(cs, st + 1);
       launch_rhs_dia(cs, c, d, B, rows, 2, st + 1, 1, nullptr, nullptr, 0, herm, herm);
     }
     big::launch_combine(cs, c, ge, 5);
+    at_time(cs, 6);
     launch_rhs_dia(cs, c, d, B, rows, 1, 6, 1, nullptr, nullptr, 0, herm, herm);
     big::launch_error(cs, c, ge);
     big::control_kernel<<<gi, 128, 0, cs>>>(c);
     big::launch_save(cs, c, ge, 1);
     big::commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
+    if (timedep) {  // the first stage of a step that starts on a discontinuity
+      at_time(cs, 7);
+      launch_rhs_dia(cs, c, d, B, rows, 0, 0, 2, nullptr, nullptr, 0, herm, herm);
+    }
   };
   if (host_loop_requested()) {
     if (run_host_loop(body, (int*)(c.iter + 1), s) != cudaSuccess) return DQB_ERR_CUDA;
@@ -1473,6 +1578,7 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
     std::memset(&key, 0, sizeof(key));
     key.c = c;
     key.d = d;
+    key.td = td;
     key.grid_e = grid_e;
     key.grid_r_x = rows;
     key.grid_r_y = fast_ok(d);
@@ -1492,4 +1598,15 @@ extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   big::launch_save(s, c, ge, 0);
   big::finalize_kernel<<<ge, T, 0, s>>>(c);
   return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
+}
+
+extern "C" int dqb_mesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* o, const dqb_outputs* out,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+  return solve_dia(p, nullptr, o, out, workspace, workspace_bytes, stream);
+}
+
+extern "C" int dqb_mesolve_dia_td(const dqb_dia_problem* p, const dqb_td_hamiltonian* td, const dqb_ode_options* o,
+                                  const dqb_outputs* out, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!td) return DQB_ERR_INVALID_ARGUMENT;
+  return solve_dia(p, td, o, out, workspace, workspace_bytes, stream);
 }

@@ -705,10 +705,14 @@ def mesolve(H, jump_ops, rho0, tsave, *, exp_ops=None, method: Method = Tsit5(),
         if _td_on_device(Hs, jump_ops, options):
             return _mesolve_td(Hs, jump_ops, rho0, tsave, exp_ops=exp_ops, method=method,
                                gradient=gradient, options=options)
+        if _td_on_dia(Hs, jump_ops, options):
+            return _mesolve_td_dia(Hs, jump_ops, rho0, tsave, exp_ops=exp_ops, method=method,
+                                   gradient=gradient, options=options)
         if not Hs.only_pwc:
-            raise NotImplementedError('Modulated Hamiltonians run on the n <= 64 kernel only '
-                                      '(at most four time-dependent terms, dense jump '
-                                      'operators, options.vectorized=False).')
+            raise NotImplementedError('Modulated Hamiltonians run on the n <= 64 kernel or, with '
+                                      'every operator in sparse-DIA storage, on the DIA stepper '
+                                      '(at most four time-dependent terms, '
+                                      'options.vectorized=False).')
         return _mesolve_piecewise(H, jump_ops, rho0, tsave, exp_ops=exp_ops, method=method,
                                   gradient=gradient, options=options, solve=mesolve)
     if getattr(H, '__class__', None).__name__.endswith('TimeQArray'):
@@ -836,6 +840,109 @@ def _mesolve_td(Hs, jump_ops, rho0, tsave, *, exp_ops, method, gradient, options
         return lib.dqb_mesolve_dense_td(prob, td, opts, outs, ws, wsb, stream)
 
     prep.fn, prep.name = fn, 'dqb_mesolve_dense_td'
+    return prep.launch().result()
+
+
+def _td_on_dia(Hs, jump_ops, options) -> bool:
+    """Whether a time-dependent H runs as one launch of the DIA stepper: every term of H and
+    every jump operator in sparse-DIA storage, at most four time-dependent terms, and their
+    diagonals together within the stepper's limit."""
+    if options.vectorized or len(Hs.td_terms) > _lib.TD_MAX_TERMS or not Hs.is_dia:
+        return False
+    if not all(isinstance(L, SparseDIA) for L in jump_ops):
+        return False
+    return len(_td_union_offsets(Hs)) <= _lib.DIA_MAX_HNH_DIAGS
+
+
+def _td_union_offsets(Hs) -> tuple:
+    offs = set()
+    for c in Hs._const_src:
+        offs.update(c.offsets)
+    for t in Hs.td_terms:
+        offs.update(t.source.offsets)
+    return tuple(sorted(offs))
+
+
+def _on_offsets(x: SparseDIA, offsets: tuple) -> np.ndarray:
+    """The diagonals of ``x`` on ``offsets`` (a superset of its own), zeros elsewhere."""
+    out = np.zeros((*x.diags.shape[:-2], len(offsets), x.diags.shape[-1]), np.complex64)
+    for d, k in enumerate(x.offsets):
+        out[..., offsets.index(k), :] += x.diags[..., d, :]
+    return out
+
+
+def _mesolve_td_dia(Hs, jump_ops, rho0, tsave, *, exp_ops, method, gradient, options):
+    """``H(t) = H0 + sum_m c_m(t) H_m`` with every operator in sparse-DIA storage, in one
+    launch of the DIA stepper (``dqb_mesolve_dia_td``): H0 and the H_m on the union of their
+    offsets, the prefactors evaluated at every stage time, the steps clipped at the
+    discontinuities as the reference's ``jump_ts`` does.  Batched PWC values are leading
+    result dimensions (cartesian batching), as on the n <= 64 kernel."""
+    import ctypes
+
+    import torch
+
+    from .time_qarray import PWCTimeQArray
+
+    Ls = list(jump_ops)
+    rho0 = _as_op(rho0)
+    tsave = np.asarray(tsave.detach().cpu().numpy() if hasattr(tsave, 'detach') else tsave,
+                       dtype=np.float64)
+    if exp_ops is not None:
+        exp_ops = [_as_op(E) for E in exp_ops] if len(exp_ops) > 0 else None
+    offs = _td_union_offsets(Hs)
+    n = Hs.constant.shape[-1]
+    bs = tuple(Hs.batch_shape)
+    if bs and not options.cartesian_batching:
+        raise NotImplementedError('Batched PWC values need cartesian batching on the B200 path.')
+    h0 = sum(_on_offsets(c, offs) for c in Hs._const_src) if Hs._const_src else \
+        np.zeros((len(offs), n), np.complex64)
+    Hb = SparseDIA(offs, np.ascontiguousarray(np.broadcast_to(h0, (*bs, len(offs), n))))
+    _check_mesolve_args(Hb, Ls, rho0, exp_ops)
+    tsave = check_times(tsave, 'tsave')
+    check_options(options, 'mesolve')
+    options = options.initialise()
+    assert_method_supported(method)
+    method.assert_supports_gradient(gradient)
+    if options.stepper == 'krylov':
+        raise NotImplementedError('The Krylov form needs a constant Hamiltonian.')
+    plan = make_batch_plan(Hb, Ls, rho0, True)
+    integ = MESolveB200Integrator(ts=tsave, y0=rho0, method=method, gradient=gradient,
+                                  options=options, H=Hb, Ls=Ls, Es=exp_ops, plan=plan)
+    lib = _lib.load()
+    prep = integ._prepare_dia(lib)
+    dev = prep.dev
+    nsets = int(np.prod(bs, dtype=np.int64)) if bs else 1
+    terms = (_lib.TdTerm * _lib.TD_MAX_TERMS)()
+    keep = []
+    for m, term in enumerate(Hs.td_terms):
+        T = terms[m]
+        if isinstance(term, PWCTimeQArray):
+            vals = np.broadcast_to(term.values, (*bs, term.values.shape[-1])).reshape(nsets, -1)
+            tt = _to_dev(term.times, torch.float64, dev)
+            vv = _to_dev(np.ascontiguousarray(vals, dtype=np.complex128), torch.complex128, dev)
+            keep += [tt, vv]
+            T.kind, T.n_times = _lib.TD_PWC, term.times.size
+            T.times, T.values = tt.data_ptr(), vv.data_ptr()
+            T.value_index = prep.bufs['H_index'].data_ptr() if bs else None
+        else:
+            f = term.f
+            T.kind = _lib.TD_WAVE
+            T.amp_re, T.amp_im = f.amplitude.real, f.amplitude.imag
+            T.omega, T.phase, T.t_center, T.sigma = f.omega, f.phase, f.t_center, f.sigma
+            T.t_start, T.t_end = f.t_start, f.t_end
+    ops_d = _to_dev(np.stack([_on_offsets(t.source, offs) for t in Hs.td_terms]), torch.complex64, dev)
+    jts = np.asarray(Hs.discontinuity_ts, dtype=np.float64)
+    jts_d = _to_dev(jts if jts.size else np.zeros(1), torch.float64, dev)
+    keep += [ops_d, jts_d]
+    td = _lib.TdHamiltonian(n_terms=len(Hs.td_terms), ops=ops_d.data_ptr(),
+                            terms=ctypes.cast(terms, ctypes.POINTER(_lib.TdTerm)),
+                            n_jump_ts=int(jts.size), jump_ts=jts_d.data_ptr())
+    prep.bufs['td'] = (td, terms, keep)
+
+    def fn(prob, opts, outs, ws, wsb, stream):
+        return lib.dqb_mesolve_dia_td(prob, td, opts, outs, ws, wsb, stream)
+
+    prep.fn, prep.name = fn, 'dqb_mesolve_dia_td'
     return prep.launch().result()
 
 

@@ -490,6 +490,19 @@ DQB_API int dqb_mesolve_dia(const dqb_dia_problem* problem, const dqb_ode_option
                             const dqb_outputs* outputs, void* workspace, size_t workspace_bytes,
                             void* stream);
 
+/* dqb_mesolve_dia with a time-dependent Hamiltonian H(t) = H + sum_m c_m(t) ops_m
+ * (dqb_td_hamiltonian; the reference's ConstantTimeQArray + PWCTimeQArray /
+ * ModulatedTimeQArray sums, time_qarray.py:497-754): td->ops holds each ops_m by its
+ * diagonals on the problem's h_offsets, device complex64 [M, h_ndiag, n] column-indexed
+ * like h_diags (zero where ops_m has no such diagonal); the prefactors are evaluated at
+ * every stage time, Hnh at that time formed from them before each right-hand side, and the
+ * controller clips its steps at td->jump_ts (PIDController jump_ts, diffrax_integrator.py:
+ * 59-72) with the first stage re-evaluated after each one.  Stage form only (a Krylov
+ * request returns DQB_ERR_UNSUPPORTED).  Workspace: dqb_mesolve_dia_workspace_size. */
+DQB_API int dqb_mesolve_dia_td(const dqb_dia_problem* problem, const dqb_td_hamiltonian* td,
+                               const dqb_ode_options* options, const dqb_outputs* outputs,
+                               void* workspace, size_t workspace_bytes, void* stream);
+
 /* One right-hand side per instance with DIA operators: out[b] = f(rho[b]).  `workspace`
  * holds the Hnh diagonals (size from dqb_mesolve_dia_workspace_size suffices). */
 DQB_API int dqb_lindblad_rhs_dia(const dqb_dia_problem* problem, int32_t form, const void* rho,

@@ -92,7 +92,9 @@ def test_quick_request_leaves_before_slow_one_of_its_wave(cuda_device):
         return dict(H=H, jump_ops=[np.float32(np.sqrt(0.1)) * a], rho0=ops.fock(n, 0),
                     tsave=np.linspace(0.0, t_end, 5), method=dq.Tsit5(rtol=1e-6, atol=1e-6))
 
-    blocker, quick, slow = kerr(0.1, 0.5), kerr(0.1, 0.05), kerr(0.5, 8.0)
+    # the blocker holds the only stream of the class while quick and slow are submitted (it
+    # must outlast two submit calls, or quick could launch alone)
+    blocker, quick, slow = kerr(0.1, 4.0), kerr(0.1, 0.05), kerr(0.5, 8.0)
     srv = MESolveServer(n_streams=2)  # one stream per class: quick and slow share a wave
     sub = [srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'], method=r['method'])
            for r in (blocker, quick, slow)]

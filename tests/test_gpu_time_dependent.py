@@ -87,3 +87,88 @@ def test_batched_pwc_values_one_launch(cuda_device):
             one = dq.mesolve(Hi, L, rho0[j], ts, method=m)
             np.testing.assert_array_equal(res.states[i, j].cpu().numpy(), one.states.cpu().numpy())
         _check(Hi, L, rho0[0], ts, None, m=m)
+
+
+# ---- the DIA stepper (dqb_mesolve_dia_td): every operator in sparse-DIA storage ----------
+
+def _dia_modes(m):
+    """Two coupled Kerr modes of m levels in DIA storage: H0, a drive operator on each mode,
+    two jump operators (dense copies for the oracle) and the first mode's photon number."""
+    a = ops.destroy(m, layout='dia')
+    eye = ops.eye(m, layout='dia')
+    a1, a2 = ops.tensor(a, eye), ops.tensor(eye, a)
+    n1 = a1.dag() @ a1
+    H0 = (a1.dag() @ a1.dag() @ a1 @ a1) * np.float32(0.05) + (a1.dag() @ a2 + a2.dag() @ a1) * \
+        np.float32(0.1) + n1 * np.float32(0.3)
+    x1 = a1 + a1.dag()
+    y2 = (a2.dag() - a2) * np.complex64(1j)
+    Ls = [a1 * np.float32(np.sqrt(0.1)), a2 * np.float32(np.sqrt(0.05))]
+    return H0, x1, y2, Ls, [L.to_dense() for L in Ls], n1.to_dense()
+
+
+def _check_dia(H, Ls, Ls_dense, rho0, ts, E, m, res=None, b=None):
+    res = res if res is not None else dq.mesolve(H, Ls, rho0, ts, exp_ops=E, method=m)
+    Hs = as_summed(H)
+    st = res.states.cpu().numpy() if b is None else res.states[b].cpu().numpy()
+    ex = None
+    if E:
+        ex = res.expects.cpu().numpy() if b is None else res.expects[b].cpu().numpy()
+    ns = int(res.infos.nsteps if b is None else res.infos.nsteps[b])
+    return assert_solve_parity(st, ex, ns, Hs, Ls_dense, rho0, ts, E, type(m).__name__, m.rtol,
+                               m.atol, jump_ts=Hs.discontinuity_ts)
+
+
+@pytest.mark.parametrize('method', ['Tsit5', 'Dopri5'])
+def test_dia_pwc_and_wave_one_launch(cuda_device, method):
+    """A PWC drive on one mode and a Gaussian-pulse Wave on the other (n = 100, DIA): one
+    launch of the DIA stepper, Hnh formed at every stage time, steps clipped at the PWC
+    times and the pulse's support edges (1.5 is also a save time), against the oracle with
+    the same jump_ts."""
+    from dynamiqs_b200.time_qarray import as_summed as _as
+
+    H0, x1, y2, Ls, Ld, n1 = _dia_modes(10)
+    pulse = dq.Wave(1.7, 0.3, 0.8 - 0.2j, t_center=1.2, sigma=0.5, t_start=0.4, t_end=2.4)
+    H = H0 + dq.pwc([0.2, 0.9, 1.5, 2.6], [0.6, -0.4, 1.1], x1) + dq.modulated(pulse, y2)
+    assert _as(H).is_dia
+    ts = np.linspace(0.0, 3.0, 13)
+    m = dq.Tsit5(rtol=1e-6, atol=1e-8) if method == 'Tsit5' else dq.Dopri5(rtol=1e-6, atol=1e-8)
+    rho0 = ops.fock(100, 0)
+    assert _check_dia(H, Ls, Ld, rho0, ts, [n1], m) == 'trajectory'
+
+
+def test_dia_td_matches_dense_kernel_at_n36(cuda_device):
+    """The same time-dependent problem (n = 36) through the DIA stepper and the n <= 64
+    kernel: step counts equal and states within 1e-5."""
+    H0, x1, y2, Ls, Ld, n1 = _dia_modes(6)
+    H_dia = H0 + dq.pwc([0.1, 0.7, 1.3], [1.0, -0.6], x1) + dq.modulated(dq.Wave(2.0, amplitude=0.4), y2)
+    H_dense = (H0.to_dense() + dq.pwc([0.1, 0.7, 1.3], [1.0, -0.6], x1.to_dense())
+               + dq.modulated(dq.Wave(2.0, amplitude=0.4), y2.to_dense()))
+    ts = np.linspace(0.0, 2.0, 9)
+    m = dq.Tsit5(rtol=1e-6, atol=1e-8)
+    rho0 = ops.fock(36, 0)
+    r_dia = dq.mesolve(H_dia, Ls, rho0, ts, method=m)
+    r_dense = dq.mesolve(H_dense, Ld, rho0, ts, method=m)
+    assert int(r_dia.infos.nsteps) == int(r_dense.infos.nsteps)
+    d = np.abs(r_dia.states.cpu().numpy() - r_dense.states.cpu().numpy()).max()
+    assert d < 1e-5
+
+
+def test_dia_batched_pwc_values(cuda_device):
+    """PWC values of shape (3, N) with two initial states on the DIA stepper: one launch
+    of 6 instances in cartesian order, each against the oracle."""
+    H0, x1, y2, Ls, Ld, n1 = _dia_modes(8)
+    vals = np.array([[1.0, -0.5, 2.0], [0.2, 0.7, -1.0], [0.0, 1.0, 0.5]])
+    times = [0.3, 0.8, 1.5, 2.2]
+    H = H0 + dq.pwc(times, vals, x1)
+    rho0 = np.stack([ops.fock(64, 0), ops.fock(64, 1)])
+    ts = np.linspace(0.0, 2.5, 11)
+    m = dq.Tsit5(rtol=1e-6, atol=1e-8)
+    res = dq.mesolve(H, Ls, rho0, ts, exp_ops=[n1], method=m)
+    assert res.states.shape == (3, 2, 11, 64, 64)
+    for i in range(3):
+        Hi = H0 + dq.pwc(times, vals[i], x1)
+        for j in range(2):
+            one = type('R', (), {})()
+            one.states, one.expects = res.states[i, j], res.expects[i, j]
+            one.infos = type('I', (), {'nsteps': res.infos.nsteps[i, j]})()
+            _check_dia(Hi, Ls, Ld, rho0[j], ts, [n1], m, res=one)

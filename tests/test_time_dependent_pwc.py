@@ -237,3 +237,30 @@ def test_dia_terms_stay_sparse_in_pieces():
         np.testing.assert_allclose(Hp.to_dense(), Hs(0.5 * (a_ + b_)), rtol=1e-6, atol=1e-6)
     dense = as_summed(np.asarray((a.dag() @ a).to_dense()) + dq.pwc([0.0, 1.0], [1.0], a))
     assert not dense.is_dia
+
+
+def test_dia_td_routing_and_union_offsets():
+    """A time-dependent H whose every term is sparse-DIA (and DIA jump operators) goes to
+    the DIA stepper in one launch: its terms are laid out on the union of their offsets,
+    each term's diagonals at their own offsets and zeros elsewhere; dense jump operators or
+    more than four terms do not qualify."""
+    from dynamiqs_b200.mesolve import _on_offsets, _td_on_dia, _td_union_offsets
+
+    a = ops.destroy(5, layout='dia')
+    n = a.dag() @ a
+    x = a + a.dag()
+    H = n * np.float32(0.5) + dq.pwc([0.0, 1.0], [1.0], x) + dq.modulated(dq.Wave(1.0), a @ a)
+    Hs = as_summed(H)
+    assert _td_union_offsets(Hs) == (-1, 0, 1, 2)
+    L = [a * np.float32(0.3)]
+    opts = dq.Options()
+    assert _td_on_dia(Hs, L, opts)
+    assert not _td_on_dia(Hs, [x.to_dense() for x in L], opts)
+    five = H + dq.pwc([0.0, 1.0], [1.0], x) + dq.pwc([0.0, 1.0], [1.0], x)
+    assert not _td_on_dia(as_summed(five + dq.pwc([0.0, 1.0], [1.0], x)), L, opts)
+    offs = (-1, 0, 1, 2)
+    laid = _on_offsets(a @ a, offs)
+    assert laid.shape == (4, 5)
+    assert np.array_equal(laid[3], (a @ a).diags[0]) and not laid[:3].any()
+    dense = sum(np.diag(laid[q, max(k, 0):5 + min(k, 0)], k) for q, k in enumerate(offs))
+    np.testing.assert_array_equal(dense, (a @ a).to_dense())

@@ -226,6 +226,12 @@ SIGNATURES = {
                                                       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                       ctypes.POINTER(OdeOptions), _P, ctypes.c_size_t, _P]),
     'dqb_mesolve_dia_workspace_size': (ctypes.c_size_t, [ctypes.POINTER(DiaProblem)]),
+    'dqb_mesolve_dense_large_td_workspace_size': (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32,
+                                                                    ctypes.c_int32, ctypes.c_int32,
+                                                                    ctypes.c_int64]),
+    'dqb_mesolve_dense_large_td': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(TdHamiltonian),
+                                                  ctypes.POINTER(OdeOptions), ctypes.POINTER(Outputs), _P,
+                                                  ctypes.c_size_t, _P]),
     'dqb_mesolve_dia_td': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.POINTER(TdHamiltonian),
                                           ctypes.POINTER(OdeOptions), ctypes.POINTER(Outputs), _P,
                                           ctypes.c_size_t, _P]),

@@ -90,6 +90,17 @@ __device__ __forceinline__ void block_atomic_add(double v, double* dst, double* 
   if (threadIdx.x == 0) atomicAdd(dst, v);
 }
 
+// Time at which instance I evaluates the right-hand side `which` of a time-dependent H,
+// or false when it evaluates none: 1..5 the stage input x_s at t + c_s h, 6 y1 at the
+// step's end, 7 the first stage re-evaluated after a discontinuity (refresh set), 8 the
+// first stage at the start, 9 the starting-step probe at t + h0.
+__device__ __forceinline__ bool td_stage_time(const Common& c, const Inst& I, int which, double* t) {
+  if (which >= 8 ? I.status != DQB_INST_OK : (!I.run || (which == 7 && !I.refresh))) return false;
+  const Tableau& T = c_tab[c.o.method];
+  *t = which <= 5 ? I.t + T.c[which] * I.h : (which == 6 ? I.tnext : (which == 9 ? I.t + I.h0 : I.t));
+  return true;
+}
+
 // ------------------------------------------------------------------------------------
 // set-up
 // ------------------------------------------------------------------------------------

@@ -19,6 +19,8 @@
 
 #include "../../include/dqb200.h"
 
+#include <cstring>
+
 namespace dqb {
 
 // ------------------------------------------------------------------------------------
@@ -252,6 +254,44 @@ __device__ __forceinline__ double2 td_coef(const TdTerm& T, long long inst, doub
     f *= exp(-0.5 * d * d);
   }
   return make_double2(T.amp_re * f, T.amp_im * f);
+}
+
+// The time-dependent terms of H for the large-problem steppers, by value in the kernel
+// arguments: ops_m in the layout of the path (dense [M, n, n] or DIA diagonals on H's
+// offsets [M, h_nd, n]).
+struct TdOps {
+  int M;
+  const float2* ops;
+  TdTerm term[DQB_TD_MAX_TERMS];
+};
+
+// TdOps of a dqb_td_hamiltonian (host side); DQB_ERR_INVALID_ARGUMENT on a malformed one.
+inline int td_ops_from(const dqb_td_hamiltonian* u, TdOps* out) {
+  std::memset(out, 0, sizeof(*out));
+  if (u->n_terms < 0 || u->n_terms > DQB_TD_MAX_TERMS || u->n_jump_ts < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if ((u->n_terms > 0 && (!u->ops || !u->terms)) || (u->n_jump_ts > 0 && !u->jump_ts)) return DQB_ERR_INVALID_ARGUMENT;
+  out->M = u->n_terms;
+  out->ops = (const float2*)u->ops;
+  for (int m = 0; m < out->M; ++m) {
+    const dqb_td_term& a = u->terms[m];
+    TdTerm& T = out->term[m];
+    if (a.kind != DQB_TD_PWC && a.kind != DQB_TD_WAVE) return DQB_ERR_INVALID_ARGUMENT;
+    if (a.kind == DQB_TD_PWC && (a.n_times < 2 || !a.times || !a.values)) return DQB_ERR_INVALID_ARGUMENT;
+    T.kind = a.kind;
+    T.n_times = a.n_times;
+    T.times = a.times;
+    T.values = (const double2*)a.values;
+    T.vidx = a.value_index;
+    T.amp_re = a.amp_re;
+    T.amp_im = a.amp_im;
+    T.omega = a.omega;
+    T.phase = a.phase;
+    T.t_center = a.t_center;
+    T.sigma = a.sigma;
+    T.t_start = a.t_start;
+    T.t_end = a.t_end;
+  }
+  return DQB_OK;
 }
 
 // First discontinuity strictly after t (or +inf).

@@ -58,7 +58,7 @@ struct GemmJob {
   int add_miH;   // epilogue: C += -i H (Hnh set-up)
   int accumulate;  // epilogue: C += result (further terms of a long sum)
   int in_sel;    // 0 = y, 1 = y1, 2 = X, 2 + q = k_q (the Krylov form's u_q)
-  int need_run;  // 1: running instances, 0: status OK, 2: all (stand-alone)
+  int need_run;  // 1: running instances, 0: status OK, 2: all (stand-alone), 3: refresh
   int kry;       // q > 0: Krylov basis right-hand side u_{q+1} = tau L u_q (skipped where the
                  // instance's basis already has it)
 };
@@ -67,6 +67,7 @@ struct GemmJob {
 __device__ __forceinline__ bool job_skips(const big::Common& c, int b, int need_run, int kry) {
   if (need_run == 2) return false;
   const big::Inst& I = c.inst[b];
+  if (need_run == 3) return !(I.run && I.refresh);  // the first stage after a discontinuity
   if (need_run == 1 ? !I.run : I.status != DQB_INST_OK) return true;
   return kry > 0 && I.kvalid >= kry + 2;
 }
@@ -817,8 +818,33 @@ GraphCache g_cache;
 struct LaunchKey {
   big::Common c;
   LargeOps d;
+  TdOps td;
+  float2* hnh0;
   int form, krylov;
 };
+
+// Hnh at the time of a right-hand side (big::td_stage_time) of a time-dependent H:
+// hnh = hnh0 - i sum_m c_m(t) ops_m, ops dense [M, n, n].  grid (tiles, B).
+__global__ void hnh_td_dense_kernel(big::Common c, LargeOps d, TdOps td, const float2* hnh0, int which) {
+  __shared__ float2 cm[DQB_TD_MAX_TERMS];
+  const int b = blockIdx.y;
+  double t;
+  if (!big::td_stage_time(c, c.inst[b], which, &t)) return;
+  if (threadIdx.x < td.M) {
+    const double2 v = td_coef(td.term[threadIdx.x], b, t);
+    cm[threadIdx.x] = make_float2((float)v.x, (float)v.y);
+  }
+  __syncthreads();
+  const long long nn = c.nn;
+  const float2* h0 = hnh0 + (long long)b * nn;
+  float2* out = d.hnh + (long long)b * nn;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn; e += (long long)gridDim.x * blockDim.x) {
+    float2 a = make_float2(0.f, 0.f);
+    for (int m = 0; m < td.M; ++m) a = cfma(cm[m], td.ops[(long long)m * nn + e], a);
+    const float2 v = h0[e];
+    out[e] = make_float2(v.x + a.y, v.y - a.x);  // hnh0 - i a
+  }
+}
 
 LargeOps make_ops(const dqb_dense_problem* p, char* ws, const LargeLayout& lay) {
   LargeOps d;
@@ -888,6 +914,7 @@ static void init_carveouts() {
     prefer_max_shared(zero_words_kernel);
     prefer_max_shared(cgemm_kernel);
     prefer_max_shared(symmetrize_kernel);
+    prefer_max_shared(hnh_td_dense_kernel);
     auto tc_attrs = [](auto kern, int smem) {
       prefer_max_shared(kern);
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -901,7 +928,9 @@ static void init_carveouts() {
   });
 }
 
-static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bool krylov) {
+// The solve; `td` (or null) with `hnh0` (B n^2 values): the time-dependent terms of H.
+static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bool krylov,
+                     const TdOps* td = nullptr, float2* hnh0 = nullptr) {
   init_carveouts();
   const int B = c.B;
   int grid_e = (int)std::min<long long>((c.nn + big::kElemThreads - 1) / big::kElemThreads, 1184);
@@ -911,9 +940,23 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bo
   const int T = big::kElemThreads;
   const int form = c.form;
 
+  const bool timedep = td != nullptr;
+  TdOps tdv;
+  std::memset(&tdv, 0, sizeof(tdv));
+  if (timedep) tdv = *td;
+  // Hnh at the time of the next right-hand side (time-dependent H only)
+  auto at_time = [&](cudaStream_t cs, int which) {
+    if (timedep) hnh_td_dense_kernel<<<ge, T, 0, cs>>>(c, d, tdv, hnh0, which);
+  };
+
   big::setup_kernel<<<gi, 128, 0, s>>>(c);
   big::load_rho0_kernel<<<ge, T, 0, s>>>(c);
-  launch_hnh(s, c, d, B, 0);
+  {
+    LargeOps d0 = d;  // the constant Hnh: into hnh, or into hnh0 when H depends on time
+    if (timedep) d0.hnh = hnh0;
+    launch_hnh(s, c, d0, B, 0);
+  }
+  at_time(s, 8);
   launch_rhs(s, c, d, B, 0, 0, 0, form, nullptr, nullptr);
   big::init_norm_kernel<<<ge, T, 0, s>>>(c, 0);
   big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 0);
@@ -923,6 +966,7 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bo
     big::init_norm_kernel<<<ge, T, 0, s>>>(c, 2);
   } else {
     big::launch_combine(s, c, ge, 6);
+    at_time(s, 9);
     launch_rhs(s, c, d, B, 2, 1, 0, form, nullptr, nullptr);
     big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
   }
@@ -941,15 +985,21 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bo
     }
     for (int st = 0; st < 5; ++st) {
       big::launch_combine(cs, c, ge, st);
+      at_time(cs, st + 1);
       launch_rhs(cs, c, d, B, 2, st + 1, 1, form, nullptr, nullptr);
     }
     big::launch_combine(cs, c, ge, 5);
+    at_time(cs, 6);
     launch_rhs(cs, c, d, B, 1, 6, 1, form, nullptr, nullptr);
     big::launch_error(cs, c, ge);
     big::control_kernel<<<gi, 128, 0, cs>>>(c);
     big::launch_save(cs, c, ge, 1);
     big::commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
     if (c.rag) big::retire_kernel<<<B, 256, 0, cs>>>(c);
+    if (timedep) {  // the first stage of a step that starts on a discontinuity
+      at_time(cs, 7);
+      launch_rhs(cs, c, d, B, 0, 0, 3, form, nullptr, nullptr);
+    }
   };
   if (host_loop_requested()) {
     if (run_host_loop(body, (int*)(c.iter + 1), s) != cudaSuccess) return DQB_ERR_CUDA;
@@ -958,6 +1008,8 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bo
     std::memset(&key, 0, sizeof(key));
     key.c = c;
     key.d = d;
+    key.td = tdv;
+    key.hnh0 = hnh0;
     key.form = form;
     key.krylov = krylov;
     cudaGraphExec_t exec = g_cache.find(&key, sizeof(key));
@@ -1058,8 +1110,8 @@ extern "C" int dqb_mesolve_dense_large_ragged(const dqb_ragged_instance* instanc
   return run_large(c, d, (cudaStream_t)stream, large_krylov(*o));
 }
 
-extern "C" int dqb_mesolve_dense_large(const dqb_dense_problem* p, const dqb_ode_options* o, const dqb_outputs* out,
-                                       void* workspace, size_t workspace_bytes, void* stream) {
+static int solve_large(const dqb_dense_problem* p, const dqb_td_hamiltonian* tdh, const dqb_ode_options* o,
+                       const dqb_outputs* out, void* workspace, size_t workspace_bytes, void* stream) {
   int rc = check_dense_large(p);
   if (rc) return rc;
   if (!o || !out || !out->states || !out->infos || !out->status || (p->n_exp > 0 && !out->expects))
@@ -1071,9 +1123,16 @@ extern "C" int dqb_mesolve_dense_large(const dqb_dense_problem* p, const dqb_ode
   if (!(o->rtol >= 0) || !(o->atol >= 0) || o->max_steps < 0) return DQB_ERR_INVALID_ARGUMENT;
   if (o->stepper < DQB_STEPPER_AUTO || o->stepper > DQB_STEPPER_KRYLOV) return DQB_ERR_INVALID_ARGUMENT;
   if (int prc = check_precision(o->precision, o->form, p->n)) return prc;
+  TdOps td;
+  if (tdh) {
+    // the Krylov form needs a constant right-hand side
+    if (large_krylov(*o)) return DQB_ERR_UNSUPPORTED;
+    if (int tr = td_ops_from(tdh, &td)) return tr;
+  }
   if (p->batch == 0) return DQB_OK;
   const LargeLayout lay = large_layout(p->n, p->n_jumps, p->n_exp, p->n_tsave, p->batch);
-  if (!workspace || workspace_bytes < lay.total) return DQB_ERR_WORKSPACE_TOO_SMALL;
+  const size_t need = tdh ? align_up(lay.total) + (size_t)p->batch * p->n * p->n * sizeof(float2) : lay.total;
+  if (!workspace || workspace_bytes < need) return DQB_ERR_WORKSPACE_TOO_SMALL;
   char* ws = (char*)workspace;
   LargeOps d = make_ops(p, ws, lay);
   d.prec = o->precision;
@@ -1101,6 +1160,26 @@ extern "C" int dqb_mesolve_dense_large(const dqb_dense_problem* p, const dqb_ode
   c.rho0 = (const float2*)p->rho0;
   c.ridx = p->rho0_index;
   c.iter = (long long*)(ws + lay.off_iter);
+  if (!tdh) return run_large(c, d, (cudaStream_t)stream, large_krylov(*o));
+  c.n_jump = tdh->n_jump_ts;
+  c.jump_ts = tdh->jump_ts;
+  return run_large(c, d, (cudaStream_t)stream, false, &td, (float2*)(ws + align_up(lay.total)));
+}
 
-  return run_large(c, d, (cudaStream_t)stream, large_krylov(*o));
+extern "C" int dqb_mesolve_dense_large(const dqb_dense_problem* p, const dqb_ode_options* o, const dqb_outputs* out,
+                                       void* workspace, size_t workspace_bytes, void* stream) {
+  return solve_large(p, nullptr, o, out, workspace, workspace_bytes, stream);
+}
+
+extern "C" size_t dqb_mesolve_dense_large_td_workspace_size(int32_t n, int32_t n_jumps, int32_t n_exp,
+                                                            int32_t n_tsave, int64_t batch) {
+  const size_t base = dqb_mesolve_dense_large_workspace_size(n, n_jumps, n_exp, n_tsave, batch);
+  return base ? align_up(base) + (size_t)batch * n * n * sizeof(float2) : 0;
+}
+
+extern "C" int dqb_mesolve_dense_large_td(const dqb_dense_problem* p, const dqb_td_hamiltonian* td,
+                                          const dqb_ode_options* o, const dqb_outputs* out, void* workspace,
+                                          size_t workspace_bytes, void* stream) {
+  if (!td) return DQB_ERR_INVALID_ARGUMENT;
+  return solve_large(p, td, o, out, workspace, workspace_bytes, stream);
 }

@@ -56,13 +56,6 @@ struct DiaOps {
                                       // on time (hnh then holds Hnh at the stage time)
 };
 
-// Time-dependent part of H for the DIA stepper: H(t) = H + sum_m c_m(t) ops_m, every ops_m
-// given by its diagonals on H's offsets ([M, h_nd, n], column-indexed like H's).
-struct DiaTd {
-  int M;
-  const float2* ops;
-  TdTerm term[DQB_TD_MAX_TERMS];
-};
 
 namespace {
 
@@ -101,20 +94,15 @@ __global__ void hnh_dia_kernel(DiaOps d, int B) {
   }
 }
 
-// Hnh at the time of a stage, for every instance that evaluates it:
-//   hnh = hnh0 - i sum_m c_m(t) ops_m    (on H's diagonals; jump terms are in hnh0)
-// which 1..5: stage input x_s at t + c_s h; 6: y1 at the step's end; 7: the first stage
-// re-evaluated after a discontinuity (instances with refresh set); 8: the first stage at
-// the start; 9: the starting-step probe at t + h0.  grid (ceil(n / 256), B).
-__global__ void hnh_td_kernel(big::Common c, DiaOps d, DiaTd td, int which) {
+// Hnh at the time of a right-hand side (big::td_stage_time), for every instance that
+// evaluates it: hnh = hnh0 - i sum_m c_m(t) ops_m on H's diagonals (ops_m given by its
+// diagonals on H's offsets, [M, h_nd, n]; the jump terms are in hnh0).  grid (ceil(n / 256), B).
+__global__ void hnh_td_kernel(big::Common c, DiaOps d, TdOps td, int which) {
   __shared__ float2 cm[DQB_TD_MAX_TERMS];
   const int b = blockIdx.y;
-  const big::Inst& I = c.inst[b];
-  if (which >= 8 ? I.status != DQB_INST_OK : (!I.run || (which == 7 && !I.refresh))) return;
+  double t;
+  if (!big::td_stage_time(c, c.inst[b], which, &t)) return;
   if (threadIdx.x < td.M) {
-    const Tableau& T = c_tab[c.o.method];
-    const double t = which <= 5 ? I.t + T.c[which] * I.h
-                                : (which == 6 ? I.tnext : (which == 9 ? I.t + I.h0 : I.t));
     const double2 v = td_coef(td.term[threadIdx.x], b, t);
     cm[threadIdx.x] = make_float2((float)v.x, (float)v.y);
   }
@@ -1311,7 +1299,7 @@ GraphCache g_cache;
 struct LaunchKey {
   big::Common c;
   DiaOps d;
-  DiaTd td;
+  TdOps td;
   int grid_e, grid_r_x, grid_r_y, krylov;
 };
 
@@ -1431,35 +1419,12 @@ static int solve_dia(const dqb_dia_problem* p, const dqb_td_hamiltonian* tdh, co
   if (o->form != DQB_FORM_HERMITIAN && o->form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
   if (!(o->rtol >= 0) || !(o->atol >= 0) || o->max_steps < 0) return DQB_ERR_INVALID_ARGUMENT;
   if (o->stepper < DQB_STEPPER_AUTO || o->stepper > DQB_STEPPER_KRYLOV) return DQB_ERR_INVALID_ARGUMENT;
-  DiaTd td;
+  TdOps td;
   std::memset(&td, 0, sizeof(td));
   if (tdh) {
     // the Krylov form needs a constant right-hand side
     if (o->stepper == DQB_STEPPER_KRYLOV) return DQB_ERR_UNSUPPORTED;
-    if (tdh->n_terms < 0 || tdh->n_terms > DQB_TD_MAX_TERMS || tdh->n_jump_ts < 0) return DQB_ERR_INVALID_ARGUMENT;
-    if ((tdh->n_terms > 0 && (!tdh->ops || !tdh->terms)) || (tdh->n_jump_ts > 0 && !tdh->jump_ts))
-      return DQB_ERR_INVALID_ARGUMENT;
-    td.M = tdh->n_terms;
-    td.ops = (const float2*)tdh->ops;
-    for (int m = 0; m < td.M; ++m) {
-      const dqb_td_term& u = tdh->terms[m];
-      TdTerm& T = td.term[m];
-      if (u.kind != DQB_TD_PWC && u.kind != DQB_TD_WAVE) return DQB_ERR_INVALID_ARGUMENT;
-      if (u.kind == DQB_TD_PWC && (u.n_times < 2 || !u.times || !u.values)) return DQB_ERR_INVALID_ARGUMENT;
-      T.kind = u.kind;
-      T.n_times = u.n_times;
-      T.times = u.times;
-      T.values = (const double2*)u.values;
-      T.vidx = u.value_index;
-      T.amp_re = u.amp_re;
-      T.amp_im = u.amp_im;
-      T.omega = u.omega;
-      T.phase = u.phase;
-      T.t_center = u.t_center;
-      T.sigma = u.sigma;
-      T.t_start = u.t_start;
-      T.t_end = u.t_end;
-    }
+    if (int tr = td_ops_from(tdh, &td)) return tr;
   }
   if (p->batch == 0) return DQB_OK;
   DiaOps d;

@@ -238,7 +238,10 @@ def _to_dev(x, dtype, device):
 
     if isinstance(x, torch.Tensor):
         return x.to(device=device, dtype=dtype).contiguous()
-    return torch.from_numpy(np.ascontiguousarray(x)).to(device=device, dtype=dtype).contiguous()
+    a = np.ascontiguousarray(x)
+    if not a.flags.writeable:  # a read-only view (e.g. a broadcast): torch wants its own copy
+        a = a.copy()
+    return torch.from_numpy(a).to(device=device, dtype=dtype).contiguous()
 
 
 class PreparedSolve:
@@ -708,11 +711,14 @@ def mesolve(H, jump_ops, rho0, tsave, *, exp_ops=None, method: Method = Tsit5(),
         if _td_on_dia(Hs, jump_ops, options):
             return _mesolve_td_dia(Hs, jump_ops, rho0, tsave, exp_ops=exp_ops, method=method,
                                    gradient=gradient, options=options)
+        if _td_on_large(Hs, jump_ops, options):
+            return _mesolve_td(Hs, jump_ops, rho0, tsave, exp_ops=exp_ops, method=method,
+                               gradient=gradient, options=options, kind='large')
         if not Hs.only_pwc:
-            raise NotImplementedError('Modulated Hamiltonians run on the n <= 64 kernel or, with '
-                                      'every operator in sparse-DIA storage, on the DIA stepper '
-                                      '(at most four time-dependent terms, '
-                                      'options.vectorized=False).')
+            raise NotImplementedError('Modulated Hamiltonians run in one launch with at most four '
+                                      'time-dependent terms, options.vectorized=False, and either '
+                                      'every operator dense or every operator in sparse-DIA '
+                                      'storage.')
         return _mesolve_piecewise(H, jump_ops, rho0, tsave, exp_ops=exp_ops, method=method,
                                   gradient=gradient, options=options, solve=mesolve)
     if getattr(H, '__class__', None).__name__.endswith('TimeQArray'):
@@ -773,12 +779,21 @@ def _td_on_device(Hs, jump_ops, options) -> bool:
     return n <= _lib.load().dqb_dense_small_max_n(len(jump_ops) + 1)
 
 
-def _mesolve_td(Hs, jump_ops, rho0, tsave, *, exp_ops, method, gradient, options):
-    """``H(t) = H0 + sum_m c_m(t) H_m`` in one launch (``dqb_mesolve_dense_td``): the
-    kernels evaluate the PWC and Wave prefactors at every stage time, and the controller
-    clips its steps at the discontinuity times as the reference's ``jump_ts`` does.
-    Batched PWC values ``(..., N)`` are the leading result dimensions (cartesian batching)
-    and run as instances of the same launch."""
+def _td_on_large(Hs, jump_ops, options) -> bool:
+    """Whether a time-dependent H with dense operators runs as one launch of the GEMM path
+    (n beyond the n <= 64 kernel's reach)."""
+    if options.vectorized or len(Hs.td_terms) > _lib.TD_MAX_TERMS or options.stepper == 'krylov':
+        return False
+    return not any(isinstance(L, SparseDIA) or np.ndim(L) != 2 for L in jump_ops)
+
+
+def _mesolve_td(Hs, jump_ops, rho0, tsave, *, exp_ops, method, gradient, options, kind='small'):
+    """``H(t) = H0 + sum_m c_m(t) H_m`` in one launch (``dqb_mesolve_dense_td`` for
+    n <= 64, ``dqb_mesolve_dense_large_td`` on the GEMM path beyond): the kernels evaluate
+    the PWC and Wave prefactors at every stage time, and the controller clips its steps at
+    the discontinuity times as the reference's ``jump_ts`` does.  Batched PWC values
+    ``(..., N)`` are the leading result dimensions (cartesian batching) and run as
+    instances of the same launch."""
     import ctypes
 
     import torch
@@ -806,7 +821,14 @@ def _mesolve_td(Hs, jump_ops, rho0, tsave, *, exp_ops, method, gradient, options
     integ = MESolveB200Integrator(ts=tsave, y0=rho0, method=method, gradient=gradient,
                                   options=options, H=Hb, Ls=Ls, Es=exp_ops, plan=plan)
     lib = _lib.load()
-    prep = integ._prepare_dense(lib, 'small', extra_mats=1)
+    if kind == 'small':
+        prep = integ._prepare_dense(lib, 'small', extra_mats=1)
+    else:  # the GEMM path also keeps the constant Hnh0 in its workspace
+        prep = integ._prepare_dense(lib, 'large')
+        n_, K_, ntsave_, B_, nE_, _ = integ._sizes()
+        wsb = lib.dqb_mesolve_dense_large_td_workspace_size(n_, K_, nE_, ntsave_, B_)
+        prep.bufs['workspace'] = torch.empty(max(wsb, 1), dtype=torch.uint8, device=prep.dev)
+        prep.ws_bytes = wsb
     dev = prep.dev
     nsets = int(np.prod(bs, dtype=np.int64)) if bs else 1
     terms = (_lib.TdTerm * _lib.TD_MAX_TERMS)()
@@ -836,10 +858,12 @@ def _mesolve_td(Hs, jump_ops, rho0, tsave, *, exp_ops, method, gradient, options
                             n_jump_ts=int(jts.size), jump_ts=jts_d.data_ptr())
     prep.bufs['td'] = (td, terms, keep)
 
-    def fn(prob, opts, outs, ws, wsb, stream):
-        return lib.dqb_mesolve_dense_td(prob, td, opts, outs, ws, wsb, stream)
+    entry = 'dqb_mesolve_dense_td' if kind == 'small' else 'dqb_mesolve_dense_large_td'
 
-    prep.fn, prep.name = fn, 'dqb_mesolve_dense_td'
+    def fn(prob, opts, outs, ws, wsb, stream):
+        return getattr(lib, entry)(prob, td, opts, outs, ws, wsb, stream)
+
+    prep.fn, prep.name = fn, entry
     return prep.launch().result()
 
 

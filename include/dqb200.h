@@ -411,6 +411,18 @@ DQB_API int dqb_mesolve_dense_large(const dqb_dense_problem* problem, const dqb_
                                     const dqb_outputs* outputs, void* workspace,
                                     size_t workspace_bytes, void* stream);
 
+/* dqb_mesolve_dense_large with a time-dependent Hamiltonian H(t) = H + sum_m c_m(t) ops_m
+ * (dqb_td_hamiltonian with dense ops [M, n, n]): Hnh at every stage time formed from the
+ * constant Hnh0 before each right-hand side, steps clipped at td->jump_ts with the first
+ * stage re-evaluated after each one, as dqb_mesolve_dense_td does for n <= 64.  Stage form
+ * only (a Krylov request returns DQB_ERR_UNSUPPORTED).  The workspace also holds Hnh0:
+ * dqb_mesolve_dense_large_td_workspace_size. */
+DQB_API size_t dqb_mesolve_dense_large_td_workspace_size(int32_t n, int32_t n_jumps, int32_t n_exp,
+                                                         int32_t n_tsave, int64_t batch);
+DQB_API int dqb_mesolve_dense_large_td(const dqb_dense_problem* problem, const dqb_td_hamiltonian* td,
+                                       const dqb_ode_options* options, const dqb_outputs* outputs,
+                                       void* workspace, size_t workspace_bytes, void* stream);
+
 /* One right-hand side per instance for any n through the GEMM path.  `workspace` needs
  * dqb_mesolve_dense_large_workspace_size(n, n_jumps, 0, 1, batch) bytes. */
 DQB_API int dqb_lindblad_rhs_dense_large(const dqb_dense_problem* problem, int32_t form,

@@ -172,3 +172,41 @@ def test_dia_batched_pwc_values(cuda_device):
             one.states, one.expects = res.states[i, j], res.expects[i, j]
             one.infos = type('I', (), {'nsteps': res.infos.nsteps[i, j]})()
             _check_dia(Hi, Ls, Ld, rho0[j], ts, [n1], m, res=one)
+
+
+# ---- the GEMM path (dqb_mesolve_dense_large_td): dense operators beyond n = 64 ----------
+
+@pytest.mark.parametrize('method', ['Tsit5', 'Dopri5'])
+def test_large_dense_pwc_and_wave_one_launch(cuda_device, method):
+    """n = 80 with dense operators: a PWC drive and a Gaussian Wave pulse in one launch of
+    the GEMM path (Hnh formed at every stage time, steps clipped at the discontinuities),
+    against the oracle with the same jump_ts."""
+    a, num, x = _osc(80)
+    pulse = dq.Wave(1.1, 0.0, 0.5 + 0.1j, t_center=1.0, sigma=0.3, t_start=0.3, t_end=1.8)
+    H = (0.4 * num + 0.01 * (ops.dag(a) @ ops.dag(a) @ a @ a)
+         + dq.pwc([0.1, 0.6, 1.2, 2.0], [0.8, -0.3, 0.5], x) + dq.modulated(pulse, 1j * (ops.dag(a) - a)))
+    ts = np.linspace(0.0, 2.4, 9)
+    m = dq.Tsit5(rtol=1e-6, atol=1e-8) if method == 'Tsit5' else dq.Dopri5(rtol=1e-6, atol=1e-8)
+    assert _check(H, [np.float32(np.sqrt(0.1)) * a], ops.fock(80, 0), ts, [num], m=m) == 'trajectory'
+
+
+def test_large_dense_batched_pwc_values(cuda_device):
+    """PWC values of shape (2, N) with two initial states on the GEMM path: one launch of
+    4 instances in cartesian order, each against the oracle."""
+    a, num, x = _osc(72)
+    vals = np.array([[1.0, -0.5, 0.7], [0.3, 0.9, -0.4]])
+    times = [0.2, 0.7, 1.1, 1.6]
+    H = 0.5 * num + dq.pwc(times, vals, x)
+    L = [np.float32(np.sqrt(0.15)) * a]
+    rho0 = np.stack([ops.fock(72, 0), ops.fock(72, 1)])
+    ts = np.linspace(0.0, 2.0, 9)
+    m = dq.Tsit5(rtol=1e-6, atol=1e-8)
+    res = dq.mesolve(H, L, rho0, ts, exp_ops=[num], method=m)
+    assert res.states.shape == (2, 2, 9, 72, 72)
+    for i in range(2):
+        Hi = 0.5 * num + dq.pwc(times, vals[i], x)
+        for j in range(2):
+            one = type('R', (), {})()
+            one.states, one.expects = res.states[i, j], res.expects[i, j]
+            one.infos = type('I', (), {'nsteps': res.infos.nsteps[i, j]})()
+            _check(Hi, L, rho0[j], ts, [num], m=m, res=one)

@@ -263,6 +263,14 @@ SIGNATURES = {
                                                ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
     'dqb_sesolve_dia': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.POINTER(OdeOptions),
                                        ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
+    'dqb_sesolve_large_td_workspace_size': (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int64, ctypes.c_int32,
+                                                              ctypes.c_int32, ctypes.c_int64]),
+    'dqb_sesolve_dense_large_td': (ctypes.c_int, [ctypes.POINTER(DenseProblem), ctypes.POINTER(TdHamiltonian),
+                                                  ctypes.POINTER(OdeOptions), ctypes.POINTER(Outputs), _P,
+                                                  ctypes.c_size_t, _P]),
+    'dqb_sesolve_dia_td': (ctypes.c_int, [ctypes.POINTER(DiaProblem), ctypes.POINTER(TdHamiltonian),
+                                          ctypes.POINTER(OdeOptions), ctypes.POINTER(Outputs), _P,
+                                          ctypes.c_size_t, _P]),
     'dqb_mesolve_vectorized': (ctypes.c_int, [ctypes.POINTER(DenseProblem), _P, ctypes.POINTER(OdeOptions),
                                               ctypes.POINTER(Outputs), _P, ctypes.c_size_t, _P]),
     'dqb_version': (ctypes.c_char_p, []),

@@ -10,6 +10,10 @@
 //     diag_d[i + k_d] x[i + k_d] with the reference's column-indexed diagonals);
 //   * the save pass: the dense output v at each save point, then <v|E|v> = sum_i
 //     conj(v_i) (E v)_i in FP64 (utils/general.py:467-474), one warp per row of E.
+// A time-dependent H(t) = H + sum_m c_m(t) ops_m (dqb_td_hamiltonian) is formed per
+// instance before every right-hand side, at that stage's time, into a workspace copy that
+// the right-hand side then reads; the controller clips its steps at the discontinuities
+// (the stepper's jump_ts handling).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,9 +35,16 @@ struct SeOps {
   int dia;           // 0: dense H [*, n, n]; 1: DIA diagonals [*, nd, n]
   int nd;
   int off[DQB_DIA_MAX_HNH_DIAGS];
-  const float2* H;
+  const float2* H;   // read by the right-hand side (H(t) of instance b at b when time-dependent)
   const int* Hidx;
+  const float2* H0;  // time-dependent H: the constant part, indexed by H0idx
+  const int* H0idx;
 };
+
+// Values of one instance's H: n^2 (dense) or nd n (DIA).
+__host__ __device__ __forceinline__ long long h_size(const SeOps& d) {
+  return d.dia ? (long long)d.nd * d.n : (long long)d.n * d.n;
+}
 
 __device__ __forceinline__ float warp_sumf(float v) {
 #pragma unroll
@@ -42,11 +53,12 @@ __device__ __forceinline__ float warp_sumf(float v) {
 }
 
 // Input and output slots of a right-hand side (in_sel 0 = y, 1 = y1, 2 = X; need_run 1 =
-// running instances, 0 = every instance whose status is OK).
+// running instances, 0 = every instance whose status is OK, 2 = the running ones whose
+// first stage is re-evaluated after a discontinuity).
 __device__ __forceinline__ bool se_io(const big::Common& c, int b, int in_sel, int out_k, int need_run,
                                       const float2*& x, float2*& out) {
   const big::Inst& I = c.inst[b];
-  if (need_run ? !I.run : I.status != DQB_INST_OK) return false;
+  if (need_run == 2 ? !(I.run && I.refresh) : (need_run ? !I.run : I.status != DQB_INST_OK)) return false;
   x = big::slot(c, b, in_sel == 0 ? I.sy : (in_sel == 1 ? I.sy1 : big::kX));
   out = big::slot(c, b, I.sk[out_k]);
   return true;
@@ -105,6 +117,28 @@ __global__ void __launch_bounds__(kSeThreads) se_rhs_dia_kernel(big::Common c, S
     if (j >= 0 && j < n) acc = cfma(__ldg(D + (long long)q * n + j), x[j], acc);
   }
   out[i] = make_float2(acc.y, -acc.x);
+}
+
+// H(t) of every instance that evaluates the right-hand side `which` (big::td_stage_time):
+// d.H[b] = H0[H0idx[b]] + sum_m c_m(t) ops_m, in the layout of the path.  grid (tiles, B).
+__global__ void se_h_td_kernel(big::Common c, SeOps d, TdOps td, int which) {
+  __shared__ float2 cm[DQB_TD_MAX_TERMS];
+  const int b = blockIdx.y;
+  double t;
+  if (!big::td_stage_time(c, c.inst[b], which, &t)) return;
+  if (threadIdx.x < td.M) {
+    const double2 v = td_coef(td.term[threadIdx.x], b, t);
+    cm[threadIdx.x] = make_float2((float)v.x, (float)v.y);
+  }
+  __syncthreads();
+  const long long hs = h_size(d);
+  const float2* h0 = d.H0 + (d.H0idx ? (long long)d.H0idx[b] : (long long)b) * hs;
+  float2* out = const_cast<float2*>(d.H) + (long long)b * hs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < hs; e += (long long)gridDim.x * blockDim.x) {
+    float2 v = h0[e];
+    for (int m = 0; m < td.M; ++m) v = cfma(cm[m], td.ops[(long long)m * hs + e], v);
+    out[e] = v;
+  }
 }
 
 // grid (tiles, B): psi0 into y, expectation sums zeroed.
@@ -208,6 +242,7 @@ GraphCache g_cache;
 struct LaunchKey {
   big::Common c;
   SeOps d;
+  TdOps td;
 };
 
 void launch_rhs(cudaStream_t s, const big::Common& c, const SeOps& d, int in_sel, int out_k, int need_run) {
@@ -230,6 +265,7 @@ void init_attrs() {
   std::call_once(once, [] {
     prefer_max_shared(se_rhs_dense_kernel);
     prefer_max_shared(se_save_kernel);
+    prefer_max_shared(se_h_td_kernel);
     cudaFuncSetAttribute(se_rhs_dense_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          kSeMaxN * (int)sizeof(float2));
     cudaFuncSetAttribute(se_save_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSeMaxN * (int)sizeof(float2));
@@ -244,13 +280,26 @@ int check_opts(const dqb_ode_options* o, const dqb_outputs* out, int n_exp) {
   return DQB_OK;
 }
 
-// The solve, once the operators are described by `d`.
-int run(const SeOps& d, int nE, int ntsave, long long B, const void* psi0, const int* pidx, const void* E,
+// The solve, once the operators are described by `d0`; `tdh` (or null): the time-dependent
+// terms of H (ops_m in the layout of d0.H) and the discontinuity times.
+int run(const SeOps& d0, int nE, int ntsave, long long B, const void* psi0, const int* pidx, const void* E,
         const double* tsave, const dqb_ode_options* o, const dqb_outputs* out, void* workspace,
-        size_t workspace_bytes, cudaStream_t s) {
-  const SeLayout lay = se_layout(d.n, nE, ntsave, B);
-  if (!workspace || workspace_bytes < lay.total) return DQB_ERR_WORKSPACE_TOO_SMALL;
+        size_t workspace_bytes, cudaStream_t s, const dqb_td_hamiltonian* tdh = nullptr) {
+  const SeLayout lay = se_layout(d0.n, nE, ntsave, B);
+  TdOps td;
+  std::memset(&td, 0, sizeof(td));
+  if (tdh)
+    if (int tr = td_ops_from(tdh, &td)) return tr;
+  const size_t need = tdh ? se_align(lay.total) + (size_t)B * h_size(d0) * sizeof(float2) : lay.total;
+  if (!workspace || workspace_bytes < need) return DQB_ERR_WORKSPACE_TOO_SMALL;
   char* ws = (char*)workspace;
+  SeOps d = d0;
+  if (tdh) {  // the right-hand side reads H(t), one copy per instance in the workspace
+    d.H0 = d0.H;
+    d.H0idx = d0.Hidx;
+    d.H = (const float2*)(ws + se_align(lay.total));
+    d.Hidx = nullptr;
+  }
   big::Common c;
   std::memset(&c, 0, sizeof(c));
   c.n = d.n;
@@ -275,6 +324,10 @@ int run(const SeOps& d, int nE, int ntsave, long long B, const void* psi0, const
   c.rho0 = (const float2*)psi0;
   c.ridx = pidx;
   c.iter = (long long*)(ws + lay.off_iter);
+  if (tdh) {
+    c.n_jump = tdh->n_jump_ts;
+    c.jump_ts = tdh->jump_ts;
+  }
 
   init_attrs();
   int grid_e = (int)std::min<long long>((c.nn + big::kElemThreads - 1) / big::kElemThreads, 1184);
@@ -282,13 +335,20 @@ int run(const SeOps& d, int nE, int ntsave, long long B, const void* psi0, const
   const dim3 ge(grid_e, c.B);
   const dim3 gi((c.B + 127) / 128);
   const int T = big::kElemThreads;
+  const dim3 gh((unsigned)std::min<long long>((h_size(d) + T - 1) / T, 1184), c.B);
+  // H at the time of the next right-hand side (time-dependent H only)
+  auto at_time = [&](cudaStream_t cs, int which) {
+    if (tdh) se_h_td_kernel<<<gh, T, 0, cs>>>(c, d, td, which);
+  };
 
   big::setup_kernel<<<gi, 128, 0, s>>>(c);
   se_load_kernel<<<ge, T, 0, s>>>(c);
+  at_time(s, 8);
   launch_rhs(s, c, d, 0, 0, 0);
   big::init_norm_kernel<<<ge, T, 0, s>>>(c, 0);
   big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 0);
   big::combine_kernel<<<ge, T, 0, s>>>(c, 6);
+  at_time(s, 9);
   launch_rhs(s, c, d, 2, 1, 0);
   big::init_norm_kernel<<<ge, T, 0, s>>>(c, 1);
   big::init_ctrl_kernel<<<gi, 128, 0, s>>>(c, 1);
@@ -297,14 +357,20 @@ int run(const SeOps& d, int nE, int ntsave, long long B, const void* psi0, const
   auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle h, int* flag) {
     for (int st = 0; st < 5; ++st) {
       big::combine_kernel<<<ge, T, 0, cs>>>(c, st);
+      at_time(cs, st + 1);
       launch_rhs(cs, c, d, 2, st + 1, 1);
     }
     big::combine_kernel<<<ge, T, 0, cs>>>(c, 5);
+    at_time(cs, 6);
     launch_rhs(cs, c, d, 1, 6, 1);
     big::error_kernel<<<ge, T, 0, cs>>>(c);
     big::control_kernel<<<gi, 128, 0, cs>>>(c);
     launch_save(cs, c, 1);
     big::commit_kernel<<<1, 1024, 0, cs>>>(c, h, flag);
+    if (tdh) {  // the first stage of a step that starts on a discontinuity
+      at_time(cs, 7);
+      launch_rhs(cs, c, d, 0, 0, 2);
+    }
   };
   if (host_loop_requested()) {
     if (run_host_loop(body, (int*)(c.iter + 1), s) != cudaSuccess) return DQB_ERR_CUDA;
@@ -313,6 +379,7 @@ int run(const SeOps& d, int nE, int ntsave, long long B, const void* psi0, const
     std::memset(&key, 0, sizeof(key));
     key.c = c;
     key.d = d;
+    key.td = td;
     cudaGraphExec_t exec = g_cache.find(&key, sizeof(key));
     if (!exec) {
       if (build_while_graph(body, &exec) != cudaSuccess) return DQB_ERR_CUDA;
@@ -338,9 +405,15 @@ extern "C" size_t dqb_sesolve_large_workspace_size(int32_t n, int32_t n_exp, int
   return se_layout(n, n_exp, n_tsave, batch).total;
 }
 
-extern "C" int dqb_sesolve_dense_large(const dqb_dense_problem* p, const dqb_ode_options* o,
-                                       const dqb_outputs* out, void* workspace, size_t workspace_bytes,
-                                       void* stream) {
+extern "C" size_t dqb_sesolve_large_td_workspace_size(int32_t n, int64_t h_values, int32_t n_exp, int32_t n_tsave,
+                                                      int64_t batch) {
+  const size_t base = dqb_sesolve_large_workspace_size(n, n_exp, n_tsave, batch);
+  if (!base || h_values < 1) return 0;
+  return se_align(base) + (size_t)batch * h_values * sizeof(float2);
+}
+
+static int sesolve_dense_large(const dqb_dense_problem* p, const dqb_td_hamiltonian* td, const dqb_ode_options* o,
+                               const dqb_outputs* out, void* workspace, size_t workspace_bytes, void* stream) {
   if (!p) return DQB_ERR_INVALID_ARGUMENT;
   if (p->n < 1 || p->n_jumps != 0 || p->n_exp < 0 || p->n_tsave < 1 || p->batch < 0) return DQB_ERR_INVALID_ARGUMENT;
   if (!p->H || !p->rho0 || !p->tsave || (p->n_exp > 0 && !p->E)) return DQB_ERR_INVALID_ARGUMENT;
@@ -355,11 +428,24 @@ extern "C" int dqb_sesolve_dense_large(const dqb_dense_problem* p, const dqb_ode
   d.H = (const float2*)p->H;
   d.Hidx = p->H_index;
   return run(d, p->n_exp, p->n_tsave, p->batch, p->rho0, p->rho0_index, p->E, p->tsave, o, out, workspace,
-             workspace_bytes, (cudaStream_t)stream);
+             workspace_bytes, (cudaStream_t)stream, td);
 }
 
-extern "C" int dqb_sesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* o, const dqb_outputs* out,
-                               void* workspace, size_t workspace_bytes, void* stream) {
+extern "C" int dqb_sesolve_dense_large(const dqb_dense_problem* p, const dqb_ode_options* o,
+                                       const dqb_outputs* out, void* workspace, size_t workspace_bytes,
+                                       void* stream) {
+  return sesolve_dense_large(p, nullptr, o, out, workspace, workspace_bytes, stream);
+}
+
+extern "C" int dqb_sesolve_dense_large_td(const dqb_dense_problem* p, const dqb_td_hamiltonian* td,
+                                          const dqb_ode_options* o, const dqb_outputs* out, void* workspace,
+                                          size_t workspace_bytes, void* stream) {
+  if (!td) return DQB_ERR_INVALID_ARGUMENT;
+  return sesolve_dense_large(p, td, o, out, workspace, workspace_bytes, stream);
+}
+
+static int sesolve_dia(const dqb_dia_problem* p, const dqb_td_hamiltonian* td, const dqb_ode_options* o,
+                       const dqb_outputs* out, void* workspace, size_t workspace_bytes, void* stream) {
   if (!p) return DQB_ERR_INVALID_ARGUMENT;
   if (p->n < 1 || p->n_jumps != 0 || p->n_exp < 0 || p->n_tsave < 1 || p->batch < 0) return DQB_ERR_INVALID_ARGUMENT;
   if (p->h_ndiag < 0 || (p->h_ndiag > 0 && (!p->h_offsets || !p->h_diags))) return DQB_ERR_INVALID_ARGUMENT;
@@ -380,5 +466,16 @@ extern "C" int dqb_sesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* 
   d.H = (const float2*)p->h_diags;
   d.Hidx = p->H_index;
   return run(d, p->n_exp, p->n_tsave, p->batch, p->rho0, p->rho0_index, p->E, p->tsave, o, out, workspace,
-             workspace_bytes, (cudaStream_t)stream);
+             workspace_bytes, (cudaStream_t)stream, td);
+}
+
+extern "C" int dqb_sesolve_dia(const dqb_dia_problem* p, const dqb_ode_options* o, const dqb_outputs* out,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+  return sesolve_dia(p, nullptr, o, out, workspace, workspace_bytes, stream);
+}
+
+extern "C" int dqb_sesolve_dia_td(const dqb_dia_problem* p, const dqb_td_hamiltonian* td, const dqb_ode_options* o,
+                                  const dqb_outputs* out, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!td) return DQB_ERR_INVALID_ARGUMENT;
+  return sesolve_dia(p, td, o, out, workspace, workspace_bytes, stream);
 }

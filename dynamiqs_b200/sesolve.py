@@ -57,6 +57,7 @@ class _Prepared:
     bufs: dict
     fn: str = 'dqb_sesolve_dense'
     host: tuple = ()  # host arrays the problem struct points to
+    td: object = None  # the dqb_td_hamiltonian of a time-dependent H
 
     def launch(self, stream=None):
         import ctypes
@@ -65,7 +66,8 @@ class _Prepared:
 
         s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
         lib = _lib.load()
-        rc = getattr(lib, self.fn)(ctypes.byref(self.prob), ctypes.byref(self.integ._ode_options()),
+        head = (ctypes.byref(self.prob),) + ((ctypes.byref(self.td),) if self.td is not None else ())
+        rc = getattr(lib, self.fn)(*head, ctypes.byref(self.integ._ode_options()),
                                    ctypes.byref(self.outs), self.bufs['workspace'].data_ptr(),
                                    self.bufs['workspace'].numel(), s)
         _lib.check(rc, self.fn)
@@ -79,7 +81,8 @@ class SESolveB200Integrator:
     """Registry-compatible integrator: ``constructor(ts=, y0=, method=, gradient=,
     options=, H=, Es=)`` then ``.run() -> SESolveResult`` (``sesolve.py:289-304``)."""
 
-    def __init__(self, *, ts, y0, method, gradient, options, H, Es, plan):
+    def __init__(self, *, ts, y0, method, gradient, options, H, Es, plan, td=None):
+        self.td = td  # a time-dependent H (SummedTimeQArray): H is then its constant part
         self.ts = ts
         self.y0 = y0
         self.method = method
@@ -112,7 +115,7 @@ class SESolveB200Integrator:
     def path(self) -> str:
         """'warp' (n <= 128), 'dia' (sparse-DIA H beyond that) or 'dense_large'."""
         n = _shape(self.H)[-1]
-        if n <= WARP_MAX_N:
+        if n <= WARP_MAX_N and self.td is None:
             return 'warp'
         return 'dia' if isinstance(self.plan.H_items, SparseDIA) else 'dense_large'
 
@@ -131,13 +134,16 @@ class SESolveB200Integrator:
         c64 = torch.complex64
         path = self.path
         lib = _lib.load()
+        dia = path == 'dia'
         if path == 'warp':
             ws_bytes = lib.dqb_sesolve_dense_workspace_size()
+        elif self.td is not None:
+            hv = len(plan.H_items.offsets) * n if dia else n * n
+            ws_bytes = lib.dqb_sesolve_large_td_workspace_size(n, hv, nE, ntsave, B)
         else:
             ws_bytes = lib.dqb_sesolve_large_workspace_size(n, nE, ntsave, B)
-            if ws_bytes == 0:
-                raise NotImplementedError(f'sesolve on the B200 path supports n <= {LARGE_MAX_N}.')
-        dia = path == 'dia'
+        if ws_bytes == 0:
+            raise NotImplementedError(f'sesolve on the B200 path supports n <= {LARGE_MAX_N}.')
         bufs = {
             'H': _to_dev(plan.H_items.diags if dia else plan.H_items_dense(), c64, dev),
             'psi0': _to_dev(plan.rho_items, c64, dev),
@@ -175,7 +181,12 @@ class SESolveB200Integrator:
         self._nE = nE
         fn = {'warp': 'dqb_sesolve_dense', 'dense_large': 'dqb_sesolve_dense_large',
               'dia': 'dqb_sesolve_dia'}[path]
-        return _Prepared(self, prob, outs, bufs, fn, host)
+        td = None
+        if self.td is not None:
+            td, keep = _td_struct(self.td, plan, bufs, dev, dia)
+            host = host + (keep,)
+            fn += '_td'
+        return _Prepared(self, prob, outs, bufs, fn, host, td)
 
     def run(self) -> SESolveResult:
         return self.prepare().launch().result()
@@ -218,14 +229,110 @@ class SESolveB200Integrator:
                              extra=extra, checks=checks)
 
 
+def _td_struct(Hs, plan, bufs, dev, dia):
+    """The dqb_td_hamiltonian of a time-dependent H: its terms' prefactors (batched PWC
+    values indexed by the instance's H index) and operators in the layout of the constant
+    part (dense, or diagonals on its offsets)."""
+    import ctypes
+
+    import torch
+
+    from .mesolve import _on_offsets
+    from .time_qarray import PWCTimeQArray
+
+    bs = tuple(Hs.batch_shape)
+    nsets = int(np.prod(bs, dtype=np.int64)) if bs else 1
+    terms = (_lib.TdTerm * _lib.TD_MAX_TERMS)()
+    keep = []
+    for m, term in enumerate(Hs.td_terms):
+        T = terms[m]
+        if isinstance(term, PWCTimeQArray):
+            vals = np.broadcast_to(term.values, (*bs, term.values.shape[-1])).reshape(nsets, -1)
+            tt = _to_dev(term.times, torch.float64, dev)
+            vv = _to_dev(np.ascontiguousarray(vals, dtype=np.complex128), torch.complex128, dev)
+            keep += [tt, vv]
+            T.kind, T.n_times = _lib.TD_PWC, term.times.size
+            T.times, T.values = tt.data_ptr(), vv.data_ptr()
+            T.value_index = bufs['H_index'].data_ptr() if bs else None
+        else:
+            f = term.f
+            T.kind = _lib.TD_WAVE
+            T.amp_re, T.amp_im = f.amplitude.real, f.amplitude.imag
+            T.omega, T.phase, T.t_center, T.sigma = f.omega, f.phase, f.t_center, f.sigma
+            T.t_start, T.t_end = f.t_start, f.t_end
+    if dia:
+        offs = tuple(plan.H_items.offsets)
+        ops = np.stack([_on_offsets(t.source, offs) for t in Hs.td_terms])
+    else:
+        ops = np.stack([t.qarray for t in Hs.td_terms])
+    ops_d = _to_dev(ops, torch.complex64, dev)
+    jts = np.asarray(Hs.discontinuity_ts, dtype=np.float64)
+    jts_d = _to_dev(jts if jts.size else np.zeros(1), torch.float64, dev)
+    keep += [ops_d, jts_d, terms]
+    td = _lib.TdHamiltonian(n_terms=len(Hs.td_terms), ops=ops_d.data_ptr(),
+                            terms=ctypes.cast(terms, ctypes.POINTER(_lib.TdTerm)),
+                            n_jump_ts=int(jts.size), jump_ts=jts_d.data_ptr())
+    return td, keep
+
+
+def _sesolve_td(Hs, psi0, tsave, *, exp_ops, method, gradient, options) -> SESolveResult:
+    """A time-dependent H (``dq.pwc`` / ``dq.modulated`` sums, at most four terms, every
+    operator dense or every one sparse-DIA) in one launch of the large-problem stepper at
+    any n: H(t) formed at every stage time, the steps clipped at the discontinuities as the
+    reference's ``jump_ts`` does; batched PWC values are leading result dimensions."""
+    from .mesolve import _td_union_offsets, _on_offsets
+    from .time_qarray import as_summed
+
+    Hs = as_summed(Hs)
+    if len(Hs.td_terms) > _lib.TD_MAX_TERMS:
+        raise NotImplementedError(f'At most {_lib.TD_MAX_TERMS} time-dependent terms on the B200 '
+                                  'path.')
+    psi0 = _as_op(psi0)
+    tsave = np.asarray(tsave.detach().cpu().numpy() if hasattr(tsave, 'detach') else tsave,
+                       dtype=np.float64)
+    if exp_ops is not None:
+        exp_ops = [_as_op(E) for E in exp_ops] if len(exp_ops) > 0 else None
+    n = Hs.constant.shape[-1]
+    bs = tuple(Hs.batch_shape)
+    if bs and not options.cartesian_batching:
+        raise NotImplementedError('Batched PWC values need cartesian batching on the B200 path.')
+    if Hs.is_dia:
+        offs = _td_union_offsets(Hs)
+        h0 = sum(_on_offsets(c, offs) for c in Hs._const_src) if Hs._const_src else \
+            np.zeros((len(offs), n), np.complex64)
+        H = SparseDIA(offs, np.ascontiguousarray(np.broadcast_to(h0, (*bs, len(offs), n))))
+    else:
+        H = np.ascontiguousarray(np.broadcast_to(Hs.constant.astype(np.complex64), (*bs, n, n)))
+    _check_sesolve_args(H, psi0, exp_ops)
+    tsave = check_times(tsave, 'tsave')
+    check_options(options, 'sesolve')
+    options = options.initialise()
+    assert_method_supported(method)
+    method.assert_supports_gradient(gradient)
+    if n > LARGE_MAX_N:
+        raise NotImplementedError(f'sesolve on the B200 path supports n <= {LARGE_MAX_N}.')
+    if _shape(psi0)[-2] != n:
+        raise ValueError(f'Argument `psi0` must have shape (..., {n}, 1).')
+    plan = make_batch_plan(H, [], psi0, True)
+    integ = SESolveB200Integrator(ts=tsave, y0=psi0, method=method, gradient=gradient,
+                                  options=options, H=H, Es=exp_ops, plan=plan, td=Hs)
+    return integ.run()
+
+
 def sesolve(H, psi0, tsave, *, exp_ops=None, method: Method = Tsit5(),  # noqa: B008
             gradient=None, options: Options = Options()) -> SESolveResult:  # noqa: B008
     r"""Solve the Schroedinger equation d psi/dt = -i H psi on the GPU (``dq.sesolve``,
     ``dynamiqs/integrators/apis/sesolve.py:35-224``).  Returns a :class:`SESolveResult`
-    with ``states`` ``(..., nsave, n, 1)`` and ``expects`` ``(..., nE, ntsave)``."""
+    with ``states`` ``(..., nsave, n, 1)`` and ``expects`` ``(..., nE, ntsave)``.  ``H`` may
+    be time-dependent (``dq.pwc`` / ``dq.modulated`` sums with a ``Wave`` prefactor)."""
+    from .time_qarray import ModulatedTimeQArray, PWCTimeQArray, SummedTimeQArray
+
+    if isinstance(H, (PWCTimeQArray, ModulatedTimeQArray, SummedTimeQArray)):
+        return _sesolve_td(H, psi0, tsave, exp_ops=exp_ops, method=method, gradient=gradient,
+                           options=options)
     if getattr(H, '__class__', None).__name__.endswith('TimeQArray'):
-        raise NotImplementedError('Time-dependent Hamiltonians are not supported by sesolve '
-                                  'on the B200 path.')
+        raise NotImplementedError('Callable time-dependent operators cannot run inside the B200 '
+                                  'kernels: use dq.pwc or dq.modulated with a Wave prefactor.')
     H = _as_op(H)
     psi0 = _as_op(psi0)
     tsave = np.asarray(tsave.detach().cpu().numpy() if hasattr(tsave, 'detach') else tsave,

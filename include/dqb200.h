@@ -334,8 +334,21 @@ DQB_API int dqb_sesolve_dense_large(const dqb_dense_problem* problem, const dqb_
                                     const dqb_outputs* outputs, void* workspace, size_t workspace_bytes,
                                     void* stream);
 
-/* (dqb_sesolve_dia, the same solve with H in sparse-DIA storage, is declared with the
- * sparse-DIA operators below.) */
+/* dqb_sesolve_dense_large with a time-dependent H(t) = H + sum_m c_m(t) ops_m
+ * (dqb_td_hamiltonian with dense ops [M, n, n]), at any 1 <= n <= 8192: H(t) is formed per
+ * instance at every stage time into the workspace, the steps are clipped at td->jump_ts
+ * with the first stage re-evaluated after each one (as dqb_mesolve_dense_td).  Workspace:
+ * dqb_sesolve_large_td_workspace_size(n, h_values = n * n, ...); with DIA storage
+ * (dqb_sesolve_dia_td, ops as diagonals on h_offsets [M, h_ndiag, n]) h_values =
+ * h_ndiag * n. */
+DQB_API size_t dqb_sesolve_large_td_workspace_size(int32_t n, int64_t h_values, int32_t n_exp, int32_t n_tsave,
+                                                   int64_t batch);
+DQB_API int dqb_sesolve_dense_large_td(const dqb_dense_problem* problem, const dqb_td_hamiltonian* td,
+                                       const dqb_ode_options* options, const dqb_outputs* outputs,
+                                       void* workspace, size_t workspace_bytes, void* stream);
+
+/* (dqb_sesolve_dia and dqb_sesolve_dia_td, the same solves with H in sparse-DIA storage,
+ * are declared with the sparse-DIA operators below.) */
 
 /* Batched adaptive solve of the vectorized master equation d vec(rho)/dt = S vec(rho)
  * (MESolveDiffraxIntegrator.vector_field_vec with options.vectorized=True,
@@ -487,6 +500,9 @@ typedef struct dqb_dia_problem {
  * (qarrays/sparsedia_primitives.py:232-246) with the column-indexed diagonals. */
 DQB_API int dqb_sesolve_dia(const dqb_dia_problem* problem, const dqb_ode_options* options,
                             const dqb_outputs* outputs, void* workspace, size_t workspace_bytes, void* stream);
+DQB_API int dqb_sesolve_dia_td(const dqb_dia_problem* problem, const dqb_td_hamiltonian* td,
+                               const dqb_ode_options* options, const dqb_outputs* outputs, void* workspace,
+                               size_t workspace_bytes, void* stream);
 
 /* Scratch bytes for dqb_mesolve_dia (10 n x n complex64 matrices per instance, plus
  * Hnh diagonals, controller state and FP64 expectation accumulators). */

@@ -211,3 +211,71 @@ def test_large_batching_and_options(cuda_device):
     assert _rel(shifted.states.cpu().numpy(), np.stack(r.ysave)).max() < 1e-5
     with pytest.raises(RuntimeError, match='maximum number of method steps'):
         dq.sesolve(Hs[0], psis[0], ts, method=dq.Tsit5(max_steps=2))
+
+
+# ---- time-dependent H (dqb_sesolve_dense_large_td, dqb_sesolve_dia_td) ------------------
+
+def _oracle_td(Hs, psi0, ts, method='Tsit5', rtol=1e-6, atol=1e-8):
+    """The Schroedinger equation with H(t) = Hs(t) in complex128 through the oracle's RK
+    engine, with the same discontinuity times handed to its controller: the saved kets and
+    the step-count slack of tests/parity.py (one step, or two when one of the oracle's
+    accept / reject decisions was borderline: a scaled error within 0.1 of 1)."""
+    from oracle.rk import solve
+
+    out = solve(lambda t, y: -1j * (np.asarray(Hs(t), dtype=complex) @ y),
+                np.asarray(psi0, dtype=complex), ts, method=method, rtol=rtol, atol=atol,
+                save_fn=lambda y: y, jump_ts=Hs.discontinuity_ts)
+    borderline = any(abs(e - 1.0) < 0.1 for (_, _, e) in out.errors)
+    return np.stack(out.ysave), out.nsteps, (max(2, int(0.01 * out.nsteps)) if borderline else 1)
+
+
+@pytest.mark.parametrize('method', ['Tsit5', 'Dopri5'])
+def test_td_dense_sesolve_matches_oracle(cuda_device, method):
+    """A PWC drive and a Gaussian Wave pulse (n = 40, dense): one launch of the
+    large-problem stepper, against the oracle with the same jump_ts at 1e-5, step counts
+    within one."""
+    from dynamiqs_b200.time_qarray import as_summed
+
+    a = ops.destroy(40, layout='dense')
+    num, x = ops.dag(a) @ a, a + ops.dag(a)
+    pulse = dq.Wave(1.4, 0.0, 0.6 - 0.2j, t_center=1.0, sigma=0.35, t_start=0.2, t_end=1.9)
+    H = 0.5 * num + dq.pwc([0.1, 0.5, 1.3, 2.0], [0.7, -0.2, 0.4], x) + dq.modulated(pulse, 1j * (ops.dag(a) - a))
+    ts = np.linspace(0.0, 2.2, 12)
+    m = dq.Tsit5(rtol=1e-6, atol=1e-8) if method == 'Tsit5' else dq.Dopri5(rtol=1e-6, atol=1e-8)
+    psi0 = ops.fock(40, 0)
+    res = dq.sesolve(H, psi0, ts, exp_ops=[num], method=m)
+    ref, nsteps, slack = _oracle_td(as_summed(H), psi0, ts, method=method)
+    assert _rel(res.states.cpu().numpy(), ref).max() < 1e-5
+    ex = np.array([[(s.conj().T @ num.astype(complex) @ s)[0, 0] for s in ref]])
+    assert (np.abs(res.expects.cpu().numpy() - ex) / np.maximum(np.abs(ex), 1.0)).max() < 1e-5
+    assert abs(int(res.infos.nsteps) - nsteps) <= slack
+
+
+def test_td_dia_sesolve_and_batched_values(cuda_device):
+    """H in DIA storage (n = 300) with batched PWC values (2 sets) and two initial kets:
+    one launch of 4 instances, each against the oracle.  atol = 1e-6: the random kets'
+    entries are ~0.06, so at atol = 1e-8 the FP32 rounding of the stage values is ~5 % of
+    the error scale and moves the first steps' sizes (the complex64 error estimate of the
+    first 0.007-long step reads 8.6e-4 where the complex128 one reads 2e-4), which changes
+    the step count by a few while the states still agree at 5e-6."""
+    from dynamiqs_b200.qarrays import SparseDIA
+    from dynamiqs_b200.time_qarray import as_summed
+
+    Hd = _banded_h(300, 3)
+    H0 = SparseDIA.from_dense(Hd)
+    a = ops.destroy(300, layout='dia')
+    x = a + a.dag()
+    vals = np.array([[0.5, -0.3, 0.8], [0.1, 0.6, -0.4]])
+    times = [0.2, 0.6, 1.0, 1.5]
+    H = H0 + dq.pwc(times, vals, x)
+    psis = np.stack([_rand_ket(300, 11), _rand_ket(300, 12)])
+    ts = np.linspace(0.0, 1.8, 7)
+    m = dq.Tsit5(rtol=1e-6, atol=1e-6)
+    res = dq.sesolve(H, psis, ts, method=m)
+    assert res.states.shape == (2, 2, 7, 300, 1)
+    for i in range(2):
+        Hi = as_summed(H0 + dq.pwc(times, vals[i], x))
+        for j in range(2):
+            ref, nsteps, slack = _oracle_td(Hi, psis[j], ts, atol=1e-6)
+            assert _rel(res.states[i, j].cpu().numpy(), ref).max() < 1e-5
+            assert abs(int(res.infos.nsteps[i, j]) - nsteps) <= slack, (i, j, nsteps, slack)

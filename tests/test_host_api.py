@@ -149,3 +149,15 @@ def test_sesolve_path_selection():
     big = SparseDIA((0,), np.ones((1, 8193), np.complex64))
     with pytest.raises(NotImplementedError, match='n <= 8192'):
         dq.sesolve(big, np.zeros((8193, 1), np.complex64), [0.0, 1.0])
+
+
+def test_sesolve_time_dependent_checks_before_the_gpu():
+    """A time-dependent sesolve with more than four time-dependent terms, or a callable
+    operator, is refused before any device work."""
+    a = ops.destroy(4, layout='dense')
+    x = a + ops.dag(a)
+    H = ops.dag(a) @ a
+    for _ in range(5):
+        H = H + dq.pwc([0.0, 1.0], [1.0], x)
+    with pytest.raises(NotImplementedError, match='At most 4'):
+        dq.sesolve(H, ops.fock(4, 0), [0.0, 1.0])

@@ -131,6 +131,11 @@ class Ticket:
     _server: object = None
     _cancel_word: int | None = None  # index of the cancel word in the pinned int32 view
     _cancel_requested: bool = False
+    # the ticket's wave has ended (its kernels no longer write the result buffers), and a
+    # release() that came before that, carried out when it ends
+    _wave_done: bool = False
+    _release_pending: bool = False
+    _release_lock: threading.Lock = field(default_factory=threading.Lock)
 
     def done(self) -> bool:
         return self._event.is_set()
@@ -155,11 +160,27 @@ class Ticket:
 
     def release(self) -> None:
         """Give the result's device memory back to the server (the result's tensors must
-        not be used afterwards)."""
+        not be used afterwards).  A ticket handed out before the rest of its wave finished
+        is released when the wave ends: until then the wave's kernels may still write its
+        buffers (the large-problem path writes every instance's outputs once more at the
+        end of the wave)."""
+        with self._release_lock:
+            if not self._wave_done:
+                self._release_pending = True
+                return
+            self._release_now()
+
+    def _release_now(self) -> None:
         if self._out is not None:
             arena, off, nb = self._out
             self._out = None
             arena.release(off, nb)
+
+    def _wave_ended(self) -> None:
+        with self._release_lock:
+            self._wave_done = True
+            if self._release_pending:
+                self._release_now()
 
 
 class _Wave:
@@ -742,5 +763,7 @@ class MESolveServer:
         for t in w.pending:  # the whole wave is done: every status word is final
             self._finish_ticket(w, t)
         w.pending = []
+        for t in w.tickets:  # releases asked for while the wave was still running
+            t._wave_ended()
         for arena, off, nb in w.keep:
             arena.release(off, nb)

@@ -53,7 +53,15 @@ def _solve_here():
 
 
 def test_host_driven_loop_equals_graph_loop(cuda_device):
+    import gc
+
+    import torch
+
     here = _solve_here()
+    # the child needs device memory that earlier tests of this process may still hold in
+    # torch's cache (a serving arena takes most of the device)
+    gc.collect()
+    torch.cuda.empty_cache()
     env = dict(os.environ, DQB_HOST_LOOP='1')
     proc = subprocess.run([sys.executable, '-c', _CHILD.format(root=ROOT)], env=env,
                           capture_output=True, text=True, timeout=600)

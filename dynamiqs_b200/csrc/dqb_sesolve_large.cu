@@ -37,6 +37,7 @@ struct SeOps {
   int off[DQB_DIA_MAX_HNH_DIAGS];
   const float2* H;   // read by the right-hand side (H(t) of instance b at b when time-dependent)
   const int* Hidx;
+  float2* Ht;        // time-dependent H: the per-instance copies H points to (workspace)
   const float2* H0;  // time-dependent H: the constant part, indexed by H0idx
   const int* H0idx;
 };
@@ -133,7 +134,7 @@ __global__ void se_h_td_kernel(big::Common c, SeOps d, TdOps td, int which) {
   __syncthreads();
   const long long hs = h_size(d);
   const float2* h0 = d.H0 + (d.H0idx ? (long long)d.H0idx[b] : (long long)b) * hs;
-  float2* out = const_cast<float2*>(d.H) + (long long)b * hs;
+  float2* out = d.Ht + (long long)b * hs;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < hs; e += (long long)gridDim.x * blockDim.x) {
     float2 v = h0[e];
     for (int m = 0; m < td.M; ++m) v = cfma(cm[m], td.ops[(long long)m * hs + e], v);
@@ -297,7 +298,8 @@ int run(const SeOps& d0, int nE, int ntsave, long long B, const void* psi0, cons
   if (tdh) {  // the right-hand side reads H(t), one copy per instance in the workspace
     d.H0 = d0.H;
     d.H0idx = d0.Hidx;
-    d.H = (const float2*)(ws + se_align(lay.total));
+    d.Ht = (float2*)(ws + se_align(lay.total));
+    d.H = d.Ht;
     d.Hidx = nullptr;
   }
   big::Common c;

@@ -6,9 +6,10 @@ same steps and results as ``dqb_mesolve_dense``), the backward pass the adjoint 
 (``dqb_mesolve_dense_adjoint``) -- the exact derivative of the discrete solve, which is
 what the reference's ``Direct`` / ``BackwardCheckpointed`` gradients compute through
 diffrax (``dynamiqs/integrators/core/diffrax_integrator.py:88-99``).  Scope: dense
-constant operators with n <= 64, unbatched jump operators; ``H`` and ``rho0`` may be
-batched (cartesian or flat).  The per-instance gradients the kernel writes are summed back
-onto the input tensors they came from.
+constant operators with n <= 64; ``H``, the jump operators and ``rho0`` may be batched
+(cartesian or flat).  The per-instance gradients the kernel writes are summed back onto the
+input tensors they came from: over the instances that share an item, and, for a jump
+operator, over the batch dimensions it was broadcast along.
 """
 
 from __future__ import annotations
@@ -56,6 +57,38 @@ def _solve_taped(integ, lib):
     return prep
 
 
+def _jump_grads(grad_L, plan, Lts, cartesian, n, dev):
+    """Per-instance jump-operator gradients ``grad_L`` (B, K, n, n) summed onto each jump
+    operator's own batch shape: first onto the jump sets the instances used (``L_index``),
+    then, for operator k, over the dimensions of the set batch that it was broadcast along
+    (cartesian: the other operators' dimensions; flat: the broadcast to the full shape)."""
+    import torch
+
+    K = len(Lts)
+    nsets = plan.L_sets.shape[0]
+    lidx = torch.as_tensor(plan.L_index, dtype=torch.long, device=dev)
+    gsets = torch.zeros((nsets, max(K, 1), n, n), dtype=grad_L.dtype, device=dev).index_add_(0, lidx, grad_L)
+    bs = [tuple(L.shape[:-2]) for L in Lts]
+    out = []
+    if cartesian:
+        lcat = tuple(d for b in bs for d in b)
+        pos = 0
+        for k, L in enumerate(Lts):
+            g = gsets[:, k].reshape(*lcat, n, n)
+            keep = set(range(pos, pos + len(bs[k])))
+            other = tuple(d for d in range(len(lcat)) if d not in keep)
+            if other:
+                g = g.sum(dim=other)
+            out.append(g.reshape(L.shape).to(L.device, L.dtype))
+            pos += len(bs[k])
+    else:
+        full = tuple(plan.bshape)
+        for k, L in enumerate(Lts):
+            g = gsets[0, k] if nsets == 1 else gsets[:, k].reshape(*full, n, n).sum_to_size(*L.shape)
+            out.append(g.reshape(L.shape).to(L.device, L.dtype))
+    return out
+
+
 def mesolve_autograd(H, jump_ops, rho0, tsave, *, exp_ops, method, gradient, options, integ_cls,
                      make_plan, check):
     """``mesolve`` with ``torch.autograd`` support; returns an ``MESolveResult`` whose
@@ -69,8 +102,6 @@ def mesolve_autograd(H, jump_ops, rho0, tsave, *, exp_ops, method, gradient, opt
     Ht = to_t(H)
     Lts = [to_t(L) for L in jump_ops]
     rt = to_t(rho0)
-    if any(L.ndim != 2 for L in Lts):
-        raise NotImplementedError('Gradients on the B200 path need unbatched jump operators.')
     H_np, Ls_np, r_np = _as_op(Ht), [_as_op(L) for L in Lts], _as_op(rt)
     Es = [_as_op(E) for E in exp_ops] if exp_ops else None
     check(H_np, Ls_np, r_np, Es)
@@ -125,7 +156,7 @@ def mesolve_autograd(H, jump_ops, rho0, tsave, *, exp_ops, method, gradient, opt
                              device=dev).index_add_(0, ridx, grad_r)
             gH = gH.reshape(Ht.shape).to(Ht.device, Ht.dtype)
             gr = gr.reshape(rt.shape).to(rt.device, rt.dtype)
-            gL = [grad_L[:, k].sum(0).to(L.device, L.dtype) for k, L in enumerate(Lts)]
+            gL = _jump_grads(grad_L, plan, Lts, options.cartesian_batching, n, dev)
             return (gH, gr, *gL)
 
     states, expects = _Solve.apply(Ht, rt, *Lts)

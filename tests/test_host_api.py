@@ -161,3 +161,39 @@ def test_sesolve_time_dependent_checks_before_the_gpu():
         H = H + dq.pwc([0.0, 1.0], [1.0], x)
     with pytest.raises(NotImplementedError, match='At most 4'):
         dq.sesolve(H, ops.fock(4, 0), [0.0, 1.0])
+
+
+@pytest.mark.parametrize('cartesian', [True, False])
+def test_jump_operator_gradients_map_back_to_batched_operators(cartesian):
+    """The per-instance jump-operator gradients of the adjoint are summed onto each jump
+    operator's own batch shape: every instance adds its gradient to the item of each
+    operator that it used (cartesian: each operator's own dimensions of the result; flat:
+    the broadcast to the full batch), checked against a brute-force sum over instances."""
+    import torch
+
+    from dynamiqs_b200.autodiff import _jump_grads
+
+    n = 3
+    rng = np.random.default_rng(0)
+    H = rng.normal(size=(2, n, n)).astype(np.complex64)
+    if cartesian:
+        Ls = [rng.normal(size=(3, n, n)).astype(np.complex64), rng.normal(size=(2, n, n)).astype(np.complex64)]
+    else:
+        Ls = [rng.normal(size=(2, n, n)).astype(np.complex64), rng.normal(size=(1, n, n)).astype(np.complex64)]
+    rho = np.eye(n, dtype=np.complex64)
+    plan = make_batch_plan(H, Ls, rho, cartesian)
+    B, K = plan.batch, len(Ls)
+    grad_L = torch.as_tensor(rng.normal(size=(B, K, n, n)) + 1j * rng.normal(size=(B, K, n, n)),
+                             dtype=torch.complex64)
+    got = _jump_grads(grad_L, plan, [torch.as_tensor(L) for L in Ls], cartesian, n, 'cpu')
+    # brute force: instance b used item idx_k(b) of operator k
+    for k, L in enumerate(Ls):
+        exp = np.zeros(L.shape, np.complex64)
+        items = L.reshape(-1, n, n)
+        sets = plan.L_sets[:, k]
+        for b in range(B):
+            s = plan.L_index[b]
+            # the item of operator k inside jump set s
+            i = next(j for j in range(items.shape[0]) if np.array_equal(items[j], sets[s]))
+            exp.reshape(-1, n, n)[i] += grad_L[b, k].numpy()
+        np.testing.assert_allclose(got[k].numpy(), exp, rtol=1e-5, atol=1e-5)

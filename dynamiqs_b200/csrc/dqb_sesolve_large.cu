@@ -87,6 +87,7 @@ __global__ void __launch_bounds__(kSeThreads) se_rhs_dense_kernel(big::Common c,
     const float2* Hi = H + (long long)i * n;
     float2 acc = make_float2(0.f, 0.f);
     if (even) {
+#pragma unroll 4  // four 16-byte loads of the row in flight per lane
       for (int j = 2 * lane; j < n; j += 64) {
         const float4 h = __ldg(reinterpret_cast<const float4*>(Hi + j));
         acc = cfma(make_float2(h.x, h.y), sx[j], acc);

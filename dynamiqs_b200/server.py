@@ -39,6 +39,7 @@ wait behind an unrelated long wave on the same queue.
 
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import dataclasses
 import threading
@@ -244,6 +245,7 @@ class MESolveServer:
         self._cancel_lock = threading.Lock()
         self._wake = threading.Condition(self._lock)
         self._closing = False
+        self._paused = False
         self._next_id = 0
         # finished tickets and per-wave launch records, the latest `history` of each (a
         # long-running server keeps a bounded window for stats())
@@ -294,6 +296,28 @@ class MESolveServer:
             self._wake.notify()
         return t
 
+    def pause(self) -> None:
+        """Stop launching new waves (running ones continue and retire); the requests
+        submitted meanwhile wait, so that :meth:`resume` launches them together, a class's
+        queue as one wave (up to the wave size) per free stream."""
+        with self._lock:
+            self._paused = True
+
+    def resume(self) -> None:
+        with self._lock:
+            self._paused = False
+            self._wake.notify()
+
+    @contextlib.contextmanager
+    def paused(self):
+        """``with server.paused(): submit(...)`` -- the requests submitted in the block
+        are launched together when it ends."""
+        self.pause()
+        try:
+            yield self
+        finally:
+            self.resume()
+
     def _cancel(self, t: Ticket) -> bool:
         with self._lock:
             if t._event.is_set():
@@ -312,6 +336,7 @@ class MESolveServer:
     def close(self, wait: bool = True) -> None:
         with self._lock:
             self._closing = True
+            self._paused = False  # a paused server still finishes what it was given
             self._wake.notify()
         if wait:
             self._thread.join()
@@ -390,6 +415,8 @@ class MESolveServer:
     def _admit(self) -> bool:
         launched = False
         with self._lock:
+            if self._paused:
+                return False
             keys = [k for k, q in self._pending.items() if q]
         for key in keys:
             while True:

@@ -92,18 +92,17 @@ def test_quick_request_leaves_before_slow_one_of_its_wave(cuda_device):
         return dict(H=H, jump_ops=[np.float32(np.sqrt(0.1)) * a], rho0=ops.fock(n, 0),
                     tsave=np.linspace(0.0, t_end, 5), method=dq.Tsit5(rtol=1e-6, atol=1e-6))
 
-    # the blocker holds the only stream of the class while quick and slow are submitted (it
-    # must outlast two submit calls, or quick could launch alone)
-    blocker, quick, slow = kerr(0.1, 4.0), kerr(0.1, 0.05), kerr(0.5, 8.0)
-    srv = MESolveServer(n_streams=2)  # one stream per class: quick and slow share a wave
-    sub = [srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'], method=r['method'])
-           for r in (blocker, quick, slow)]
+    quick, slow = kerr(0.1, 0.05), kerr(0.5, 8.0)
+    srv = MESolveServer(n_streams=2)  # one stream per class
+    with srv.paused():  # submitted while paused: launched together, as one wave
+        sub = [srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'], method=r['method'])
+               for r in (quick, slow)]
     res = [t.result(timeout=600) for t in sub]
     srv.close()
-    t_b, t_q, t_s = sub
+    t_q, t_s = sub
     assert t_q.t_launch == t_s.t_launch  # the same wave
     assert t_s.t_done - t_q.t_done > 0.05, (t_q.t_done, t_s.t_done)
-    for r, got in zip((quick, slow), res[1:]):
+    for r, got in zip((quick, slow), res):
         alone = dq.mesolve(r['H'], r['jump_ops'], r['rho0'], r['tsave'], method=r['method'])
         assert _rel(got.states.cpu().numpy(), alone.states.cpu().numpy()) < 1e-5
         assert int(got.infos.nsteps) == int(alone.infos.nsteps)
@@ -126,31 +125,30 @@ def test_cancel_running_and_waiting_requests(cuda_device):
 
     srv = MESolveServer(n_streams=2)  # one stream per class
     for n in (64, 80):
-        blocker, slow, quick = kerr(n, 0.1, 0.5), kerr(n, 0.5, 400.0), kerr(n, 0.1, 0.05)
-        # the blocker holds the class's only stream, so slow and quick form the next wave
-        ts = [srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'], method=r['method'])
-              for r in (blocker, slow, quick)]
+        slow, quick = kerr(n, 0.5, 400.0), kerr(n, 0.1, 0.05)
+        with srv.paused():  # slow and quick are launched together, as one wave
+            ts = [srv.submit(r['H'], r['jump_ops'], r['rho0'], r['tsave'], method=r['method'])
+                  for r in (slow, quick)]
         t0 = time.perf_counter()
-        while ts[1].t_launch == 0.0 and time.perf_counter() - t0 < 120:
+        while ts[0].t_launch == 0.0 and time.perf_counter() - t0 < 120:
             time.sleep(0.01)
-        assert ts[1].t_launch > 0.0 and ts[2].t_launch == ts[1].t_launch
-        # a request that arrives now waits: the class's stream runs the slow wave
+        assert ts[0].t_launch > 0.0 and ts[1].t_launch == ts[0].t_launch
+        # a request that arrives now waits: the class's only stream runs the slow wave
         waiting = srv.submit(quick['H'], quick['jump_ops'], quick['rho0'], quick['tsave'],
                              method=quick['method'])
         assert waiting.cancel()
         with pytest.raises(CancelledError):
             waiting.result(timeout=1)
         assert waiting.t_launch == 0.0
-        got_quick = ts[2].result(timeout=600)
+        got_quick = ts[1].result(timeout=600)
         t_cancel = time.perf_counter()
-        assert ts[1].cancel()
+        assert ts[0].cancel()
         with pytest.raises(CancelledError):
-            ts[1].result(timeout=60)
-        assert ts[1].t_done - t_cancel < 5.0
-        assert not ts[1].cancel()  # already finished
+            ts[0].result(timeout=60)
+        assert ts[0].t_done - t_cancel < 5.0
+        assert not ts[0].cancel()  # already finished
         alone = dq.mesolve(quick['H'], quick['jump_ops'], quick['rho0'], quick['tsave'],
                            method=quick['method'])
         assert _rel(got_quick.states.cpu().numpy(), alone.states.cpu().numpy()) < 1e-5
-        for t in (ts[0], ts[2]):
-            t.release()
+        ts[1].release()  # (carried out when the wave ends)
     srv.close()

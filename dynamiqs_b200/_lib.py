@@ -148,6 +148,7 @@ class RaggedInstance(ctypes.Structure):
 
 TD_PWC = 0
 TD_WAVE = 1
+TD_CONST = 2
 TD_MAX_TERMS = 4
 DIA_MAX_HNH_DIAGS = 64  # DQB_DIA_MAX_HNH_DIAGS
 
@@ -177,6 +178,7 @@ class TdHamiltonian(ctypes.Structure):
         ('terms', ctypes.POINTER(TdTerm)),
         ('n_jump_ts', ctypes.c_int32),
         ('jump_ts', ctypes.c_void_p),
+        ('jump_terms', ctypes.POINTER(TdTerm)),
     ]
 
 

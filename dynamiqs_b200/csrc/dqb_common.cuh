@@ -236,6 +236,7 @@ struct TdTerm {
 
 // c_m(t) of term T for instance `inst`.
 __device__ __forceinline__ double2 td_coef(const TdTerm& T, long long inst, double t) {
+  if (T.kind == DQB_TD_CONST) return make_double2(1.0, 0.0);
   if (T.kind == DQB_TD_PWC) {
     const int nt = T.n_times;
     if (!(t >= T.times[0]) || !(t < T.times[nt - 1])) return make_double2(0.0, 0.0);
@@ -265,6 +266,26 @@ struct TdOps {
   TdTerm term[DQB_TD_MAX_TERMS];
 };
 
+// One dqb_td_term as a TdTerm (host side); DQB_ERR_INVALID_ARGUMENT on a malformed one.
+inline int td_term_from(const dqb_td_term& a, TdTerm* T) {
+  if (a.kind != DQB_TD_PWC && a.kind != DQB_TD_WAVE && a.kind != DQB_TD_CONST) return DQB_ERR_INVALID_ARGUMENT;
+  if (a.kind == DQB_TD_PWC && (a.n_times < 2 || !a.times || !a.values)) return DQB_ERR_INVALID_ARGUMENT;
+  T->kind = a.kind;
+  T->n_times = a.n_times;
+  T->times = a.times;
+  T->values = (const double2*)a.values;
+  T->vidx = a.value_index;
+  T->amp_re = a.amp_re;
+  T->amp_im = a.amp_im;
+  T->omega = a.omega;
+  T->phase = a.phase;
+  T->t_center = a.t_center;
+  T->sigma = a.sigma;
+  T->t_start = a.t_start;
+  T->t_end = a.t_end;
+  return DQB_OK;
+}
+
 // TdOps of a dqb_td_hamiltonian (host side); DQB_ERR_INVALID_ARGUMENT on a malformed one.
 inline int td_ops_from(const dqb_td_hamiltonian* u, TdOps* out) {
   std::memset(out, 0, sizeof(*out));
@@ -272,25 +293,8 @@ inline int td_ops_from(const dqb_td_hamiltonian* u, TdOps* out) {
   if ((u->n_terms > 0 && (!u->ops || !u->terms)) || (u->n_jump_ts > 0 && !u->jump_ts)) return DQB_ERR_INVALID_ARGUMENT;
   out->M = u->n_terms;
   out->ops = (const float2*)u->ops;
-  for (int m = 0; m < out->M; ++m) {
-    const dqb_td_term& a = u->terms[m];
-    TdTerm& T = out->term[m];
-    if (a.kind != DQB_TD_PWC && a.kind != DQB_TD_WAVE) return DQB_ERR_INVALID_ARGUMENT;
-    if (a.kind == DQB_TD_PWC && (a.n_times < 2 || !a.times || !a.values)) return DQB_ERR_INVALID_ARGUMENT;
-    T.kind = a.kind;
-    T.n_times = a.n_times;
-    T.times = a.times;
-    T.values = (const double2*)a.values;
-    T.vidx = a.value_index;
-    T.amp_re = a.amp_re;
-    T.amp_im = a.amp_im;
-    T.omega = a.omega;
-    T.phase = a.phase;
-    T.t_center = a.t_center;
-    T.sigma = a.sigma;
-    T.t_start = a.t_start;
-    T.t_end = a.t_end;
-  }
+  for (int m = 0; m < out->M; ++m)
+    if (int rc = td_term_from(u->terms[m], &out->term[m])) return rc;
   return DQB_OK;
 }
 

@@ -1126,7 +1126,7 @@ static int solve_large(const dqb_dense_problem* p, const dqb_td_hamiltonian* tdh
   TdOps td;
   if (tdh) {
     // the Krylov form needs a constant right-hand side
-    if (large_krylov(*o)) return DQB_ERR_UNSUPPORTED;
+    if (large_krylov(*o) || tdh->jump_terms) return DQB_ERR_UNSUPPORTED;
     if (int tr = td_ops_from(tdh, &td)) return tr;
   }
   if (p->batch == 0) return DQB_OK;

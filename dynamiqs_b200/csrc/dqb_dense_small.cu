@@ -515,6 +515,7 @@ extern "C" int dqb_mesolve_dense_td(const dqb_dense_problem* p, const dqb_td_ham
   if (!out || !out->states || !out->infos || !out->status || (p->n_exp > 0 && !out->expects))
     return DQB_ERR_INVALID_ARGUMENT;
   if (!td || td->n_terms < 0 || td->n_terms > DQB_TD_MAX_TERMS || td->n_jump_ts < 0) return DQB_ERR_INVALID_ARGUMENT;
+  if (td->jump_terms) return DQB_ERR_UNSUPPORTED;  // time-dependent jump operators: the DIA path
   if ((td->n_terms > 0 && (!td->ops || !td->terms)) || (td->n_jump_ts > 0 && !td->jump_ts))
     return DQB_ERR_INVALID_ARGUMENT;
   for (int m = 0; m < td->n_terms; ++m) {

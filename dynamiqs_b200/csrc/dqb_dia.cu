@@ -54,6 +54,16 @@ struct DiaOps {
   float2* hnh;                        // [B, nh, n]
   float2* hnh0;                       // [B, nh, n]: the constant part of Hnh when H depends
                                       // on time (hnh then holds Hnh at the stage time)
+  // time-dependent jump operators: L above points to the per-instance copies c_k(t) L_k
+  // ([B, nl, n], Lidx null) that the stencils read; L0 / L0idx are the given diagonals
+  const float2* L0;
+  const int* L0idx;
+};
+
+// Prefactors c_k(t) of the jump operators (time-dependent jump operators), by value.
+struct DiaJumpTd {
+  int on;
+  TdTerm term[DQB_DIA_MAX_JUMPS];
 };
 
 
@@ -120,6 +130,65 @@ __global__ void hnh_td_kernel(big::Common c, DiaOps d, TdOps td, int which) {
       for (int m = 0; m < td.M; ++m) a = cfma(cm[m], td.ops[((long long)m * d.h_nd + d.hmap[q]) * n + col], a);
       v.x += a.y;  // -i a
       v.y -= a.x;
+    }
+    out[q * n + col] = v;
+  }
+}
+
+// Time-dependent jump operators L_k(t) = c_k(t) L_k (and H(t) as hnh_td_kernel): at the
+// time of a right-hand side (big::td_stage_time) every instance that evaluates it gets
+//   L(t)   = c_k(t) L_k on jump k's diagonals (the copies the stencils read), and
+//   Hnh(t) = -i (H + sum_m c_m(t) ops_m) - 1/2 sum_k |c_k(t)|^2 L_k^+ L_k
+// on Hnh's diagonals, the L^+ L products formed from the given diagonals as
+// hnh_dia_kernel does.  grid (ceil(n / 256), B).
+__global__ void hnh_td_jump_kernel(big::Common c, DiaOps d, TdOps td, DiaJumpTd jt, int which) {
+  __shared__ float2 cm[DQB_TD_MAX_TERMS];
+  __shared__ float2 ck[DQB_DIA_MAX_JUMPS];
+  __shared__ float wk[DQB_DIA_MAX_JUMPS];
+  const int b = blockIdx.y;
+  double t;
+  if (!big::td_stage_time(c, c.inst[b], which, &t)) return;
+  if (threadIdx.x < td.M) {
+    const double2 v = td_coef(td.term[threadIdx.x], b, t);
+    cm[threadIdx.x] = make_float2((float)v.x, (float)v.y);
+  }
+  if (threadIdx.x < d.K) {
+    const double2 v = td_coef(jt.term[threadIdx.x], b, t);
+    ck[threadIdx.x] = make_float2((float)v.x, (float)v.y);
+    wk[threadIdx.x] = (float)(v.x * v.x + v.y * v.y);
+  }
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = d.n;
+  if (col >= n) return;
+  const long long hi = d.Hidx ? d.Hidx[b] : b;
+  const long long li = d.L0idx ? d.L0idx[b] : b;
+  const float2* H = d.H + hi * d.h_nd * n;
+  const float2* L = d.L0 + li * d.nl * n;
+  float2* Lt = const_cast<float2*>(d.L) + (long long)b * d.nl * n;
+  for (int k = 0; k < d.K; ++k)
+    for (int p = d.lstart[k]; p < d.lstart[k + 1]; ++p) Lt[(long long)p * n + col] = cmul(ck[k], L[(long long)p * n + col]);
+  float2* out = d.hnh + (long long)b * d.nh * n;
+  for (int q = 0; q < d.nh; ++q) {
+    const int k = d.hoff[q];
+    float2 v = make_float2(0.f, 0.f);
+    if (col - k >= 0 && col - k < n) {
+      if (d.hmap[q] >= 0) {
+        float2 h = H[d.hmap[q] * n + col];
+        for (int m = 0; m < td.M; ++m) h = cfma(cm[m], td.ops[((long long)m * d.h_nd + d.hmap[q]) * n + col], h);
+        v = make_float2(h.y, -h.x);  // -i h
+      }
+      for (int jk = 0; jk < d.K; ++jk) {
+        for (int p = d.lstart[jk]; p < d.lstart[jk + 1]; ++p) {
+          for (int r = d.lstart[jk]; r < d.lstart[jk + 1]; ++r) {
+            if (d.loff[r] - d.loff[p] != k) continue;
+            // |c_k|^2 (L^+ L)[col - k][col] += conj(l_p[col - k]) l_r[col]
+            const float2 u = cmul(cconj(L[p * n + (col - k)]), L[r * n + col]);
+            v.x -= 0.5f * wk[jk] * u.x;
+            v.y -= 0.5f * wk[jk] * u.y;
+          }
+        }
+      }
     }
     out[q * n + col] = v;
   }
@@ -898,7 +967,7 @@ __global__ void __launch_bounds__(kBulkW, 1) rhs_dia_bulk_kernel(big::Common c, 
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct DiaLayout {
-  size_t off_iter, off_inst, off_eacc, off_hnh, off_hnh0, off_mats, total;
+  size_t off_iter, off_inst, off_eacc, off_hnh, off_hnh0, off_lt, off_mats, total;
 };
 
 int build_ops(const dqb_dia_problem* p, DiaOps* d) {
@@ -969,7 +1038,10 @@ DiaLayout layout_for(const dqb_dia_problem* p, int nh) {
   l.off_eacc = align_up(l.off_inst + B * sizeof(big::Inst));
   l.off_hnh = align_up(l.off_eacc + B * (size_t)p->n_exp * p->n_tsave * sizeof(double2));
   l.off_hnh0 = align_up(l.off_hnh + B * (size_t)nh * n * sizeof(float2));
-  l.off_mats = align_up(l.off_hnh0 + B * (size_t)nh * n * sizeof(float2));
+  size_t nl = 0;
+  for (int k = 0; k < p->n_jumps; ++k) nl += (size_t)p->l_ndiag[k];
+  l.off_lt = align_up(l.off_hnh0 + B * (size_t)nh * n * sizeof(float2));
+  l.off_mats = align_up(l.off_lt + B * nl * n * sizeof(float2));
   l.total = l.off_mats + B * big::kSlots * n * n * sizeof(float2);
   return l;
 }
@@ -1300,6 +1372,7 @@ struct LaunchKey {
   big::Common c;
   DiaOps d;
   TdOps td;
+  DiaJumpTd jt;
   int grid_e, grid_r_x, grid_r_y, krylov;
 };
 
@@ -1336,6 +1409,7 @@ static void init_carveouts() {
     prefer_max_shared(zero_words_kernel);
     prefer_max_shared(hnh_dia_kernel);
     prefer_max_shared(hnh_td_kernel);
+    prefer_max_shared(hnh_td_jump_kernel);
     prefer_max_shared(rhs_dia_generic_kernel);
     prefer_max_shared(rhs_dia_tiled_kernel<4>);
     prefer_max_shared(rhs_dia_tiled_kernel<8>);
@@ -1421,10 +1495,17 @@ static int solve_dia(const dqb_dia_problem* p, const dqb_td_hamiltonian* tdh, co
   if (o->stepper < DQB_STEPPER_AUTO || o->stepper > DQB_STEPPER_KRYLOV) return DQB_ERR_INVALID_ARGUMENT;
   TdOps td;
   std::memset(&td, 0, sizeof(td));
+  DiaJumpTd jt;
+  std::memset(&jt, 0, sizeof(jt));
   if (tdh) {
     // the Krylov form needs a constant right-hand side
     if (o->stepper == DQB_STEPPER_KRYLOV) return DQB_ERR_UNSUPPORTED;
     if (int tr = td_ops_from(tdh, &td)) return tr;
+    if (tdh->jump_terms) {
+      jt.on = 1;
+      for (int k = 0; k < p->n_jumps; ++k)
+        if (int tr = td_term_from(tdh->jump_terms[k], &jt.term[k])) return tr;
+    }
   }
   if (p->batch == 0) return DQB_OK;
   DiaOps d;
@@ -1436,6 +1517,12 @@ static int solve_dia(const dqb_dia_problem* p, const dqb_td_hamiltonian* tdh, co
   d.hnh = (float2*)(ws + lay.off_hnh);
   d.hnh0 = (float2*)(ws + lay.off_hnh0);
   const bool timedep = tdh != nullptr;
+  if (jt.on) {  // the stencils read the per-instance copies c_k(t) L_k
+    d.L0 = d.L;
+    d.L0idx = d.Lidx;
+    d.L = (const float2*)(ws + lay.off_lt);
+    d.Lidx = nullptr;
+  }
 
   big::Common c;
   std::memset(&c, 0, sizeof(c));
@@ -1481,15 +1568,19 @@ static int solve_dia(const dqb_dia_problem* p, const dqb_td_hamiltonian* tdh, co
   // ---- set-up and starting step (outside the graph) ----------------------------------
   init_carveouts();
   big::setup_kernel<<<gi, 128, 0, s>>>(c);
-  {
+  if (!jt.on) {  // (with time-dependent jump operators every Hnh is formed at its time)
     DiaOps d0 = d;  // the constant Hnh: into hnh, or into hnh0 when H depends on time
     if (timedep) d0.hnh = d.hnh0;
     hnh_dia_kernel<<<dim3((p->n + 255) / 256, B), 256, 0, s>>>(d0, B);
   }
   const dim3 gh((p->n + 255) / 256, B);
-  // Hnh at the time of the next right-hand side (time-dependent H only)
+  // Hnh (and the jump operators) at the time of the next right-hand side (time-dependent
+  // operators only)
   auto at_time = [&](cudaStream_t cs, int which) {
-    if (timedep) hnh_td_kernel<<<gh, 256, 0, cs>>>(c, d, td, which);
+    if (jt.on)
+      hnh_td_jump_kernel<<<gh, 256, 0, cs>>>(c, d, td, jt, which);
+    else if (timedep)
+      hnh_td_kernel<<<gh, 256, 0, cs>>>(c, d, td, which);
   };
   big::load_rho0_kernel<<<ge, T, 0, s>>>(c);
   at_time(s, 8);
@@ -1544,6 +1635,7 @@ static int solve_dia(const dqb_dia_problem* p, const dqb_td_hamiltonian* tdh, co
     key.c = c;
     key.d = d;
     key.td = td;
+    key.jt = jt;
     key.grid_e = grid_e;
     key.grid_r_x = rows;
     key.grid_r_y = fast_ok(d);

@@ -290,8 +290,10 @@ int run(const SeOps& d0, int nE, int ntsave, long long B, const void* psi0, cons
   const SeLayout lay = se_layout(d0.n, nE, ntsave, B);
   TdOps td;
   std::memset(&td, 0, sizeof(td));
-  if (tdh)
+  if (tdh) {
+    if (tdh->jump_terms) return DQB_ERR_UNSUPPORTED;  // the Schroedinger equation has no jumps
     if (int tr = td_ops_from(tdh, &td)) return tr;
+  }
   const size_t need = tdh ? se_align(lay.total) + (size_t)B * h_size(d0) * sizeof(float2) : lay.total;
   if (!workspace || workspace_bytes < need) return DQB_ERR_WORKSPACE_TOO_SMALL;
   char* ws = (char*)workspace;

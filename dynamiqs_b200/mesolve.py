@@ -701,8 +701,14 @@ def mesolve(H, jump_ops, rho0, tsave, *, exp_ops=None, method: Method = Tsit5(),
 
     td_types = (PWCTimeQArray, ModulatedTimeQArray, SummedTimeQArray)
     if any(isinstance(L, td_types) for L in jump_ops):
-        raise NotImplementedError('Time-dependent jump operators are not supported on the B200 '
-                                  'path.')
+        Hs = as_summed(H if isinstance(H, td_types) else _as_op(H))
+        if not _td_on_dia(Hs, jump_ops, options):
+            raise NotImplementedError('Time-dependent jump operators run on the DIA stepper: every '
+                                      'operator in sparse-DIA storage, each time-dependent jump '
+                                      'operator one dq.pwc / dq.modulated term with unbatched '
+                                      'values, at most four time-dependent terms in H.')
+        return _mesolve_td_dia(Hs, jump_ops, rho0, tsave, exp_ops=exp_ops, method=method,
+                               gradient=gradient, options=options)
     if isinstance(H, td_types):
         Hs = as_summed(H)
         if _td_on_device(Hs, jump_ops, options):
@@ -873,9 +879,21 @@ def _td_on_dia(Hs, jump_ops, options) -> bool:
     diagonals together within the stepper's limit."""
     if options.vectorized or len(Hs.td_terms) > _lib.TD_MAX_TERMS or not Hs.is_dia:
         return False
-    if not all(isinstance(L, SparseDIA) for L in jump_ops):
+    if not all(isinstance(_jump_source(L), SparseDIA) for L in jump_ops):
         return False
     return len(_td_union_offsets(Hs)) <= _lib.DIA_MAX_HNH_DIAGS
+
+
+def _jump_source(L):
+    """The operator of a jump operator that is constant or one dq.pwc / dq.modulated term with
+    unbatched values (None for anything else)."""
+    from .time_qarray import ModulatedTimeQArray, PWCTimeQArray
+
+    if isinstance(L, PWCTimeQArray):
+        return L.source if not L.batch_shape else None
+    if isinstance(L, ModulatedTimeQArray):
+        return L.source
+    return L if not getattr(L, '__class__', type(None)).__name__.endswith('TimeQArray') else None
 
 
 def _td_union_offsets(Hs) -> tuple:
@@ -905,9 +923,10 @@ def _mesolve_td_dia(Hs, jump_ops, rho0, tsave, *, exp_ops, method, gradient, opt
 
     import torch
 
-    from .time_qarray import PWCTimeQArray
+    from .time_qarray import ModulatedTimeQArray, PWCTimeQArray
 
-    Ls = list(jump_ops)
+    td_jumps = [L for L in jump_ops if isinstance(L, (PWCTimeQArray, ModulatedTimeQArray))]
+    Ls = [_jump_source(L) for L in jump_ops]
     rho0 = _as_op(rho0)
     tsave = np.asarray(tsave.detach().cpu().numpy() if hasattr(tsave, 'detach') else tsave,
                        dtype=np.float64)
@@ -954,14 +973,41 @@ def _mesolve_td_dia(Hs, jump_ops, rho0, tsave, *, exp_ops, method, gradient, opt
             T.amp_re, T.amp_im = f.amplitude.real, f.amplitude.imag
             T.omega, T.phase, T.t_center, T.sigma = f.omega, f.phase, f.t_center, f.sigma
             T.t_start, T.t_end = f.t_start, f.t_end
-    ops_d = _to_dev(np.stack([_on_offsets(t.source, offs) for t in Hs.td_terms]), torch.complex64, dev)
-    jts = np.asarray(Hs.discontinuity_ts, dtype=np.float64)
+    ops_d = (_to_dev(np.stack([_on_offsets(t.source, offs) for t in Hs.td_terms]), torch.complex64, dev)
+             if Hs.td_terms else torch.zeros(1, dtype=torch.complex64, device=dev))
+    # prefactors of the jump operators (constant ones: 1)
+    jterms = None
+    disc = [np.asarray(Hs.discontinuity_ts, dtype=np.float64)]
+    if td_jumps:
+        jterms = (_lib.TdTerm * max(len(jump_ops), 1))()
+        for k, L in enumerate(jump_ops):
+            T = jterms[k]
+            if isinstance(L, PWCTimeQArray):
+                tt = _to_dev(L.times, torch.float64, dev)
+                vv = _to_dev(np.ascontiguousarray(L.values.reshape(1, -1), dtype=np.complex128),
+                             torch.complex128, dev)
+                keep += [tt, vv]
+                T.kind, T.n_times = _lib.TD_PWC, L.times.size
+                T.times, T.values, T.value_index = tt.data_ptr(), vv.data_ptr(), None
+                disc.append(np.asarray(L.discontinuity_ts, dtype=np.float64))
+            elif isinstance(L, ModulatedTimeQArray):
+                f = L.f
+                T.kind = _lib.TD_WAVE
+                T.amp_re, T.amp_im = f.amplitude.real, f.amplitude.imag
+                T.omega, T.phase, T.t_center, T.sigma = f.omega, f.phase, f.t_center, f.sigma
+                T.t_start, T.t_end = f.t_start, f.t_end
+                disc.append(np.asarray(L.discontinuity_ts, dtype=np.float64))
+            else:
+                T.kind = _lib.TD_CONST
+    jts = np.unique(np.concatenate(disc)) if disc else np.zeros(0)
     jts_d = _to_dev(jts if jts.size else np.zeros(1), torch.float64, dev)
     keep += [ops_d, jts_d]
     td = _lib.TdHamiltonian(n_terms=len(Hs.td_terms), ops=ops_d.data_ptr(),
                             terms=ctypes.cast(terms, ctypes.POINTER(_lib.TdTerm)),
-                            n_jump_ts=int(jts.size), jump_ts=jts_d.data_ptr())
-    prep.bufs['td'] = (td, terms, keep)
+                            n_jump_ts=int(jts.size), jump_ts=jts_d.data_ptr(),
+                            jump_terms=(ctypes.cast(jterms, ctypes.POINTER(_lib.TdTerm))
+                                        if jterms is not None else None))
+    prep.bufs['td'] = (td, terms, jterms, keep)
 
     def fn(prob, opts, outs, ws, wsb, stream):
         return lib.dqb_mesolve_dia_td(prob, td, opts, outs, ws, wsb, stream)

@@ -271,6 +271,7 @@ DQB_API int dqb_probe_bounded_wait(uint64_t limit_ns, int32_t* result, void* str
                          t_start <= t < t_end, else 0; env(t) = exp(-(t - t_center)^2 /
                          (2 sigma^2)) when sigma > 0, else 1 (a ModulatedTimeQArray whose
                          prefactor is one of these closed forms) */
+#define DQB_TD_CONST 2 /* c(t) = 1 (a jump operator without time dependence)                */
 #define DQB_TD_MAX_TERMS 4
 
 typedef struct dqb_td_term {
@@ -293,6 +294,10 @@ typedef struct dqb_td_hamiltonian {
                                   crosses one; it ends just before it, the next starts on
                                   it with its first stage re-evaluated, and the next step
                                   size scales the proposal, not the clipped step          */
+  const dqb_td_term* jump_terms; /* host array [n_jumps] or NULL: jump operator k is
+                                    c_k(t) L_k with c_k of jump_terms[k] (DQB_TD_CONST: 1);
+                                    dqb_mesolve_dia_td only (the other entry points return
+                                    DQB_ERR_UNSUPPORTED when it is set)                    */
 } dqb_td_hamiltonian;
 
 /* dqb_mesolve_dense with a time-dependent Hamiltonian: problem->H is the constant part;

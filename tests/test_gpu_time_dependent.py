@@ -210,3 +210,62 @@ def test_large_dense_batched_pwc_values(cuda_device):
             one.states, one.expects = res.states[i, j], res.expects[i, j]
             one.infos = type('I', (), {'nsteps': res.infos.nsteps[i, j]})()
             _check(Hi, L, rho0[j], ts, [num], m=m, res=one)
+
+
+# ---- time-dependent jump operators (DIA stepper) --------------------------------------
+
+def _oracle_td_jumps(Hs, Ls, cfs, rho0, ts, jts, rtol=1e-6, atol=1e-8):
+    """The Lindblad equation with H(t) = Hs(t) and jump operators c_k(t) L_k in complex128
+    through the oracle's RK engine and hermitian vector field
+    (diffrax_integrator.py:319-323), with the discontinuity times handed to its controller;
+    returns the saved states, the step count and the parity step slack."""
+    from oracle import lindblad as lb
+    from oracle.rk import solve
+
+    Ls = [np.asarray(L, dtype=complex) for L in Ls]
+
+    def f(t, y):
+        Lt = [complex(c(t)) * L for c, L in zip(cfs, Ls)]
+        Hnh = lb.hnh_dense(np.asarray(Hs(t), dtype=complex), Lt)
+        tmp = Hnh @ y
+        for L in Lt:
+            tmp = tmp + 0.5 * (L @ y @ L.conj().T)
+        return tmp + tmp.conj().T
+
+    psi = np.asarray(rho0, dtype=complex)
+    rho = psi @ psi.conj().T if psi.shape[-1] == 1 else psi
+    out = solve(f, rho, ts, rtol=rtol, atol=atol, save_fn=lambda y: y, jump_ts=jts)
+    borderline = any(abs(e - 1.0) < 0.1 for (_, _, e) in out.errors)
+    return np.stack(out.ysave), out.nsteps, (max(2, int(0.01 * out.nsteps)) if borderline else 1)
+
+
+@pytest.mark.parametrize('td_h', [False, True])
+def test_dia_time_dependent_jump_operators(cuda_device, td_h):
+    """Jump operators with PWC and Wave prefactors (and one constant), with a constant or a
+    time-dependent H, on the DIA stepper (n = 100): L_k(t) and Hnh(t) formed at every stage
+    time, steps clipped at every discontinuity; against the oracle at 1e-5."""
+    from dynamiqs_b200.time_qarray import as_summed
+
+    H0, x1, y2, Ls, Ld, n1 = _dia_modes(10)
+    a = ops.destroy(10, layout='dia')
+    eye = ops.eye(10, layout='dia')
+    a1, a2 = ops.tensor(a, eye), ops.tensor(eye, a)
+    decay1 = dq.pwc([0.0, 0.7, 1.4], [1.0, 0.3], a1 * np.float32(np.sqrt(0.2)))
+    decay2 = dq.modulated(dq.Wave(1.5, amplitude=1.0), a2 * np.float32(np.sqrt(0.1)))
+    deph = (a1.dag() @ a1) * np.float32(0.05)
+    jumps = [decay1, decay2, deph]
+    H = H0 + dq.pwc([0.2, 0.9, 1.6], [0.5, -0.4], x1) if td_h else H0
+    ts = np.linspace(0.0, 2.0, 9)
+    m = dq.Tsit5(rtol=1e-6, atol=1e-8)
+    rho0 = ops.fock(100, 0)
+    res = dq.mesolve(H, jumps, rho0, ts, method=m)
+    Hs = as_summed(H)
+    jts = np.unique(np.concatenate([Hs.discontinuity_ts, decay1.discontinuity_ts,
+                                    decay2.discontinuity_ts]))
+    cfs = [decay1.prefactor, decay2.prefactor, lambda t: 1.0]
+    ref, nsteps, slack = _oracle_td_jumps(Hs, [decay1.qarray, decay2.qarray, deph.to_dense()], cfs,
+                                          rho0, ts, jts)
+    err = np.linalg.norm(res.states.cpu().numpy() - ref, axis=(-2, -1)) / np.linalg.norm(ref, axis=(-2, -1))
+    assert err.max() < 1e-5, err
+    assert abs(int(res.infos.nsteps) - nsteps) <= slack, (int(res.infos.nsteps), nsteps)
+

@@ -197,3 +197,11 @@ def test_jump_operator_gradients_map_back_to_batched_operators(cartesian):
             i = next(j for j in range(items.shape[0]) if np.array_equal(items[j], sets[s]))
             exp.reshape(-1, n, n)[i] += grad_L[b, k].numpy()
         np.testing.assert_allclose(got[k].numpy(), exp, rtol=1e-5, atol=1e-5)
+
+
+def test_time_dependent_jump_operators_need_dia_storage():
+    """A time-dependent jump operator with dense operators is refused (before any GPU work)."""
+    a = ops.destroy(6, layout='dense')
+    L = dq.pwc([0.0, 1.0], [1.0], a)
+    with pytest.raises(NotImplementedError, match='DIA stepper'):
+        dq.mesolve(ops.dag(a) @ a, [L], ops.fock(6, 0), [0.0, 1.0])

@@ -815,13 +815,44 @@ int check_precision(int prec, int form, int n) {
 
 GraphCache g_cache;
 
+// Prefactors c_k(t) of the jump operators (time-dependent jump operators), by value.
+struct JumpTd {
+  int on;
+  TdTerm term[16];
+};
+
 struct LaunchKey {
   big::Common c;
   LargeOps d;
   TdOps td;
+  JumpTd jt;
   float2* hnh0;
+  const float2* L0;
   int form, krylov;
 };
+
+// Time-dependent jump operators: the per-instance copies L_k(t) = c_k(t) L_k that the
+// products read (L0: the given operators, indexed by L0idx), at the time of a right-hand
+// side (big::td_stage_time).  grid (tiles, B).
+__global__ void lt_td_dense_kernel(big::Common c, LargeOps d, JumpTd jt, const float2* L0, const int* L0idx,
+                                   int which) {
+  __shared__ float2 ck[16];
+  const int b = blockIdx.y;
+  double t;
+  if (!big::td_stage_time(c, c.inst[b], which, &t)) return;
+  if (threadIdx.x < d.K) {
+    const double2 v = td_coef(jt.term[threadIdx.x], b, t);
+    ck[threadIdx.x] = make_float2((float)v.x, (float)v.y);
+  }
+  __syncthreads();
+  const long long nn = c.nn;
+  const long long li = L0idx ? L0idx[b] : b;
+  const float2* src = L0 + li * d.K * nn;
+  float2* dst = const_cast<float2*>(d.L) + (long long)b * d.K * nn;
+  for (int k = 0; k < d.K; ++k)
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn; e += (long long)gridDim.x * blockDim.x)
+      dst[k * nn + e] = cmul(ck[k], src[k * nn + e]);
+}
 
 // Hnh at the time of a right-hand side (big::td_stage_time) of a time-dependent H:
 // hnh = hnh0 - i sum_m c_m(t) ops_m, ops dense [M, n, n].  grid (tiles, B).
@@ -915,6 +946,7 @@ static void init_carveouts() {
     prefer_max_shared(cgemm_kernel);
     prefer_max_shared(symmetrize_kernel);
     prefer_max_shared(hnh_td_dense_kernel);
+    prefer_max_shared(lt_td_dense_kernel);
     auto tc_attrs = [](auto kern, int smem) {
       prefer_max_shared(kern);
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -928,10 +960,24 @@ static void init_carveouts() {
   });
 }
 
-// The solve; `td` (or null) with `hnh0` (B n^2 values): the time-dependent terms of H.
-static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bool krylov,
-                     const TdOps* td = nullptr, float2* hnh0 = nullptr) {
+// The solve; `td` (or null) with `hnh0` (B n^2 values): the time-dependent terms of H;
+// `jt` (or null) with `Lt` (B K n^2 values): time-dependent jump operators, whose copies
+// c_k(t) L_k the products then read (and Hnh is formed by the GEMM from them at every
+// right-hand side).
+static int run_large(const big::Common& c, const LargeOps& d_in, cudaStream_t s, bool krylov,
+                     const TdOps* td = nullptr, float2* hnh0 = nullptr, const JumpTd* jt = nullptr,
+                     float2* Lt = nullptr) {
   init_carveouts();
+  LargeOps d = d_in;
+  JumpTd jtv;
+  std::memset(&jtv, 0, sizeof(jtv));
+  const float2* L0 = d_in.L;
+  const int* L0idx = d_in.Lidx;
+  if (jt && jt->on) {
+    jtv = *jt;
+    d.L = Lt;
+    d.Lidx = nullptr;
+  }
   const int B = c.B;
   int grid_e = (int)std::min<long long>((c.nn + big::kElemThreads - 1) / big::kElemThreads, 1184);
   if (grid_e < 1) grid_e = 1;
@@ -944,14 +990,22 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bo
   TdOps tdv;
   std::memset(&tdv, 0, sizeof(tdv));
   if (timedep) tdv = *td;
-  // Hnh at the time of the next right-hand side (time-dependent H only)
+  // Hnh (and the jump operators) at the time of the next right-hand side (time-dependent
+  // operators only)
   auto at_time = [&](cudaStream_t cs, int which) {
-    if (timedep) hnh_td_dense_kernel<<<ge, T, 0, cs>>>(c, d, tdv, hnh0, which);
+    if (jtv.on) {
+      lt_td_dense_kernel<<<ge, T, 0, cs>>>(c, d, jtv, L0, L0idx, which);
+      // Hnh = -iH - 1/2 sum L(t)^+ L(t) by the GEMM, for the instances that evaluate it
+      launch_hnh(cs, c, d, B, which >= 8 ? 0 : (which == 7 ? 3 : 1));
+      if (tdv.M > 0) hnh_td_dense_kernel<<<ge, T, 0, cs>>>(c, d, tdv, d.hnh, which);  // in place
+    } else if (timedep) {
+      hnh_td_dense_kernel<<<ge, T, 0, cs>>>(c, d, tdv, hnh0, which);
+    }
   };
 
   big::setup_kernel<<<gi, 128, 0, s>>>(c);
   big::load_rho0_kernel<<<ge, T, 0, s>>>(c);
-  {
+  if (!jtv.on) {  // (with time-dependent jump operators every Hnh is formed at its time)
     LargeOps d0 = d;  // the constant Hnh: into hnh, or into hnh0 when H depends on time
     if (timedep) d0.hnh = hnh0;
     launch_hnh(s, c, d0, B, 0);
@@ -1009,7 +1063,9 @@ static int run_large(const big::Common& c, const LargeOps& d, cudaStream_t s, bo
     key.c = c;
     key.d = d;
     key.td = tdv;
+    key.jt = jtv;
     key.hnh0 = hnh0;
+    key.L0 = L0;
     key.form = form;
     key.krylov = krylov;
     cudaGraphExec_t exec = g_cache.find(&key, sizeof(key));
@@ -1124,14 +1180,23 @@ static int solve_large(const dqb_dense_problem* p, const dqb_td_hamiltonian* tdh
   if (o->stepper < DQB_STEPPER_AUTO || o->stepper > DQB_STEPPER_KRYLOV) return DQB_ERR_INVALID_ARGUMENT;
   if (int prc = check_precision(o->precision, o->form, p->n)) return prc;
   TdOps td;
+  JumpTd jt;
+  std::memset(&jt, 0, sizeof(jt));
   if (tdh) {
     // the Krylov form needs a constant right-hand side
-    if (large_krylov(*o) || tdh->jump_terms) return DQB_ERR_UNSUPPORTED;
+    if (large_krylov(*o)) return DQB_ERR_UNSUPPORTED;
     if (int tr = td_ops_from(tdh, &td)) return tr;
+    if (tdh->jump_terms) {
+      if (p->n_jumps > 16) return DQB_ERR_UNSUPPORTED;
+      jt.on = 1;
+      for (int k = 0; k < p->n_jumps; ++k)
+        if (int tr = td_term_from(tdh->jump_terms[k], &jt.term[k])) return tr;
+    }
   }
   if (p->batch == 0) return DQB_OK;
   const LargeLayout lay = large_layout(p->n, p->n_jumps, p->n_exp, p->n_tsave, p->batch);
-  const size_t need = tdh ? align_up(lay.total) + (size_t)p->batch * p->n * p->n * sizeof(float2) : lay.total;
+  const size_t nnb = (size_t)p->batch * p->n * p->n * sizeof(float2);
+  const size_t need = tdh ? align_up(lay.total) + nnb * (1 + std::max(p->n_jumps, 1)) : lay.total;
   if (!workspace || workspace_bytes < need) return DQB_ERR_WORKSPACE_TOO_SMALL;
   char* ws = (char*)workspace;
   LargeOps d = make_ops(p, ws, lay);
@@ -1163,7 +1228,8 @@ static int solve_large(const dqb_dense_problem* p, const dqb_td_hamiltonian* tdh
   if (!tdh) return run_large(c, d, (cudaStream_t)stream, large_krylov(*o));
   c.n_jump = tdh->n_jump_ts;
   c.jump_ts = tdh->jump_ts;
-  return run_large(c, d, (cudaStream_t)stream, false, &td, (float2*)(ws + align_up(lay.total)));
+  return run_large(c, d, (cudaStream_t)stream, false, &td, (float2*)(ws + align_up(lay.total)), &jt,
+                   (float2*)(ws + align_up(lay.total) + nnb));
 }
 
 extern "C" int dqb_mesolve_dense_large(const dqb_dense_problem* p, const dqb_ode_options* o, const dqb_outputs* out,
@@ -1174,7 +1240,7 @@ extern "C" int dqb_mesolve_dense_large(const dqb_dense_problem* p, const dqb_ode
 extern "C" size_t dqb_mesolve_dense_large_td_workspace_size(int32_t n, int32_t n_jumps, int32_t n_exp,
                                                             int32_t n_tsave, int64_t batch) {
   const size_t base = dqb_mesolve_dense_large_workspace_size(n, n_jumps, n_exp, n_tsave, batch);
-  return base ? align_up(base) + (size_t)batch * n * n * sizeof(float2) : 0;
+  return base ? align_up(base) + (size_t)batch * n * n * sizeof(float2) * (1 + std::max(n_jumps, 1)) : 0;
 }
 
 extern "C" int dqb_mesolve_dense_large_td(const dqb_dense_problem* p, const dqb_td_hamiltonian* td,

@@ -702,13 +702,17 @@ def mesolve(H, jump_ops, rho0, tsave, *, exp_ops=None, method: Method = Tsit5(),
     td_types = (PWCTimeQArray, ModulatedTimeQArray, SummedTimeQArray)
     if any(isinstance(L, td_types) for L in jump_ops):
         Hs = as_summed(H if isinstance(H, td_types) else _as_op(H))
-        if not _td_on_dia(Hs, jump_ops, options):
-            raise NotImplementedError('Time-dependent jump operators run on the DIA stepper: every '
-                                      'operator in sparse-DIA storage, each time-dependent jump '
-                                      'operator one dq.pwc / dq.modulated term with unbatched '
-                                      'values, at most four time-dependent terms in H.')
-        return _mesolve_td_dia(Hs, jump_ops, rho0, tsave, exp_ops=exp_ops, method=method,
-                               gradient=gradient, options=options)
+        if _td_on_dia(Hs, jump_ops, options):
+            return _mesolve_td_dia(Hs, jump_ops, rho0, tsave, exp_ops=exp_ops, method=method,
+                                   gradient=gradient, options=options)
+        if _td_jumps_on_large(Hs, jump_ops, options):
+            return _mesolve_td(Hs, jump_ops, rho0, tsave, exp_ops=exp_ops, method=method,
+                               gradient=gradient, options=options, kind='large')
+        raise NotImplementedError('Time-dependent jump operators need every operator dense (the '
+                                  'GEMM path) or every one in sparse-DIA storage (the DIA '
+                                  'stepper), each time-dependent jump operator one dq.pwc / '
+                                  'dq.modulated term with unbatched values, and at most four '
+                                  'time-dependent terms in H.')
     if isinstance(H, td_types):
         Hs = as_summed(H)
         if _td_on_device(Hs, jump_ops, options):
@@ -806,7 +810,7 @@ def _mesolve_td(Hs, jump_ops, rho0, tsave, *, exp_ops, method, gradient, options
 
     from .time_qarray import PWCTimeQArray
 
-    Ls = [_as_op(L) for L in jump_ops]
+    Ls = [_as_op(_jump_source(L)) for L in jump_ops]
     rho0 = _as_op(rho0)
     tsave = np.asarray(tsave.detach().cpu().numpy() if hasattr(tsave, 'detach') else tsave,
                        dtype=np.float64)
@@ -855,13 +859,17 @@ def _mesolve_td(Hs, jump_ops, rho0, tsave, *, exp_ops, method, gradient, options
             T.amp_re, T.amp_im = f.amplitude.real, f.amplitude.imag
             T.omega, T.phase, T.t_center, T.sigma = f.omega, f.phase, f.t_center, f.sigma
             T.t_start, T.t_end = f.t_start, f.t_end
-    ops_d = _to_dev(np.stack([t.qarray for t in Hs.td_terms]), torch.complex64, dev)
-    jts = np.asarray(Hs.discontinuity_ts, dtype=np.float64)
+    ops_d = (_to_dev(np.stack([t.qarray for t in Hs.td_terms]), torch.complex64, dev)
+             if Hs.td_terms else torch.zeros(1, dtype=torch.complex64, device=dev))
+    jterms, disc = _jump_prefactors(jump_ops, dev, keep)
+    jts = np.unique(np.concatenate([np.asarray(Hs.discontinuity_ts, dtype=np.float64)] + disc))
     jts_d = _to_dev(jts if jts.size else np.zeros(1), torch.float64, dev)
     keep += [ops_d, jts_d]
     td = _lib.TdHamiltonian(n_terms=len(Hs.td_terms), ops=ops_d.data_ptr(),
                             terms=ctypes.cast(terms, ctypes.POINTER(_lib.TdTerm)),
-                            n_jump_ts=int(jts.size), jump_ts=jts_d.data_ptr())
+                            n_jump_ts=int(jts.size), jump_ts=jts_d.data_ptr(),
+                            jump_terms=(ctypes.cast(jterms, ctypes.POINTER(_lib.TdTerm))
+                                        if jterms is not None else None))
     prep.bufs['td'] = (td, terms, keep)
 
     entry = 'dqb_mesolve_dense_td' if kind == 'small' else 'dqb_mesolve_dense_large_td'
@@ -882,6 +890,53 @@ def _td_on_dia(Hs, jump_ops, options) -> bool:
     if not all(isinstance(_jump_source(L), SparseDIA) for L in jump_ops):
         return False
     return len(_td_union_offsets(Hs)) <= _lib.DIA_MAX_HNH_DIAGS
+
+
+def _jump_prefactors(jump_ops, dev, keep):
+    """The dqb_td_term array of the jump operators' prefactors c_k(t) (constant operators:
+    DQB_TD_CONST), or None when none depends on time, and their discontinuity times."""
+    import torch
+
+    from .time_qarray import ModulatedTimeQArray, PWCTimeQArray
+
+    if not any(isinstance(L, (PWCTimeQArray, ModulatedTimeQArray)) for L in jump_ops):
+        return None, []
+    jterms = (_lib.TdTerm * max(len(jump_ops), 1))()
+    disc = []
+    for k, L in enumerate(jump_ops):
+        T = jterms[k]
+        if isinstance(L, PWCTimeQArray):
+            tt = _to_dev(L.times, torch.float64, dev)
+            vv = _to_dev(np.ascontiguousarray(L.values.reshape(1, -1), dtype=np.complex128),
+                         torch.complex128, dev)
+            keep += [tt, vv]
+            T.kind, T.n_times = _lib.TD_PWC, L.times.size
+            T.times, T.values, T.value_index = tt.data_ptr(), vv.data_ptr(), None
+            disc.append(np.asarray(L.discontinuity_ts, dtype=np.float64))
+        elif isinstance(L, ModulatedTimeQArray):
+            f = L.f
+            T.kind = _lib.TD_WAVE
+            T.amp_re, T.amp_im = f.amplitude.real, f.amplitude.imag
+            T.omega, T.phase, T.t_center, T.sigma = f.omega, f.phase, f.t_center, f.sigma
+            T.t_start, T.t_end = f.t_start, f.t_end
+            disc.append(np.asarray(L.discontinuity_ts, dtype=np.float64))
+        else:
+            T.kind = _lib.TD_CONST
+    keep.append(jterms)
+    return jterms, disc
+
+
+def _td_jumps_on_large(Hs, jump_ops, options) -> bool:
+    """Whether time-dependent jump operators with dense operators run on the GEMM path:
+    dense H (constant part and terms) and jump operators, at most four time-dependent
+    terms in H."""
+    if options.vectorized or len(Hs.td_terms) > _lib.TD_MAX_TERMS or options.stepper == 'krylov':
+        return False
+    if any(isinstance(c, SparseDIA) for c in Hs._const_src) or \
+            any(isinstance(t.source, SparseDIA) for t in Hs.td_terms):
+        return False
+    srcs = [_jump_source(L) for L in jump_ops]
+    return all(s is not None and not isinstance(s, SparseDIA) and np.ndim(s) == 2 for s in srcs)
 
 
 def _jump_source(L):
@@ -923,9 +978,8 @@ def _mesolve_td_dia(Hs, jump_ops, rho0, tsave, *, exp_ops, method, gradient, opt
 
     import torch
 
-    from .time_qarray import ModulatedTimeQArray, PWCTimeQArray
+    from .time_qarray import PWCTimeQArray
 
-    td_jumps = [L for L in jump_ops if isinstance(L, (PWCTimeQArray, ModulatedTimeQArray))]
     Ls = [_jump_source(L) for L in jump_ops]
     rho0 = _as_op(rho0)
     tsave = np.asarray(tsave.detach().cpu().numpy() if hasattr(tsave, 'detach') else tsave,
@@ -976,30 +1030,8 @@ def _mesolve_td_dia(Hs, jump_ops, rho0, tsave, *, exp_ops, method, gradient, opt
     ops_d = (_to_dev(np.stack([_on_offsets(t.source, offs) for t in Hs.td_terms]), torch.complex64, dev)
              if Hs.td_terms else torch.zeros(1, dtype=torch.complex64, device=dev))
     # prefactors of the jump operators (constant ones: 1)
-    jterms = None
-    disc = [np.asarray(Hs.discontinuity_ts, dtype=np.float64)]
-    if td_jumps:
-        jterms = (_lib.TdTerm * max(len(jump_ops), 1))()
-        for k, L in enumerate(jump_ops):
-            T = jterms[k]
-            if isinstance(L, PWCTimeQArray):
-                tt = _to_dev(L.times, torch.float64, dev)
-                vv = _to_dev(np.ascontiguousarray(L.values.reshape(1, -1), dtype=np.complex128),
-                             torch.complex128, dev)
-                keep += [tt, vv]
-                T.kind, T.n_times = _lib.TD_PWC, L.times.size
-                T.times, T.values, T.value_index = tt.data_ptr(), vv.data_ptr(), None
-                disc.append(np.asarray(L.discontinuity_ts, dtype=np.float64))
-            elif isinstance(L, ModulatedTimeQArray):
-                f = L.f
-                T.kind = _lib.TD_WAVE
-                T.amp_re, T.amp_im = f.amplitude.real, f.amplitude.imag
-                T.omega, T.phase, T.t_center, T.sigma = f.omega, f.phase, f.t_center, f.sigma
-                T.t_start, T.t_end = f.t_start, f.t_end
-                disc.append(np.asarray(L.discontinuity_ts, dtype=np.float64))
-            else:
-                T.kind = _lib.TD_CONST
-    jts = np.unique(np.concatenate(disc)) if disc else np.zeros(0)
+    jterms, disc = _jump_prefactors(jump_ops, dev, keep)
+    jts = np.unique(np.concatenate([np.asarray(Hs.discontinuity_ts, dtype=np.float64)] + disc))
     jts_d = _to_dev(jts if jts.size else np.zeros(1), torch.float64, dev)
     keep += [ops_d, jts_d]
     td = _lib.TdHamiltonian(n_terms=len(Hs.td_terms), ops=ops_d.data_ptr(),

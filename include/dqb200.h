@@ -296,8 +296,8 @@ typedef struct dqb_td_hamiltonian {
                                   size scales the proposal, not the clipped step          */
   const dqb_td_term* jump_terms; /* host array [n_jumps] or NULL: jump operator k is
                                     c_k(t) L_k with c_k of jump_terms[k] (DQB_TD_CONST: 1);
-                                    dqb_mesolve_dia_td only (the other entry points return
-                                    DQB_ERR_UNSUPPORTED when it is set)                    */
+                                    dqb_mesolve_dia_td and dqb_mesolve_dense_large_td only
+                                    (the others return DQB_ERR_UNSUPPORTED when it is set) */
 } dqb_td_hamiltonian;
 
 /* dqb_mesolve_dense with a time-dependent Hamiltonian: problem->H is the constant part;
@@ -433,7 +433,8 @@ DQB_API int dqb_mesolve_dense_large(const dqb_dense_problem* problem, const dqb_
  * (dqb_td_hamiltonian with dense ops [M, n, n]): Hnh at every stage time formed from the
  * constant Hnh0 before each right-hand side, steps clipped at td->jump_ts with the first
  * stage re-evaluated after each one, as dqb_mesolve_dense_td does for n <= 64.  Stage form
- * only (a Krylov request returns DQB_ERR_UNSUPPORTED).  The workspace also holds Hnh0:
+ * only (a Krylov request returns DQB_ERR_UNSUPPORTED).  The workspace also holds Hnh0 and the
+ * per-instance copies c_k(t) L_k of time-dependent jump operators (td->jump_terms):
  * dqb_mesolve_dense_large_td_workspace_size. */
 DQB_API size_t dqb_mesolve_dense_large_td_workspace_size(int32_t n, int32_t n_jumps, int32_t n_exp,
                                                          int32_t n_tsave, int64_t batch);

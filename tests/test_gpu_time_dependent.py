@@ -269,3 +269,29 @@ def test_dia_time_dependent_jump_operators(cuda_device, td_h):
     assert err.max() < 1e-5, err
     assert abs(int(res.infos.nsteps) - nsteps) <= slack, (int(res.infos.nsteps), nsteps)
 
+
+
+@pytest.mark.parametrize('n', [12, 80])
+def test_dense_time_dependent_jump_operators(cuda_device, n):
+    """Dense operators with a PWC-modulated decay and a Wave-modulated dephasing, with a
+    PWC drive on H, on the GEMM path (any n; n = 12 goes there too): the copies c_k(t) L_k
+    and Hnh(t) = -iH(t) - 1/2 sum |c_k|^2 L_k^+ L_k formed at every stage time; against the
+    oracle at 1e-5."""
+    from dynamiqs_b200.time_qarray import as_summed
+
+    a, num, x = _osc(n)
+    decay = dq.pwc([0.0, 0.6, 1.3], [1.0, 0.4], np.float32(np.sqrt(0.2)) * a)
+    deph = dq.modulated(dq.Wave(2.0, amplitude=0.8), np.float32(np.sqrt(0.02)) * num)
+    H = 0.4 * num + dq.pwc([0.3, 0.9, 1.5], [0.6, -0.3], x)
+    ts = np.linspace(0.0, 1.8, 7)
+    m = dq.Tsit5(rtol=1e-6, atol=1e-8)
+    rho0 = ops.fock(n, 1)
+    res = dq.mesolve(H, [decay, deph], rho0, ts, exp_ops=[num], method=m)
+    Hs = as_summed(H)
+    jts = np.unique(np.concatenate([Hs.discontinuity_ts, decay.discontinuity_ts,
+                                    deph.discontinuity_ts]))
+    ref, nsteps, slack = _oracle_td_jumps(Hs, [decay.qarray, deph.qarray],
+                                          [decay.prefactor, deph.prefactor], rho0, ts, jts)
+    err = np.linalg.norm(res.states.cpu().numpy() - ref, axis=(-2, -1)) / np.linalg.norm(ref, axis=(-2, -1))
+    assert err.max() < 1e-5, err
+    assert abs(int(res.infos.nsteps) - nsteps) <= slack, (int(res.infos.nsteps), nsteps)

@@ -199,9 +199,14 @@ def test_jump_operator_gradients_map_back_to_batched_operators(cartesian):
         np.testing.assert_allclose(got[k].numpy(), exp, rtol=1e-5, atol=1e-5)
 
 
-def test_time_dependent_jump_operators_need_dia_storage():
-    """A time-dependent jump operator with dense operators is refused (before any GPU work)."""
+def test_time_dependent_jump_operators_need_one_storage():
+    """Time-dependent jump operators run with every operator dense (GEMM path) or every one
+    in sparse-DIA storage (DIA stepper); a dense H with a DIA jump operator, or a jump
+    operator with batched prefactor values, is refused before any GPU work."""
     a = ops.destroy(6, layout='dense')
-    L = dq.pwc([0.0, 1.0], [1.0], a)
-    with pytest.raises(NotImplementedError, match='DIA stepper'):
-        dq.mesolve(ops.dag(a) @ a, [L], ops.fock(6, 0), [0.0, 1.0])
+    a_dia = ops.destroy(6, layout='dia')
+    with pytest.raises(NotImplementedError, match='every operator dense'):
+        dq.mesolve(ops.dag(a) @ a, [dq.pwc([0.0, 1.0], [1.0], a_dia)], ops.fock(6, 0), [0.0, 1.0])
+    with pytest.raises(NotImplementedError, match='unbatched values'):
+        dq.mesolve(ops.dag(a) @ a, [dq.pwc([0.0, 1.0], [[1.0], [0.5]], a)], ops.fock(6, 0),
+                   [0.0, 1.0])

@@ -607,8 +607,8 @@ __device__ __forceinline__ void wide_load(const float2* __restrict__ rp, int col
 // and above the diagonal and nothing else -- every element (i, j) with j >= 32 floor(i / 32),
 // the set the hermitian-half elementwise kernels read -- and no mirror, for a stage slot
 // that only those kernels consume.
-template <int R, int NR, int NP, int C, bool HERM, int U = 1>
-__global__ void __launch_bounds__(kRhsCols, 4) rhs_dia_wide_kernel(big::Common c, DiaOps d, DiaWide w, int in_sel,
+template <int R, int NR, int NP, int C, bool HERM, int U = 1, int MB = 4>
+__global__ void __launch_bounds__(kRhsCols, MB) rhs_dia_wide_kernel(big::Common c, DiaOps d, DiaWide w, int in_sel,
                                                                   int out_k, int need_run, int kry,
                                                                   const float2* ext_in, float2* ext_out,
                                                                   int half) {
@@ -1221,19 +1221,23 @@ int wide_nr(int nr) { return nr <= 4 ? 4 : 8; }
 int wide_np(int np) { return np <= 2 ? 2 : 4; }
 
 // Shape codes of the wide kernel: 200 + R (C = 4 columns per thread) or 300 + R (C = 2),
-// R = 8 or 16 rows per CTA.
+// R = 8 or 16 rows per CTA; 408 / 508: 8 rows, two rows' loads in flight per thread;
+// 708: 8 rows with C = 2, registers capped for 6 resident CTAs per SM (instead of 4) so
+// that more warps hide the shifted loads' latency (C = 4 capped for 5 CTAs spills).
 bool is_wide(int rows) {
-  return rows == 208 || rows == 216 || rows == 308 || rows == 316 || rows == 408 || rows == 508;
+  return rows == 208 || rows == 216 || rows == 308 || rows == 316 || rows == 408 || rows == 508 ||
+         rows == 708;
 }
 bool is_bulk(int rows) { return rows == 604 || rows == 608; }
-int wide_c(int rows) { return (rows / 100) % 2 == 1 ? 2 : 4; }  // 2xx, 4xx: 4; 3xx, 5xx: 2
+int wide_c(int rows) { return (rows / 100) % 2 == 1 ? 2 : 4; }  // 2xx, 4xx: 4; 3xx, 5xx, 7xx: 2
 int wide_r(int rows) { return rows % 100; }
 
 // Launch shape of the stencil from `tile`: 4, 8 or 16 = the tiled kernel with that many rows
 // per thread (when the operators have at most kTiledMaxTerms diagonal terms); 108 or 116 =
 // the staged kernel with 8 or 16 rows per CTA (when its plan fits); 208 or 216 (4 columns
 // per thread), 308 or 316 (2 columns) = the wide kernel with 8 or 16 rows per CTA, 408 /
-// 508 = 8 rows with two rows in flight per thread (when its plan fits); anything else (0 =
+// 508 = 8 rows with two rows in flight per thread, 708 = 8 rows (2 columns) with registers
+// capped for more resident CTAs (when its plan fits); anything else (0 =
 // default, 1) = the generic kernel.  The autotuner picks among them per problem shape.
 // Returns the shape code (1 = generic).
 int rows_for(const DiaOps& d, int tile) {
@@ -1266,23 +1270,23 @@ dim3 rhs_grid(const DiaOps& d, int rows, int B) {
   return dim3((d.n + kRhsCols - 1) / kRhsCols, (d.n + r - 1) / r, B);
 }
 
-template <int R, int C, bool HERM, int U>
+template <int R, int C, bool HERM, int U, int MB>
 void launch_wide_form(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, const DiaWide& w,
                       int in_sel, int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out,
                       int half) {
   const int nr = wide_nr(w.nr), np = wide_np(w.np);
   const size_t sm = HERM && !half ? (size_t)R * (kRhsCols * C + 1) * sizeof(float2) : 0;
   if (nr == 4 && np == 2)
-    rhs_dia_wide_kernel<R, 4, 2, C, HERM, U><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
+    rhs_dia_wide_kernel<R, 4, 2, C, HERM, U, MB><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
                                                                     ext_in, ext_out, half);
   else if (nr == 4)
-    rhs_dia_wide_kernel<R, 4, 4, C, HERM, U><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
+    rhs_dia_wide_kernel<R, 4, 4, C, HERM, U, MB><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
                                                                     ext_in, ext_out, half);
   else if (np == 2)
-    rhs_dia_wide_kernel<R, 8, 2, C, HERM, U><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
+    rhs_dia_wide_kernel<R, 8, 2, C, HERM, U, MB><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
                                                                     ext_in, ext_out, half);
   else
-    rhs_dia_wide_kernel<R, 8, 4, C, HERM, U><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
+    rhs_dia_wide_kernel<R, 8, 4, C, HERM, U, MB><<<g, kRhsCols, sm, s>>>(c, d, w, in_sel, out_k, need_run, kry,
                                                                     ext_in, ext_out, half);
 }
 
@@ -1303,13 +1307,13 @@ void launch_bulk(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, 
     rhs_dia_bulk_kernel<R, 8, 4><<<g, kBulkW, sm, s>>>(c, d, w, pl, in_sel, out_k, need_run, kry, ext_in, ext_out);
 }
 
-template <int R, int C, int U = 1>
+template <int R, int C, int U = 1, int MB = 4>
 void launch_wide(cudaStream_t s, dim3 g, const big::Common& c, const DiaOps& d, const DiaWide& w, int in_sel,
                  int out_k, int need_run, int kry, const float2* ext_in, float2* ext_out, bool herm, bool half) {
   if (herm)
-    launch_wide_form<R, C, true, U>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, half ? 1 : 0);
+    launch_wide_form<R, C, true, U, MB>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, half ? 1 : 0);
   else
-    launch_wide_form<R, C, false, U>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, 0);
+    launch_wide_form<R, C, false, U, MB>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, 0);
 }
 
 // One right-hand side of every instance: k[out_k] = f(input), through the kernel the shape
@@ -1340,6 +1344,7 @@ void launch_rhs_dia(cudaStream_t s, const big::Common& c, const DiaOps& d, int B
       case 308: launch_wide<8, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm, half); break;
       case 408: launch_wide<8, 4, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm, half); break;
       case 508: launch_wide<8, 2, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm, half); break;
+      case 708: launch_wide<8, 2, 1, 6>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm, half); break;
       default: launch_wide<16, 2>(s, g, c, d, w, in_sel, out_k, need_run, kry, ext_in, ext_out, herm, half);
     }
     return;

@@ -276,9 +276,10 @@ class PreparedSolve:
 # Shape codes of the sparse-DIA stencil (dqb_ode_options.tile) the autotuner times: the
 # generic kernel, the tiled one with 4, 8, 16 rows per thread, the staged one with 8 or 16
 # rows per CTA, the wide one with 4 or 2 columns per thread and 8 or 16 rows per CTA (and
-# 8 rows with two rows' loads in flight per thread: 408, 508), and the bulk-staged one with
+# 8 rows with two rows' loads in flight per thread: 408, 508; 8 rows and 2 columns with
+# registers capped for more resident CTAs: 708), and the bulk-staged one with
 # stages of 4 or 8 rows (604, 608; hermitian form).
-DIA_STENCIL_SHAPES = (1, 4, 8, 16, 108, 116, 208, 216, 308, 316, 408, 508, 604, 608)
+DIA_STENCIL_SHAPES = (1, 4, 8, 16, 108, 116, 208, 216, 308, 316, 408, 508, 604, 608, 708)
 
 
 def _stepper_code(o) -> int:

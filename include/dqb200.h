@@ -91,7 +91,9 @@ typedef struct dqb_ode_options {
                               staged kernel with 8 or 16 rows per CTA; 208 or 216 (4
                               columns per thread), 308 or 316 (2 columns) = wide kernel
                               with 8 or 16 rows per CTA, 408 / 508 = 8 rows with two
-                              rows in flight per thread; 604 / 608 = bulk-staged kernel
+                              rows in flight per thread, 708 = 8 rows, 2 columns,
+                              registers capped for 6 CTAs per SM;
+                              604 / 608 = bulk-staged kernel
                               (rows of X copied into shared memory by the bulk-copy
                               engine, stages of 4 / 8 rows; hermitian form, else 308);
                               0 (default) or 1 = generic

@@ -51,7 +51,7 @@ def _problem_struct(H, Ls, n, batch):
     return p, [h_off, l_nd, l_off, H_d, L_d]
 
 
-@pytest.mark.parametrize('tile', [0, 8, 108, 116, 208, 316, 408, 508, 604, 608])
+@pytest.mark.parametrize('tile', [0, 8, 108, 116, 208, 316, 408, 508, 604, 608, 708])
 @pytest.mark.parametrize('form', [_lib.FORM_HERMITIAN, _lib.FORM_STANDARD])
 @pytest.mark.parametrize('n', [10, 77, 300])
 def test_rhs_dia_matches_oracle(cuda_device, form, n, tile):
@@ -107,7 +107,7 @@ def test_coupled_kerr_dia_small_vs_oracle(cuda_device):
         _oracle_compare(res, w, b)
 
 
-@pytest.mark.parametrize('tile', [1, 8, 208, 216, 308, 316, 408, 508, 608])
+@pytest.mark.parametrize('tile', [1, 8, 208, 216, 308, 316, 408, 508, 608, 708])
 @pytest.mark.parametrize('m', [10, 18])
 def test_dia_solve_every_stencil_shape_vs_oracle(cuda_device, m, tile):
     """The DIA solve with the stencil shape forced, hermitian form: the wide shapes
@@ -186,7 +186,7 @@ def coupled_kerr_4096_rhs():
     return w, X, ref
 
 
-@pytest.mark.parametrize('tile', [0, 4, 8, 16, 108, 116, 208, 216, 308, 316, 408, 508, 604, 608])
+@pytest.mark.parametrize('tile', [0, 4, 8, 16, 108, 116, 208, 216, 308, 316, 408, 508, 604, 608, 708])
 def test_rhs_dia_full_size_every_stencil(cuda_device, coupled_kerr_4096_rhs, tile):
     """One right-hand side at n = 4096 with the workload's own offsets (+-63/+-64 select
     other row groups in the staged kernel and other halos in the tiled one than the small

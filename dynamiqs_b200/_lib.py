@@ -40,6 +40,7 @@ METHOD_TSIT5 = 0
 METHOD_DOPRI5 = 1
 FORM_HERMITIAN = 0
 FORM_STANDARD = 1
+FORM_HERMITIAN_UPPER = 2  # DIA right-hand-side entry points only: upper 32 x 32 tiles
 PREC_FP32 = 0
 PREC_TF32X3 = 1
 PREC_BF16X3 = 2

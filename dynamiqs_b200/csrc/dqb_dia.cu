@@ -1464,7 +1464,8 @@ extern "C" int dqb_lindblad_rhs_dia_tiled(const dqb_dia_problem* p, int32_t form
   int rc = check_ops(p);
   if (rc) return rc;
   if (!rho || !outp) return DQB_ERR_INVALID_ARGUMENT;
-  if (form != DQB_FORM_HERMITIAN && form != DQB_FORM_STANDARD) return DQB_ERR_INVALID_ARGUMENT;
+  if (form != DQB_FORM_HERMITIAN && form != DQB_FORM_STANDARD && form != DQB_FORM_HERMITIAN_UPPER)
+    return DQB_ERR_INVALID_ARGUMENT;
   if (p->batch == 0) return DQB_OK;
   DiaOps d;
   rc = build_ops(p, &d);
@@ -1482,7 +1483,7 @@ extern "C" int dqb_lindblad_rhs_dia_tiled(const dqb_dia_problem* p, int32_t form
       ((reinterpret_cast<uintptr_t>(rho) | reinterpret_cast<uintptr_t>(outp)) & 15))
     rows = 1;
   launch_rhs_dia(s, c, d, (int)p->batch, rows, 2, 0, 0, (const float2*)rho, (float2*)outp, 0,
-                 form == DQB_FORM_HERMITIAN);
+                 form != DQB_FORM_STANDARD, form == DQB_FORM_HERMITIAN_UPPER);
   return cudaGetLastError() == cudaSuccess ? DQB_OK : DQB_ERR_CUDA;
 }
 

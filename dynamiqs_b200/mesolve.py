@@ -591,7 +591,9 @@ class MESolveB200Integrator:
 
     def _tune_dia_tile(self, lib, prob, ws, ws_bytes, dev, pattern) -> None:
         """Launch shape of the DIA stencil for this (n, sparsity pattern), among
-        ``DIA_STENCIL_SHAPES``, timed on one right-hand side of one instance."""
+        ``DIA_STENCIL_SHAPES``, timed on one right-hand side of the instances that run
+        together (the solve's first instances, at most 1 GiB of states): the grid the solve
+        launches, so that its tail and occupancy effects are the ones timed."""
         import ctypes
 
         import torch
@@ -599,22 +601,29 @@ class MESolveB200Integrator:
         from . import autotune
 
         n = prob.n
+        # the form the solve's stencils write in: the stage form of the hermitian form
+        # fills only the stage slots' upper 32 x 32 tiles; the Krylov basis and the
+        # standard form write whole matrices
+        form = self._form()
+        if form == _lib.FORM_HERMITIAN and _stepper_code(self.options) != _lib.STEPPER_KRYLOV:
+            form = _lib.FORM_HERMITIAN_UPPER
+        bt = int(max(1, min(prob.batch, (1 << 30) // (8 * n * n))))
         pt = _lib.DiaProblem.from_buffer_copy(prob)
-        pt.batch = 1
+        pt.batch = bt
         g = torch.Generator(device='cpu').manual_seed(0)
-        rho = (torch.randn(1, n, n, dtype=torch.complex64, generator=g) / n).to(dev)
+        rho = (torch.randn(bt, n, n, dtype=torch.complex64, generator=g) / n).to(dev)
         out = torch.empty_like(rho)
         stream = torch.cuda.current_stream(dev).cuda_stream
 
         def make_run(t):
             def run():
                 _lib.check(lib.dqb_lindblad_rhs_dia_tiled(
-                    ctypes.byref(pt), _lib.FORM_HERMITIAN, t, rho.data_ptr(), out.data_ptr(),
+                    ctypes.byref(pt), form, t, rho.data_ptr(), out.data_ptr(),
                     ws.data_ptr(), ws_bytes, stream), 'dqb_lindblad_rhs_dia_tiled')
             return run
 
         key = ('dia_stencil', torch.cuda.get_device_name(dev), n, prob.n_jumps, pattern,
-               autotune.batch_bucket(prob.batch))
+               autotune.batch_bucket(prob.batch), form)
         self._tuned['tile'] = autotune.choose(key, list(DIA_STENCIL_SHAPES), make_run, 1)
 
     # kept for callers that select a path explicitly (tests)

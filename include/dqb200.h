@@ -55,6 +55,12 @@ extern "C" {
 #define DQB_METHOD_DOPRI5 1
 #define DQB_FORM_HERMITIAN 0 /* tmp = Hnh rho + 1/2 sum L rho L^+ ; out = tmp + tmp^+ */
 #define DQB_FORM_STANDARD 1  /* Hnh rho + rho Hnh^+ + sum L rho L^+                 */
+/* dqb_lindblad_rhs_dia(_tiled) only: the hermitian form with out[b] defined on the 32 x 32
+ * tiles on and above the diagonal alone (every element (i, j) with j >= 32 floor(i / 32);
+ * the rest is left as it was, except by stencil shapes that always write the whole
+ * matrix): the layout of the stage slots in dqb_mesolve_dia's stage form, which the
+ * autotuner times. */
+#define DQB_FORM_HERMITIAN_UPPER 2
 
 /* Arithmetic of the complex products.  The tensor-core modes run tcgen05 MMAs with FP32
  * accumulation in tensor memory, on each operand split into hi + lo parts (three products
@@ -539,8 +545,9 @@ DQB_API int dqb_mesolve_dia_td(const dqb_dia_problem* problem, const dqb_td_hami
                                const dqb_ode_options* options, const dqb_outputs* outputs,
                                void* workspace, size_t workspace_bytes, void* stream);
 
-/* One right-hand side per instance with DIA operators: out[b] = f(rho[b]).  `workspace`
- * holds the Hnh diagonals (size from dqb_mesolve_dia_workspace_size suffices). */
+/* One right-hand side per instance with DIA operators: out[b] = f(rho[b]).  `form`:
+ * DQB_FORM_HERMITIAN, DQB_FORM_STANDARD or DQB_FORM_HERMITIAN_UPPER.  `workspace` holds
+ * the Hnh diagonals (size from dqb_mesolve_dia_workspace_size suffices). */
 DQB_API int dqb_lindblad_rhs_dia(const dqb_dia_problem* problem, int32_t form, const void* rho,
                                  void* out, void* workspace, size_t workspace_bytes, void* stream);
 

@@ -209,6 +209,35 @@ def test_rhs_dia_full_size_every_stencil(cuda_device, coupled_kerr_4096_rhs, til
         assert np.array_equal(got, np.conj(got.T))
 
 
+@pytest.mark.parametrize('tile', [8, 208, 708])
+def test_rhs_dia_upper_tiles_form(cuda_device, coupled_kerr_4096_rhs, tile):
+    """DQB_FORM_HERMITIAN_UPPER (the stage slots' layout, the form the autotuner times) at
+    n = 4096: on the 32 x 32 tiles on and above the diagonal the output matches the oracle
+    at 2e-6, and on and above the diagonal it equals the hermitian form's output bit for
+    bit (the same arithmetic, only the lower triangle is not mirrored)."""
+    w, X, ref = coupled_kerr_4096_rhs
+    n = 4096
+    Ls = [SparseDIA(L.offsets, L.diags[None]) for L in w['jump_ops']]
+    p, keep = _problem_struct(w['H'], Ls, n, 1)
+    r_d = torch.from_numpy(np.ascontiguousarray(X[None])).to('cuda')
+    full = torch.empty_like(r_d)
+    upper = torch.zeros_like(r_d)
+    ws = torch.empty(1 << 20, dtype=torch.uint8, device='cuda')
+    lib = _lib.load()
+    stream = torch.cuda.current_stream().cuda_stream
+    for form, out in ((_lib.FORM_HERMITIAN, full), (_lib.FORM_HERMITIAN_UPPER, upper)):
+        _lib.check(lib.dqb_lindblad_rhs_dia_tiled(p, form, tile, r_d.data_ptr(), out.data_ptr(),
+                                                  ws.data_ptr(), ws.numel(), stream), 'rhs_dia')
+    got_f = full[0].cpu().numpy()
+    got_u = upper[0].cpu().numpy()
+    i = np.arange(n)
+    tiles = i[None, :] >= 32 * (i[:, None] // 32)
+    diff = np.linalg.norm((got_u - ref)[tiles]) / np.linalg.norm(ref[tiles])
+    assert diff < 2e-6
+    triu = i[None, :] >= i[:, None]
+    assert np.array_equal(got_u[triu], got_f[triu])
+
+
 def test_dia_full_size_short_solve_vs_oracle(cuda_device):
     """The n = 4096 coupled-Kerr solve (Tsit5 1e-5/1e-7) over t in [0, 0.05] against the
     oracle (complex128 state) at 1e-5 on every saved state, with equal step counts."""

@@ -60,3 +60,34 @@ def test_argument_validation_without_gpu():
     # workspace query of a complete problem is host arithmetic
     p.n_tsave, p.rho0, p.tsave = 3, 1, 1
     assert lib.dqb_mesolve_dia_workspace_size(p) > 10 * 64 * 8
+
+
+def header_int_constants():
+    """Every ``#define DQB_<NAME> <integer>`` of include/*.h."""
+    consts = {}
+    for h in sorted((ROOT / 'include').glob('*.h')):
+        text = re.sub(r'/\*.*?\*/', '', h.read_text(), flags=re.S)
+        for name, val in re.findall(r'^\s*#define\s+(DQB_\w+)\s+(-?\d+)\s*$', text, flags=re.M):
+            consts[name] = int(val)
+    return consts
+
+
+def test_binding_constants_match_header():
+    """The ctypes mirror's constants (named as in the header, or without its ``DQB_``
+    prefix) hold the header's values: a value that drifts on one side would silently
+    select another form, method, precision or stepper."""
+    consts = header_int_constants()
+    assert consts['DQB_FORM_HERMITIAN_UPPER'] == 2 and consts['DQB_STEPPER_KRYLOV'] == 2
+    checked, wrong = 0, []
+    for name, val in consts.items():
+        for py in (name, name[len('DQB_'):]):
+            if hasattr(_lib, py):
+                checked += 1
+                if getattr(_lib, py) != val:
+                    wrong.append((name, val, py, getattr(_lib, py)))
+                break
+    assert not wrong, wrong
+    for must in ('FORM_HERMITIAN', 'FORM_STANDARD', 'FORM_HERMITIAN_UPPER', 'METHOD_TSIT5',
+                 'METHOD_DOPRI5', 'PREC_TF32X3', 'STEPPER_KRYLOV', 'INST_CANCELLED', 'TD_CONST'):
+        assert 'DQB_' + must in consts and hasattr(_lib, must), must
+    assert checked >= 20

@@ -12,9 +12,11 @@ Choices tuned:
 
 * sparse DIA (``dqb_mesolve_dia``): the stencil kernel and its rows -- the generic kernel,
   the tiled one (coefficient tables) with 4, 8 or 16 rows per thread, the staged one
-  (rows of X in shared memory) with 8 or 16 rows per CTA, or the wide one (4 or 2 columns
-  per thread, column factors in registers) with 8 or 16 rows per CTA
-  (``dqb_ode_options.tile``).
+  (rows of X in shared memory) with 8 or 16 rows per CTA, the wide one (4 or 2 columns
+  per thread, column factors in registers) with 8 or 16 rows per CTA, two rows in flight
+  or registers capped for more resident CTAs, or the bulk-staged one
+  (``dqb_ode_options.tile``); timed on the instances that run together and in the form
+  the solve's stencils write (the stage slots' upper tiles in the hermitian stage form).
 * dense GEMM path (n > 64) with ``Options(precision='auto')``: FP32 CUDA-core products or
   3xTF32 tensor-core products, the two arithmetic modes that meet the 1e-5 relative error
   bar; the tensor-core mode needs the hermitian form and an even n, else FP32 is used.

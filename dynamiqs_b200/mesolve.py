@@ -291,6 +291,15 @@ def _stepper_code(o) -> int:
                          f'got {o.stepper!r}.') from None
 
 
+def _dia_tune_form(form: int, stepper: int) -> int:
+    """Form in which the DIA solve's stencils write, for the autotuner to time: the stage
+    form of the hermitian form fills only the stage slots' upper 32 x 32 tiles
+    (FORM_HERMITIAN_UPPER); the Krylov basis and the standard form write whole matrices."""
+    if form == _lib.FORM_HERMITIAN and stepper != _lib.STEPPER_KRYLOV:
+        return _lib.FORM_HERMITIAN_UPPER
+    return form
+
+
 def _precision_code(o, form: int, path: str = 'large') -> int:
     """DQB_PREC_* for ``Options.precision`` on `path` ('small': the n <= 64 kernel,
     'large': the GEMM path, 'dia'); the tensor-core modes need the hermitian form.
@@ -601,12 +610,7 @@ class MESolveB200Integrator:
         from . import autotune
 
         n = prob.n
-        # the form the solve's stencils write in: the stage form of the hermitian form
-        # fills only the stage slots' upper 32 x 32 tiles; the Krylov basis and the
-        # standard form write whole matrices
-        form = self._form()
-        if form == _lib.FORM_HERMITIAN and _stepper_code(self.options) != _lib.STEPPER_KRYLOV:
-            form = _lib.FORM_HERMITIAN_UPPER
+        form = _dia_tune_form(self._form(), _stepper_code(self.options))
         bt = int(max(1, min(prob.batch, (1 << 30) // (8 * n * n))))
         pt = _lib.DiaProblem.from_buffer_copy(prob)
         pt.batch = bt

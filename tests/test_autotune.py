@@ -41,6 +41,20 @@ def test_disabled_returns_default(monkeypatch):
 
 
 @pytest.mark.gpu
+def test_dia_tune_form():
+    """The DIA stencil is timed in the form the solve writes: upper tiles for the stage form
+    of the hermitian form (every stepper but Krylov), whole matrices otherwise."""
+    from dynamiqs_b200 import _lib
+    from dynamiqs_b200.mesolve import _dia_tune_form
+
+    H, S, U = _lib.FORM_HERMITIAN, _lib.FORM_STANDARD, _lib.FORM_HERMITIAN_UPPER
+    assert _dia_tune_form(H, _lib.STEPPER_AUTO) == U
+    assert _dia_tune_form(H, _lib.STEPPER_STAGES) == U
+    assert _dia_tune_form(H, _lib.STEPPER_KRYLOV) == H
+    for st in (_lib.STEPPER_AUTO, _lib.STEPPER_STAGES, _lib.STEPPER_KRYLOV):
+        assert _dia_tune_form(S, st) == S
+
+
 def test_dia_tiles_equal_and_cached(cuda_device, tmp_path, monkeypatch):
     import torch
 

@@ -40,7 +40,6 @@ def test_disabled_returns_default(monkeypatch):
     assert got == 2 and not called
 
 
-@pytest.mark.gpu
 def test_dia_tune_form():
     """The DIA stencil is timed in the form the solve writes: upper tiles for the stage form
     of the hermitian form (every stepper but Krylov), whole matrices otherwise."""
@@ -55,6 +54,7 @@ def test_dia_tune_form():
         assert _dia_tune_form(S, st) == S
 
 
+@pytest.mark.gpu
 def test_dia_tiles_equal_and_cached(cuda_device, tmp_path, monkeypatch):
     import torch
 
